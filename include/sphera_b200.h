@@ -1,0 +1,260 @@
+/*
+ * sphera_b200.h -- C ABI of the B200 (sm_100a) implementation of SPHERA's
+ * per-step particle hot path (SA-SPH, leapfrog, linear barotropic EoS).
+ *
+ * Every entry point is extern "C", takes plain pointers, sizes and POD
+ * structs with fixed-width members, and returns an int status (SPH_OK = 0),
+ * so a Fortran `bind(C)` interface can map it one to one.
+ *
+ * The reference (SPHERA v10.0.0, Fortran 90 + OpenMP) implements the same
+ * path as argument-less subroutines that read and write module globals
+ * (pg(:), Icont, NPartOrd, PartIntorno, PartKernel, rag,
+ * BoundaryDataPointer, BoundaryDataTab).  Each fine-grained entry point below
+ * replaces one call site of src/Main_algorithm/time_step_loop.f90; the cited
+ * file:line is the reference unit it stands in for.
+ *
+ * Ownership: the library owns device memory and the handle.  Host buffers
+ * passed in are caller-owned and only read or written during the call.  The
+ * library keeps particles in its own cell-sorted order on the device and
+ * reads/writes host arrays in the caller's particle order (index npi-1 of
+ * pg(npi)), keeping the permutation itself.
+ *
+ * Threading: a handle is not re-entrant (the reference calls these units
+ * from the master thread).  Separate handles may be driven from separate
+ * host threads; each handle owns its CUDA stream.
+ */
+#ifndef SPHERA_B200_H
+#define SPHERA_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------------- */
+/* Status codes.  Codes >= 100 mirror the reference's fatal                */
+/* diagnostic(arg1,arg2) pairs as 100*arg1 + arg2                          */
+/* (src/Memory_I_O/diagnostic.f90); the library never aborts or traps.     */
+/* ---------------------------------------------------------------------- */
+#define SPH_OK                       0
+#define SPH_ERR_INVALID_ARGUMENT     1   /* bad pointer, size or parameter          */
+#define SPH_ERR_UNSUPPORTED          2   /* feature outside the implemented path    */
+#define SPH_ERR_CUDA                 3   /* a CUDA runtime call failed              */
+#define SPH_ERR_NO_DEVICE            5   /* no sm_100 device visible                */
+#define SPH_ERR_TIMEOUT              6   /* a bounded device wait gave up           */
+#define SPH_ERR_ALLOC              400   /* diagnostic(4): allocation failure       */
+#define SPH_ERR_BDT_OVERFLOW       802   /* diagnostic(8,2): BoundaryDataTab full   */
+#define SPH_ERR_CLOSE_FACES        807   /* diagnostic(8,7): > MAXCLOSEBOUNDFACES   */
+#define SPH_ERR_CLOSE_SIDES        808   /* diagnostic(8,8): > MAXCLOSEBOUNDSIDES   */
+#define SPH_ERR_NCBF_MAX           904   /* diagnostic(9,4): Ncbf_Max too large     */
+
+/* Warning bits (non-fatal; the reference writes a message and continues). */
+#define SPH_WARN_NEIGHBOURS_TRUNCATED  0x1  /* CalcVarLength.f90:197-205 list cap  */
+#define SPH_WARN_PARTICLES_REMOVED     0x2  /* OrdGrid1.f90:71-82 out of grid     */
+
+/* Precision forms. */
+#define SPH_PREC_FP64   0   /* plain FP64, the reference's arithmetic           */
+#define SPH_PREC_FP32C  1   /* FP32 pair sums with compensated accumulation,
+                               FP64 positions/integration                        */
+
+/* Boundary zone types (Tratto%tipo).  Only solid walls are on this path.  */
+#define SPH_ZONE_FIXE   1   /* "fixe": fixed wall                                */
+#define SPH_ZONE_TAPI   2   /* "tapi": wall translating at constant velocity     */
+
+/* ---------------------------------------------------------------------- */
+/* Parameters: the subset of Domain, Med(1) and input_any_t the hot path    */
+/* reads (src/Modules/Hybrid_allocation_module.f90, ReadInput*.f90).        */
+/* ---------------------------------------------------------------------- */
+typedef struct SphParams {
+    int32_t dim;                    /* 2 (SPACE_2D, x-z plane) or 3 (SPACE_3D)        */
+    int32_t precision;              /* SPH_PREC_FP64 or SPH_PREC_FP32C                */
+    double  dx;                     /* Domain%dx                                      */
+    double  trunc;                  /* Domain%trunc = h/dx                            */
+    double  coef_nmaxpartj;         /* input_any_t%COEFNMAXPARTJ                      */
+    int32_t max_close_bound_faces;  /* input_any_t%MAXCLOSEBOUNDFACES (3D)            */
+    int32_t dt_alfa_mon;            /* logical dt_alfa_Mon                            */
+    double  domain_lo[3];           /* Domain%coord(:,1)                              */
+    double  domain_hi[3];           /* Domain%coord(:,2)                              */
+    double  den0;                   /* Med%den0                                       */
+    double  eps;                    /* Med%eps, bulk modulus K                        */
+    double  alfa_mon;               /* Med%alfaMon                                    */
+    double  kin_visc;               /* Med%kin_visc = mu/den0                         */
+    double  p_ref;                  /* Domain%prif                                    */
+    double  grav[3];                /* Domain%grav                                    */
+    double  cfl;                    /* input_any_t%CFL                                */
+    double  vsc_coeff;              /* input_any_t%vsc_coeff                          */
+    double  pesodt;                 /* pesodt                                         */
+    int32_t density_thresholds;     /* input_any_t%density_thresholds (0/1)           */
+    int32_t bdt_capacity;           /* BoundaryDataTab entries to reserve, 0 = n      */
+    double  teta_p;                 /* input_any_t%TetaP (must be 0 on this path)     */
+    double  teta_v;                 /* input_any_t%TetaV (must be 0 on this path)     */
+} SphParams;
+
+/* One boundary zone (Tratto). */
+typedef struct SphZone {
+    int32_t type;                   /* SPH_ZONE_FIXE / SPH_ZONE_TAPI                  */
+    int32_t slip_coefficient_mode;  /* Partz%slip_coefficient_mode (1 only)           */
+    double  velocity[3];            /* Tratto%velocity (tapi)                         */
+    double  bc_shear_stress_input;  /* Partz%BC_shear_stress_input: slip coefficient  */
+    int32_t laminar_no_slip_check;  /* Tratto%laminar_no_slip_check (logical)         */
+    int32_t reserved;
+} SphZone;
+
+/* Boundary geometry.  Indices are 1-based, as in the input deck.          */
+typedef struct SphGeometry {
+    int32_t        n_vertices;
+    const double*  vertices;        /* [n_vertices][3]                                */
+    int32_t        n_zones;
+    const SphZone* zones;           /* [n_zones]                                      */
+    /* 3D: quadrilateral or triangular faces (BoundaryFace) */
+    int32_t        n_faces;
+    const int32_t* face_nodes;      /* [n_faces][4] vertex ids, 0 pads a triangle     */
+    const int32_t* face_zone;       /* [n_faces] zone id                              */
+    /* 2D: boundary sides (BoundarySide), vertex 1 -> vertex 2 */
+    int32_t        n_sides;
+    const int32_t* side_vertices;   /* [n_sides][2] vertex ids                        */
+    const int32_t* side_zone;       /* [n_sides] zone id                              */
+} SphGeometry;
+
+/* Particle state in the caller's order (pg(1:n)). */
+typedef struct SphState {
+    int32_t n;
+    double* x;                      /* [n][3] pg%coord                                */
+    double* v;                      /* [n][3] pg%vel (pg%var equals it, TetaV = 0)    */
+    double* rho;                    /* [n]    pg%dens                                 */
+    double* p;                      /* [n]    pg%pres                                 */
+    double* m;                      /* [n]    pg%mass                                 */
+} SphState;
+
+typedef struct SphStepInfo {
+    double  time;                   /* simulation_time after the steps                */
+    double  dt;                     /* dt of the last completed step                  */
+    int32_t step;                   /* on_going_time_step                             */
+    int32_t n;                      /* nag (particles still in the grid)              */
+    int32_t warnings;               /* SPH_WARN_* bits accumulated                    */
+    int32_t max_neighbours;         /* largest neighbour count seen (incl. self)      */
+} SphStepInfo;
+
+typedef struct SphDiagnostics {
+    int32_t warnings;               /* SPH_WARN_* bits                                */
+    int32_t status;                 /* first fatal device status, SPH_OK if none      */
+    int32_t removed_out_of_grid;    /* EpOrdGrid                                      */
+    int32_t ncbf_max;               /* Ncbf_Max of the last boundary pass             */
+    int32_t bdt_entries;            /* BoundaryDataTab entries in use                 */
+    int32_t nmaxpartj;              /* NMAXPARTJ                                      */
+    int32_t grid_ncd[3];            /* Grid%ncd                                       */
+    int32_t n_cells;                /* Grid%nmax                                      */
+} SphDiagnostics;
+
+typedef struct SphHandle SphHandle;
+
+/* ---------------------------------------------------------------------- */
+/* Life cycle                                                              */
+/* ---------------------------------------------------------------------- */
+
+/* Builds the grid (CreaGrid.f90:51-74), the boundary geometry
+ * (DefineLocalSystemVersors.f90, GridCellBoundaryFacesIntersections3D.f90 /
+ * DefineBoundarySideGeometry2D.f90) and the IC integral tables
+ * (ComputeKernelTable.f90, ComputeBoundaryIntegralTab.f90) and reserves
+ * device memory for up to n_capacity particles.                           */
+int  sph_create(const SphParams* params, const SphGeometry* geometry,
+                int32_t n_capacity, SphHandle** out);
+void sph_destroy(SphHandle* h);
+
+/* Uploads pg(1:n) and performs the IC part of time_step_loop.f90:82-173:
+ * OrdGrid1, neighbour search, ComputeBoundaryDataTab and the IC
+ * time_step_duration.  v doubles as pg%var.                               */
+int  sph_upload(SphHandle* h, const SphState* state);
+/* Copies pg(1:n) back in the caller's order (after removals, the
+ * reference's swap-with-last order).  Any of x, v, rho, p, m may be NULL.  */
+int  sph_download(SphHandle* h, SphState* state);
+
+/* One or more whole leapfrog steps: time_step_loop.f90:175-405 with
+ * time_split = 1, Domain%tipo = "semi", TetaP = TetaV = 0.                 */
+int  sph_step(SphHandle* h, int32_t nsteps, SphStepInfo* info);
+
+int  sph_get_diagnostics(SphHandle* h, SphDiagnostics* diag);
+
+/* Enqueue nsteps whole steps on the handle's stream without waiting, and
+ * wait for them (and read back the device status).  The step is replayed
+ * from a CUDA graph built on the first call.                              */
+int  sph_step_async(SphHandle* h, int32_t nsteps);
+int  sph_sync(SphHandle* h);
+/* The handle's cudaStream_t, for callers that order their own work after
+ * the library's.                                                          */
+void* sph_stream(SphHandle* h);
+
+/* ---------------------------------------------------------------------- */
+/* Batches: several independent simulations advanced by the same launches  */
+/* (no reference counterpart; the reference runs one case per process).    */
+/* All simulations of a batch share dim and precision.                     */
+/* ---------------------------------------------------------------------- */
+int  sph_batch_create(int32_t nsims, const SphParams* params, const SphGeometry* geometries,
+                      const int32_t* n_capacity, SphHandle** out);
+int  sph_batch_upload(SphHandle* h, int32_t nsims, const SphState* states);
+int  sph_batch_download(SphHandle* h, int32_t sim, SphState* state);
+/* A simulation whose time reaches t_end (> 0) stops advancing; its state
+ * stays on the device for download while the others continue.             */
+int  sph_batch_set_end_time(SphHandle* h, int32_t sim, double t_end);
+int  sph_batch_info(SphHandle* h, int32_t sim, SphStepInfo* info, int32_t* frozen);
+
+/* ---------------------------------------------------------------------- */
+/* Fine-grained calls, one per replaced Fortran call site                  */
+/* ---------------------------------------------------------------------- */
+
+/* time_step_duration.f90:59-123 (time_step_loop.f90:185). */
+int  sph_time_step_duration(SphHandle* h, double* dt_out);
+/* RHS_momentum_equation.f90:87-179 with inter_EqMoto.f90:108-263,
+ * viscomon.f90:54-73, viscomorris.f90:60-71,
+ * AddBoundaryContributions_to_ME3D.f90:105-336 / ..._ME2D.f90:96-402 and
+ * AddElasticBoundaryReaction_3D.f90:67-154 / ..._2D.f90:63-97
+ * (time_step_loop.f90:222).  acc_out ([n][3], caller order) may be NULL.  */
+int  sph_rhs_momentum(SphHandle* h, double* acc_out);
+/* Leapfrog_momentum.f90:66-99 (time_step_loop.f90:241) using the
+ * accelerations of the last sph_rhs_momentum, then velocity_smoothing_2
+ * with TetaV = 0 (var = vel).                                             */
+int  sph_leapfrog_momentum(SphHandle* h);
+/* Leapfrog_trajectories.f90:52-66 (time_step_loop.f90:262). */
+int  sph_leapfrog_trajectories(SphHandle* h);
+/* OrdGrid1.f90:50-105 followed by the list-free replacement of
+ * CalcVarLength.f90:133-269 (time_step_loop.f90:286,292).                 */
+int  sph_ord_grid(SphHandle* h);
+/* ComputeBoundaryDataTab_3D.f90:67-105 / _2D.f90:70-157
+ * (time_step_loop.f90:322/324).                                           */
+int  sph_boundary_data_tab(SphHandle* h);
+/* The OMP block time_step_loop.f90:338-360: dden = 0, SASPH_continuity
+ * (SASPH_continuity.f90:89-169 with AddBoundaryContribution_to_CE3D/2D)
+ * and Continuity_Equation.f90:90-249.  dden_out ([n]) may be NULL.        */
+int  sph_continuity(SphHandle* h, double* dden_out);
+/* Leapfrog_continuity.f90:54-68 (time_step_loop.f90:382). */
+int  sph_leapfrog_continuity(SphHandle* h);
+/* EoS_fluid_loop.f90:59-69 with EoS_barotropic_linear.f90:49-55
+ * (time_step_loop.f90:386).                                               */
+int  sph_eos(SphHandle* h);
+
+/* ---------------------------------------------------------------------- */
+/* Verification                                                            */
+/* ---------------------------------------------------------------------- */
+
+/* The reference's grid arrays for the current positions: pg%cella ([n],
+ * caller order), Icont ([n_cells+1], 1-based starts) and NPartOrd ([n],
+ * 1-based caller indices), exactly as OrdGrid1.f90:58-105 builds them.
+ * Any pointer may be NULL.                                                */
+int  sph_dump_grid(SphHandle* h, int32_t* cella, int32_t* icont, int32_t* npartord);
+/* The neighbour lists CalcVarLength.f90:173-269 would build:
+ * counts ([n], nPartIntorno) and lists ([n][nmaxj], PartIntorno, 1-based
+ * caller indices in the reference's visiting order).                      */
+int  sph_dump_neighbours(SphHandle* h, int32_t nmaxj, int32_t* counts, int32_t* lists);
+/* BoundaryDataTab in caller order: ncb ([n], BoundaryDataPointer(1,:) in
+ * 3D, IntNcbs in 2D), and for each particle up to max_per entries of
+ * clobonum ([n][max_per]) and the 20 doubles LocXYZ(3), BoundaryIntegral(8),
+ * IntGiWrRdV(3,3) column-major ([n][max_per][20]).                        */
+int  sph_dump_boundary(SphHandle* h, int32_t max_per, int32_t* ncb,
+                       int32_t* clobonum, double* values);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SPHERA_B200_H */

@@ -1,0 +1,270 @@
+"""sphera_b200 -- B200 (sm_100a) implementation of SPHERA's per-step particle path.
+
+Python host mirror of the C ABI declared in include/sphera_b200.h.  The
+method names follow the reference subroutines each call replaces
+(src/Main_algorithm/time_step_loop.f90), so a test reads like the
+reference's time loop:
+
+    sim = Simulation(case)            # CreaGrid + IC tables, device memory
+    sim.upload(case.state)            # OrdGrid1 + CalcVarLength + ComputeBoundaryDataTab + dt
+    sim.step(100)                     # whole leapfrog steps (CUDA graph)
+    st = sim.download()
+
+The compute runs only in libsphera_b200.so; if the library is missing the
+import of the CUDA path fails loudly (there is no CPU fallback).
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import abi
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libsphera_b200.so")
+_lib = None
+
+
+class SphError(RuntimeError):
+    def __init__(self, code, what):
+        self.code = code
+        super().__init__(f"{what}: status {code} ({abi.STATUS_NAMES.get(code, 'unknown')})")
+
+
+def lib():
+    """Loads libsphera_b200.so (built by sphera_b200/build.py)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: build it with `python sphera_b200/build.py` "
+                          "(the CUDA library is the only implementation)")
+    L = C.CDLL(LIB_PATH)
+    vp = C.c_void_p
+    dp = C.POINTER(C.c_double)
+    ip = C.POINTER(C.c_int32)
+    hp = C.POINTER(vp)
+    sig = {
+        "sph_create": ([C.POINTER(abi.SphParams), C.POINTER(abi.SphGeometry), C.c_int32, hp], C.c_int),
+        "sph_batch_create": ([C.c_int32, C.POINTER(abi.SphParams), C.POINTER(abi.SphGeometry), ip, hp], C.c_int),
+        "sph_destroy": ([vp], None),
+        "sph_upload": ([vp, C.POINTER(abi.SphState)], C.c_int),
+        "sph_batch_upload": ([vp, C.c_int32, C.POINTER(abi.SphState)], C.c_int),
+        "sph_download": ([vp, C.POINTER(abi.SphState)], C.c_int),
+        "sph_batch_download": ([vp, C.c_int32, C.POINTER(abi.SphState)], C.c_int),
+        "sph_batch_set_end_time": ([vp, C.c_int32, C.c_double], C.c_int),
+        "sph_batch_info": ([vp, C.c_int32, C.POINTER(abi.SphStepInfo), ip], C.c_int),
+        "sph_step": ([vp, C.c_int32, C.POINTER(abi.SphStepInfo)], C.c_int),
+        "sph_step_async": ([vp, C.c_int32], C.c_int),
+        "sph_sync": ([vp], C.c_int),
+        "sph_stream": ([vp], vp),
+        "sph_get_diagnostics": ([vp, C.POINTER(abi.SphDiagnostics)], C.c_int),
+        "sph_time_step_duration": ([vp, dp], C.c_int),
+        "sph_rhs_momentum": ([vp, dp], C.c_int),
+        "sph_leapfrog_momentum": ([vp], C.c_int),
+        "sph_leapfrog_trajectories": ([vp], C.c_int),
+        "sph_ord_grid": ([vp], C.c_int),
+        "sph_boundary_data_tab": ([vp], C.c_int),
+        "sph_continuity": ([vp, dp], C.c_int),
+        "sph_leapfrog_continuity": ([vp], C.c_int),
+        "sph_eos": ([vp], C.c_int),
+        "sph_dump_grid": ([vp, ip, ip, ip], C.c_int),
+        "sph_dump_neighbours": ([vp, C.c_int32, ip, ip], C.c_int),
+        "sph_dump_boundary": ([vp, C.c_int32, ip, ip, dp], C.c_int),
+    }
+    for name, (args, res) in sig.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = res
+    _lib = L
+    return L
+
+
+def _chk(code, what):
+    if code != abi.SPH_OK:
+        raise SphError(code, what)
+
+
+class Simulation:
+    """One simulation on the device (a one-entry batch of the C ABI)."""
+
+    def __init__(self, case=None, params=None, geometry=None, capacity=None):
+        if case is not None:
+            params, geometry = case.params, case.geometry
+            capacity = capacity or case.n
+        self.params = params
+        self.geometry = geometry
+        self.capacity = int(capacity)
+        self._h = C.c_void_p()
+        _chk(lib().sph_create(C.byref(params), C.byref(geometry.struct), self.capacity, C.byref(self._h)),
+             "sph_create")
+        self.n = 0
+
+    def close(self):
+        if self._h:
+            lib().sph_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # ----------------------------------------------------------------- state
+    def upload(self, state):
+        _chk(lib().sph_upload(self._h, C.byref(state.struct)), "sph_upload")
+        self.n = state.n
+
+    def download(self):
+        info = self.diagnostics()
+        n = self.n
+        st = abi.State.empty(n)
+        _chk(lib().sph_download(self._h, C.byref(st.struct)), "sph_download")
+        n2 = st.struct.n
+        if n2 != n:
+            st = abi.State(st.x[:n2], st.v[:n2], st.rho[:n2], st.p[:n2], st.m[:n2])
+            self.n = n2
+        del info
+        return st
+
+    def step(self, nsteps=1):
+        info = abi.SphStepInfo()
+        _chk(lib().sph_step(self._h, int(nsteps), C.byref(info)), "sph_step")
+        self.n = info.n
+        return info
+
+    def step_async(self, nsteps=1):
+        _chk(lib().sph_step_async(self._h, int(nsteps)), "sph_step_async")
+
+    def sync(self):
+        _chk(lib().sph_sync(self._h), "sph_sync")
+
+    @property
+    def stream(self):
+        return lib().sph_stream(self._h)
+
+    def diagnostics(self):
+        d = abi.SphDiagnostics()
+        _chk(lib().sph_get_diagnostics(self._h, C.byref(d)), "sph_get_diagnostics")
+        return d
+
+    # ------------------------------------------- one call per Fortran call site
+    def time_step_duration(self):
+        dt = C.c_double()
+        _chk(lib().sph_time_step_duration(self._h, C.byref(dt)), "sph_time_step_duration")
+        return dt.value
+
+    def rhs_momentum(self, want=True):
+        acc = np.zeros((self.n, 3)) if want else None
+        _chk(lib().sph_rhs_momentum(self._h, abi.dptr(acc)), "sph_rhs_momentum")
+        return acc
+
+    def leapfrog_momentum(self):
+        _chk(lib().sph_leapfrog_momentum(self._h), "sph_leapfrog_momentum")
+
+    def leapfrog_trajectories(self):
+        _chk(lib().sph_leapfrog_trajectories(self._h), "sph_leapfrog_trajectories")
+
+    def ord_grid(self):
+        _chk(lib().sph_ord_grid(self._h), "sph_ord_grid")
+
+    def boundary_data_tab(self):
+        _chk(lib().sph_boundary_data_tab(self._h), "sph_boundary_data_tab")
+
+    def continuity(self, want=True):
+        dden = np.zeros(self.n) if want else None
+        _chk(lib().sph_continuity(self._h, abi.dptr(dden)), "sph_continuity")
+        return dden
+
+    def leapfrog_continuity(self):
+        _chk(lib().sph_leapfrog_continuity(self._h), "sph_leapfrog_continuity")
+
+    def eos(self):
+        _chk(lib().sph_eos(self._h), "sph_eos")
+
+    # --------------------------------------------------------- verification
+    def dump_grid(self):
+        d = self.diagnostics()
+        cella = np.zeros(self.n, np.int32)
+        icont = np.zeros(d.n_cells + 1, np.int32)
+        npo = np.zeros(self.n, np.int32)
+        _chk(lib().sph_dump_grid(self._h, abi.iptr(cella), abi.iptr(icont), abi.iptr(npo)), "sph_dump_grid")
+        return cella, icont, npo
+
+    def dump_neighbours(self, nmaxj=None):
+        nmaxj = nmaxj or self.diagnostics().nmaxpartj
+        counts = np.zeros(self.n, np.int32)
+        lists = np.zeros((self.n, nmaxj), np.int32)
+        _chk(lib().sph_dump_neighbours(self._h, nmaxj, abi.iptr(counts), abi.iptr(lists)), "sph_dump_neighbours")
+        return counts, lists
+
+    def dump_boundary(self, max_per=4):
+        ncb = np.zeros(self.n, np.int32)
+        clob = np.zeros((self.n, max_per), np.int32)
+        vals = np.zeros((self.n, max_per, 20))
+        _chk(lib().sph_dump_boundary(self._h, max_per, abi.iptr(ncb), abi.iptr(clob), abi.dptr(vals)),
+             "sph_dump_boundary")
+        return ncb, clob, vals
+
+
+class Batch:
+    """Several independent simulations advanced by the same launches."""
+
+    def __init__(self, cases):
+        self.cases = list(cases)
+        n = len(self.cases)
+        self._params = (abi.SphParams * n)(*[c.params for c in self.cases])
+        self._geoms = (abi.SphGeometry * n)(*[c.geometry.struct for c in self.cases])
+        self._caps = np.array([c.n for c in self.cases], np.int32)
+        self._h = C.c_void_p()
+        _chk(lib().sph_batch_create(n, self._params, self._geoms, abi.iptr(self._caps), C.byref(self._h)),
+             "sph_batch_create")
+
+    def close(self):
+        if self._h:
+            lib().sph_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def upload(self, states=None):
+        states = states or [c.state for c in self.cases]
+        arr = (abi.SphState * len(states))(*[s.struct for s in states])
+        _chk(lib().sph_batch_upload(self._h, len(states), arr), "sph_batch_upload")
+
+    def set_end_time(self, sim, t_end):
+        _chk(lib().sph_batch_set_end_time(self._h, int(sim), float(t_end)), "sph_batch_set_end_time")
+
+    def step(self, nsteps=1):
+        info = abi.SphStepInfo()
+        _chk(lib().sph_step(self._h, int(nsteps), C.byref(info)), "sph_step")
+
+    def step_async(self, nsteps=1):
+        _chk(lib().sph_step_async(self._h, int(nsteps)), "sph_step_async")
+
+    def sync(self):
+        _chk(lib().sph_sync(self._h), "sph_sync")
+
+    def info(self, sim):
+        info = abi.SphStepInfo()
+        fr = C.c_int32()
+        _chk(lib().sph_batch_info(self._h, int(sim), C.byref(info), C.byref(fr)), "sph_batch_info")
+        return info, bool(fr.value)
+
+    def download(self, sim):
+        n = self.cases[sim].n
+        st = abi.State.empty(n)
+        _chk(lib().sph_batch_download(self._h, int(sim), C.byref(st.struct)), "sph_batch_download")
+        n2 = st.struct.n
+        return abi.State(st.x[:n2], st.v[:n2], st.rho[:n2], st.p[:n2], st.m[:n2])

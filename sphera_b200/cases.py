@@ -1,0 +1,159 @@
+"""Seeded synthetic initial states for the workloads of this path.
+
+The reference builds its initial lattice in src/IC (GeneratePart.f90,
+SetParticleParameters.f90:55-131, SubCalcPreIdro.f90:98-196) with an
+unseeded white-noise jitter (pos_plus_white_noise.f90:48-55).  These
+generators restate the same conventions -- particle centres at (i+1/2)dx,
+mass = dx**D * den0, hydrostatic pressure of type "pl" (level = highest
+particle + dx/2) and density from the inverse linear EoS -- with a seeded
+jitter so every run sees the identical state.
+
+Workloads (all synthetic, no external dataset):
+  * dam_break_2d:  4.0 x 3.0 m tank, 1.0 x 2.0 m column, dx 0.02 (5,000 particles)
+  * dam_break_3d:  1.6 x 0.6 x 0.6 m tank, 0.6 x 0.3 x 0.6 m block, dx 0.005
+                   (864,000 particles)
+  * random_box:    N particles uniform in a cube at mean spacing 0.01 m,
+                   rho = 1000 (1 + N(0, 1e-3)), v ~ N(0, 0.1), no walls
+  * ensemble_2d:   dam breaks with column width U[0.5, 2.0] and height
+                   U[0.5, 2.5] in the 2D tank at dx 0.01
+"""
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import abi
+
+G = 9.81
+
+
+@dataclass
+class Case:
+    name: str
+    params: abi.SphParams
+    geometry: abi.Geometry
+    state: abi.State
+    meta: dict = field(default_factory=dict)
+
+    @property
+    def n(self):
+        return self.state.n
+
+
+def _params(dim, dx, lo, hi, cfl=0.1, precision=abi.SPH_PREC_FP64, **extra):
+    den0 = 1000.0
+    c0 = 40.0
+    kw = dict(
+        dim=dim, precision=precision, dx=dx, trunc=1.3, coef_nmaxpartj=2.0,
+        max_close_bound_faces=100, dt_alfa_mon=0,
+        domain_lo=lo, domain_hi=hi, den0=den0, eps=den0 * c0 * c0,
+        alfa_mon=0.05, kin_visc=1.0e-6, p_ref=0.0,
+        grav=(0.0, 0.0, -G), cfl=cfl, vsc_coeff=0.05, pesodt=0.0,
+        density_thresholds=0, bdt_capacity=0, teta_p=0.0, teta_v=0.0)
+    kw.update(extra)
+    return abi.make_params(**kw)
+
+
+def _hydrostatic(z, dx, den0, eps, p_ref, g=G):
+    # SubCalcPreIdro.f90:182-196, pressure type "pl" (coshor = 1, senhor = 0)
+    level = z.max() + dx / 2.0
+    p = (level - z) * 1.0 * den0 * g + p_ref
+    # EoS_barotropic_linear.f90:49-55, inverse form
+    rho = den0 * (1.0 + (p - p_ref) / eps)
+    return p, rho
+
+
+def _box_faces(lx, ly, lz):
+    """Six quads of the box [0,lx]x[0,ly]x[0,lz], each with its normal
+    (V1-V4)x(V3-V4) pointing into the box (DefineLocalSystemVersors.f90)."""
+    V = np.array([[0, 0, 0], [lx, 0, 0], [lx, ly, 0], [0, ly, 0],
+                  [0, 0, lz], [lx, 0, lz], [lx, ly, lz], [0, ly, lz]], dtype=np.float64)
+    quads = [(1, 2, 3, 4), (5, 8, 7, 6), (1, 5, 6, 2), (4, 3, 7, 8), (1, 4, 8, 5), (2, 6, 7, 3)]
+    centre = V.mean(axis=0)
+    faces = []
+    for q in quads:
+        a, b, c, d = (V[i - 1] for i in q)
+        nrm = np.cross(a - d, c - d)
+        fc = (a + b + c + d) / 4.0
+        if np.dot(nrm, centre - fc) < 0:
+            q = q[::-1]
+        faces.append(q)
+    return V, np.array(faces, dtype=np.int32)
+
+
+def tank_3d(lx, ly, lz, zone=None):
+    V, F = _box_faces(lx, ly, lz)
+    z = zone or abi.make_zone()
+    return abi.Geometry(V, [z], faces=F, face_zone=np.ones(len(F), dtype=np.int32))
+
+
+def tank_2d(lx, lz, zone=None):
+    # counter-clockwise in the x-z plane: the side normal (-sz, sx) points inside
+    V = np.array([[0, 0, 0], [lx, 0, 0], [lx, 0, lz], [0, 0, lz]], dtype=np.float64)
+    S = np.array([[1, 2], [2, 3], [3, 4], [4, 1]], dtype=np.int32)
+    z = zone or abi.make_zone()
+    return abi.Geometry(V, [z], sides=S, side_zone=np.ones(len(S), dtype=np.int32))
+
+
+def _jitter(rng, shape, dx, frac):
+    return rng.uniform(-frac * dx, frac * dx, size=shape)
+
+
+def dam_break_2d(dx=0.02, tank=(4.0, 3.0), column=(1.0, 2.0), jitter=0.01, seed=0xC0,
+                 precision=abi.SPH_PREC_FP64, cfl=0.1):
+    rng = np.random.Generator(np.random.PCG64(seed))
+    nx, nz = int(round(column[0] / dx)), int(round(column[1] / dx))
+    i, k = np.meshgrid(np.arange(nx), np.arange(nz), indexing="ij")
+    x = np.zeros((nx * nz, 3))
+    x[:, 0] = (i.ravel() + 0.5) * dx
+    x[:, 2] = (k.ravel() + 0.5) * dx
+    j = _jitter(rng, (nx * nz, 2), dx, jitter)
+    x[:, 0] += j[:, 0]
+    x[:, 2] += j[:, 1]
+    prm = _params(2, dx, (0.0, 0.0, 0.0), (tank[0], 0.0, tank[1]), cfl=cfl, precision=precision)
+    p, rho = _hydrostatic(x[:, 2], dx, prm.den0, prm.eps, prm.p_ref)
+    m = np.full(len(p), dx * dx * prm.den0)
+    st = abi.State(x, np.zeros_like(x), rho, p, m)
+    return Case("dam_break_2d", prm, tank_2d(*tank), st,
+                dict(dx=dx, tank=tank, column=column, seed=seed, t_end=1.0))
+
+
+def dam_break_3d(dx=0.005, tank=(1.6, 0.6, 0.6), block=(0.6, 0.3, 0.6), jitter=0.01, seed=0xC1,
+                 precision=abi.SPH_PREC_FP64, cfl=0.1):
+    rng = np.random.Generator(np.random.PCG64(seed))
+    nx, ny, nz = (int(round(b / dx)) for b in block)
+    i, j, k = np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing="ij")
+    x = np.stack([(i.ravel() + 0.5) * dx, (j.ravel() + 0.5) * dx, (k.ravel() + 0.5) * dx], axis=1)
+    x += _jitter(rng, x.shape, dx, jitter)
+    prm = _params(3, dx, (0.0, 0.0, 0.0), tank, cfl=cfl, precision=precision)
+    p, rho = _hydrostatic(x[:, 2], dx, prm.den0, prm.eps, prm.p_ref)
+    m = np.full(len(p), dx ** 3 * prm.den0)
+    st = abi.State(x, np.zeros_like(x), rho, p, m)
+    return Case("dam_break_3d", prm, tank_3d(*tank), st,
+                dict(dx=dx, tank=tank, block=block, seed=seed, t_end=0.5))
+
+
+def random_box(n=16_000_000, spacing=0.01, seed=0xC2, precision=abi.SPH_PREC_FP64):
+    rng = np.random.Generator(np.random.PCG64(seed))
+    L = (n * spacing ** 3) ** (1.0 / 3.0)
+    x = rng.uniform(0.0, L, size=(n, 3))
+    prm = _params(3, spacing, (0.0, 0.0, 0.0), (L, L, L), precision=precision)
+    rho = prm.den0 * (1.0 + rng.normal(0.0, 1.0e-3, size=n))
+    v = rng.normal(0.0, 0.1, size=(n, 3))
+    p = prm.eps / prm.den0 * (rho - prm.den0) + prm.p_ref
+    m = np.full(n, spacing ** 3 * prm.den0)
+    geo = abi.Geometry(np.zeros((1, 3)), [abi.make_zone()])
+    return Case("random_box", prm, geo, abi.State(x, v, rho, p, m),
+                dict(spacing=spacing, side=L, seed=seed))
+
+
+def ensemble_2d(n_sims=256, dx=0.01, seed=0xC3, precision=abi.SPH_PREC_FP32C):
+    rng = np.random.Generator(np.random.PCG64(seed))
+    out = []
+    for s in range(n_sims):
+        w = rng.uniform(0.5, 2.0)
+        hgt = rng.uniform(0.5, 2.5)
+        w = round(w / dx) * dx
+        hgt = round(hgt / dx) * dx
+        out.append(dam_break_2d(dx=dx, column=(w, hgt), seed=int(rng.integers(1 << 31)),
+                                precision=precision))
+    return out

@@ -1,0 +1,1020 @@
+// C ABI of the library (include/sphera_b200.h) and its host-side runtime:
+// IC-time geometry and integral tables, device memory, the per-step launch
+// sequence and its CUDA graph.
+//
+// Host arithmetic that feeds the kernels (grid, face frames, tables) is
+// compiled with -ffp-contract=off and written in the reference's evaluation
+// order, so the device sees the same constants the reference computes.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <cstdlib>
+#include <algorithm>
+#include <new>
+#include <vector>
+
+#include "../../include/sphera_b200.h"
+#include "sph_internal.cuh"
+#include "sph_launch.h"
+
+namespace sph {
+
+// BoundIntegralTab2D, SA_SPH_module.f90:29-54.  The DATA statement's values
+// are default-REAL (single precision) literals, so the reference's double
+// array holds their float roundings; kept here as float literals.
+static const float kBit2dLiterals[22][6] = {
+    {-9.900000E-02f, 6.916001E-01f, 5.671769E-01f, 1.614238E+00f, 7.329450E-01f, 8.813822E-01f},
+    {1.000000E-03f, 6.820633E-01f, 4.993001E-01f, 1.426603E+00f, 7.142813E-01f, 7.123606E-01f},
+    {1.010000E-01f, 6.725266E-01f, 4.314232E-01f, 1.238968E+00f, 6.956176E-01f, 5.433391E-01f},
+    {2.010000E-01f, 6.452481E-01f, 3.653947E-01f, 1.057834E+00f, 6.492812E-01f, 4.085521E-01f},
+    {3.010000E-01f, 6.025034E-01f, 3.028878E-01f, 8.871524E-01f, 5.851007E-01f, 3.020341E-01f},
+    {4.010000E-01f, 5.473293E-01f, 2.453079E-01f, 7.296175E-01f, 5.106232E-01f, 2.189841E-01f},
+    {5.010000E-01f, 4.832434E-01f, 1.937172E-01f, 5.872117E-01f, 4.319031E-01f, 1.553082E-01f},
+    {6.010000E-01f, 4.139976E-01f, 1.488267E-01f, 4.612826E-01f, 3.538107E-01f, 1.074685E-01f},
+    {7.010000E-01f, 3.434138E-01f, 1.109601E-01f, 3.526284E-01f, 2.802530E-01f, 7.237218E-02f},
+    {8.010000E-01f, 2.751568E-01f, 8.006434E-02f, 2.615428E-01f, 2.142205E-01f, 4.732315E-02f},
+    {9.010000E-01f, 2.125249E-01f, 5.573915E-02f, 1.877770E-01f, 1.577964E-01f, 2.998003E-02f},
+    {1.001000E+00f, 1.581202E-01f, 3.728314E-02f, 1.304301E-01f, 1.120873E-01f, 1.834320E-02f},
+    {1.101000E+00f, 1.131765E-01f, 2.379696E-02f, 8.756287E-02f, 7.679627E-02f, 1.076657E-02f},
+    {1.201000E+00f, 7.737532E-02f, 1.434262E-02f, 5.638309E-02f, 5.038764E-02f, 5.995379E-03f},
+    {1.301000E+00f, 4.995510E-02f, 8.042085E-03f, 3.441001E-02f, 3.129118E-02f, 3.118804E-03f},
+    {1.401000E+00f, 2.994721E-02f, 4.104289E-03f, 1.956203E-02f, 1.807987E-02f, 1.482120E-03f},
+    {1.501000E+00f, 1.623613E-02f, 1.842642E-03f, 1.008625E-02f, 9.464607E-03f, 6.216584E-04f},
+    {1.601000E+00f, 7.615461E-03f, 6.873181E-04f, 4.510624E-03f, 4.293336E-03f, 2.172841E-04f},
+    {1.701000E+00f, 2.842820E-03f, 1.913104E-04f, 1.609094E-03f, 1.552266E-03f, 5.682598E-05f},
+    {1.801000E+00f, 6.998383E-04f, 3.120105E-05f, 3.793334E-04f, 3.706037E-04f, 8.729655E-06f},
+    {1.901000E+00f, 6.214235E-05f, 1.372448E-06f, 3.231651E-05f, 3.195398E-05f, 3.625237E-07f},
+    {2.001000E+00f, 0.000000E+00f, 0.000000E+00f, 0.000000E+00f, 0.000000E+00f, 0.000000E+00f}};
+
+namespace {
+
+constexpr double kPi = 3.14159265358979e0;   // PIGRECO, Static_allocation_module.f90:50
+
+// One simulation as prepared on the host.
+struct HostSim {
+  SphParams prm{};
+  SimDev dev{};
+  std::vector<FaceDev> faces;
+  std::vector<SideDev> sides;
+  std::vector<double> bit;             // 256 x 7
+  std::vector<int> cf_count, cf_start, cf_list;
+  std::vector<uint8_t> near;
+  int cap = 0;
+};
+
+struct FaceGeo {   // host copy of a face for the cell-intersection test
+  int nodes;
+  double GX[6][3];
+  double T[3][3];
+  int zone;
+};
+
+// JdWsRn.f90 (beta-spline kernel, n = 1..3)
+double jdwsrn(double ro, int n) {
+  const double KS3D = 0.31830989;
+  double ro2 = ro * ro, ro3 = ro2 * ro, ro4 = ro2 * ro2, ro5 = ro4 * ro;
+  double J = 0.0;
+  if (n == 1) {
+    if (ro >= 0.0 && ro < 1.0) J = -0.75 + (1.0 - 0.5625 * ro) * ro3;
+    else if (ro >= 1.0 && ro < 2.0) J = -1.0 + (1.5 - 1.0 * ro + 0.1875 * ro2) * ro2;
+  } else if (n == 2) {
+    if (ro >= 0.0 && ro < 1.0) J = -0.7 + (0.75 - 0.45 * ro) * ro4;
+    else if (ro >= 1.0 && ro < 2.0) J = -0.8 + (1.0 - 0.75 * ro + 0.15 * ro2) * ro3;
+  } else if (n == 3) {
+    if (ro >= 0.0 && ro < 1.0) J = -0.75 + (0.6 - 0.375 * ro) * ro5;
+    else if (ro >= 1.0 && ro < 2.0) J = -0.8 + (0.75 - 0.6 * ro + 0.125 * ro2) * ro4;
+  }
+  return J * KS3D;
+}
+
+// IWro2dro.f90:60-74
+double iwro2dro(double ro) {
+  const double a1 = 0.333333333333333, a2 = 0.3, a3 = 0.125, a4 = 0.25;
+  const double b1 = 0.0625, b2 = 0.025, b3 = 4.16666666666667e-03;
+  const double kc = 1.0 / kPi;
+  if (ro >= 0.0 && ro < 1.0) {
+    double ro2 = ro * ro, ro3 = ro2 * ro;
+    double I1 = (a1 - a2 * ro2 + a3 * ro3) * ro3;
+    return kc * (a4 - I1);
+  }
+  if (ro >= 1.0 && ro < 2.0) {
+    double ro2 = ro * ro, d = 2.0 - ro, d2 = d * d, d4 = d2 * d2;
+    double I2 = -(b1 * ro2 + b2 * d * ro + b3 * d2) * d4;
+    return kc * (-I2);
+  }
+  return 0.0;
+}
+
+void cross(const double* u, const double* v, double* w) {   // Vector_Product.f90
+  const int iseg[3] = {1, 2, 0};
+  for (int i = 0; i < 3; ++i) {
+    int j = iseg[i], k = iseg[j];
+    w[i] = u[j] * v[k] - u[k] * v[j];
+  }
+}
+
+int cell_indices(const SimDev& s, int nc, int& i, int& j, int& k) {   // CellIndices.f90
+  int ni = s.ncd[0], nj = s.ncd[1];
+  int nij = ni * nj;
+  k = (nc - 1) / nij + 1;
+  int ncij = nc - nij * (k - 1);
+  j = (ncij - 1) / ni + 1;
+  i = ncij - ni * (j - 1);
+  return ncij;
+}
+
+int prepare_sim(const SphParams& prm, const SphGeometry& g, int cap, HostSim& hs) {
+  if (prm.dim != 2 && prm.dim != 3) return SPH_ERR_INVALID_ARGUMENT;
+  if (!(prm.dx > 0.0) || !(prm.trunc > 0.0) || !(prm.den0 > 0.0) || !(prm.eps > 0.0)) return SPH_ERR_INVALID_ARGUMENT;
+  if (prm.teta_p != 0.0 || prm.teta_v != 0.0) return SPH_ERR_UNSUPPORTED;
+  if (prm.precision != SPH_PREC_FP64 && prm.precision != SPH_PREC_FP32C) return SPH_ERR_INVALID_ARGUMENT;
+  if (g.n_zones < 0 || (g.n_zones > 0 && !g.zones)) return SPH_ERR_INVALID_ARGUMENT;
+  for (int z = 0; z < g.n_zones; ++z) {
+    if (g.zones[z].type != SPH_ZONE_FIXE && g.zones[z].type != SPH_ZONE_TAPI) return SPH_ERR_UNSUPPORTED;
+    if (g.zones[z].slip_coefficient_mode != 1) return SPH_ERR_UNSUPPORTED;
+  }
+  hs.prm = prm;
+  hs.cap = cap;
+  SimDev& s = hs.dev;
+  std::memset(&s, 0, sizeof(s));
+  s.dim = prm.dim;
+  // ReadInput.f90:198-205
+  s.h = prm.dx * prm.trunc;
+  s.doubleh = 2.0 * s.h;
+  s.squareh = s.h * s.h;
+  s.square_doubleh = s.doubleh * s.doubleh;
+  s.eta = 1.0e-3 * s.h;
+  s.eta2 = 1.0e-2 * s.squareh;
+  double unosuh = 1.0 / s.h, unosusquareh = 1.0 / s.squareh;
+  // Gest_Input.f90:266-289
+  double hp = (s.dim == 3) ? (s.h * s.h) * s.h : s.h * s.h;
+  s.coefke = ((s.dim == 3) ? 0.477464 : 0.682093) / hp;
+  s.coefkacl = ((s.dim == 3) ? 0.074603 : 0.099472) / hp;
+  s.ke_coef = s.coefke / s.h;
+  s.kacl_coef = s.coefkacl / s.h;
+  double r = s.h * 4.0 / prm.dx;
+  double rp = (s.dim == 3) ? (r * r) * r : r * r;
+  s.nmaxpartj = (int)(prm.coef_nmaxpartj * rp) + 1;
+  s.maxcb = (s.dim == 3) ? prm.max_close_bound_faces : kMaxCloseSides;
+  if (s.maxcb <= 0) return SPH_ERR_INVALID_ARGUMENT;
+  s.dx = prm.dx;
+  s.den0 = prm.den0;
+  s.eps = prm.eps;
+  s.k_over_rho0 = prm.eps / prm.den0;
+  s.celerita = std::sqrt(prm.eps / prm.den0);   // ReadInputMedium.f90:156
+  s.alfa_mon = prm.alfa_mon;
+  s.kin_visc = prm.kin_visc;
+  s.p_ref = prm.p_ref;
+  for (int d = 0; d < 3; ++d) s.grav[d] = prm.grav[d];
+  s.cfl = prm.cfl;
+  s.vsc_coeff = prm.vsc_coeff;
+  s.pesodt = prm.pesodt;
+  s.dt_alfa_mon = prm.dt_alfa_mon;
+  s.density_thresholds = prm.density_thresholds;
+  s.zpmin = 0.05 * s.h;
+  // CreaGrid.f90:51-74
+  double epsi = 0.01 * prm.dx;
+  for (int d = 0; d < 3; ++d) {
+    double lo = prm.domain_lo[d] - s.doubleh - epsi;
+    double hi = prm.domain_hi[d] + s.doubleh + epsi;
+    double dextr = hi - lo;
+    s.extr_lo[d] = lo;
+    s.ncd[d] = (int)std::lround(dextr / s.doubleh);
+    if (s.ncd[d] < 1) return SPH_ERR_INVALID_ARGUMENT;
+    s.dcd[d] = dextr / s.ncd[d];
+  }
+  if (s.dim == 2) s.ncd[1] = 1;
+  long long ncells = (long long)s.ncd[0] * s.ncd[1] * s.ncd[2];
+  if (ncells > (1LL << 30)) return SPH_ERR_INVALID_ARGUMENT;
+  s.ncells = (int)ncells;
+  // ComputeKernelTable.f90:58-71
+  s.ktdelta = 2.0 / kKtRows;
+  for (int nr = 0; nr <= kKtRows; ++nr) {
+    double rob = s.ktdelta * nr;
+    s.kerneltab[nr][0] = rob;
+    s.kerneltab[nr][1] = iwro2dro(rob);
+    s.kerneltab[nr][2] = jdwsrn(rob, 1) * unosusquareh;
+    s.kerneltab[nr][3] = jdwsrn(rob, 2) * unosuh;
+    s.kerneltab[nr][4] = jdwsrn(rob, 3);
+  }
+  // ComputeBoundaryIntegralTab.f90:61-86
+  hs.bit.assign(kBitRows * 7, 0.0);
+  {
+    double delta_fi = (kPi / 2.0) / 8;
+    double duesendelta_fimz = 2.0 * std::sin(0.5 * delta_fi);
+    double delta_teta = (kPi + kPi) / 32;
+    double fi = -0.5 * delta_fi;
+    int pts = 0;
+    for (int i = 1; i <= 8; ++i) {
+      fi = fi + delta_fi;
+      double teta = -0.5 * delta_teta;
+      double zp = -(s.doubleh * std::cos(fi));
+      for (int j = 1; j <= 32; ++j) {
+        teta = teta + delta_teta;
+        double xp = s.doubleh * std::sin(fi) * std::cos(teta);
+        double yp = s.doubleh * std::sin(fi) * std::sin(teta);
+        double* row = &hs.bit[pts * 7];
+        row[0] = xp;
+        row[1] = yp;
+        row[2] = zp;
+        row[3] = delta_teta * duesendelta_fimz * std::sin(fi);
+        row[4] = xp / s.doubleh;
+        row[5] = yp / s.doubleh;
+        row[6] = zp / s.doubleh;
+        pts++;
+      }
+    }
+  }
+  auto vtx = [&](int id, int d) { return g.vertices[3 * (id - 1) + d]; };
+  if (s.dim == 3) {
+    // DefineLocalSystemVersors.f90 + DefineBoundaryFaceGeometry3D.f90
+    std::vector<FaceGeo> geo(g.n_faces);
+    hs.faces.resize(g.n_faces);
+    for (int f = 0; f < g.n_faces; ++f) {
+      int name[4], nn = 0;
+      for (int k = 0; k < 4; ++k) {
+        name[k] = g.face_nodes[4 * f + k];
+        if (name[k] > 0) {
+          if (name[k] > g.n_vertices) return SPH_ERR_INVALID_ARGUMENT;
+          nn++;
+        }
+      }
+      if (nn < 3) return SPH_ERR_INVALID_ARGUMENT;
+      int zone = g.face_zone[f];
+      if (zone < 1 || zone > g.n_zones) return SPH_ERR_INVALID_ARGUMENT;
+      FaceGeo& F = geo[f];
+      F.nodes = nn;
+      F.zone = zone;
+      for (int n = 0; n < nn; ++n)
+        for (int d = 0; d < 3; ++d) F.GX[n][d] = vtx(name[n], d);
+      const int nindex[2][3] = {{1, 2, 3}, {1, 3, 4}};
+      int sidek = nn - 2;
+      double U1[3], U2[3], RR[3], W12[3], nrm[3], ss[3];
+      for (int d = 0; d < 3; ++d) {
+        U1[d] = F.GX[nindex[sidek - 1][0] - 1][d] - F.GX[nindex[sidek - 1][2] - 1][d];
+        U2[d] = F.GX[nindex[sidek - 1][1] - 1][d] - F.GX[nindex[sidek - 1][2] - 1][d];
+      }
+      double U1len = std::sqrt(U1[0] * U1[0] + U1[1] * U1[1] + U1[2] * U1[2]);
+      for (int d = 0; d < 3; ++d) RR[d] = U1[d] / U1len;
+      cross(U1, U2, W12);
+      double W12len = std::sqrt(W12[0] * W12[0] + W12[1] * W12[1] + W12[2] * W12[2]);
+      if (!(W12len > 1.0e-9)) return SPH_ERR_INVALID_ARGUMENT;
+      double area = W12len / (double)(float)(3 - sidek);
+      for (int d = 0; d < 3; ++d) nrm[d] = W12[d] / W12len;
+      cross(nrm, RR, ss);
+      for (int d = 0; d < 3; ++d) {
+        F.T[d][0] = RR[d];
+        F.T[d][1] = ss[d];
+        F.T[d][2] = nrm[d];
+      }
+      double LX[4][2];
+      for (int n = 0; n < nn - 1; ++n)
+        for (int i = 0; i < 2; ++i) {
+          double a = 0.0;
+          for (int j = 0; j < 3; ++j) a = a + F.T[j][i] * (F.GX[n][j] - F.GX[nn - 1][j]);
+          LX[n][i] = a;
+        }
+      LX[nn - 1][0] = 0.0;
+      LX[nn - 1][1] = 0.0;
+      FaceDev& D = hs.faces[f];
+      std::memset(&D, 0, sizeof(D));
+      std::memcpy(D.T, F.T, sizeof(D.T));
+      for (int d = 0; d < 3; ++d) D.GXref[d] = F.GX[nn - 1][d];
+      // LocalNormalCoordinates.f90:59-87 line coefficients
+      int fkod = nn - 2;
+      const int iseg[3] = {2, 3, 1};
+      const int mainod[2][3] = {{1, 2, 3}, {1, 3, 4}};
+      D.usu_due_area = 1.0 / ((double)(3 - fkod) * area);
+      for (int ii = 1; ii <= 2; ++ii) {
+        int jj = iseg[ii - 1], kk = iseg[jj - 1];
+        double xj = LX[mainod[fkod - 1][jj - 1] - 1][0], yj = LX[mainod[fkod - 1][jj - 1] - 1][1];
+        double xk = LX[mainod[fkod - 1][kk - 1] - 1][0], yk = LX[mainod[fkod - 1][kk - 1] - 1][1];
+        D.AA[ii - 1] = xj * yk - xk * yj;
+        D.BB[ii - 1] = yj - yk;
+        D.CC[ii - 1] = xk - xj;
+      }
+      D.fkod = fkod;
+      const SphZone& z = g.zones[zone - 1];
+      for (int d = 0; d < 3; ++d) D.velocity[d] = (z.type == SPH_ZONE_TAPI) ? z.velocity[d] : 0.0;
+      D.slip = z.bc_shear_stress_input;
+      D.laminar_no_slip_check = z.laminar_no_slip_check;
+      D.zone_type = z.type;
+    }
+    // CompleteBoundaries3D.f90: BFaceList ordered by zone
+    std::vector<int> bface;
+    for (int nt = 1; nt <= g.n_zones; ++nt)
+      for (int f = 0; f < g.n_faces; ++f)
+        if (geo[f].zone == nt) bface.push_back(f + 1);
+    // GridCellBoundaryFacesIntersections3D.f90:89-210, stored by sort key
+    hs.cf_count.assign(s.ncells + 1, 0);
+    hs.cf_start.assign(s.ncells + 1, 0);
+    hs.cf_list.clear();
+    std::vector<std::vector<int>> per(s.ncells);
+    for (int nc = 1; nc <= s.ncells && !bface.empty(); ++nc) {
+      int i, j, k;
+      cell_indices(s, nc, i, j, k);
+      double cxyz[3][2];
+      int idx[3] = {i, j, k};
+      for (int d = 0; d < 3; ++d) {
+        cxyz[d][0] = s.extr_lo[d] + s.dcd[d] * (idx[d] - 1);
+        cxyz[d][1] = s.extr_lo[d] + s.dcd[d] * idx[d];
+      }
+      double cn[8][3];
+      int nv = 0;
+      for (int ii = 0; ii < 2; ++ii)
+        for (int jj = 0; jj < 2; ++jj)
+          for (int kk = 0; kk < 2; ++kk) {
+            cn[nv][0] = cxyz[0][ii];
+            cn[nv][1] = cxyz[1][jj];
+            cn[nv][2] = cxyz[2][kk];
+            nv++;
+          }
+      std::vector<int>& lst = per[cell_key_local(s, i, j, k)];
+      for (int nf : bface) {
+        const FaceGeo& F = geo[nf - 1];
+        int nodes = F.nodes;
+        bool found = true;
+        for (int sd = 0; sd < 3 && found; ++sd) {
+          int sc[5] = {0, 0, 0, 0, 0};
+          for (int no = 0; no < nodes; ++no) {
+            double X = F.GX[no][sd];
+            if (X < cxyz[sd][0]) sc[0]++;
+            else if (X == cxyz[sd][0]) sc[1]++;
+            else if (X < cxyz[sd][1]) sc[2]++;
+            else if (X == cxyz[sd][1]) sc[3]++;
+            else if (X > cxyz[sd][1]) sc[4]++;
+          }
+          if ((sc[0] + sc[1]) == nodes && !(sc[1] == nodes)) found = false;
+          else if ((sc[4] + sc[3]) == nodes && !(sc[3] == nodes)) found = false;
+        }
+        if (!found) continue;
+        int c3[3] = {0, 0, 0};
+        for (nv = 0; nv < 8; ++nv) {
+          double zita = 0.0;
+          for (int sd = 0; sd < 3; ++sd) zita = zita + F.T[sd][2] * (cn[nv][sd] - F.GX[nodes - 1][sd]);
+          if (zita < 0.0) c3[0]++;
+          else if (zita == 0.0) c3[1]++;
+          else c3[2]++;
+        }
+        if ((c3[0] + c3[1]) == 8 && !(c3[1] == 4)) found = false;
+        else if ((c3[2] + c3[1]) == 8 && !(c3[1] == 4)) found = false;
+        if (found) {
+          if ((int)lst.size() >= prm.max_close_bound_faces) return SPH_ERR_ALLOC;
+          lst.push_back(nf);
+        }
+      }
+    }
+    for (int key = 0; key < s.ncells; ++key) {
+      hs.cf_start[key] = (int)hs.cf_list.size();
+      hs.cf_count[key] = (int)per[key].size();
+      hs.cf_list.insert(hs.cf_list.end(), per[key].begin(), per[key].end());
+    }
+    // a cell needs the face search when any of its 27 neighbours is cut
+    hs.near.assign(s.ncells + 1, 0);
+    for (int k = 1; k <= s.ncd[2]; ++k)
+      for (int j = 1; j <= s.ncd[1]; ++j)
+        for (int i = 1; i <= s.ncd[0]; ++i) {
+          uint8_t any = 0;
+          for (int di = -1; di <= 1 && !any; ++di)
+            for (int dj = -1; dj <= 1 && !any; ++dj)
+              for (int dk = -1; dk <= 1 && !any; ++dk) {
+                int a = i + di, bq = j + dj, c = k + dk;
+                if (a < 1 || a > s.ncd[0] || bq < 1 || bq > s.ncd[1] || c < 1 || c > s.ncd[2]) continue;
+                if (hs.cf_count[cell_key_local(s, a, bq, c)] > 0) any = 1;
+              }
+          hs.near[cell_key_local(s, i, j, k)] = any;
+        }
+    s.nfaces = g.n_faces;
+  } else {
+    // DefineBoundarySideGeometry2D.f90 + BoundaryMassForceMatrix2D.f90 +
+    // DefineBoundarySideRelativeAngles2D.f90
+    int ns = g.n_sides;
+    hs.sides.resize(ns);
+    std::vector<double> T11(ns), T31(ns);
+    for (int q = 0; q < ns; ++q) {
+      int v1 = g.side_vertices[2 * q], v2 = g.side_vertices[2 * q + 1];
+      int zone = g.side_zone[q];
+      if (v1 < 1 || v2 < 1 || v1 > g.n_vertices || v2 > g.n_vertices || zone < 1 || zone > g.n_zones)
+        return SPH_ERR_INVALID_ARGUMENT;
+      double Dx = vtx(v2, 0) - vtx(v1, 0);
+      double Dz = vtx(v2, 2) - vtx(v1, 2);
+      double L = std::sqrt(Dx * Dx + Dz * Dz);
+      double sx = Dx / L, sz = Dz / L;
+      SideDev& S = hs.sides[q];
+      std::memset(&S, 0, sizeof(S));
+      S.v1[0] = vtx(v1, 0);
+      S.v1[1] = vtx(v1, 2);
+      S.sss[0] = sx;
+      S.sss[1] = sz;
+      S.nnn[0] = -sz;
+      S.nnn[1] = sx;
+      S.length = L;
+      double FiS = 1.0, FiN = 1.0;
+      S.RN[0][0] = FiS * sx * sx + FiN * sz * sz;
+      S.RN[0][1] = (FiS - FiN) * sx * sz;
+      S.RN[1][0] = S.RN[0][1];
+      S.RN[1][1] = FiS * sz * sz + FiN * sx * sx;
+      const SphZone& z = g.zones[zone - 1];
+      for (int d = 0; d < 3; ++d) S.velocity[d] = (z.type == SPH_ZONE_TAPI) ? z.velocity[d] : 0.0;
+      S.slip = z.bc_shear_stress_input;
+      S.laminar_no_slip_check = z.laminar_no_slip_check;
+      S.zone_type = z.type;
+      T11[q] = sx;
+      T31[q] = sz;
+    }
+    for (int isi = 0; isi < ns; ++isi) {
+      int ksi = 0;
+      for (int jsi = 0; jsi < ns; ++jsi)
+        if (g.side_vertices[2 * jsi + 1] == g.side_vertices[2 * isi]) { ksi = jsi + 1; break; }
+      hs.sides[isi].angle = 0.0;
+      if (ksi > 0) {
+        double sinangle = T11[ksi - 1] * T31[isi] - T31[ksi - 1] * T11[isi];
+        double cosangle = T11[ksi - 1] * T11[isi] + T31[ksi - 1] * T31[isi];
+        hs.sides[isi].angle = std::atan2(sinangle, cosangle);
+      }
+      hs.sides[isi].previous_side = ksi;
+    }
+    s.nsides = ns;
+    hs.cf_count.assign(s.ncells + 1, 0);
+    hs.cf_start.assign(s.ncells + 1, 0);
+    hs.near.assign(s.ncells + 1, 0);
+  }
+  return SPH_OK;
+}
+
+template <class T>
+int dalloc(T** p, size_t n) {
+  *p = nullptr;
+  if (n == 0) n = 1;
+  cudaError_t e = cudaMalloc((void**)p, n * sizeof(T));
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return SPH_ERR_ALLOC;
+  }
+  return SPH_OK;
+}
+
+}  // namespace
+}  // namespace sph
+
+using namespace sph;
+
+struct SphHandle {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int nsims = 0;
+  int dim = 3;
+  int precision = SPH_PREC_FP64;
+  std::vector<HostSim> sims;
+  std::vector<int> n_of;            // particles uploaded per simulation
+  int total_slots = 0;
+  int total_cells = 0;
+  int total_faces = 0, total_sides = 0;
+  // device memory
+  SimDev* d_sims = nullptr;
+  SimDyn* d_dyn = nullptr;
+  Tile* d_tiles = nullptr;
+  FaceDev* d_faces = nullptr;
+  SideDev* d_sides = nullptr;
+  double* d_bit = nullptr;
+  int *d_cf_start = nullptr, *d_cf_count = nullptr, *d_cf_list = nullptr;
+  uint8_t* d_near = nullptr;
+  int* d_scan = nullptr;
+  Particles P{};
+  std::vector<void*> owned;
+  // caller-order staging
+  double *d_cx = nullptr, *d_cv = nullptr, *d_crho = nullptr, *d_cp = nullptr, *d_cm = nullptr;
+  double *d_cacc = nullptr, *d_cdden = nullptr;
+  int *d_ci1 = nullptr, *d_ci2 = nullptr, *d_ci3 = nullptr;
+  double* d_cvals = nullptr;
+  size_t cvals_n = 0;
+  DevBatch db{};
+  cudaGraphExec_t graph = nullptr;
+  bool uploaded = false;
+  std::vector<SimDyn> h_dyn;
+};
+
+namespace {
+
+int cuda_status(cudaError_t e) {
+  if (e == cudaSuccess) return SPH_OK;
+  cudaGetLastError();
+  return SPH_ERR_CUDA;
+}
+
+#define SPH_TRY(x)                  \
+  do {                              \
+    int _st = (x);                  \
+    if (_st != SPH_OK) return _st;  \
+  } while (0)
+#define SPH_CUDA(x) SPH_TRY(cuda_status(x))
+
+template <class T>
+int halloc(SphHandle* h, T** p, size_t n) {
+  int st = dalloc(p, n);
+  if (st == SPH_OK) h->owned.push_back((void*)*p);
+  return st;
+}
+
+int sync_dyn(SphHandle* h) {
+  SPH_CUDA(cudaMemcpyAsync(h->h_dyn.data(), h->d_dyn, sizeof(SimDyn) * (h->nsims + 1), cudaMemcpyDeviceToHost,
+                           h->stream));
+  SPH_CUDA(cudaStreamSynchronize(h->stream));
+  for (int s = 0; s < h->nsims; ++s)
+    if (h->h_dyn[s].status != 0) return h->h_dyn[s].status;
+  return SPH_OK;
+}
+
+void sort_sequence(SphHandle* h, cudaStream_t st) {
+  launch_sort_reset(h->db, st);
+  launch_bin(h->db, KeyKind::Sort, st);
+  launch_removal(h->db, st);
+  launch_scan(h->db, h->P.cell_start, st);
+  launch_place(h->db, st);
+  launch_rank_permute(h->db, st);
+}
+
+void step_sequence(SphHandle* h, cudaStream_t st) {
+  launch_momentum(h->db, true, st);
+  sort_sequence(h, st);
+  launch_boundary(h->db, st);
+  launch_continuity(h->db, true, st);
+  launch_finalize(h->db, 1, st);
+}
+
+int build_graph(SphHandle* h) {
+  if (h->graph) return SPH_OK;
+  cudaGraph_t g = nullptr;
+  SPH_CUDA(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+  step_sequence(h, h->stream);
+  cudaError_t e = cudaStreamEndCapture(h->stream, &g);
+  if (e != cudaSuccess) return cuda_status(e);
+  e = cudaGraphInstantiate(&h->graph, g, 0);
+  cudaGraphDestroy(g);
+  return cuda_status(e);
+}
+
+int create_batch(int nsims, const SphParams* params, const SphGeometry* geoms, const int32_t* caps,
+                 SphHandle** out) {
+  if (!out || nsims <= 0 || !params || !geoms || !caps) return SPH_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) { cudaGetLastError(); return SPH_ERR_NO_DEVICE; }
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, dev) != cudaSuccess) { cudaGetLastError(); return SPH_ERR_NO_DEVICE; }
+  if (prop.major != 10) return SPH_ERR_NO_DEVICE;
+  SphHandle* h = new (std::nothrow) SphHandle();
+  if (!h) return SPH_ERR_ALLOC;
+  h->device = dev;
+  h->nsims = nsims;
+  h->dim = params[0].dim;
+  h->precision = params[0].precision;
+  h->sims.resize(nsims);
+  h->n_of.assign(nsims, 0);
+  for (int s = 0; s < nsims; ++s) {
+    if (params[s].dim != h->dim || params[s].precision != h->precision || caps[s] <= 0) {
+      delete h;
+      return SPH_ERR_INVALID_ARGUMENT;
+    }
+    int st = prepare_sim(params[s], geoms[s], caps[s], h->sims[s]);
+    if (st != SPH_OK) { delete h; return st; }
+  }
+  // layout of the concatenated arrays; simulations start on tile boundaries
+  std::vector<Tile> tiles;
+  int poff = 0, coff = 0, foff = 0, soff = 0;
+  size_t bdt_cap = 0;
+  for (int s = 0; s < nsims; ++s) {
+    HostSim& hs = h->sims[s];
+    hs.dev.p_off = poff;
+    hs.dev.cap = hs.cap;
+    hs.dev.cell_off = coff;
+    hs.dev.face_off = foff;
+    hs.dev.side_off = soff;
+    for (int t = 0; t < hs.cap; t += kBlock) {
+      Tile tl;
+      tl.sim = s;
+      tl.start = poff + t;
+      tl.count = std::min(kBlock, hs.cap - t);
+      tl.pad = 0;
+      tiles.push_back(tl);
+    }
+    int padded = (hs.cap + kBlock - 1) / kBlock * kBlock;
+    poff += padded;
+    coff += hs.dev.ncells + 1;
+    foff += (int)hs.faces.size();
+    soff += (int)hs.sides.size();
+    bdt_cap += hs.prm.bdt_capacity > 0 ? (size_t)hs.prm.bdt_capacity : (size_t)hs.cap;
+  }
+  h->total_slots = poff;
+  h->total_cells = coff;
+  h->total_faces = foff;
+  h->total_sides = soff;
+  int st = SPH_OK;
+  cudaError_t e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) { delete h; return cuda_status(e); }
+  size_t N = poff, C = coff;
+  Particles& P = h->P;
+#define A(ptr, n) if (st == SPH_OK) st = halloc(h, &(ptr), (n))
+  A(h->d_sims, nsims);
+  A(h->d_dyn, nsims + 1);
+  A(h->d_tiles, tiles.size());
+  A(h->d_faces, foff);
+  A(h->d_sides, soff);
+  A(h->d_bit, (size_t)nsims * kBitRows * 7);
+  A(h->d_cf_start, C);
+  A(h->d_cf_count, C);
+  A(h->d_near, C);
+  A(P.X, N); A(P.V, N); A(P.RP, N); A(P.I, N); A(P.L, N);
+  A(P.X2, N); A(P.V2, N); A(P.P2, N); A(P.I2, N); A(P.L2, N);
+  A(P.bdt_count, N); A(P.bdt_start, N); A(P.bdt, bdt_cap);
+  A(P.key, N); A(P.slot, N); A(P.cell_count, C + 1); A(P.cell_start, C + 1);
+  A(P.tmp_src, N); A(P.tmp_id, N); A(P.tmp_key, N);
+  A(P.ACC, N); A(P.DDEN, N);
+  A(P.out_flag, N); A(P.id_remap, N); A(P.cur_of, N);
+  A(h->d_cx, 3 * N); A(h->d_cv, 3 * N); A(h->d_crho, N); A(h->d_cp, N); A(h->d_cm, N);
+  A(h->d_cacc, 3 * N); A(h->d_cdden, N);
+  A(h->d_ci1, N); A(h->d_ci2, C + 1); A(h->d_ci3, N);
+  int nb = (int)((C + 4095) / 4096) + 1;
+  A(h->d_scan, nb);
+#undef A
+  if (st != SPH_OK) { sph_destroy(h); return st; }
+  P.bdt_cap = (int)std::min(bdt_cap, (size_t)0x7fffffff);
+  P.total_cells = coff;
+  P.total_slots = poff;
+  // host tables -> device
+  std::vector<SimDev> hsd(nsims);
+  std::vector<FaceDev> hf;
+  std::vector<SideDev> hsi;
+  std::vector<double> hbit;
+  std::vector<int> cfs(C, 0), cfc(C, 0), cfl;
+  std::vector<uint8_t> nr(C, 0);
+  for (int s = 0; s < nsims; ++s) {
+    HostSim& hs = h->sims[s];
+    hsd[s] = hs.dev;
+    hf.insert(hf.end(), hs.faces.begin(), hs.faces.end());
+    hsi.insert(hsi.end(), hs.sides.begin(), hs.sides.end());
+    hbit.insert(hbit.end(), hs.bit.begin(), hs.bit.end());
+    int base = (int)cfl.size();
+    for (int k = 0; k < hs.dev.ncells; ++k) {
+      cfs[hs.dev.cell_off + k] = base + hs.cf_start[k];
+      cfc[hs.dev.cell_off + k] = hs.cf_count[k];
+      nr[hs.dev.cell_off + k] = hs.near[k];
+    }
+    cfl.insert(cfl.end(), hs.cf_list.begin(), hs.cf_list.end());
+  }
+  if (st == SPH_OK) st = halloc(h, &h->d_cf_list, cfl.size());
+  if (st != SPH_OK) { sph_destroy(h); return st; }
+  cudaStream_t q = h->stream;
+  std::vector<SimDyn> dyn0(nsims + 1);
+  std::memset(dyn0.data(), 0, sizeof(SimDyn) * (nsims + 1));
+  for (auto& d : dyn0) d.dtmin_bits = 0x7FF0000000000000ull;
+  h->h_dyn = dyn0;
+  double bit2d[22][6];
+  for (int i = 0; i < 22; ++i)
+    for (int j = 0; j < 6; ++j) bit2d[i][j] = (double)kBit2dLiterals[i][j];
+  e = cudaMemcpyAsync(h->d_sims, hsd.data(), sizeof(SimDev) * nsims, cudaMemcpyHostToDevice, q);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(h->d_dyn, dyn0.data(), sizeof(SimDyn) * (nsims + 1), cudaMemcpyHostToDevice, q);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(h->d_tiles, tiles.data(), sizeof(Tile) * tiles.size(), cudaMemcpyHostToDevice, q);
+  if (e == cudaSuccess && !hf.empty()) e = cudaMemcpyAsync(h->d_faces, hf.data(), sizeof(FaceDev) * hf.size(), cudaMemcpyHostToDevice, q);
+  if (e == cudaSuccess && !hsi.empty()) e = cudaMemcpyAsync(h->d_sides, hsi.data(), sizeof(SideDev) * hsi.size(), cudaMemcpyHostToDevice, q);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(h->d_bit, hbit.data(), sizeof(double) * hbit.size(), cudaMemcpyHostToDevice, q);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(h->d_cf_start, cfs.data(), sizeof(int) * C, cudaMemcpyHostToDevice, q);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(h->d_cf_count, cfc.data(), sizeof(int) * C, cudaMemcpyHostToDevice, q);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(h->d_near, nr.data(), C, cudaMemcpyHostToDevice, q);
+  if (e == cudaSuccess && !cfl.empty()) e = cudaMemcpyAsync(h->d_cf_list, cfl.data(), sizeof(int) * cfl.size(), cudaMemcpyHostToDevice, q);
+  if (e == cudaSuccess) e = cudaMemsetAsync(P.cell_count, 0, sizeof(int) * (C + 1), q);
+  if (e == cudaSuccess) e = cudaMemsetAsync(P.out_flag, 0, N, q);
+  if (e == cudaSuccess) e = cudaMemsetAsync(P.bdt_count, 0, sizeof(int) * N, q);
+  if (e == cudaSuccess) e = cudaMemsetAsync(P.ACC, 0, sizeof(double4) * N, q);
+  if (e == cudaSuccess) e = cudaMemsetAsync(P.DDEN, 0, sizeof(double) * N, q);
+  if (e == cudaSuccess) upload_bit2d(&bit2d[0][0], q);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(q);
+  if (e != cudaSuccess) { sph_destroy(h); return cuda_status(e); }
+  DevBatch& b = h->db;
+  b.sims = h->d_sims;
+  b.dyn = h->d_dyn;
+  b.tiles = h->d_tiles;
+  b.ntiles = (int)tiles.size();
+  b.nsims = nsims;
+  b.dim = h->dim;
+  b.P = P;
+  b.faces = h->d_faces;
+  b.sides = h->d_sides;
+  b.bit = h->d_bit;
+  b.cf_start = h->d_cf_start;
+  b.cf_count = h->d_cf_count;
+  b.cf_list = h->d_cf_list;
+  b.cell_near = h->d_near;
+  b.scan_block_sums = h->d_scan;
+  b.scan_nblocks = nb;
+  b.grid_blocks = prop.multiProcessorCount * 8;
+  *out = h;
+  return SPH_OK;
+}
+
+int upload_sim(SphHandle* h, int sim, const SphState* st) {
+  if (!h || !st || sim < 0 || sim >= h->nsims) return SPH_ERR_INVALID_ARGUMENT;
+  HostSim& hs = h->sims[sim];
+  if (st->n < 0 || st->n > hs.cap || !st->x || !st->v || !st->rho || !st->p || !st->m) return SPH_ERR_INVALID_ARGUMENT;
+  size_t o = hs.dev.p_off, n = st->n;
+  cudaStream_t q = h->stream;
+  SPH_CUDA(cudaMemcpyAsync(h->d_cx + 3 * o, st->x, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, q));
+  SPH_CUDA(cudaMemcpyAsync(h->d_cv + 3 * o, st->v, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, q));
+  SPH_CUDA(cudaMemcpyAsync(h->d_crho + o, st->rho, sizeof(double) * n, cudaMemcpyHostToDevice, q));
+  SPH_CUDA(cudaMemcpyAsync(h->d_cp + o, st->p, sizeof(double) * n, cudaMemcpyHostToDevice, q));
+  SPH_CUDA(cudaMemcpyAsync(h->d_cm + o, st->m, sizeof(double) * n, cudaMemcpyHostToDevice, q));
+  h->n_of[sim] = st->n;
+  return SPH_OK;
+}
+
+// IC of all simulations: sort, boundary data, IC time step.
+int initialise(SphHandle* h) {
+  cudaStream_t q = h->stream;
+  for (int s = 0; s < h->nsims; ++s) {
+    std::memset(&h->h_dyn[s], 0, sizeof(SimDyn));
+    h->h_dyn[s].nag = h->n_of[s];
+    h->h_dyn[s].dtmin_bits = 0x7FF0000000000000ull;
+    h->h_dyn[s].t_end = 0.0;
+  }
+  std::memset(&h->h_dyn[h->nsims], 0, sizeof(SimDyn));
+  SPH_CUDA(cudaMemcpyAsync(h->d_dyn, h->h_dyn.data(), sizeof(SimDyn) * (h->nsims + 1), cudaMemcpyHostToDevice, q));
+  launch_init_from_caller(h->db, h->d_cx, h->d_cv, h->d_crho, h->d_cp, h->d_cm, q);
+  sort_sequence(h, q);
+  launch_boundary(h->db, q);
+  launch_dt_reduce(h->db, q);
+  launch_finalize(h->db, 0, q);
+  SPH_CUDA(cudaGetLastError());
+  h->uploaded = true;
+  return sync_dyn(h);
+}
+
+}  // namespace
+
+// ==========================================================================
+// C ABI
+// ==========================================================================
+extern "C" {
+
+int sph_create(const SphParams* params, const SphGeometry* geometry, int32_t n_capacity, SphHandle** out) {
+  if (!params || !geometry) return SPH_ERR_INVALID_ARGUMENT;
+  return create_batch(1, params, geometry, &n_capacity, out);
+}
+
+int sph_batch_create(int32_t nsims, const SphParams* params, const SphGeometry* geometries,
+                     const int32_t* n_capacity, SphHandle** out) {
+  return create_batch(nsims, params, geometries, n_capacity, out);
+}
+
+void sph_destroy(SphHandle* h) {
+  if (!h) return;
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  if (h->graph) cudaGraphExecDestroy(h->graph);
+  for (void* p : h->owned) cudaFree(p);
+  if (h->stream) cudaStreamDestroy(h->stream);
+  cudaGetLastError();
+  delete h;
+}
+
+int sph_upload(SphHandle* h, const SphState* state) {
+  if (!h || h->nsims != 1) return SPH_ERR_INVALID_ARGUMENT;
+  SPH_TRY(upload_sim(h, 0, state));
+  return initialise(h);
+}
+
+int sph_batch_upload(SphHandle* h, int32_t nsims, const SphState* states) {
+  if (!h || nsims != h->nsims || !states) return SPH_ERR_INVALID_ARGUMENT;
+  for (int s = 0; s < nsims; ++s) SPH_TRY(upload_sim(h, s, &states[s]));
+  return initialise(h);
+}
+
+int sph_batch_set_end_time(SphHandle* h, int32_t sim, double t_end) {
+  if (!h || sim < 0 || sim >= h->nsims || !h->uploaded) return SPH_ERR_INVALID_ARGUMENT;
+  SPH_CUDA(cudaMemcpyAsync(&h->d_dyn[sim].t_end, &t_end, sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  return cuda_status(cudaStreamSynchronize(h->stream));
+}
+
+static int download_impl(SphHandle* h, int sim, SphState* state, double* acc, double* dden) {
+  if (!h || !h->uploaded || sim < 0 || sim >= h->nsims) return SPH_ERR_INVALID_ARGUMENT;
+  SPH_TRY(sync_dyn(h));
+  HostSim& hs = h->sims[sim];
+  int n = h->h_dyn[sim].nag;
+  cudaStream_t q = h->stream;
+  launch_to_caller(h->db, h->d_cx, h->d_cv, h->d_crho, h->d_cp, h->d_cm, acc ? h->d_cacc : nullptr,
+                   dden ? h->d_cdden : nullptr, q);
+  SPH_CUDA(cudaGetLastError());
+  size_t o = hs.dev.p_off;
+  if (state) {
+    state->n = n;
+    if (state->x) SPH_CUDA(cudaMemcpyAsync(state->x, h->d_cx + 3 * o, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, q));
+    if (state->v) SPH_CUDA(cudaMemcpyAsync(state->v, h->d_cv + 3 * o, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, q));
+    if (state->rho) SPH_CUDA(cudaMemcpyAsync(state->rho, h->d_crho + o, sizeof(double) * n, cudaMemcpyDeviceToHost, q));
+    if (state->p) SPH_CUDA(cudaMemcpyAsync(state->p, h->d_cp + o, sizeof(double) * n, cudaMemcpyDeviceToHost, q));
+    if (state->m) SPH_CUDA(cudaMemcpyAsync(state->m, h->d_cm + o, sizeof(double) * n, cudaMemcpyDeviceToHost, q));
+  }
+  if (acc) SPH_CUDA(cudaMemcpyAsync(acc, h->d_cacc + 3 * o, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, q));
+  if (dden) SPH_CUDA(cudaMemcpyAsync(dden, h->d_cdden + o, sizeof(double) * n, cudaMemcpyDeviceToHost, q));
+  return cuda_status(cudaStreamSynchronize(q));
+}
+
+int sph_download(SphHandle* h, SphState* state) {
+  if (!h || h->nsims != 1 || !state) return SPH_ERR_INVALID_ARGUMENT;
+  return download_impl(h, 0, state, nullptr, nullptr);
+}
+
+int sph_batch_download(SphHandle* h, int32_t sim, SphState* state) { return download_impl(h, sim, state, nullptr, nullptr); }
+
+static void fill_info(SphHandle* h, int sim, SphStepInfo* info) {
+  const SimDyn& d = h->h_dyn[sim];
+  info->time = d.time;
+  info->dt = d.dt_prev;
+  info->step = d.step;
+  info->n = d.nag;
+  info->warnings = d.warnings;
+  info->max_neighbours = d.max_neigh;
+}
+
+int sph_step(SphHandle* h, int32_t nsteps, SphStepInfo* info) {
+  if (!h || !h->uploaded || nsteps < 0) return SPH_ERR_INVALID_ARGUMENT;
+  SPH_TRY(build_graph(h));
+  for (int s = 0; s < nsteps; ++s) SPH_CUDA(cudaGraphLaunch(h->graph, h->stream));
+  SPH_TRY(sync_dyn(h));
+  if (info) fill_info(h, 0, info);
+  return SPH_OK;
+}
+
+// Enqueue steps without waiting (the caller synchronises through sph_sync).
+int sph_step_async(SphHandle* h, int32_t nsteps) {
+  if (!h || !h->uploaded || nsteps < 0) return SPH_ERR_INVALID_ARGUMENT;
+  SPH_TRY(build_graph(h));
+  for (int s = 0; s < nsteps; ++s) SPH_CUDA(cudaGraphLaunch(h->graph, h->stream));
+  return SPH_OK;
+}
+
+int sph_sync(SphHandle* h) {
+  if (!h) return SPH_ERR_INVALID_ARGUMENT;
+  return sync_dyn(h);
+}
+
+int sph_batch_info(SphHandle* h, int32_t sim, SphStepInfo* info, int32_t* frozen) {
+  if (!h || sim < 0 || sim >= h->nsims || !info) return SPH_ERR_INVALID_ARGUMENT;
+  SPH_TRY(sync_dyn(h));
+  fill_info(h, sim, info);
+  if (frozen) *frozen = h->h_dyn[sim].frozen;
+  return SPH_OK;
+}
+
+void* sph_stream(SphHandle* h) { return h ? (void*)h->stream : nullptr; }
+
+int sph_get_diagnostics(SphHandle* h, SphDiagnostics* diag) {
+  if (!h || !diag) return SPH_ERR_INVALID_ARGUMENT;
+  int st = sync_dyn(h);
+  const SimDyn& d = h->h_dyn[0];
+  const SimDev& s = h->sims[0].dev;
+  diag->warnings = d.warnings;
+  diag->status = d.status;
+  diag->removed_out_of_grid = d.removed_total;
+  diag->ncbf_max = d.ncbf_max;
+  diag->bdt_entries = h->h_dyn[h->nsims].bdt_used;
+  diag->nmaxpartj = s.nmaxpartj;
+  for (int k = 0; k < 3; ++k) diag->grid_ncd[k] = s.ncd[k];
+  diag->n_cells = s.ncells;
+  return st == SPH_ERR_CUDA ? st : SPH_OK;
+}
+
+// ---------------------------------------------------------------- fine-grained
+int sph_time_step_duration(SphHandle* h, double* dt_out) {
+  if (!h || !h->uploaded) return SPH_ERR_INVALID_ARGUMENT;
+  SPH_TRY(sync_dyn(h));
+  if (dt_out) *dt_out = h->h_dyn[0].dt;
+  return SPH_OK;
+}
+
+int sph_rhs_momentum(SphHandle* h, double* acc_out) {
+  if (!h || !h->uploaded) return SPH_ERR_INVALID_ARGUMENT;
+  launch_momentum(h->db, false, h->stream);
+  SPH_CUDA(cudaGetLastError());
+  if (acc_out) return download_impl(h, 0, nullptr, acc_out, nullptr);
+  return sync_dyn(h);
+}
+
+int sph_leapfrog_momentum(SphHandle* h) {
+  if (!h || !h->uploaded) return SPH_ERR_INVALID_ARGUMENT;
+  launch_leapfrog_momentum(h->db, h->stream);
+  SPH_CUDA(cudaGetLastError());
+  return sync_dyn(h);
+}
+
+int sph_leapfrog_trajectories(SphHandle* h) {
+  if (!h || !h->uploaded) return SPH_ERR_INVALID_ARGUMENT;
+  launch_leapfrog_trajectories(h->db, h->stream);
+  SPH_CUDA(cudaGetLastError());
+  return sync_dyn(h);
+}
+
+int sph_ord_grid(SphHandle* h) {
+  if (!h || !h->uploaded) return SPH_ERR_INVALID_ARGUMENT;
+  launch_stage(h->db, h->stream);
+  sort_sequence(h, h->stream);
+  SPH_CUDA(cudaGetLastError());
+  return sync_dyn(h);
+}
+
+int sph_boundary_data_tab(SphHandle* h) {
+  if (!h || !h->uploaded) return SPH_ERR_INVALID_ARGUMENT;
+  launch_boundary(h->db, h->stream);
+  SPH_CUDA(cudaGetLastError());
+  return sync_dyn(h);
+}
+
+int sph_continuity(SphHandle* h, double* dden_out) {
+  if (!h || !h->uploaded) return SPH_ERR_INVALID_ARGUMENT;
+  launch_continuity(h->db, false, h->stream);
+  SPH_CUDA(cudaGetLastError());
+  if (dden_out) return download_impl(h, 0, nullptr, nullptr, dden_out);
+  return sync_dyn(h);
+}
+
+int sph_leapfrog_continuity(SphHandle* h) {
+  if (!h || !h->uploaded) return SPH_ERR_INVALID_ARGUMENT;
+  launch_leapfrog_continuity(h->db, h->stream);
+  SPH_CUDA(cudaGetLastError());
+  return sync_dyn(h);
+}
+
+int sph_eos(SphHandle* h) {
+  if (!h || !h->uploaded) return SPH_ERR_INVALID_ARGUMENT;
+  launch_eos(h->db, h->stream);
+  launch_dt_reduce(h->db, h->stream);
+  launch_finalize(h->db, 1, h->stream);
+  SPH_CUDA(cudaGetLastError());
+  return sync_dyn(h);
+}
+
+// ---------------------------------------------------------------- verification
+int sph_dump_grid(SphHandle* h, int32_t* cella, int32_t* icont, int32_t* npartord) {
+  if (!h || !h->uploaded || h->nsims != 1) return SPH_ERR_INVALID_ARGUMENT;
+  SPH_TRY(sync_dyn(h));
+  int n = h->h_dyn[0].nag;
+  int ncells = h->sims[0].dev.ncells;
+  cudaStream_t q = h->stream;
+  if (cella) {
+    launch_dump_cella(h->db, h->d_ci1, q);
+    SPH_CUDA(cudaMemcpyAsync(cella, h->d_ci1, sizeof(int) * n, cudaMemcpyDeviceToHost, q));
+  }
+  if (icont || npartord) {
+    launch_sort_reset(h->db, q);
+    launch_bin(h->db, KeyKind::Reference, q);
+    launch_scan(h->db, h->d_ci2, q);
+    launch_rank_reference(h->db, h->d_ci2, h->d_ci3, q);
+    SPH_CUDA(cudaGetLastError());
+    if (icont) {
+      std::vector<int> cs(ncells + 1);
+      SPH_CUDA(cudaMemcpyAsync(cs.data(), h->d_ci2, sizeof(int) * (ncells + 1), cudaMemcpyDeviceToHost, q));
+      SPH_CUDA(cudaStreamSynchronize(q));
+      for (int c = 0; c <= ncells; ++c) icont[c] = cs[c] + 1;   // Icont is 1-based
+    }
+    if (npartord) SPH_CUDA(cudaMemcpyAsync(npartord, h->d_ci3, sizeof(int) * n, cudaMemcpyDeviceToHost, q));
+  }
+  return cuda_status(cudaStreamSynchronize(q));
+}
+
+int sph_dump_neighbours(SphHandle* h, int32_t nmaxj, int32_t* counts, int32_t* lists) {
+  if (!h || !h->uploaded || h->nsims != 1 || nmaxj <= 0 || !counts || !lists) return SPH_ERR_INVALID_ARGUMENT;
+  SPH_TRY(sync_dyn(h));
+  int n = h->h_dyn[0].nag;
+  int* dl = nullptr;
+  SPH_TRY(dalloc(&dl, (size_t)n * nmaxj));
+  cudaStream_t q = h->stream;
+  cudaMemsetAsync(dl, 0, sizeof(int) * (size_t)n * nmaxj, q);
+  launch_dump_neighbours(h->db, nmaxj, h->d_ci1, dl, q);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpyAsync(counts, h->d_ci1, sizeof(int) * n, cudaMemcpyDeviceToHost, q);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(lists, dl, sizeof(int) * (size_t)n * nmaxj, cudaMemcpyDeviceToHost, q);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(q);
+  cudaFree(dl);
+  return cuda_status(e);
+}
+
+int sph_dump_boundary(SphHandle* h, int32_t max_per, int32_t* ncb, int32_t* clobonum, double* values) {
+  if (!h || !h->uploaded || h->nsims != 1 || max_per <= 0 || !ncb || !clobonum || !values) return SPH_ERR_INVALID_ARGUMENT;
+  SPH_TRY(sync_dyn(h));
+  int n = h->h_dyn[0].nag;
+  int *dc = nullptr;
+  double* dv = nullptr;
+  SPH_TRY(dalloc(&dc, (size_t)n * max_per));
+  if (dalloc(&dv, (size_t)n * max_per * 20) != SPH_OK) { cudaFree(dc); return SPH_ERR_ALLOC; }
+  cudaStream_t q = h->stream;
+  cudaMemsetAsync(dc, 0, sizeof(int) * (size_t)n * max_per, q);
+  cudaMemsetAsync(dv, 0, sizeof(double) * (size_t)n * max_per * 20, q);
+  launch_dump_boundary(h->db, max_per, h->d_ci1, dc, dv, q);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpyAsync(ncb, h->d_ci1, sizeof(int) * n, cudaMemcpyDeviceToHost, q);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(clobonum, dc, sizeof(int) * (size_t)n * max_per, cudaMemcpyDeviceToHost, q);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(values, dv, sizeof(double) * (size_t)n * max_per * 20, cudaMemcpyDeviceToHost, q);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(q);
+  cudaFree(dc);
+  cudaFree(dv);
+  return cuda_status(e);
+}
+
+}  // extern "C"

@@ -1,0 +1,1640 @@
+// Device kernels of the FP64 path: cell binning and sort, SA-SPH boundary
+// data, continuity and momentum pair passes, leapfrog, EoS and time step.
+//
+// Compiled with --fmad=false: every FP64 expression below is evaluated in
+// the reference's left-to-right order without contraction, like the
+// gfortran -O2 x86-64 build of the reference (src/Makefile:124), so the
+// pair sums reproduce the reference's rounding.
+#include <cstdint>
+#include <cfloat>
+#include "../../include/sphera_b200.h"
+#include "sph_internal.cuh"
+#include "sph_launch.h"
+
+namespace sph {
+
+// BoundIntegralTab2D (SA_SPH_module.f90:29-54), filled by the host with the
+// single-precision roundings of the table's default-REAL literals.
+__constant__ double c_bit2d[22][6];
+
+namespace {
+
+constexpr double kMaxPositive = 3.4e+38;       // max_positive_number
+constexpr double kPigreco = 3.14159265358979e0;
+constexpr double kKernelConst2D = 0.454728408833987e0;
+constexpr double kDeltaXBit = 0.1;
+
+// --------------------------------------------------------------------------
+// small helpers
+// --------------------------------------------------------------------------
+
+__device__ __forceinline__ void load_sim(SimDev& dst, const SimDev* src, int sim, int& cur) {
+  if (cur == sim) return;
+  __syncthreads();
+  const unsigned long long* s = reinterpret_cast<const unsigned long long*>(src + sim);
+  unsigned long long* d = reinterpret_cast<unsigned long long*>(&dst);
+  constexpr int n = sizeof(SimDev) / 8;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) d[i] = s[i];
+  cur = sim;
+  __syncthreads();
+}
+
+// ParticleCellNumber.f90:52-62 + CellNumber.f90:53-59: 1-based (i,j,k),
+// false if outside the grid.
+__device__ __forceinline__ bool particle_cell(const SimDev& s, double x, double y, double z, int& i, int& j,
+                                              int& k) {
+  double ci = ceil((x - s.extr_lo[0]) / s.dcd[0]);
+  double ck = ceil((z - s.extr_lo[2]) / s.dcd[2]);
+  double cj = (s.dim == 3) ? ceil((y - s.extr_lo[1]) / s.dcd[1]) : 1.0;
+  if (!(ci >= 1.0 && ci <= (double)s.ncd[0] && cj >= 1.0 && cj <= (double)s.ncd[1] && ck >= 1.0 &&
+        ck <= (double)s.ncd[2]))
+    return false;
+  i = (int)ci;
+  j = (int)cj;
+  k = (int)ck;
+  return true;
+}
+
+// Contiguous slot range of neighbour column r (reference order: y, then x).
+template <int DIM>
+__device__ __forceinline__ void neighbour_run(const SimDev& s, const int* __restrict__ cell_start, int ci, int cj,
+                                              int ck, int r, int& b, int& e) {
+  int jr = (DIM == 3) ? cj - 1 + r / 3 : cj;
+  int ir = ci - 1 + ((DIM == 3) ? r % 3 : r);
+  b = 0;
+  e = 0;
+  if (ir < 1 || ir > s.ncd[0] || jr < 1 || jr > s.ncd[1]) return;
+  int klo = ck > 1 ? ck - 1 : 1;
+  int khi = ck < s.ncd[2] ? ck + 1 : s.ncd[2];
+  int base = s.cell_off + ((jr - 1) * s.ncd[0] + (ir - 1)) * s.ncd[2];
+  b = __ldg(cell_start + base + klo - 1);
+  e = __ldg(cell_start + base + khi);
+}
+
+// Kernel values of CalcVarLength.f90:242-269 for an accepted pair.
+__device__ __forceinline__ void kernel_values(const SimDev& s, double rijtemp2, double& PK1, double& PK2,
+                                              double& PK3) {
+  double rijtemp = sqrt(rijtemp2);
+  double rij_su_h = rijtemp / s.h;
+  double rij_su_h_quad = rijtemp2 / s.squareh;
+  int index_rij_su_h = (int)rij_su_h;
+  double denom = 1.0 / (rijtemp + s.eta);
+  PK1 = 0.0;
+  PK2 = 0.0;
+  PK3 = 0.0;
+  if (index_rij_su_h >= 2) return;
+  double gradmod = -(2.0 * rij_su_h) + 1.5 * rij_su_h_quad;
+  double gradmodwacl = -12.0 - 3.0 * rij_su_h_quad + 12.0 * rij_su_h;
+  if (index_rij_su_h > 0) gradmod = -gradmod + rij_su_h_quad - 2.0;
+  gradmod = gradmod * s.ke_coef;
+  gradmodwacl = gradmodwacl * s.kacl_coef;
+  PK1 = gradmod * denom;
+  PK2 = PK1 / (rijtemp2 + s.eta2);
+  PK3 = gradmodwacl * denom;
+}
+
+__device__ __forceinline__ void set_status(SimDyn* d, int code) { atomicCAS(&d->status, 0, code); }
+
+__device__ __forceinline__ double warp_min(double v) {
+  for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+__device__ __forceinline__ int warp_max(int v) {
+  for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+// InterpolateTable.f90:58-82 on columns 1..4.
+__device__ __forceinline__ void interpolate_table(const SimDev& s, double xval, double* iv) {
+  double deltaX = s.ktdelta;
+  double xval0 = s.kerneltab[0][0];
+  int nr0 = (int)((xval - xval0) / deltaX);
+  if (nr0 <= 0) {
+    for (int c = 0; c < 4; ++c) iv[c] = s.kerneltab[0][c + 1];
+  } else if (nr0 >= kKtRows) {
+    for (int c = 0; c < 4; ++c) iv[c] = s.kerneltab[kKtRows][c + 1];
+  } else {
+    double csi = (xval - s.kerneltab[nr0][0]) / deltaX;
+    for (int c = 0; c < 4; ++c)
+      iv[c] = s.kerneltab[nr0][c + 1] + csi * (s.kerneltab[nr0 + 1][c + 1] - s.kerneltab[nr0][c + 1]);
+  }
+}
+
+// LocalNormalCoordinates.f90:59-87 + IsPointInternal.f90:54-72.
+__device__ __forceinline__ bool point_internal(const FaceDev& f, double px, double py) {
+  double c0 = (f.AA[0] + f.BB[0] * px + f.CC[0] * py) * f.usu_due_area;
+  double c1 = (f.AA[1] + f.BB[1] * px + f.CC[1] * py) * f.usu_due_area;
+  if (f.fkod == 2) return !(c0 < 0.0 || c0 > 1.0 || c1 < 0.0 || c1 > 1.0);
+  if (f.fkod == 1) {
+    double c2 = 1.0 - (c0 + c1);
+    return !(c0 < 0.0 || c0 > 1.0 || c1 < 0.0 || c1 > 1.0 || c2 < 0.0 || c2 > 1.0);
+  }
+  return false;
+}
+
+// w.f90:48-57
+__device__ __forceinline__ double w_kernel(double r, double h, double coef) {
+  double s = r / h, q;
+  if (s <= 1.0) q = 0.666666667 + s * s * (s * 0.5 - 1.0);
+  else if (s >= 2.0) q = 0.0;
+  else {
+    double dms = 2.0 - s;
+    q = dms * dms * dms / 6.0;
+  }
+  return q * coef;
+}
+
+// WIntegr.f90:57-74
+__device__ __forceinline__ double w_integr(double ri, double hh) {
+  double ro = ri / hh;
+  if (0.0 <= ro && ro < 1.0) {
+    double ro2 = ro * ro, ro3 = ro2 * ro;
+    double W1 = (0.5 + -0.375 * ro2 + 0.15 * ro3) * ro2;
+    return kKernelConst2D * (0.35 - W1);
+  } else if (1.0 <= ro && ro < 2.0) {
+    double q1 = 2.0 - ro, q2 = q1 * q1, q4 = q2 * q2;
+    double W2 = (-0.125 + 0.05 * q1) * q4;
+    return -kKernelConst2D * W2;
+  }
+  return 0.0;
+}
+
+// J2Wro2.f90:50-63
+__device__ __forceinline__ double j2_wro2(double ro) {
+  const double a1 = 0.00833333333333333, a2 = 0.26666666666666667;
+  double ro2 = ro * ro, ro3 = ro2 * ro;
+  if (0.0 <= ro && ro < 1.0) return kKernelConst2D * (0.25 - (a1 * (40.0 - 36.0 * ro2 + 15.0 * ro3) * ro3));
+  if (1.0 <= ro && ro < 2.0)
+    return kKernelConst2D * (a2 - (a1 * (80.0 - 90.0 * ro + 36.0 * ro2 - 5.0 * ro3) * ro3));
+  return 0.0;
+}
+
+// InterpolateBoundaryIntegrals2D.f90:61-69
+__device__ __forceinline__ void interp_bit2d(int ncols, const int* col, double xx, double* func) {
+  if (xx < c_bit2d[0][0]) xx = c_bit2d[0][0];
+  int ii = (int)((xx - c_bit2d[0][0]) / kDeltaXBit) + 1;
+  if (ii > 21) ii = 21;  // the table ends at 2.001; deltai < 2 on this path
+  double xi = c_bit2d[ii - 1][0];
+  for (int nc = 0; nc < ncols; ++nc) {
+    double fi = c_bit2d[ii - 1][col[nc]];
+    double fip1 = c_bit2d[ii][col[nc]];
+    func[nc] = fi + (fip1 - fi) * (xx - xi) / kDeltaXBit;
+  }
+}
+
+}  // namespace
+
+// ==========================================================================
+// Sorting (OrdGrid1 replacement)
+// ==========================================================================
+
+// Copies the sorted state into the scratch record the sort consumes.
+__global__ void k_stage(DevBatch b) {
+  __shared__ SimDev s;
+  int cur = -1;
+  for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
+    Tile tl = b.tiles[t];
+    load_sim(s, b.sims, tl.sim, cur);
+    int p = tl.start + threadIdx.x;
+    if (threadIdx.x >= tl.count) continue;
+    const Particles& P = b.P;
+    double4 x = P.X[p];
+    double4 v = P.V[p];
+    double2 rp = P.RP[p];
+    P.X2[p] = x;
+    P.V2[p] = make_double4(v.x, v.y, v.z, rp.x);
+    P.P2[p] = rp.y;
+    P.I2[p] = P.I[p];
+    P.L2[p] = P.L[p];
+  }
+}
+
+// Cell key of every slot + atomic histogram.  KeyKind::Sort bins the
+// scratch record by the z-fastest layout key; KeyKind::Reference bins the
+// sorted state by CellNumber.f90's numbering for the grid dump.
+template <KeyKind KIND>
+__global__ void k_bin(DevBatch b) {
+  __shared__ SimDev s;
+  int cur = -1;
+  const Particles& P = b.P;
+  for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
+    Tile tl = b.tiles[t];
+    load_sim(s, b.sims, tl.sim, cur);
+    if (threadIdx.x >= tl.count) continue;
+    int p = tl.start + threadIdx.x;
+    SimDyn* dyn = b.dyn + tl.sim;
+    int nag = dyn->nag;
+    int key = s.cell_off + s.ncells;  // removal bin
+    if (p < s.p_off + nag) {
+      double4 x = (KIND == KeyKind::Sort) ? P.X2[p] : P.X[p];
+      int i, j, k;
+      if (particle_cell(s, x.x, x.y, x.z, i, j, k)) {
+        key = s.cell_off + ((KIND == KeyKind::Sort) ? cell_key_local(s, i, j, k)
+                                                     : ((k - 1) * s.ncd[1] + (j - 1)) * s.ncd[0] + (i - 1));
+      } else if (KIND == KeyKind::Sort) {
+        atomicAdd(&dyn->n_out, 1);
+        P.out_flag[s.p_off + P.I2[p] - 1] = 1;
+      }
+    }
+    P.key[p] = key;
+    P.slot[p] = atomicAdd(P.cell_count + key, 1);
+  }
+}
+
+// OrdGrid1.f90:58-82: particles out of the grid are removed by moving the
+// last particle into their place, in increasing particle index.  Replayed
+// exactly (one thread per simulation, only when a removal happened).
+__global__ void k_removal(DevBatch b) {
+  int sim = blockIdx.x;
+  if (threadIdx.x != 0 || sim >= b.nsims) return;
+  SimDyn* d = b.dyn + sim;
+  if (d->n_out == 0) return;
+  const SimDev& s = b.sims[sim];
+  uint8_t* out = b.P.out_flag + s.p_off - 1;   // 1-based by caller index
+  int* cur_of = b.P.cur_of + s.p_off - 1;
+  int* remap = b.P.id_remap + s.p_off - 1;
+  int n0 = d->nag;
+  int n = n0;
+  for (int id = 1; id <= n0; ++id) { cur_of[id] = id; remap[id] = 0; }
+  int npi = 0;
+  while (n > 0 && npi < n) {
+    npi = npi + 1;
+    if (out[npi]) {
+      out[npi] = out[n];
+      cur_of[npi] = cur_of[n];
+      n = n - 1;
+      npi = npi - 1;
+    }
+  }
+  for (int id = 1; id <= n; ++id) remap[cur_of[id]] = id;
+  for (int id = 1; id <= n0; ++id) out[id] = 0;
+  d->removed_total += n0 - n;
+  d->nag = n;
+  d->warnings |= SPH_WARN_PARTICLES_REMOVED;
+}
+
+// Exclusive scan of the cell histogram (3 phases), clearing the histogram.
+__device__ __forceinline__ int block_excl_scan(int v, int* warp_sums, int& total) {
+  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  int x = v;
+  for (int o = 1; o < 32; o <<= 1) {
+    int y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) warp_sums[wid] = x;
+  __syncthreads();
+  if (wid == 0) {
+    int nw = blockDim.x >> 5;
+    int ws = lane < nw ? warp_sums[lane] : 0;
+    for (int o = 1; o < 32; o <<= 1) {
+      int y = __shfl_up_sync(0xffffffffu, ws, o);
+      if (lane >= o) ws += y;
+    }
+    if (lane < nw) warp_sums[lane] = ws;
+  }
+  __syncthreads();
+  int base = wid > 0 ? warp_sums[wid - 1] : 0;
+  total = warp_sums[(blockDim.x >> 5) - 1];
+  __syncthreads();
+  return base + x - v;
+}
+
+constexpr int kScanThreads = 1024;
+constexpr int kScanPer = 4;
+constexpr int kScanChunk = kScanThreads * kScanPer;
+
+__global__ void __launch_bounds__(kScanThreads) k_scan1(const int* __restrict__ cnt, int n, int* block_sums) {
+  __shared__ int ws[32];
+  int base = blockIdx.x * kScanChunk + threadIdx.x * kScanPer;
+  int v = 0;
+  for (int q = 0; q < kScanPer; ++q) v += (base + q < n) ? cnt[base + q] : 0;
+  int total;
+  block_excl_scan(v, ws, total);
+  if (threadIdx.x == 0) block_sums[blockIdx.x] = total;
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_scan2(int* block_sums, int nb, int* cell_start, int n) {
+  __shared__ int ws[32];
+  int carry = 0;
+  for (int c0 = 0; c0 < nb; c0 += kScanThreads) {
+    int i = c0 + threadIdx.x;
+    int v = i < nb ? block_sums[i] : 0;
+    int total;
+    int ex = block_excl_scan(v, ws, total);
+    if (i < nb) block_sums[i] = ex + carry;
+    carry += total;
+  }
+  if (threadIdx.x == 0) cell_start[n] = carry;
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_scan3(int* cnt, int n, const int* block_sums, int* cell_start) {
+  __shared__ int ws[32];
+  int base = blockIdx.x * kScanChunk + threadIdx.x * kScanPer;
+  int vals[kScanPer];
+  int v = 0;
+  for (int q = 0; q < kScanPer; ++q) {
+    vals[q] = (base + q < n) ? cnt[base + q] : 0;
+    v += vals[q];
+  }
+  int total;
+  int ex = block_excl_scan(v, ws, total) + block_sums[blockIdx.x];
+  for (int q = 0; q < kScanPer; ++q) {
+    if (base + q < n) {
+      cell_start[base + q] = ex;
+      cnt[base + q] = 0;
+    }
+    ex += vals[q];
+  }
+}
+
+// Unstable placement by cell (the atomic slot), remembering the source.
+__global__ void k_place(DevBatch b, const int* __restrict__ cstart, int use_scratch_ids) {
+  __shared__ SimDev s;
+  int cur = -1;
+  const Particles& P = b.P;
+  for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
+    Tile tl = b.tiles[t];
+    load_sim(s, b.sims, tl.sim, cur);
+    if (threadIdx.x >= tl.count) continue;
+    int p = tl.start + threadIdx.x;
+    int key = P.key[p];
+    int dst = cstart[key] + P.slot[p];
+    int id = use_scratch_ids ? P.I2[p] : P.I[p];
+    if (use_scratch_ids && b.dyn[tl.sim].n_out > 0 && id > 0) id = P.id_remap[s.p_off + id - 1];
+    P.tmp_src[dst] = p;
+    P.tmp_id[dst] = id;
+    P.tmp_key[dst] = key;
+  }
+}
+
+// Rank inside the cell by caller index (OrdGrid1.f90:100-105 stable
+// scatter) and gather the scratch record into the sorted state.
+__global__ void k_rank_permute(DevBatch b) {
+  __shared__ SimDev s;
+  int cur = -1;
+  const Particles& P = b.P;
+  for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
+    Tile tl = b.tiles[t];
+    load_sim(s, b.sims, tl.sim, cur);
+    if (threadIdx.x >= tl.count) continue;
+    int d = tl.start + threadIdx.x;
+    int key = P.tmp_key[d];
+    int myid = P.tmp_id[d];
+    int fin = d;
+    if (key != s.cell_off + s.ncells) {
+      int cs = P.cell_start[key], ce = P.cell_start[key + 1];
+      int rank = 0;
+      for (int q = cs; q < ce; ++q) rank += (P.tmp_id[q] < myid) ? 1 : 0;
+      fin = cs + rank;
+    }
+    int src = P.tmp_src[d];
+    double4 x = P.X2[src];
+    double4 v = P.V2[src];
+    P.X[fin] = x;
+    P.V[fin] = make_double4(v.x, v.y, v.z, x.w / v.w);
+    P.RP[fin] = make_double2(v.w, P.P2[src]);
+    P.I[fin] = myid;
+    P.L[fin] = P.L2[src];
+  }
+}
+
+// NPartOrd of the reference numbering (verification only).
+__global__ void k_rank_reference(DevBatch b, const int* __restrict__ cstart, int* npartord) {
+  __shared__ SimDev s;
+  int cur = -1;
+  const Particles& P = b.P;
+  for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
+    Tile tl = b.tiles[t];
+    load_sim(s, b.sims, tl.sim, cur);
+    if (threadIdx.x >= tl.count) continue;
+    int d = tl.start + threadIdx.x;
+    int key = P.tmp_key[d];
+    if (key == s.cell_off + s.ncells) continue;
+    int myid = P.tmp_id[d];
+    int cs = cstart[key], ce = cstart[key + 1];
+    int rank = 0;
+    for (int q = cs; q < ce; ++q) rank += (P.tmp_id[q] < myid) ? 1 : 0;
+    npartord[cs + rank - s.p_off] = myid;
+  }
+}
+
+// ==========================================================================
+// SA-SPH boundary data (ComputeBoundaryDataTab_3D / _2D)
+// ==========================================================================
+
+// ComputeBoundaryVolumeIntegrals_P0.f90:81-155 for one (particle, face).
+__device__ void face_integrals(const SimDev& s, const double* __restrict__ bit, const FaceDev& f,
+                               const double* locx, BdtEntry& e) {
+  double IntWdV = 0.0, IntdWrm1dV = 0.0, IntGWZrm1dV = 0.0;
+  double G0 = 0.0, G1 = 0.0, G2 = 0.0;
+  double R00 = 0.0, R01 = 0.0, R02 = 0.0, R11 = 0.0, R12 = 0.0, R22 = 0.0;
+  double J0 = 0.0, J1 = 0.0, J2 = 0.0, J3 = 0.0;
+  double L0 = locx[0], L1 = locx[1], L2 = locx[2];
+  if (!(L2 < 0.0)) {
+    if (L2 < s.zpmin) L2 = s.zpmin;
+    double robpre = 2.1;
+    for (int ring = 0; ring < 8; ++ring) {
+      const double* row0 = bit + ring * 32 * 7;
+      double zp = row0[2];
+      double lpj2 = L2 + zp;
+      if (!(lpj2 <= 0.0)) continue;       // the whole ring lies above the face plane
+      double tsegnato = L2 / (L2 - lpj2);
+      for (int q = 0; q < 32; ++q) {
+        const double* row = row0 + q * 7;
+        double lpj0 = L0 + row[0];
+        double lpj1 = L1 + row[1];
+        double px0 = L0 + (lpj0 - L0) * tsegnato;
+        double px1 = L1 + (lpj1 - L1) * tsegnato;
+        if (!point_internal(f, px0, px1)) continue;
+        double d0 = px0 - L0, d1 = px1 - L1, d2 = 0.0 - L2;
+        double dist = sqrt(d0 * d0 + d1 * d1 + d2 * d2);
+        double rob = dist / s.h;
+        if (fabs(rob - robpre) > 1.0e-3) {
+          double iv[4];
+          interpolate_table(s, rob, iv);
+          double da = row[3];
+          J0 = iv[0] * da;
+          J1 = iv[1] * da;
+          J2 = iv[2] * da;
+          J3 = iv[3] * da;
+          robpre = rob;
+        }
+        double r0 = row[4], r1 = row[5], r2 = row[6];
+        double RZ2 = r2 * r2;
+        IntWdV = IntWdV + J0;
+        IntdWrm1dV = IntdWrm1dV + J1;
+        IntGWZrm1dV = IntGWZrm1dV + RZ2 * J1;
+        G0 = G0 + r0 * J2;
+        R00 = R00 + r0 * r0 * J3;
+        R01 = R01 + r0 * r1 * J3;
+        R02 = R02 + r0 * r2 * J3;
+        G1 = G1 + r1 * J2;
+        R11 = R11 + r1 * r1 * J3;
+        R12 = R12 + r1 * r2 * J3;
+        G2 = G2 + r2 * J2;
+        R22 = R22 + r2 * r2 * J3;
+      }
+    }
+    if (L2 == s.zpmin) IntWdV = point_internal(f, L0, L1) ? 0.5 : 0.0;
+  }
+  e.bi[0] = 0.0;
+  e.bi[1] = IntWdV;
+  e.bi[2] = IntdWrm1dV;
+  e.bi[3] = G0;
+  e.bi[4] = G1;
+  e.bi[5] = G2;
+  e.bi[6] = IntGWZrm1dV;
+  e.bi[7] = 0.0;
+  e.ig[0] = R00; e.ig[1] = R01; e.ig[2] = R02;
+  e.ig[3] = R01; e.ig[4] = R11; e.ig[5] = R12;
+  e.ig[6] = R02; e.ig[7] = R12; e.ig[8] = R22;
+}
+
+// ComputeBoundaryDataTab_3D.f90:67-105 with FindCloseBoundaryFaces3D.f90:79-188.
+__global__ void __launch_bounds__(kBlock) k_boundary3d(DevBatch b) {
+  __shared__ SimDev s;
+  int cur = -1;
+  const Particles& P = b.P;
+  for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
+    Tile tl = b.tiles[t];
+    load_sim(s, b.sims, tl.sim, cur);
+    if (threadIdx.x >= tl.count) continue;
+    int p = tl.start + threadIdx.x;
+    SimDyn* dyn = b.dyn + tl.sim;
+    P.bdt_count[p] = 0;
+    if (p >= s.p_off + dyn->nag || s.nfaces == 0) continue;
+    double4 x = P.X[p];
+    int ic, jc, kc;
+    if (!particle_cell(s, x.x, x.y, x.z, ic, jc, kc)) continue;
+    if (!b.cell_near[s.cell_off + cell_key_local(s, ic, jc, kc)]) continue;
+    int clob[kMaxLocalFaces];
+    double pin[kMaxLocalFaces];
+    int ncbf = 0;
+    bool overflow = false;
+    for (int i = ic - 1; i <= ic + 1; ++i)
+      for (int j = jc - 1; j <= jc + 1; ++j)
+        for (int k = kc - 1; k <= kc + 1; ++k) {
+          if (i < 1 || i > s.ncd[0] || j < 1 || j > s.ncd[1] || k < 1 || k > s.ncd[2]) continue;
+          int gk = s.cell_off + cell_key_local(s, i, j, k);
+          int nf = b.cf_count[gk];
+          int fs = b.cf_start[gk];
+          for (int q = 0; q < nf; ++q) {
+            int fid = b.cf_list[fs + q];
+            bool there = false;
+            for (int u = 0; u < ncbf && u < kMaxLocalFaces; ++u) there |= (clob[u] == fid);
+            if (there) continue;
+            const FaceDev& f = b.faces[s.face_off + fid - 1];
+            double pn = 0.0;
+            pn = pn + f.T[0][2] * (x.x - f.GXref[0]);
+            pn = pn + f.T[1][2] * (x.y - f.GXref[1]);
+            pn = pn + f.T[2][2] * (x.z - f.GXref[2]);
+            if (pn >= 0.0 && pn < s.doubleh) {
+              if (ncbf >= s.maxcb || ncbf >= kMaxLocalFaces) {
+                overflow = true;
+              } else {
+                clob[ncbf] = fid;
+                pin[ncbf] = pn;
+              }
+              ncbf++;
+            }
+          }
+        }
+    if (overflow) {
+      set_status(dyn, SPH_ERR_CLOSE_FACES);
+      continue;
+    }
+    if (ncbf == 0) continue;
+    int gbase = atomicAdd(&b.dyn[b.nsims].bdt_used, ncbf);  // global allocation counter
+    if (gbase + ncbf > P.bdt_cap) {
+      set_status(dyn, SPH_ERR_BDT_OVERFLOW);
+      continue;
+    }
+    atomicMax(&dyn->ncbf_max, ncbf);
+    P.bdt_count[p] = ncbf;
+    P.bdt_start[p] = gbase;
+    const double* bit = b.bit + (size_t)tl.sim * kBitRows * 7;
+    for (int u = 0; u < ncbf; ++u) {
+      const FaceDev& f = b.faces[s.face_off + clob[u] - 1];
+      double locx[3];
+      for (int sdi = 0; sdi < 2; ++sdi) {
+        double acc = 0.0;
+        acc = acc + f.T[0][sdi] * (x.x - f.GXref[0]);
+        acc = acc + f.T[1][sdi] * (x.y - f.GXref[1]);
+        acc = acc + f.T[2][sdi] * (x.z - f.GXref[2]);
+        locx[sdi] = acc;
+      }
+      locx[2] = pin[u];
+      BdtEntry e;
+      face_integrals(s, bit, f, locx, e);
+      e.loc[0] = locx[0];
+      e.loc[1] = locx[1];
+      e.loc[2] = locx[2];
+      e.clobonum = clob[u];
+      e.pad = 0;
+      P.bdt[gbase + u] = e;
+    }
+  }
+}
+
+// ComputeBoundaryDataTab_2D.f90:70-157 with FindCloseBoundarySides2D,
+// SelectCloseBoundarySides2D, FindBoundaryIntersection2D,
+// ComputeSurfaceIntegral_WdS2D, BoundaryVolumeIntegrals2D,
+// ComputeVolumeIntegral_WdV2D and InterpolateBoundaryIntegrals2D.
+__global__ void __launch_bounds__(kBlock) k_boundary2d(DevBatch b) {
+  __shared__ SimDev s;
+  int cur = -1;
+  const Particles& P = b.P;
+  for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
+    Tile tl = b.tiles[t];
+    load_sim(s, b.sims, tl.sim, cur);
+    if (threadIdx.x >= tl.count) continue;
+    int p = tl.start + threadIdx.x;
+    SimDyn* dyn = b.dyn + tl.sim;
+    P.bdt_count[p] = 0;
+    if (p >= s.p_off + dyn->nag || s.nsides == 0) continue;
+    double4 x = P.X[p];
+    const SideDev* sd = b.sides + s.side_off;
+    int clob[kMaxCloseSides];
+    double lx[kMaxCloseSides], ly[kMaxCloseSides];
+    int ncbs = 0;
+    bool overflow = false;
+    for (int isi = 1; isi <= s.nsides; ++isi) {
+      const SideDev& S = sd[isi - 1];
+      double P1P0 = x.x - S.v1[0], P1P1 = x.z - S.v1[1];
+      double sidel = S.length;
+      double xp = P1P0 * S.sss[0] + P1P1 * S.sss[1];
+      double yp = P1P0 * S.nnn[0] + P1P1 * S.nnn[1];
+      double xpmin = -s.doubleh, xpmax = sidel + s.doubleh;
+      double ypmin = -s.doubleh, ypmax = s.doubleh;
+      if ((xpmin < xp && xp < xpmax) && (ypmin < yp && yp < ypmax)) {
+        double ypmx = 0.0, ypmn = 0.0;
+        if (xp < 0.0) {
+          ypmx = sqrt(s.square_doubleh - xp * xp);
+          ypmn = -ypmx;
+        } else if (xp <= sidel) {
+          ypmx = ypmax;
+          ypmn = ypmin;
+        } else if (xp < xpmax) {
+          double L = (sidel - xp) * (sidel - xp);
+          ypmx = sqrt(s.square_doubleh - L);
+          ypmn = -ypmx;
+        }
+        if (ypmn < yp && yp < ypmx) {
+          if (ncbs >= kMaxCloseSides) {
+            overflow = true;
+          } else {
+            clob[ncbs] = isi;
+            lx[ncbs] = xp;
+            ly[ncbs] = yp;
+          }
+          ncbs++;
+        }
+      }
+    }
+    if (overflow) {
+      set_status(dyn, SPH_ERR_CLOSE_SIDES);
+      continue;
+    }
+    if (ncbs == 0) continue;
+    if (ncbs == 2) {
+      if (sd[clob[0] - 1].previous_side == clob[1]) lx[1] = sd[clob[1] - 1].length - lx[1];
+      else if (sd[clob[1] - 1].previous_side == clob[0]) lx[0] = sd[clob[0] - 1].length - lx[0];
+    }
+    // SelectCloseBoundarySides2D: fixe / tapi sides in front of the particle
+    int ib[kMaxCloseSides];
+    double ix[kMaxCloseSides], iy[kMaxCloseSides];
+    int nint = 0;
+    for (int c = 0; c < ncbs; ++c)
+      if (ly[c] > 0.0) {
+        ib[nint] = clob[c];
+        ix[nint] = lx[c];
+        iy[nint] = ly[c];
+        nint++;
+      }
+    if (nint == 0) continue;
+    int gbase = atomicAdd(&b.dyn[b.nsims].bdt_used, nint);
+    if (gbase + nint > P.bdt_cap) {
+      set_status(dyn, SPH_ERR_BDT_OVERFLOW);
+      continue;
+    }
+    P.bdt_count[p] = nint;
+    P.bdt_start[p] = gbase;
+    for (int c = 0; c < nint; ++c) {
+      BdtEntry e;
+      for (int q = 0; q < 9; ++q) e.ig[q] = 0.0;
+      for (int q = 0; q < 8; ++q) e.bi[q] = 0.0;
+      e.clobonum = ib[c];
+      e.pad = 0;
+      e.loc[0] = ix[c];
+      e.loc[1] = iy[c];
+      e.loc[2] = 0.0;
+      double func[5] = {0, 0, 0, 0, 0};
+      if (nint == 2) {
+        // FindBoundaryIntersection2D.f90:61-92
+        double minlen = 0.01 * s.h;
+        double xpi = ix[c], ypi = iy[c];
+        if (ypi < 0.0) ypi = 0.0;
+        double halfchord = sqrt(s.square_doubleh - ypi * ypi);
+        double XA = xpi - halfchord, XB = xpi + halfchord;
+        double xpmin = 0.0;
+        if (XA > xpmin) xpmin = XA;
+        double xpmax = sd[ib[c] - 1].length;
+        if (XB < xpmax) xpmax = XB;
+        double interlen = xpmax - xpmin;
+        if (interlen <= minlen) interlen = 0.0;
+        // ComputeSurfaceIntegral_WdS2D.f90:57-83
+        double IntWdS = 0.0;
+        if (interlen > 0.0) {
+          double dsrif = s.h / 2;
+          double ypc = iy[c] < 0.0 ? 0.0 : iy[c];
+          double ypiq = ypc * ypc;
+          int ndiv = (int)(interlen / dsrif + 0.5);
+          if (ndiv < 2) ndiv = 2;
+          double deltas = interlen / ndiv;
+          double xpip = xpmin - 0.5 * deltas;
+          for (int ipt = 1; ipt <= ndiv; ++ipt) {
+            xpip = xpip + deltas;
+            double dxpip = xpip - ix[c];
+            double ris = sqrt(dxpip * dxpip + ypiq);
+            IntWdS = IntWdS + w_kernel(ris, s.h, s.coefke) * deltas;
+          }
+        }
+        // BoundaryVolumeIntegrals2D.f90
+        double IntWdV = 0.0, D0 = 0.0, D1 = 0.0;
+        double dalfarif = kPigreco / 10;
+        double yplimite = 0.05 * s.h;
+        if (interlen > 0.0) {
+          double ypb = iy[c];
+          if (ypb < yplimite) ypb = yplimite;
+          double alfaA = atan2(xpmin - ix[c], ypb), alfaB = atan2(xpmax - ix[c], ypb);
+          double Intalfa = alfaB - alfaA;
+          int ndiv = (int)(Intalfa / dalfarif + 0.5);
+          if (ndiv < 1) ndiv = 1;
+          double dalfa = Intalfa / ndiv;
+          double alfa_k = alfaA - 0.5 * dalfa;
+          for (int k = 1; k <= ndiv; ++k) {
+            alfa_k = alfa_k + dalfa;
+            double sa = sin(alfa_k), ca = cos(alfa_k);
+            double rb = ypb / ca;
+            double rob = rb / s.h;
+            double mult = s.h * j2_wro2(rob) * dalfa;
+            D0 = D0 + sa * mult;
+            D1 = D1 - ca * mult;
+            IntWdV = IntWdV + w_integr(rb, s.h) * dalfa;
+          }
+          if (ypb == yplimite) IntWdV = 0.5;
+        }
+        // ComputeVolumeIntegral_WdV2D.f90
+        double IntWdV1 = 0.0;
+        if (interlen > 0.0) {
+          double ypv = iy[c];
+          if (ypv >= yplimite) {
+            double alfaA = atan2(xpmin - ix[c], ypv), alfaB = atan2(xpmax - ix[c], ypv);
+            double Intalfa = alfaB - alfaA;
+            int ndiv = (int)(Intalfa / dalfarif + 0.5);
+            if (ndiv < 2) ndiv = 2;
+            double dalfa = Intalfa / ndiv;
+            double alfa = alfaA - 0.5 * dalfa;
+            for (int ipt = 1; ipt <= ndiv; ++ipt) {
+              alfa = alfa + dalfa;
+              double ta = tan(alfa);
+              double ris = ypv * sqrt(1.0 + ta * ta);
+              IntWdV1 = IntWdV1 + w_integr(ris, s.h) * dalfa;
+            }
+          } else {
+            int jc = 1 - c;  // the other side (nint == 2)
+            double ypj = iy[jc];
+            if (ypj <= yplimite) {
+              double angle = 0.0;
+              if (sd[ib[0] - 1].previous_side == ib[1]) angle = sd[ib[0] - 1].angle;
+              else if (sd[ib[1] - 1].previous_side == ib[0]) angle = sd[ib[1] - 1].angle;
+              else set_status(dyn, 804);
+              IntWdV1 = 0.5 * (angle + kPigreco) / (2.0 * kPigreco);
+            } else {
+              IntWdV1 = (xpmin >= ix[c] && ix[c] <= xpmax) ? 0.5 : 0.0;
+            }
+          }
+        }
+        const int col[3] = {3, 4, 5};
+        interp_bit2d(3, col, iy[c] / s.h, func);
+        e.bi[0] = IntWdS;
+        e.bi[1] = IntWdV;
+        e.bi[2] = IntWdV1;
+        e.bi[3] = D0;
+        e.bi[4] = D1;
+        e.bi[5] = func[0] / s.squareh;
+        e.bi[6] = func[1] / s.squareh;
+        e.bi[7] = func[2] / s.squareh;
+      } else if (nint == 1) {
+        const int col[5] = {1, 2, 3, 4, 5};
+        interp_bit2d(5, col, iy[c] / s.h, func);
+        e.bi[0] = func[0] / s.h;
+        e.bi[1] = func[1];
+        e.bi[2] = func[1];
+        e.bi[3] = 0.0;
+        e.bi[4] = 0.0;
+        e.bi[5] = func[2] / s.squareh;
+        e.bi[6] = func[3] / s.squareh;
+        e.bi[7] = func[4] / s.squareh;
+      }
+      P.bdt[gbase + c] = e;
+    }
+  }
+}
+
+// ==========================================================================
+// Momentum: RHS_momentum_equation + inter_EqMoto + viscomon + viscomorris
+// + AddBoundaryContributions_to_ME3D/2D + AddElasticBoundaryReaction_3D/2D,
+// optionally fused with Leapfrog_momentum, velocity_smoothing_2 (TetaV=0),
+// Leapfrog_trajectories and the CFL part of time_step_duration.
+// ==========================================================================
+
+// AddBoundaryContributions_to_ME3D.f90:105-336 (fixe/tapi, slip mode 1).
+__device__ void me_boundary3d(const SimDev& s, const DevBatch& b, int nb, int start, const double* vi, double rhoi,
+                              double pres, int lam, double* tpres, double* tdiss, double* tvisc) {
+  double ALEt[3] = {0, 0, 0}, gradpt[3] = {0, 0, 0}, VMon[3] = {0, 0, 0}, VShear[3] = {0, 0, 0};
+  for (int u = 0; u < nb; ++u) {
+    const BdtEntry& e = b.P.bdt[start + u];
+    const FaceDev& f = b.faces[s.face_off + e.clobonum - 1];
+    if (!(e.loc[2] > 0.0)) continue;
+    double dvn = 0.0;
+    for (int SD = 0; SD < 3; ++SD) {
+      double dvij = 2.0 * (vi[SD] - f.velocity[SD]);
+      dvn = dvn + f.T[SD][2] * dvij;
+    }
+    double gl[3];
+    for (int SD = 0; SD < 3; ++SD) {
+      double a = 0.0;
+      for (int sdj = 0; sdj < 3; ++sdj) a = a + f.T[sdj][SD] * s.grav[sdj];
+      gl[SD] = a;
+    }
+    double loc[3];
+    for (int i = 0; i < 3; ++i) {
+      double a = 0.0;
+      for (int k = 0; k < 3; ++k) a = a + e.ig[3 * i + k] * gl[k];
+      loc[i] = a;
+    }
+    for (int i = 0; i < 3; ++i) {
+      double a = 0.0;
+      for (int k = 0; k < 3; ++k) a = a + f.T[i][k] * loc[k];
+      gradpt[i] = gradpt[i] + a;
+    }
+    double aloc[3];
+    for (int k = 0; k < 3; ++k) aloc[k] = 2.0 * pres / rhoi * e.bi[3 + k];
+    for (int i = 0; i < 3; ++i) {
+      double a = 0.0;
+      for (int k = 0; k < 3; ++k) a = a + f.T[i][k] * aloc[k];
+      ALEt[i] = ALEt[i] + a;
+    }
+    double IntGWZrm1dV = e.bi[6];
+    double IntdWrm1dV = e.bi[2];
+    if (s.alfa_mon > 0.0) {
+      double Monvisc = s.alfa_mon * s.celerita * s.h;
+      double Mmult = -(Monvisc * dvn * IntGWZrm1dV);
+      for (int d = 0; d < 3; ++d) VMon[d] = VMon[d] + Mmult * f.T[d][2];
+    }
+    double cinvisci = s.kin_visc;
+    if (cinvisci > 0.0 && (lam == 1 || !f.laminar_no_slip_check)) {
+      double cinviscmult = cinvisci * IntdWrm1dV * f.slip;
+      for (int d = 0; d < 3; ++d) VShear[d] = VShear[d] + cinviscmult * (2.0 * (vi[d] - f.velocity[d]));
+    }
+  }
+  for (int d = 0; d < 3; ++d) {
+    tpres[d] = tpres[d] + ALEt[d] + gradpt[d];
+    tdiss[d] = tdiss[d] - VMon[d];
+    tvisc[d] = tvisc[d] + VShear[d];
+  }
+}
+
+// AddBoundaryContributions_to_ME2D.f90:96-402 (fixe/tapi, slip mode 1).
+__device__ void me_boundary2d(const SimDev& s, const DevBatch& b, int nb, int start, const double* vi, double roi,
+                              double pressi, int lam, double* tpres, double* tdiss, double* tvisc) {
+  const double pibmink = 10.0;
+  double ro0 = s.den0, distpimin = s.dx;
+  double VMon[2] = {0, 0}, VShear[2] = {0, 0}, RG_sum[2] = {0, 0}, ALEt[2] = {0, 0};
+  const double g2[2] = {s.grav[0], s.grav[2]};
+  const double v2[2] = {vi[0], vi[2]};
+  for (int u = 0; u < nb; ++u) {
+    const BdtEntry& e = b.P.bdt[start + u];
+    const SideDev& S = b.sides[s.side_off + e.clobonum - 1];
+    double xpi = e.loc[0], ypi = e.loc[1];
+    double IntWdS = e.bi[0], IntWdV = e.bi[2], IntWd1s0 = e.bi[5], IntWd3s0 = e.bi[6];
+    double GravN = 0.0;
+    for (int i = 0; i < 2; ++i) GravN = GravN + g2[i] * S.nnn[i];
+    double sidevel[2] = {0.0, 0.0};
+    if (S.zone_type == SPH_ZONE_TAPI) {
+      sidevel[0] = S.velocity[0];
+      sidevel[1] = S.velocity[2];
+    }
+    double Dvel0 = 2.0 * (v2[0] - sidevel[0]), Dvel1 = 2.0 * (v2[1] - sidevel[1]);
+    double DvelN = Dvel0 * S.nnn[0] + Dvel1 * S.nnn[1];
+    double distpi = fmax(ypi, distpimin);
+    double pressib = pressi;
+    double pressibmin = pibmink * ro0 * distpimin;
+    if (DvelN <= 0.0 && pressib < pressibmin) pressib = pressibmin;
+    double PressB = pressib - ro0 * GravN * distpi;
+    double QiiIntWdS = IntWdS * (pressib + PressB) / roi;
+    for (int i = 0; i < 2; ++i) {
+      double RG = 0.0;
+      for (int j = 0; j < 2; ++j) RG = RG + S.RN[i][j] * g2[j];
+      RG = RG * IntWdV;
+      RG_sum[i] = RG_sum[i] + RG;
+    }
+    ALEt[0] = ALEt[0] - S.nnn[0] * QiiIntWdS;
+    ALEt[1] = ALEt[1] - S.nnn[1] * QiiIntWdS;
+    if (xpi >= 0.0 && xpi <= S.length) {
+      double Monvisc = s.alfa_mon * s.celerita * s.h;
+      double TN = Monvisc * DvelN * IntWd3s0;
+      double SVforce;
+      if (lam == 1 || !S.laminar_no_slip_check) SVforce = 2.0 * s.kin_visc * S.slip * IntWd1s0;
+      else SVforce = 0.0;
+      for (int i = 0; i < 2; ++i) {
+        VMon[i] = VMon[i] + TN * S.nnn[i];
+        VShear[i] = VShear[i] + (2.0 * v2[i]) * SVforce;
+      }
+    }
+  }
+  const int acix[2] = {0, 2};
+  for (int i = 0; i < 2; ++i) {
+    tpres[acix[i]] = tpres[acix[i]] - RG_sum[i] - ALEt[i];
+    tdiss[acix[i]] = tdiss[acix[i]] - VMon[i];
+    tvisc[acix[i]] = tvisc[acix[i]] - VShear[i];
+  }
+}
+
+// AddElasticBoundaryReaction_3D.f90:67-154 (no convex edges) / _2D.f90:63-97.
+template <int DIM>
+__device__ void elastic_reaction(const SimDev& s, const DevBatch& b, int nb, int start, const double* vi, double* R) {
+  R[0] = R[1] = R[2] = 0.0;
+  double zimin = 0.25 * s.dx;
+  double celer02 = s.eps / s.den0;
+  for (int u = 0; u < nb; ++u) {
+    const BdtEntry& e = b.P.bdt[start + u];
+    if (DIM == 3) {
+      const FaceDev& f = b.faces[s.face_off + e.clobonum - 1];
+      double zi = e.loc[2];
+      if (zi < zimin && point_internal(f, e.loc[0], e.loc[1])) {
+        double vin = 0.0;
+        for (int sd = 0; sd < 3; ++sd) vin = vin + vi[sd] * f.T[sd][2];
+        if (vin < 0.0) {
+          double normreact = -(1.0 * celer02 * log((s.h + zi - zimin) / s.h) / s.h);
+          for (int d = 0; d < 3; ++d) R[d] = R[d] + normreact * f.T[d][2];
+        }
+      }
+    } else {
+      const SideDev& S = b.sides[s.side_off + e.clobonum - 1];
+      double xpi = e.loc[0], ypi = e.loc[1];
+      if (ypi < zimin && xpi > 0.0 && xpi < S.length) {
+        double vin = 0.0;
+        vin = vin + vi[0] * S.nnn[0];
+        vin = vin + vi[1] * 0.0;
+        vin = vin + vi[2] * S.nnn[1];
+        if (vin < 0.0) {
+          double normreact = -(1.0 * celer02 * log((s.h + ypi - zimin) / s.h) / s.h);
+          R[0] = R[0] + normreact * S.nnn[0];
+          R[2] = R[2] + normreact * S.nnn[1];
+        }
+      }
+    }
+  }
+}
+
+template <int DIM, bool FUSED>
+__global__ void __launch_bounds__(kBlock) k_momentum(DevBatch b) {
+  __shared__ SimDev s;
+  __shared__ double red[kBlock / 32];
+  int cur = -1;
+  const Particles& P = b.P;
+  const double GI = (double)9.80665f;   // Static_allocation_module.f90:72, a default-REAL literal
+  for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
+    Tile tl = b.tiles[t];
+    load_sim(s, b.sims, tl.sim, cur);
+    SimDyn* dyn = b.dyn + tl.sim;
+    int p = tl.start + threadIdx.x;
+    bool active = threadIdx.x < tl.count && p < s.p_off + dyn->nag;
+    double dtc = 1.0e300;
+    int nneigh = 0;
+    if (FUSED && active && dyn->frozen) {
+      // a finished simulation of a batch: carry the record through the sort
+      double4 v4 = P.V[p];
+      double2 rp = P.RP[p];
+      P.X2[p] = P.X[p];
+      P.V2[p] = make_double4(v4.x, v4.y, v4.z, rp.x);
+      P.P2[p] = rp.y;
+      P.I2[p] = P.I[p];
+      P.L2[p] = P.L[p];
+      active = false;
+    }
+    if (active) {
+      double4 xi = P.X[p];
+      double4 v4 = P.V[p];
+      double2 rp = P.RP[p];
+      double vi[3] = {v4.x, v4.y, v4.z};
+      double rhoi = rp.x, pi = rp.y;
+      int lam = P.L[p];
+      double tpres[3] = {0, 0, 0}, tdiss[3] = {0, 0, 0}, tvisc[3] = {0, 0, 0};
+      int nb = P.bdt_count[p];
+      int bstart = nb > 0 ? P.bdt_start[p] : 0;
+      if (nb > 0) {
+        if (DIM == 3) me_boundary3d(s, b, nb, bstart, vi, rhoi, pi, lam, tpres, tdiss, tvisc);
+        else me_boundary2d(s, b, nb, bstart, vi, rhoi, pi, lam, tpres, tdiss, tvisc);
+      }
+      int ci, cj, ck;
+      particle_cell(s, xi.x, xi.y, xi.z, ci, cj, ck);
+      double tp0 = 0, tp1 = 0, tp2 = 0, al0 = 0, al1 = 0, al2 = 0;
+      double td0 = tdiss[0], td1 = tdiss[1], td2 = tdiss[2];
+      double tv0 = tvisc[0], tv1 = tvisc[1], tv2 = tvisc[2];
+      double rs0 = 0, rs1 = 0, rs2 = 0;
+      const double celt = s.celerita + s.celerita;
+      const bool morris = s.kin_visc > 1.0e-12;
+      const double nu = s.kin_visc;
+      bool trunc = false;
+      constexpr int NR = (DIM == 3) ? 9 : 3;
+      for (int r = 0; r < NR && !trunc; ++r) {
+        int qb, qe;
+        neighbour_run<DIM>(s, P.cell_start, ci, cj, ck, r, qb, qe);
+        for (int q = qb; q < qe; ++q) {
+          if (nneigh >= s.nmaxpartj) { trunc = true; break; }
+          double4 xj = P.X[q];
+          double r0 = xi.x - xj.x, r1 = xi.y - xj.y, r2 = xi.z - xj.z;
+          double rr = r0 * r0 + r1 * r1 + r2 * r2;
+          if (rr > s.square_doubleh) continue;
+          nneigh++;
+          if (q == p) continue;
+          double PK1, PK2, PK3;
+          kernel_values(s, rr, PK1, PK2, PK3);
+          double4 vj = P.V[q];
+          double2 rpj = P.RP[q];
+          double rhoj = rpj.x, pj = rpj.y, amassj = xj.w;
+          double dv0 = vj.x - vi[0], dv1 = vj.y - vi[1], dv2 = vj.z - vi[2];
+          // pressure gradient and ALE1 terms, inter_EqMoto.f90:195-221
+          double alpha = (pj - pi) / (rhoi * rhoj);
+          tp0 = tp0 + -(amassj * alpha * r0 * PK3);
+          if (DIM == 3) tp1 = tp1 + -(amassj * alpha * r1 * PK3);
+          tp2 = tp2 + -(amassj * alpha * r2 * PK3);
+          double alpha2 = (pi * (rhoj / rhoi + 1.0) + pj * (rhoi / rhoj - 1.0)) / (rhoi * rhoj);
+          al0 = al0 - amassj * alpha2 * r0 * PK3;
+          if (DIM == 3) al1 = al1 - amassj * alpha2 * r1 * PK3;
+          al2 = al2 - amassj * alpha2 * r2 * PK3;
+          // viscomon.f90:54-73
+          double vrij = (DIM == 3) ? -(dv0 * r0) - dv1 * r1 - dv2 * r2 : -(dv0 * r0) - dv2 * r2;
+          double TermMon = s.alfa_mon * celt * s.h / (rhoi + rhoj);
+          double mtv = amassj * TermMon * vrij;
+          td0 = td0 + (mtv * r0 * PK2 + 0.0);
+          if (DIM == 3) td1 = td1 + (mtv * r1 * PK2 + 0.0);
+          td2 = td2 + (mtv * r2 * PK2 + 0.0);
+          // viscomorris.f90:60-71
+          if (morris) {
+            double rt = nu * rhoi + nu * rhoj + 1.0e-3;
+            double anuitilde = 4.0 * (nu * nu);
+            double factivis = amassj * anuitilde / rt;
+            double w0 = factivis * (-(dv0 * PK2 * rr));
+            double w2 = factivis * (-(dv2 * PK2 * rr));
+            tv0 = tv0 + w0;
+            rs0 = rs0 + w0;
+            if (DIM == 3) {
+              double w1 = factivis * (-(dv1 * PK2 * rr));
+              tv1 = tv1 + w1;
+              rs1 = rs1 + w1;
+            }
+            tv2 = tv2 + w2;
+            rs2 = rs2 + w2;
+          }
+        }
+      }
+      if (trunc) atomicOr(&dyn->warnings, SPH_WARN_NEIGHBOURS_TRUNCATED);
+      tpres[0] = tpres[0] + tp0 + al0;
+      tpres[1] = tpres[1] + tp1 + al1;
+      tpres[2] = tpres[2] + tp2 + al2;
+      // laminar_flag, inter_EqMoto.f90:269-283
+      int lam_new = 0;
+      if (s.kin_visc > 0.0) {
+        double absv_pres = sqrt(tpres[0] * tpres[0] + tpres[1] * tpres[1] + tpres[2] * tpres[2]) + GI;
+        double absv_morris = sqrt(rs0 * rs0 + rs1 * rs1 + rs2 * rs2);
+        double weight = 0.0;
+        if (absv_pres != 0.0) weight = absv_morris / absv_pres * 100.0;
+        lam_new = (weight > 5.0 || absv_pres == 0.0) ? 1 : 0;
+      }
+      double acc[3];
+      acc[0] = tpres[0] + td0 + tv0 + s.grav[0];
+      acc[1] = tpres[1] + td1 + tv1 + s.grav[1];
+      acc[2] = tpres[2] + td2 + tv2 + s.grav[2];
+      if (nb > 0) {
+        double R[3];
+        elastic_reaction<DIM>(s, b, nb, bstart, vi, R);
+        for (int d = 0; d < 3; ++d) acc[d] = acc[d] + R[d];
+      }
+      if (FUSED) {
+        double dtvel = dyn->dtvel, dt = dyn->dt;
+        double vn[3], xn[3];
+        for (int d = 0; d < 3; ++d) vn[d] = vi[d] + dtvel * acc[d];
+        xn[0] = xi.x + dt * vn[0];
+        xn[1] = xi.y + dt * vn[1];
+        xn[2] = xi.z + dt * vn[2];
+        P.X2[p] = make_double4(xn[0], xn[1], xn[2], xi.w);
+        P.V2[p] = make_double4(vn[0], vn[1], vn[2], rhoi);
+        P.P2[p] = pi;
+        P.I2[p] = P.I[p];
+        P.L2[p] = (uint8_t)lam_new;
+        double U = sqrt(vn[0] * vn[0] + vn[1] * vn[1] + vn[2] * vn[2]);
+        dtc = s.cfl * 2.0 * s.h / (s.celerita + U);
+      } else {
+        P.ACC[p] = make_double4(acc[0], acc[1], acc[2], 0.0);
+        P.L[p] = (uint8_t)lam_new;
+      }
+    }
+    if (FUSED) {
+      double m = warp_min(dtc);
+      int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+      if (lane == 0) red[wid] = m;
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        double mm = red[0];
+        for (int w = 1; w < kBlock / 32; ++w) mm = fmin(mm, red[w]);
+        if (mm < 1.0e300) atomicMin(&dyn->dtmin_bits, (unsigned long long)__double_as_longlong(mm));
+      }
+      __syncthreads();
+    }
+  }
+}
+
+// ==========================================================================
+// Continuity: SASPH_continuity + AddBoundaryContribution_to_CE3D/2D +
+// Continuity_Equation, optionally fused with Leapfrog_continuity and the EoS.
+// ==========================================================================
+template <int DIM, bool FUSED>
+__global__ void __launch_bounds__(kBlock) k_continuity(DevBatch b) {
+  __shared__ SimDev s;
+  __shared__ int redi[kBlock / 32];
+  int cur = -1;
+  const Particles& P = b.P;
+  for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
+    Tile tl = b.tiles[t];
+    load_sim(s, b.sims, tl.sim, cur);
+    SimDyn* dyn = b.dyn + tl.sim;
+    int p = tl.start + threadIdx.x;
+    bool active = threadIdx.x < tl.count && p < s.p_off + dyn->nag && !(FUSED && dyn->frozen);
+    int nneigh = 0;
+    if (active) {
+      double4 xi = P.X[p];
+      double4 vi = P.V[p];
+      double rhoi = P.RP[p].x;
+      double dden = 0.0;
+      int nb = P.bdt_count[p];
+      if (nb > 0) {
+        int bstart = P.bdt_start[p];
+        double gu0 = 0, gv1 = 0, gw2 = 0;
+        if (DIM == 3) {
+          double gu[3] = {0, 0, 0}, gv[3] = {0, 0, 0}, gw[3] = {0, 0, 0};
+          const double var[3] = {vi.x, vi.y, vi.z};
+          for (int u = 0; u < nb; ++u) {
+            const BdtEntry& e = P.bdt[bstart + u];
+            const FaceDev& f = b.faces[s.face_off + e.clobonum - 1];
+            if (!(e.loc[2] > 0.0)) continue;
+            double dp = 0.0;
+            for (int d = 0; d < 3; ++d) dp = dp + (2.0 * (f.velocity[d] - var[d])) * f.T[d][2];
+            double dvel[3] = {dp * f.T[0][2], dp * f.T[1][2], dp * f.T[2][2]};
+            double av[3];
+            for (int i = 0; i < 3; ++i) {
+              double a = 0.0;
+              for (int k = 0; k < 3; ++k) a = a + f.T[i][k] * e.bi[3 + k];
+              av[i] = a;
+            }
+            for (int d = 0; d < 3; ++d) {
+              gu[d] = gu[d] - dvel[0] * av[d];
+              gv[d] = gv[d] - dvel[1] * av[d];
+              gw[d] = gw[d] - dvel[2] * av[d];
+            }
+          }
+          gu0 = gu[0];
+          gv1 = gv[1];
+          gw2 = gw[2];
+          atomicMax(&dyn->ncbf_max, nb);
+        } else {
+          const double var2[2] = {vi.x, vi.z};
+          double gu_x = 0.0, gw_z = 0.0;
+          for (int u = 0; u < nb; ++u) {
+            const BdtEntry& e = P.bdt[bstart + u];
+            const SideDev& S = b.sides[s.side_off + e.clobonum - 1];
+            double IntWdS = e.bi[0];
+            double dvel0, dvel1;
+            if (S.zone_type == SPH_ZONE_TAPI) {
+              dvel0 = 2.0 * (S.velocity[0] - var2[0]);
+              dvel1 = 2.0 * (S.velocity[2] - var2[1]);
+            } else {
+              dvel0 = 2.0 * (-var2[0]);
+              dvel1 = 2.0 * (-var2[1]);
+            }
+            gu_x = gu_x - dvel0 * S.nnn[0] * IntWdS;
+            gw_z = gw_z - dvel1 * S.nnn[1] * IntWdS;
+          }
+          gu0 = gu_x;
+          gw2 = gw_z;
+        }
+        dden = dden - rhoi * (gu0 + gv1 + gw2);
+      }
+      int ci, cj, ck;
+      particle_cell(s, xi.x, xi.y, xi.z, ci, cj, ck);
+      double a1 = 0.0, a2 = 0.0, a3 = 0.0;
+      bool trunc = false;
+      constexpr int NR = (DIM == 3) ? 9 : 3;
+      for (int r = 0; r < NR && !trunc; ++r) {
+        int qb, qe;
+        neighbour_run<DIM>(s, P.cell_start, ci, cj, ck, r, qb, qe);
+        for (int q = qb; q < qe; ++q) {
+          if (nneigh >= s.nmaxpartj) { trunc = true; break; }
+          double4 xj = P.X[q];
+          double r0 = xi.x - xj.x, r1 = xi.y - xj.y, r2 = xi.z - xj.z;
+          double rr = r0 * r0 + r1 * r1 + r2 * r2;
+          if (rr > s.square_doubleh) continue;
+          nneigh++;
+          if (q == p) continue;   // dvar = 0 for the particle itself
+          double PK1, PK2, PK3;
+          kernel_values(s, rr, PK1, PK2, PK3);
+          double4 vj = P.V[q];
+          double c = rhoi * vj.w * PK1;     // rhoi * (amassj / rhoj) * PK1
+          a1 = a1 + c * (vj.x - vi.x) * r0;
+          if (DIM == 3) a2 = a2 + c * (vj.y - vi.y) * r1;
+          a3 = a3 + c * (vj.z - vi.z) * r2;
+        }
+      }
+      if (trunc) atomicOr(&dyn->warnings, SPH_WARN_NEIGHBOURS_TRUNCATED);
+      if (DIM == 3) dden = dden - (a1 + a2 + a3);
+      else dden = dden - (a1 + a3);
+      if (FUSED) {
+        // Leapfrog_continuity.f90:54-68, EoS_barotropic_linear.f90:49-55
+        double rho = rhoi + dyn->dt * dden;
+        if (s.density_thresholds == 1) {
+          if (rho < 0.9 * s.den0) rho = 0.9 * s.den0;
+          if (rho > 1.1 * s.den0) rho = 1.1 * s.den0;
+        }
+        double pr = s.k_over_rho0 * (rho - s.den0) + s.p_ref;
+        P.RP[p] = make_double2(rho, pr);
+      } else {
+        P.DDEN[p] = dden;
+      }
+    }
+    int m = warp_max(nneigh);
+    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) redi[wid] = m;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int mm = redi[0];
+      for (int w = 1; w < kBlock / 32; ++w) mm = max(mm, redi[w]);
+      if (mm > 0) atomicMax(&dyn->max_neigh, mm);
+    }
+    __syncthreads();
+  }
+}
+
+// ==========================================================================
+// Fine-grained integration kernels (used by the per-call C ABI)
+// ==========================================================================
+__global__ void k_leapfrog_momentum(DevBatch b) {
+  __shared__ SimDev s;
+  int cur = -1;
+  for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
+    Tile tl = b.tiles[t];
+    load_sim(s, b.sims, tl.sim, cur);
+    int p = tl.start + threadIdx.x;
+    if (threadIdx.x >= tl.count || p >= s.p_off + b.dyn[tl.sim].nag) continue;
+    double dtvel = b.dyn[tl.sim].dtvel;
+    double4 v = b.P.V[p];
+    double4 a = b.P.ACC[p];
+    v.x = v.x + dtvel * a.x;
+    v.y = v.y + dtvel * a.y;
+    v.z = v.z + dtvel * a.z;
+    b.P.V[p] = v;
+  }
+}
+
+__global__ void k_leapfrog_trajectories(DevBatch b) {
+  __shared__ SimDev s;
+  int cur = -1;
+  for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
+    Tile tl = b.tiles[t];
+    load_sim(s, b.sims, tl.sim, cur);
+    int p = tl.start + threadIdx.x;
+    if (threadIdx.x >= tl.count || p >= s.p_off + b.dyn[tl.sim].nag) continue;
+    double dt = b.dyn[tl.sim].dt;
+    double4 x = b.P.X[p];
+    double4 v = b.P.V[p];
+    x.x = x.x + dt * v.x;
+    x.y = x.y + dt * v.y;
+    x.z = x.z + dt * v.z;
+    b.P.X[p] = x;
+  }
+}
+
+__global__ void k_leapfrog_continuity(DevBatch b) {
+  __shared__ SimDev s;
+  int cur = -1;
+  for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
+    Tile tl = b.tiles[t];
+    load_sim(s, b.sims, tl.sim, cur);
+    int p = tl.start + threadIdx.x;
+    if (threadIdx.x >= tl.count || p >= s.p_off + b.dyn[tl.sim].nag) continue;
+    double2 rp = b.P.RP[p];
+    double rho = rp.x + b.dyn[tl.sim].dt * b.P.DDEN[p];
+    if (s.density_thresholds == 1) {
+      if (rho < 0.9 * s.den0) rho = 0.9 * s.den0;
+      if (rho > 1.1 * s.den0) rho = 1.1 * s.den0;
+    }
+    b.P.RP[p] = make_double2(rho, rp.y);
+    double4 v = b.P.V[p];
+    v.w = b.P.X[p].w / rho;
+    b.P.V[p] = v;
+  }
+}
+
+__global__ void k_eos(DevBatch b) {
+  __shared__ SimDev s;
+  int cur = -1;
+  for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
+    Tile tl = b.tiles[t];
+    load_sim(s, b.sims, tl.sim, cur);
+    int p = tl.start + threadIdx.x;
+    if (threadIdx.x >= tl.count || p >= s.p_off + b.dyn[tl.sim].nag) continue;
+    if (b.dyn[tl.sim].step < 0) continue;   // EoS_fluid_loop.f90:61 (on_going_time_step > 0)
+    double2 rp = b.P.RP[p];
+    rp.y = s.k_over_rho0 * (rp.x - s.den0) + s.p_ref;
+    b.P.RP[p] = rp;
+  }
+}
+
+// CFL minimum of time_step_duration.f90:86-110 over the current velocities.
+__global__ void k_dt_reduce(DevBatch b) {
+  __shared__ SimDev s;
+  __shared__ double red[kBlock / 32];
+  int cur = -1;
+  for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
+    Tile tl = b.tiles[t];
+    load_sim(s, b.sims, tl.sim, cur);
+    int p = tl.start + threadIdx.x;
+    double dtc = 1.0e300;
+    if (threadIdx.x < tl.count && p < s.p_off + b.dyn[tl.sim].nag) {
+      double4 v = b.P.V[p];
+      double U = sqrt(v.x * v.x + v.y * v.y + v.z * v.z);
+      dtc = s.cfl * 2.0 * s.h / (s.celerita + U);
+    }
+    double m = warp_min(dtc);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double mm = red[0];
+      for (int w = 1; w < kBlock / 32; ++w) mm = fmin(mm, red[w]);
+      if (mm < 1.0e300) atomicMin(&b.dyn[tl.sim].dtmin_bits, (unsigned long long)__double_as_longlong(mm));
+    }
+    __syncthreads();
+  }
+}
+
+// time_step_duration.f90:74-123 closing formula for on_going_time_step.
+__device__ void tsd_close(const SimDev& s, SimDyn& d, double dtmin_cfl, int on_going) {
+  double dtmin = kMaxPositive;
+  double dt_vis = kMaxPositive;
+  double dt;
+  if (d.nag == 0) {
+    dt = 0.0;
+  } else {
+    if (s.kin_visc > 1.0e-24) {
+      dt_vis = s.vsc_coeff * s.squareh / (0.5 * s.kin_visc);
+      dtmin = fmin(dtmin, dt_vis);
+    }
+    dtmin = fmin(dtmin, fmin(dtmin_cfl, dt_vis));
+    if (s.dt_alfa_mon) {
+      double visc_mon = s.alfa_mon * s.celerita * s.h / s.den0;
+      double dt_mon = s.squareh / (0.5 * visc_mon);
+      dtmin = fmin(dtmin, fmin(kMaxPositive, dt_mon));
+    }
+    if (on_going == 0) dt = dtmin;
+    else dt = (1.0 - s.pesodt) * dtmin + s.pesodt * d.dt_average;
+  }
+  if (on_going == 0) d.dt_average = dt;
+  else d.dt_average = (d.dt_average * (on_going - 1) + dt) / on_going;
+  d.dt = dt;
+}
+
+// mode 0: IC.  time_step_loop.f90:173 evaluates dt with on_going_time_step
+//         = -999, then the first iteration (time_step_loop.f90:182-185)
+//         evaluates it again for step 1 from the same velocities.
+// mode 1: end of a step: advance the simulation time and evaluate the dt of
+//         the next iteration (its time_step_duration sees the velocities
+//         this step left).
+// Between steps the state keeps: step = completed steps, time = sum of their
+// dt, dt = dt of the next step, dt_prev = dt of the last step.
+__global__ void k_finalize(DevBatch b, int mode) {
+  int sim = blockIdx.x * blockDim.x + threadIdx.x;
+  if (sim >= b.nsims) return;
+  const SimDev& s = b.sims[sim];
+  SimDyn& d = b.dyn[sim];
+  unsigned long long bits = d.dtmin_bits;
+  double dtmin_cfl = (bits == 0x7FF0000000000000ull) ? kMaxPositive : __longlong_as_double((long long)bits);
+  d.dtmin_bits = 0x7FF0000000000000ull;
+  if (mode == 0) {
+    d.dt_average = 0.0;
+    tsd_close(s, d, dtmin_cfl, -999);
+    double dt_ic = d.dt;
+    tsd_close(s, d, dtmin_cfl, 1);
+    d.dt_prev = dt_ic;
+    d.step = 0;
+    d.time = 0.0;
+    d.frozen = 0;
+  } else {
+    if (d.frozen) return;
+    d.time = d.time + d.dt;
+    d.step = d.step + 1;
+    double dt_cur = d.dt;
+    tsd_close(s, d, dtmin_cfl, d.step + 1);
+    d.dt_prev = dt_cur;
+    if (d.t_end > 0.0 && d.time >= d.t_end) d.frozen = 1;
+  }
+  d.dtvel = 0.5 * (d.dt + d.dt_prev);
+}
+
+__global__ void k_sort_reset(DevBatch b) {
+  int sim = blockIdx.x * blockDim.x + threadIdx.x;
+  if (sim < b.nsims) b.dyn[sim].n_out = 0;
+}
+
+__global__ void k_bdt_reset(DevBatch b) {
+  int sim = blockIdx.x * blockDim.x + threadIdx.x;
+  if (sim < b.nsims) b.dyn[sim].ncbf_max = 0;
+  if (sim == 0) b.dyn[b.nsims].bdt_used = 0;
+}
+
+// ==========================================================================
+// Caller-order transfer and verification dumps
+// ==========================================================================
+__global__ void k_init_from_caller(DevBatch b, const double* x, const double* v, const double* rho, const double* p,
+                                   const double* m) {
+  __shared__ SimDev s;
+  int cur = -1;
+  const Particles& P = b.P;
+  for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
+    Tile tl = b.tiles[t];
+    load_sim(s, b.sims, tl.sim, cur);
+    if (threadIdx.x >= tl.count) continue;
+    int q = tl.start + threadIdx.x;           // caller order slot
+    int i = q - s.p_off;                       // caller index - 1
+    if (i < b.dyn[tl.sim].nag) {
+      P.X2[q] = make_double4(x[3 * (size_t)q], x[3 * (size_t)q + 1], x[3 * (size_t)q + 2], m[q]);
+      P.V2[q] = make_double4(v[3 * (size_t)q], v[3 * (size_t)q + 1], v[3 * (size_t)q + 2], rho[q]);
+      P.P2[q] = p[q];
+      P.I2[q] = i + 1;
+    } else {
+      P.X2[q] = make_double4(0, 0, 0, 0);
+      P.V2[q] = make_double4(0, 0, 0, 1.0);
+      P.P2[q] = 0.0;
+      P.I2[q] = 0;
+    }
+    P.L2[q] = 0;
+  }
+}
+
+__global__ void k_to_caller(DevBatch b, double* x, double* v, double* rho, double* p, double* m, double* acc,
+                            double* dden) {
+  __shared__ SimDev s;
+  int cur = -1;
+  const Particles& P = b.P;
+  for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
+    Tile tl = b.tiles[t];
+    load_sim(s, b.sims, tl.sim, cur);
+    int q = tl.start + threadIdx.x;
+    if (threadIdx.x >= tl.count || q >= s.p_off + b.dyn[tl.sim].nag) continue;
+    size_t o = (size_t)s.p_off + P.I[q] - 1;
+    double4 xx = P.X[q];
+    double4 vv = P.V[q];
+    double2 rp = P.RP[q];
+    if (x) { x[3 * o] = xx.x; x[3 * o + 1] = xx.y; x[3 * o + 2] = xx.z; }
+    if (v) { v[3 * o] = vv.x; v[3 * o + 1] = vv.y; v[3 * o + 2] = vv.z; }
+    if (rho) rho[o] = rp.x;
+    if (p) p[o] = rp.y;
+    if (m) m[o] = xx.w;
+    if (acc) { double4 a = P.ACC[q]; acc[3 * o] = a.x; acc[3 * o + 1] = a.y; acc[3 * o + 2] = a.z; }
+    if (dden) dden[o] = P.DDEN[q];
+  }
+}
+
+template <int DIM>
+__global__ void k_dump_neighbours(DevBatch b, int nmaxj, int* counts, int* lists) {
+  __shared__ SimDev s;
+  int cur = -1;
+  const Particles& P = b.P;
+  for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
+    Tile tl = b.tiles[t];
+    load_sim(s, b.sims, tl.sim, cur);
+    int p = tl.start + threadIdx.x;
+    if (threadIdx.x >= tl.count || p >= s.p_off + b.dyn[tl.sim].nag) continue;
+    double4 xi = P.X[p];
+    size_t row = (size_t)s.p_off + P.I[p] - 1;
+    int ci, cj, ck;
+    particle_cell(s, xi.x, xi.y, xi.z, ci, cj, ck);
+    int n = 0;
+    bool stop = false;
+    constexpr int NR = (DIM == 3) ? 9 : 3;
+    for (int r = 0; r < NR && !stop; ++r) {
+      int qb, qe;
+      neighbour_run<DIM>(s, P.cell_start, ci, cj, ck, r, qb, qe);
+      for (int q = qb; q < qe; ++q) {
+        if (n >= s.nmaxpartj) { stop = true; break; }
+        double4 xj = P.X[q];
+        double r0 = xi.x - xj.x, r1 = xi.y - xj.y, r2 = xi.z - xj.z;
+        double rr = r0 * r0 + r1 * r1 + r2 * r2;
+        if (rr > s.square_doubleh) continue;
+        if (n < nmaxj) lists[row * nmaxj + n] = P.I[q];
+        n++;
+      }
+    }
+    counts[row] = n;
+  }
+}
+
+__global__ void k_dump_boundary(DevBatch b, int max_per, int* ncb, int* clob, double* vals) {
+  __shared__ SimDev s;
+  int cur = -1;
+  const Particles& P = b.P;
+  for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
+    Tile tl = b.tiles[t];
+    load_sim(s, b.sims, tl.sim, cur);
+    int p = tl.start + threadIdx.x;
+    if (threadIdx.x >= tl.count || p >= s.p_off + b.dyn[tl.sim].nag) continue;
+    size_t row = (size_t)s.p_off + P.I[p] - 1;
+    int n = P.bdt_count[p];
+    ncb[row] = n;
+    for (int k = 0; k < n && k < max_per; ++k) {
+      const BdtEntry& e = P.bdt[P.bdt_start[p] + k];
+      clob[row * max_per + k] = e.clobonum;
+      double* d = vals + (row * max_per + k) * 20;
+      for (int q = 0; q < 3; ++q) d[q] = e.loc[q];
+      for (int q = 0; q < 8; ++q) d[3 + q] = e.bi[q];
+      // IntGiWrRdV(3,3) column-major
+      for (int c = 0; c < 3; ++c)
+        for (int r = 0; r < 3; ++r) d[11 + 3 * c + r] = e.ig[3 * r + c];
+    }
+  }
+}
+
+__global__ void k_dump_cella(DevBatch b, int* cella) {
+  __shared__ SimDev s;
+  int cur = -1;
+  const Particles& P = b.P;
+  for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
+    Tile tl = b.tiles[t];
+    load_sim(s, b.sims, tl.sim, cur);
+    int p = tl.start + threadIdx.x;
+    if (threadIdx.x >= tl.count || p >= s.p_off + b.dyn[tl.sim].nag) continue;
+    double4 xi = P.X[p];
+    int i, j, k;
+    int c = 0;
+    if (particle_cell(s, xi.x, xi.y, xi.z, i, j, k)) c = ((k - 1) * s.ncd[1] + (j - 1)) * s.ncd[0] + i;
+    cella[(size_t)s.p_off + P.I[p] - 1] = c;
+  }
+}
+
+// ==========================================================================
+// launch wrappers
+// ==========================================================================
+static inline int blocks_for(const DevBatch& b) { return b.ntiles < b.grid_blocks ? b.ntiles : b.grid_blocks; }
+
+void launch_stage(const DevBatch& b, cudaStream_t st) { k_stage<<<blocks_for(b), kBlock, 0, st>>>(b); }
+
+void launch_bin(const DevBatch& b, KeyKind kind, cudaStream_t st) {
+  if (kind == KeyKind::Sort) k_bin<KeyKind::Sort><<<blocks_for(b), kBlock, 0, st>>>(b);
+  else k_bin<KeyKind::Reference><<<blocks_for(b), kBlock, 0, st>>>(b);
+}
+
+void launch_removal(const DevBatch& b, cudaStream_t st) { k_removal<<<b.nsims, 32, 0, st>>>(b); }
+
+void launch_scan(const DevBatch& b, int* cell_start, cudaStream_t st) {
+  int n = b.P.total_cells;
+  int nb = (n + kScanChunk - 1) / kScanChunk;
+  k_scan1<<<nb, kScanThreads, 0, st>>>(b.P.cell_count, n, b.scan_block_sums);
+  k_scan2<<<1, kScanThreads, 0, st>>>(b.scan_block_sums, nb, cell_start, n);
+  k_scan3<<<nb, kScanThreads, 0, st>>>(b.P.cell_count, n, b.scan_block_sums, cell_start);
+}
+
+void launch_sort_reset(const DevBatch& b, cudaStream_t st) {
+  k_sort_reset<<<(b.nsims + 127) / 128, 128, 0, st>>>(b);
+}
+
+void upload_bit2d(const double* tab, cudaStream_t st) {
+  cudaMemcpyToSymbolAsync(c_bit2d, tab, sizeof(double) * 22 * 6, 0, cudaMemcpyHostToDevice, st);
+}
+
+void launch_place(const DevBatch& b, cudaStream_t st) {
+  k_place<<<blocks_for(b), kBlock, 0, st>>>(b, b.P.cell_start, 1);
+}
+
+void launch_rank_permute(const DevBatch& b, cudaStream_t st) {
+  k_rank_permute<<<blocks_for(b), kBlock, 0, st>>>(b);
+}
+
+void launch_rank_reference(const DevBatch& b, const int* cell_start_ref, int* npartord, cudaStream_t st) {
+  k_place<<<blocks_for(b), kBlock, 0, st>>>(b, cell_start_ref, 0);
+  k_rank_reference<<<blocks_for(b), kBlock, 0, st>>>(b, cell_start_ref, npartord);
+}
+
+void launch_boundary(const DevBatch& b, cudaStream_t st) {
+  k_bdt_reset<<<(b.nsims + 127) / 128, 128, 0, st>>>(b);
+  if (b.dim == 3) k_boundary3d<<<blocks_for(b), kBlock, 0, st>>>(b);
+  else k_boundary2d<<<blocks_for(b), kBlock, 0, st>>>(b);
+}
+
+void launch_momentum(const DevBatch& b, bool fused, cudaStream_t st) {
+  int g = blocks_for(b);
+  if (b.dim == 3) {
+    if (fused) k_momentum<3, true><<<g, kBlock, 0, st>>>(b);
+    else k_momentum<3, false><<<g, kBlock, 0, st>>>(b);
+  } else {
+    if (fused) k_momentum<2, true><<<g, kBlock, 0, st>>>(b);
+    else k_momentum<2, false><<<g, kBlock, 0, st>>>(b);
+  }
+}
+
+void launch_continuity(const DevBatch& b, bool fused, cudaStream_t st) {
+  int g = blocks_for(b);
+  if (b.dim == 3) {
+    if (fused) k_continuity<3, true><<<g, kBlock, 0, st>>>(b);
+    else k_continuity<3, false><<<g, kBlock, 0, st>>>(b);
+  } else {
+    if (fused) k_continuity<2, true><<<g, kBlock, 0, st>>>(b);
+    else k_continuity<2, false><<<g, kBlock, 0, st>>>(b);
+  }
+}
+
+void launch_leapfrog_momentum(const DevBatch& b, cudaStream_t st) {
+  k_leapfrog_momentum<<<blocks_for(b), kBlock, 0, st>>>(b);
+}
+void launch_leapfrog_trajectories(const DevBatch& b, cudaStream_t st) {
+  k_leapfrog_trajectories<<<blocks_for(b), kBlock, 0, st>>>(b);
+}
+void launch_leapfrog_continuity(const DevBatch& b, cudaStream_t st) {
+  k_leapfrog_continuity<<<blocks_for(b), kBlock, 0, st>>>(b);
+}
+void launch_eos(const DevBatch& b, cudaStream_t st) { k_eos<<<blocks_for(b), kBlock, 0, st>>>(b); }
+void launch_dt_reduce(const DevBatch& b, cudaStream_t st) { k_dt_reduce<<<blocks_for(b), kBlock, 0, st>>>(b); }
+void launch_finalize(const DevBatch& b, int mode, cudaStream_t st) {
+  k_finalize<<<(b.nsims + 127) / 128, 128, 0, st>>>(b, mode);
+}
+
+void launch_init_from_caller(const DevBatch& b, const double* x, const double* v, const double* rho,
+                             const double* p, const double* m, cudaStream_t st) {
+  k_init_from_caller<<<blocks_for(b), kBlock, 0, st>>>(b, x, v, rho, p, m);
+}
+void launch_to_caller(const DevBatch& b, double* x, double* v, double* rho, double* p, double* m, double* acc,
+                      double* dden, cudaStream_t st) {
+  k_to_caller<<<blocks_for(b), kBlock, 0, st>>>(b, x, v, rho, p, m, acc, dden);
+}
+void launch_dump_neighbours(const DevBatch& b, int nmaxj, int* counts, int* lists, cudaStream_t st) {
+  if (b.dim == 3) k_dump_neighbours<3><<<blocks_for(b), kBlock, 0, st>>>(b, nmaxj, counts, lists);
+  else k_dump_neighbours<2><<<blocks_for(b), kBlock, 0, st>>>(b, nmaxj, counts, lists);
+}
+void launch_dump_boundary(const DevBatch& b, int max_per, int* ncb, int* clob, double* vals, cudaStream_t st) {
+  k_dump_boundary<<<blocks_for(b), kBlock, 0, st>>>(b, max_per, ncb, clob, vals);
+}
+void launch_dump_cella(const DevBatch& b, int* cella, cudaStream_t st) {
+  k_dump_cella<<<blocks_for(b), kBlock, 0, st>>>(b, cella);
+}
+
+}  // namespace sph

@@ -1,0 +1,60 @@
+// Host-side launch wrappers of the device kernels (C++ linkage, internal).
+#pragma once
+#include <cuda_runtime.h>
+#include "sph_internal.cuh"
+
+namespace sph {
+
+struct DevBatch {
+  const SimDev* sims;      // [nsims]
+  SimDyn* dyn;             // [nsims]
+  const Tile* tiles;       // [ntiles]
+  int ntiles;
+  int nsims;
+  int dim;
+  Particles P;
+  const FaceDev* faces;
+  const SideDev* sides;
+  const double* bit;       // per-sim BoundIntegralTab, 256 x 7 each
+  const int* cf_start;     // per global cell: first entry in cf_list
+  const int* cf_count;     // per global cell: faces cutting the cell
+  const int* cf_list;      // face ids (1-based within the simulation)
+  const uint8_t* cell_near;  // per global cell: faces cut the 27-cell block
+  int* scan_block_sums;    // scan scratch
+  int scan_nblocks;
+  int grid_blocks;         // blocks of the persistent particle kernels
+};
+
+enum class KeyKind { Sort = 0, Reference = 1 };
+
+// sorting
+void launch_stage(const DevBatch& b, cudaStream_t st);
+void launch_bin(const DevBatch& b, KeyKind kind, cudaStream_t st);
+void launch_removal(const DevBatch& b, cudaStream_t st);
+void launch_scan(const DevBatch& b, int* cell_start, cudaStream_t st);
+void launch_sort_reset(const DevBatch& b, cudaStream_t st);
+void upload_bit2d(const double* tab, cudaStream_t st);
+void launch_place(const DevBatch& b, cudaStream_t st);
+void launch_rank_permute(const DevBatch& b, cudaStream_t st);
+void launch_rank_reference(const DevBatch& b, const int* cell_start_ref, int* npartord, cudaStream_t st);
+// physics (FP64)
+void launch_boundary(const DevBatch& b, cudaStream_t st);
+void launch_momentum(const DevBatch& b, bool fused, cudaStream_t st);
+void launch_continuity(const DevBatch& b, bool fused, cudaStream_t st);
+void launch_leapfrog_momentum(const DevBatch& b, cudaStream_t st);
+void launch_leapfrog_trajectories(const DevBatch& b, cudaStream_t st);
+void launch_leapfrog_continuity(const DevBatch& b, cudaStream_t st);
+void launch_eos(const DevBatch& b, cudaStream_t st);
+void launch_dt_reduce(const DevBatch& b, cudaStream_t st);
+void launch_finalize(const DevBatch& b, int mode, cudaStream_t st);
+// host <-> device in caller order
+void launch_init_from_caller(const DevBatch& b, const double* x, const double* v, const double* rho,
+                             const double* p, const double* m, cudaStream_t st);
+void launch_to_caller(const DevBatch& b, double* x, double* v, double* rho, double* p, double* m,
+                      double* acc, double* dden, cudaStream_t st);
+// verification
+void launch_dump_neighbours(const DevBatch& b, int nmaxj, int* counts, int* lists, cudaStream_t st);
+void launch_dump_boundary(const DevBatch& b, int max_per, int* ncb, int* clob, double* vals, cudaStream_t st);
+void launch_dump_cella(const DevBatch& b, int* cella, cudaStream_t st);
+
+}  // namespace sph
