@@ -979,8 +979,9 @@ __global__ void __launch_bounds__(kBlock) k_momentum(DevBatch b) {
         if (DIM == 3) me_boundary3d(s, b, nb, bstart, vi, rhoi, pi, lam, tpres, tdiss, tvisc);
         else me_boundary2d(s, b, nb, bstart, vi, rhoi, pi, lam, tpres, tdiss, tvisc);
       }
-      int ci, cj, ck;
-      particle_cell(s, xi.x, xi.y, xi.z, ci, cj, ck);
+      int ci = 0, cj = 0, ck = 0;
+      bool in_grid = particle_cell(s, xi.x, xi.y, xi.z, ci, cj, ck);
+      if (!in_grid) set_status(dyn, SPH_ERR_INVALID_ARGUMENT);   // state not re-sorted after a move
       double tp0 = 0, tp1 = 0, tp2 = 0, al0 = 0, al1 = 0, al2 = 0;
       double td0 = tdiss[0], td1 = tdiss[1], td2 = tdiss[2];
       double tv0 = tvisc[0], tv1 = tvisc[1], tv2 = tvisc[2];
@@ -990,7 +991,7 @@ __global__ void __launch_bounds__(kBlock) k_momentum(DevBatch b) {
       const double nu = s.kin_visc;
       bool trunc = false;
       constexpr int NR = (DIM == 3) ? 9 : 3;
-      for (int r = 0; r < NR && !trunc; ++r) {
+      for (int r = 0; r < NR && !trunc && in_grid; ++r) {
         int qb, qe;
         neighbour_run<DIM>(s, P.cell_start, ci, cj, ck, r, qb, qe);
         for (int q = qb; q < qe; ++q) {
@@ -1173,12 +1174,13 @@ __global__ void __launch_bounds__(kBlock) k_continuity(DevBatch b) {
         }
         dden = dden - rhoi * (gu0 + gv1 + gw2);
       }
-      int ci, cj, ck;
-      particle_cell(s, xi.x, xi.y, xi.z, ci, cj, ck);
+      int ci = 0, cj = 0, ck = 0;
+      bool in_grid = particle_cell(s, xi.x, xi.y, xi.z, ci, cj, ck);
+      if (!in_grid) set_status(dyn, SPH_ERR_INVALID_ARGUMENT);   // state not re-sorted after a move
       double a1 = 0.0, a2 = 0.0, a3 = 0.0;
       bool trunc = false;
       constexpr int NR = (DIM == 3) ? 9 : 3;
-      for (int r = 0; r < NR && !trunc; ++r) {
+      for (int r = 0; r < NR && !trunc && in_grid; ++r) {
         int qb, qe;
         neighbour_run<DIM>(s, P.cell_start, ci, cj, ck, r, qb, qe);
         for (int q = qb; q < qe; ++q) {
@@ -1468,10 +1470,9 @@ __global__ void k_dump_neighbours(DevBatch b, int nmaxj, int* counts, int* lists
     if (threadIdx.x >= tl.count || p >= s.p_off + b.dyn[tl.sim].nag) continue;
     double4 xi = P.X[p];
     size_t row = (size_t)s.p_off + P.I[p] - 1;
-    int ci, cj, ck;
-    particle_cell(s, xi.x, xi.y, xi.z, ci, cj, ck);
+    int ci = 0, cj = 0, ck = 0;
     int n = 0;
-    bool stop = false;
+    bool stop = !particle_cell(s, xi.x, xi.y, xi.z, ci, cj, ck);
     constexpr int NR = (DIM == 3) ? 9 : 3;
     for (int r = 0; r < NR && !stop; ++r) {
       int qb, qe;
