@@ -1,0 +1,335 @@
+#!/usr/bin/env python
+"""Benchmark of the SPHERA per-step particle path on B200.
+
+Workload: the 3D dam break (tank 1.6 x 0.6 x 0.6 m, block 0.6 x 0.3 x 0.6 m,
+dx = 0.005 m, 864,000 particles, seeded +-0.01 dx jitter, SA-SPH fixe
+walls), synthetic state generated in-repo.  A step is one whole leapfrog
+step of time_step_loop.f90 (momentum + leapfrog, cell sort, SA-SPH boundary
+data, continuity + EoS, time step), replayed from a CUDA graph.
+
+  value       particle-steps/s over all ranks, state resident on the device
+              (device time, CUDA events on the library's stream, max over ranks)
+  e2e         the same metric through the C ABI with the state in pinned host
+              memory: every step uploads pg(:), advances and downloads it
+  roofline    dominant kernel (momentum pass) against the measured HBM copy
+              bandwidth; fp64 gives the same kernel against the measured FP64
+              FMA rate, the bound that actually applies to the pair passes
+  cpu_baseline  the oracle (FP64 OpenMP restatement) on the host cores
+
+`--impl reference` times the oracle alone (the reference is Fortran and
+cannot be built here) on the same workload.  Multi-GPU (torchrun) runs one
+independent replica per rank (no data-path collective: weak scaling).
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+METRIC = "particle-steps/s FP32c vs FP64 at ≤1e-3 rel L2; ensemble p50/p99 time-to-result"
+UNIT = "particle-steps/s"
+KERNELS_PER_STEP = 13          # momentum, 7 sort, 2 boundary, continuity, finalize... counted in step_sequence
+# algorithmic bytes of the fused momentum kernel per particle: reads X 32,
+# V 32, RP 16, L 1, bdt_count 4, I 4; writes X2 32, V2 32, P2 8, I2 4, L2 1
+MOM_BYTES_PER_PARTICLE = 166
+BDT_ENTRY_BYTES = 168
+# FP64 operations: 9 per candidate distance test, 107 per accepted non-self
+# pair in the momentum pass, 34 in the continuity pass (sqrt and divide
+# counted as one)
+FLOP_CAND, FLOP_MOM_PAIR, FLOP_CONT_PAIR = 9, 107, 34
+
+
+def _dist():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import torch.distributed as dist
+        dist.init_process_group("gloo", init_method="env://")
+    return ws, rank, local
+
+
+def _barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def _max_over_ranks(ws, v):
+    if ws == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(index), f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        time.sleep(0.25)
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        self.f.flush()
+        rows = []
+        with open(self.f.name) as fh:
+            for line in fh:
+                parts = [t.strip() for t in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.f.name)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            for nm, val in zip(names, r[5:9]):
+                if val.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": float(rows[0][2]) if rows[0][2].replace(".", "").isdigit() else None,
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            pk = json.load(f)
+        return float(pk["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def _traffic(workload):
+    """DRAM bytes per momentum launch from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        with open(path) as f:
+            t = json.load(f)
+        return t.get(workload)
+    except (OSError, ValueError):
+        return None
+
+
+def cpu_oracle_rate(case, steps, threads):
+    from oracle.pyoracle import Oracle
+    o = Oracle(case, nthreads=threads)
+    o.prepare()
+    t0 = time.perf_counter()
+    o.step(steps)
+    dt = time.perf_counter() - t0
+    n = o.n
+    o.close()
+    return n * steps / dt, dt
+
+
+def run_reference(args, ws, rank):
+    if rank != 0:
+        return 0
+    from sphera_b200 import cases
+    threads = os.cpu_count() or 1
+    case = cases.dam_break_3d()
+    steps = max(1, min(args.steps, 20))
+    from oracle.pyoracle import Oracle
+    o = Oracle(case, nthreads=threads)
+    o.prepare()
+    o.step(max(0, min(args.warmup, 3)))
+    t0 = time.perf_counter()
+    o.step(steps)
+    el = time.perf_counter() - t0
+    v = case.n * steps / el
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": steps, "warmup": min(args.warmup, 3), "ms_per_step": el / steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded 3D dam break generated in-repo)",
+        "config": {"workload": "dam_break_3d: tank 1.6x0.6x0.6 m, block 0.6x0.3x0.6 m, dx 0.005 m, "
+                               "864000 particles, SA-SPH walls, FP64", "particles": case.n},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"{steps} leapfrog steps of the full 864000-particle state after the IC "
+                                   f"(timed steps capped at 20 so the run stays within minutes)"},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "the reference is Fortran 90 and no Fortran compiler exists on these machines; "
+                "timed: the oracle's C++ OpenMP restatement of the same subroutines",
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--e2e-steps", type=int, default=10)
+    ap.add_argument("--cpu-steps", type=int, default=3)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+    ws, rank, local = _dist()
+    if args.impl == "reference":
+        rc = run_reference(args, ws, rank)
+        if ws > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return rc
+
+    import torch
+    torch.cuda.set_device(local)
+    from sphera_b200 import Simulation, cases, measure_fp64_peak
+
+    case = cases.dam_break_3d()
+    n = case.n
+    sim = Simulation(case)
+    sim.upload(case.state)
+    sim.step(args.warmup)
+    stream = torch.cuda.ExternalStream(sim.stream)
+    fp64_peak = measure_fp64_peak()
+
+    try:
+        gpu_id = "GPU-" + str(torch.cuda.get_device_properties(local).uuid)
+    except Exception:
+        gpu_id = str(local)
+    sampler = ClockSampler(gpu_id)
+    _barrier(ws)
+    torch.cuda.synchronize()
+    sim.sync()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    sim.step_async(args.steps)
+    e1.record(stream)
+    e1.synchronize()
+    sim.sync()
+    torch.cuda.synchronize()
+    _barrier(ws)
+    ms = e0.elapsed_time(e1)
+    clocks = sampler.stop()
+    ms_max = _max_over_ranks(ws, ms)
+    value = ws * n * args.steps / (ms_max * 1e-3)
+
+    # phase times and counters of the same workload (un-graphed steps)
+    sim.counters(reset=True)
+    nprof = 10
+    phases = sim.profile_phases(nprof)
+    cnt = sim.counters(reset=True)
+    diag = sim.diagnostics()
+    mom_ms = phases["momentum"] / nprof
+    alg_bytes = n * MOM_BYTES_PER_PARTICLE + diag.bdt_entries * BDT_ENTRY_BYTES
+    hbm_peak, peak_kind = _peaks()
+    achieved_gbs = alg_bytes / (mom_ms * 1e-3) / 1e9
+    mom_flops = (cnt["mom_candidates"] * FLOP_CAND + (cnt["mom_pairs"] - n * nprof) * FLOP_MOM_PAIR) / nprof
+    cont_flops = (cnt["cont_candidates"] * FLOP_CAND + (cnt["cont_pairs"] - n * nprof) * FLOP_CONT_PAIR) / nprof
+    mom_tflops = mom_flops / (mom_ms * 1e-3) / 1e12
+    workload = "dam_break_3d"
+    traffic = _traffic(workload)
+
+    # end to end through the C ABI with pinned host buffers
+    pin = {k: torch.empty(sh, dtype=torch.float64, pin_memory=True)
+           for k, sh in (("x", (n, 3)), ("v", (n, 3)), ("rho", (n,)), ("p", (n,)), ("m", (n,)))}
+    st0 = sim.download()
+    for k in pin:
+        pin[k].numpy()[...] = getattr(st0, k)
+    from sphera_b200 import abi
+    import ctypes as C
+    hs = abi.SphState()
+    hs.n = n
+    for k in pin:
+        setattr(hs, k, C.cast(pin[k].data_ptr(), C.POINTER(C.c_double)))
+
+    lib = __import__("sphera_b200").lib()
+    _barrier(ws)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e0.record(stream)
+    for _ in range(args.e2e_steps):
+        if lib.sph_upload(sim._h, C.byref(hs)) != 0:
+            raise RuntimeError("sph_upload failed")
+        if lib.sph_step_async(sim._h, 1) != 0:
+            raise RuntimeError("sph_step failed")
+        if lib.sph_download(sim._h, C.byref(hs)) != 0:
+            raise RuntimeError("sph_download failed")
+    e1.record(stream)
+    e1.synchronize()
+    wall_e2e = time.perf_counter() - t0
+    e2e_ms = max(e0.elapsed_time(e1), wall_e2e * 1e3)
+    e2e_ms = _max_over_ranks(ws, e2e_ms)
+    e2e_value = ws * n * args.e2e_steps / (e2e_ms * 1e-3)
+    state_bytes = n * (3 + 3 + 1 + 1 + 1) * 8
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        threads = os.cpu_count() or 1
+        rate, el = cpu_oracle_rate(case, args.cpu_steps, threads)
+        cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": f"{args.cpu_steps} leapfrog steps of the full 864000-particle 3D dam break after "
+                         f"its IC ({el:.1f} s), FP64 oracle, OpenMP on all host threads"}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded 3D dam break generated in-repo)",
+        "config": {"workload": "dam_break_3d: tank 1.6x0.6x0.6 m, block 0.6x0.3x0.6 m, dx 0.005 m, "
+                               "864000 particles per GPU, SA-SPH walls, FP64 form",
+                   "particles_per_gpu": n, "form": "fp64",
+                   "l2": "state and scratch (~250 MB per step) exceed the 126 MB L2; no flush",
+                   "parallelism": f"replicas x{ws} (independent simulations, no collective)"},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": state_bytes,
+                "d2h_bytes_per_step": state_bytes, "steps": args.e2e_steps,
+                "path": "sph_upload + sph_step_async(1) + sph_download per step, pinned host buffers"},
+        "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": hbm_peak, "unit": "GB/s",
+                     "frac": achieved_gbs / hbm_peak, "traffic": traffic,
+                     "kernel": "k_momentum<3,true> (fused momentum + leapfrog)",
+                     "peak_kind": f"{peak_kind} HBM copy bandwidth",
+                     "fp64": {"achieved_tflops": mom_tflops, "peak_tflops": fp64_peak,
+                              "frac": mom_tflops / fp64_peak, "peak_kind": "measured FP64 FMA rate (in-run)"}},
+        "phases_ms_per_step": {k: v / nprof for k, v in phases.items()},
+        "pairs_per_particle": cnt["mom_pairs"] / nprof / n,
+        "candidates_per_particle": cnt["mom_candidates"] / nprof / n,
+        "continuity_tflops": cont_flops / (phases["continuity"] / nprof * 1e-3) / 1e12,
+        "gpu_launches": KERNELS_PER_STEP * args.steps,
+        "clocks": clocks,
+        "cpu_baseline": cpu,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    sim.close()
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

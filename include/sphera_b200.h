@@ -253,6 +253,22 @@ int  sph_dump_neighbours(SphHandle* h, int32_t nmaxj, int32_t* counts, int32_t* 
 int  sph_dump_boundary(SphHandle* h, int32_t max_per, int32_t* ncb,
                        int32_t* clobonum, double* values);
 
+/* ---------------------------------------------------------------------- */
+/* Profiling (the counterpart of the reference's start_and_stop phase      */
+/* timers, src/Post_processing/elapsed_time/start_and_stop.f90:65-152)      */
+/* ---------------------------------------------------------------------- */
+
+/* Runs nsteps whole steps without the graph, timing each phase with CUDA
+ * events on the handle's stream; ms[0..4] receive the summed milliseconds of
+ * momentum (+leapfrog, trajectories), OrdGrid1, ComputeBoundaryDataTab,
+ * continuity (+Leapfrog_continuity, EoS) and the time-step closing.       */
+int  sph_profile_phases(SphHandle* h, int32_t nsteps, double* ms);
+/* Neighbour candidates and accepted pairs (incl. self) counted by the pair
+ * passes: c[0..1] momentum, c[2..3] continuity; reset != 0 zeroes them.   */
+int  sph_get_counters(SphHandle* h, uint64_t* c, int32_t reset);
+/* Measured dense FP64 FMA throughput of the current device in TFLOP/s.    */
+int  sph_measure_fp64_peak(double* tflops);
+
 #ifdef __cplusplus
 }
 #endif

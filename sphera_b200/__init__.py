@@ -71,6 +71,9 @@ def lib():
         "sph_dump_grid": ([vp, ip, ip, ip], C.c_int),
         "sph_dump_neighbours": ([vp, C.c_int32, ip, ip], C.c_int),
         "sph_dump_boundary": ([vp, C.c_int32, ip, ip, dp], C.c_int),
+        "sph_profile_phases": ([vp, C.c_int32, dp], C.c_int),
+        "sph_get_counters": ([vp, C.POINTER(C.c_uint64), C.c_int32], C.c_int),
+        "sph_measure_fp64_peak": ([dp], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -189,6 +192,19 @@ class Simulation:
     def eos(self):
         _chk(lib().sph_eos(self._h), "sph_eos")
 
+    # ------------------------------------------------------------ profiling
+    PHASES = ("momentum", "ord_grid", "boundary_data_tab", "continuity", "time_step")
+
+    def profile_phases(self, nsteps):
+        ms = np.zeros(5)
+        _chk(lib().sph_profile_phases(self._h, int(nsteps), abi.dptr(ms)), "sph_profile_phases")
+        return dict(zip(self.PHASES, ms))
+
+    def counters(self, reset=False):
+        c = (C.c_uint64 * 4)()
+        _chk(lib().sph_get_counters(self._h, c, int(bool(reset))), "sph_get_counters")
+        return dict(mom_candidates=c[0], mom_pairs=c[1], cont_candidates=c[2], cont_pairs=c[3])
+
     # --------------------------------------------------------- verification
     def dump_grid(self):
         d = self.diagnostics()
@@ -212,6 +228,13 @@ class Simulation:
         _chk(lib().sph_dump_boundary(self._h, max_per, abi.iptr(ncb), abi.iptr(clob), abi.dptr(vals)),
              "sph_dump_boundary")
         return ncb, clob, vals
+
+
+def measure_fp64_peak():
+    """Dense FP64 FMA throughput of the current device, TFLOP/s."""
+    t = C.c_double()
+    _chk(lib().sph_measure_fp64_peak(C.byref(t)), "sph_measure_fp64_peak")
+    return t.value
 
 
 class Batch:

@@ -480,6 +480,7 @@ struct SphHandle {
   int *d_cf_start = nullptr, *d_cf_count = nullptr, *d_cf_list = nullptr;
   uint8_t* d_near = nullptr;
   int* d_scan = nullptr;
+  unsigned long long* d_counters = nullptr;
   Particles P{};
   std::vector<void*> owned;
   // caller-order staging
@@ -636,6 +637,7 @@ int create_batch(int nsims, const SphParams* params, const SphGeometry* geoms, c
   A(h->d_ci1, N); A(h->d_ci2, C + 1); A(h->d_ci3, N);
   int nb = (int)((C + 4095) / 4096) + 1;
   A(h->d_scan, nb);
+  A(h->d_counters, 4);
 #undef A
   if (st != SPH_OK) { sph_destroy(h); return st; }
   P.bdt_cap = (int)std::min(bdt_cap, (size_t)0x7fffffff);
@@ -687,6 +689,7 @@ int create_batch(int nsims, const SphParams* params, const SphGeometry* geoms, c
   if (e == cudaSuccess) e = cudaMemsetAsync(P.bdt_count, 0, sizeof(int) * N, q);
   if (e == cudaSuccess) e = cudaMemsetAsync(P.ACC, 0, sizeof(double4) * N, q);
   if (e == cudaSuccess) e = cudaMemsetAsync(P.DDEN, 0, sizeof(double) * N, q);
+  if (e == cudaSuccess) e = cudaMemsetAsync(h->d_counters, 0, sizeof(unsigned long long) * 4, q);
   if (e == cudaSuccess) upload_bit2d(&bit2d[0][0], q);
   if (e == cudaSuccess) e = cudaStreamSynchronize(q);
   if (e != cudaSuccess) { sph_destroy(h); return cuda_status(e); }
@@ -706,6 +709,7 @@ int create_batch(int nsims, const SphParams* params, const SphGeometry* geoms, c
   b.cf_list = h->d_cf_list;
   b.cell_near = h->d_near;
   b.scan_block_sums = h->d_scan;
+  b.counters = h->d_counters;
   b.scan_nblocks = nb;
   b.grid_blocks = prop.multiProcessorCount * 8;
   *out = h;
@@ -1015,6 +1019,94 @@ int sph_dump_boundary(SphHandle* h, int32_t max_per, int32_t* ncb, int32_t* clob
   cudaFree(dc);
   cudaFree(dv);
   return cuda_status(e);
+}
+
+// ---------------------------------------------------------------- profiling
+// Per-phase device time of nsteps un-graphed steps (CUDA events on the
+// handle's stream; the replacement of the reference's start_and_stop timers,
+// src/Post_processing/elapsed_time/start_and_stop.f90):
+//   ms[0] momentum (RHS_momentum_equation + leapfrog + trajectories)
+//   ms[1] OrdGrid1 (bin, removals, scan, place, rank/permute)
+//   ms[2] ComputeBoundaryDataTab
+//   ms[3] continuity + Leapfrog_continuity + EoS
+//   ms[4] time_step_duration closing
+int sph_profile_phases(SphHandle* h, int32_t nsteps, double* ms) {
+  if (!h || !h->uploaded || nsteps <= 0 || !ms) return SPH_ERR_INVALID_ARGUMENT;
+  cudaEvent_t ev[6];
+  for (int i = 0; i < 6; ++i)
+    if (cudaEventCreate(&ev[i]) != cudaSuccess) { cudaGetLastError(); return SPH_ERR_CUDA; }
+  for (int i = 0; i < 5; ++i) ms[i] = 0.0;
+  cudaStream_t q = h->stream;
+  cudaError_t e = cudaSuccess;
+  for (int s = 0; s < nsteps && e == cudaSuccess; ++s) {
+    cudaEventRecord(ev[0], q);
+    launch_momentum(h->db, true, q);
+    cudaEventRecord(ev[1], q);
+    sort_sequence(h, q);
+    cudaEventRecord(ev[2], q);
+    launch_boundary(h->db, q);
+    cudaEventRecord(ev[3], q);
+    launch_continuity(h->db, true, q);
+    cudaEventRecord(ev[4], q);
+    launch_finalize(h->db, 1, q);
+    cudaEventRecord(ev[5], q);
+    e = cudaEventSynchronize(ev[5]);
+    for (int i = 0; i < 5 && e == cudaSuccess; ++i) {
+      float t = 0.f;
+      e = cudaEventElapsedTime(&t, ev[i], ev[i + 1]);
+      ms[i] += t;
+    }
+  }
+  for (int i = 0; i < 6; ++i) cudaEventDestroy(ev[i]);
+  if (e != cudaSuccess) return cuda_status(e);
+  return sync_dyn(h);
+}
+
+// Candidate and accepted-pair counts accumulated by the pair passes:
+// c[0] momentum candidates, c[1] momentum pairs (incl. the particle
+// itself), c[2] continuity candidates, c[3] continuity pairs.
+int sph_get_counters(SphHandle* h, uint64_t* c, int32_t reset) {
+  if (!h || !c) return SPH_ERR_INVALID_ARGUMENT;
+  unsigned long long t[4];
+  SPH_CUDA(cudaMemcpyAsync(t, h->d_counters, sizeof(t), cudaMemcpyDeviceToHost, h->stream));
+  if (reset) SPH_CUDA(cudaMemsetAsync(h->d_counters, 0, sizeof(t), h->stream));
+  SPH_CUDA(cudaStreamSynchronize(h->stream));
+  for (int i = 0; i < 4; ++i) c[i] = t[i];
+  return SPH_OK;
+}
+
+// Dense FP64 FMA throughput of the current device (TFLOP/s), the FP64
+// roofline of the pair passes.
+int sph_measure_fp64_peak(double* tflops) {
+  if (!tflops) return SPH_ERR_INVALID_ARGUMENT;
+  int dev = 0, sms = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
+    cudaGetLastError();
+    return SPH_ERR_NO_DEVICE;
+  }
+  double* sink = nullptr;
+  int blocks = sms * 16;
+  SPH_TRY(dalloc(&sink, blocks));
+  cudaStream_t q;
+  if (cudaStreamCreateWithFlags(&q, cudaStreamNonBlocking) != cudaSuccess) { cudaFree(sink); cudaGetLastError(); return SPH_ERR_CUDA; }
+  cudaEvent_t a, b;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  double flops = 0.0;
+  for (int w = 0; w < 3; ++w) launch_fp64_probe(sink, blocks, q);
+  cudaEventRecord(a, q);
+  for (int r = 0; r < 10; ++r) flops += launch_fp64_probe(sink, blocks, q);
+  cudaEventRecord(b, q);
+  cudaError_t e = cudaEventSynchronize(b);
+  float ms = 0.f;
+  if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, a, b);
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  cudaStreamDestroy(q);
+  cudaFree(sink);
+  if (e != cudaSuccess) return cuda_status(e);
+  *tflops = flops / (ms * 1e-3) / 1e12;
+  return SPH_OK;
 }
 
 }  // extern "C"

@@ -104,6 +104,20 @@ __device__ __forceinline__ int warp_max(int v) {
   return v;
 }
 
+// Adds two per-thread counts of the block to counters[0..1] (one atomic per
+// block and counter).
+__device__ __forceinline__ void block_count2(unsigned long long* counters, int a, int c) {
+  unsigned long long sa = (unsigned long long)a, sc = (unsigned long long)c;
+  for (int o = 16; o > 0; o >>= 1) {
+    sa += __shfl_xor_sync(0xffffffffu, sa, o);
+    sc += __shfl_xor_sync(0xffffffffu, sc, o);
+  }
+  if ((threadIdx.x & 31) == 0 && (sa | sc)) {
+    atomicAdd(counters, sa);
+    atomicAdd(counters + 1, sc);
+  }
+}
+
 // InterpolateTable.f90:58-82 on columns 1..4.
 __device__ __forceinline__ void interpolate_table(const SimDev& s, double xval, double* iv) {
   double deltaX = s.ktdelta;
@@ -954,6 +968,7 @@ __global__ void __launch_bounds__(kBlock) k_momentum(DevBatch b) {
     bool active = threadIdx.x < tl.count && p < s.p_off + dyn->nag;
     double dtc = 1.0e300;
     int nneigh = 0;
+    int cnt_cand = 0, cnt_pairs = 0;
     if (FUSED && active && dyn->frozen) {
       // a finished simulation of a batch: carry the record through the sort
       double4 v4 = P.V[p];
@@ -994,6 +1009,7 @@ __global__ void __launch_bounds__(kBlock) k_momentum(DevBatch b) {
       for (int r = 0; r < NR && !trunc && in_grid; ++r) {
         int qb, qe;
         neighbour_run<DIM>(s, P.cell_start, ci, cj, ck, r, qb, qe);
+        cnt_cand += qe - qb;
         for (int q = qb; q < qe; ++q) {
           if (nneigh >= s.nmaxpartj) { trunc = true; break; }
           double4 xj = P.X[q];
@@ -1044,6 +1060,7 @@ __global__ void __launch_bounds__(kBlock) k_momentum(DevBatch b) {
         }
       }
       if (trunc) atomicOr(&dyn->warnings, SPH_WARN_NEIGHBOURS_TRUNCATED);
+      cnt_pairs = nneigh;
       tpres[0] = tpres[0] + tp0 + al0;
       tpres[1] = tpres[1] + tp1 + al1;
       tpres[2] = tpres[2] + tp2 + al2;
@@ -1084,6 +1101,7 @@ __global__ void __launch_bounds__(kBlock) k_momentum(DevBatch b) {
         P.L[p] = (uint8_t)lam_new;
       }
     }
+    block_count2(b.counters, cnt_cand, cnt_pairs);
     if (FUSED) {
       double m = warp_min(dtc);
       int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -1116,6 +1134,7 @@ __global__ void __launch_bounds__(kBlock) k_continuity(DevBatch b) {
     int p = tl.start + threadIdx.x;
     bool active = threadIdx.x < tl.count && p < s.p_off + dyn->nag && !(FUSED && dyn->frozen);
     int nneigh = 0;
+    int cnt_cand = 0;
     if (active) {
       double4 xi = P.X[p];
       double4 vi = P.V[p];
@@ -1183,6 +1202,7 @@ __global__ void __launch_bounds__(kBlock) k_continuity(DevBatch b) {
       for (int r = 0; r < NR && !trunc && in_grid; ++r) {
         int qb, qe;
         neighbour_run<DIM>(s, P.cell_start, ci, cj, ck, r, qb, qe);
+        cnt_cand += qe - qb;
         for (int q = qb; q < qe; ++q) {
           if (nneigh >= s.nmaxpartj) { trunc = true; break; }
           double4 xj = P.X[q];
@@ -1216,6 +1236,7 @@ __global__ void __launch_bounds__(kBlock) k_continuity(DevBatch b) {
         P.DDEN[p] = dden;
       }
     }
+    block_count2(b.counters + 2, cnt_cand, nneigh);
     int m = warp_max(nneigh);
     int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     if (lane == 0) redi[wid] = m;
@@ -1531,6 +1552,25 @@ __global__ void k_dump_cella(DevBatch b, int* cella) {
     if (particle_cell(s, xi.x, xi.y, xi.z, i, j, k)) c = ((k - 1) * s.ncd[1] + (j - 1)) * s.ncd[0] + i;
     cella[(size_t)s.p_off + P.I[p] - 1] = c;
   }
+}
+
+// FP64 fused multiply-add throughput probe (8 independent chains per thread).
+__global__ void __launch_bounds__(256) k_fp64_probe(double* sink, int iters) {
+  double a0 = threadIdx.x * 1e-9, a1 = a0 + 1e-9, a2 = a0 + 2e-9, a3 = a0 + 3e-9;
+  double a4 = a0 + 4e-9, a5 = a0 + 5e-9, a6 = a0 + 6e-9, a7 = a0 + 7e-9;
+  const double m = 0.999999999, c = 1e-12;
+  for (int i = 0; i < iters; ++i) {
+    a0 = fma(a0, m, c); a1 = fma(a1, m, c); a2 = fma(a2, m, c); a3 = fma(a3, m, c);
+    a4 = fma(a4, m, c); a5 = fma(a5, m, c); a6 = fma(a6, m, c); a7 = fma(a7, m, c);
+  }
+  double r = a0 + a1 + a2 + a3 + a4 + a5 + a6 + a7;
+  if (r == 12345.0) sink[blockIdx.x] = r;
+}
+
+double launch_fp64_probe(double* sink, int blocks, cudaStream_t st) {
+  const int iters = 4096;
+  k_fp64_probe<<<blocks, 256, 0, st>>>(sink, iters);
+  return 2.0 * 8.0 * iters * 256.0 * blocks;
 }
 
 // ==========================================================================

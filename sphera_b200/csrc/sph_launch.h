@@ -20,6 +20,8 @@ struct DevBatch {
   const int* cf_count;     // per global cell: faces cutting the cell
   const int* cf_list;      // face ids (1-based within the simulation)
   const uint8_t* cell_near;  // per global cell: faces cut the 27-cell block
+  unsigned long long* counters;  // [0] momentum candidates, [1] momentum pairs,
+                                 // [2] continuity candidates, [3] continuity pairs
   int* scan_block_sums;    // scan scratch
   int scan_nblocks;
   int grid_blocks;         // blocks of the persistent particle kernels
@@ -56,5 +58,7 @@ void launch_to_caller(const DevBatch& b, double* x, double* v, double* rho, doub
 void launch_dump_neighbours(const DevBatch& b, int nmaxj, int* counts, int* lists, cudaStream_t st);
 void launch_dump_boundary(const DevBatch& b, int max_per, int* ncb, int* clob, double* vals, cudaStream_t st);
 void launch_dump_cella(const DevBatch& b, int* cella, cudaStream_t st);
+// FP64 FMA throughput probe: returns flops per launch
+double launch_fp64_probe(double* sink, int blocks, cudaStream_t st);
 
 }  // namespace sph
