@@ -88,6 +88,13 @@ class ClockSampler:
                                       stdout=self.f, stderr=subprocess.DEVNULL)
         except OSError:
             self.p = None
+        # nvidia-smi's first query can stall the driver for seconds on a box
+        # without persistence mode: wait for its first sample before timing
+        t0 = time.time()
+        while self.p is not None and time.time() - t0 < 10.0:
+            if os.path.getsize(self.f.name) > 0:
+                break
+            time.sleep(0.05)
 
     def stop(self):
         if self.p is None:

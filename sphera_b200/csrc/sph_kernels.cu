@@ -953,22 +953,82 @@ __device__ void elastic_reaction(const SimDev& s, const DevBatch& b, int nb, int
   }
 }
 
+// Accepted-neighbour FIFO per thread.  The candidate scan (cheap, divergent:
+// about one candidate in six lies within 2h) fills it in the reference's
+// visiting order; the pair arithmetic then drains it with the whole warp in
+// lockstep, so the expensive FP64 work runs on (nearly) all lanes.
+constexpr int kBuf = 16;
+
+template <int DIM>
+struct NeighbourScan {
+  int r, q, qe, ci, cj, ck, nacc, cand;
+  bool done, trunc;
+
+  __device__ __forceinline__ void init(bool on, int ci_, int cj_, int ck_) {
+    ci = ci_;
+    cj = cj_;
+    ck = ck_;
+    r = 0;
+    q = 0;
+    qe = 0;
+    nacc = 0;
+    cand = 0;
+    trunc = false;
+    done = !on;
+  }
+
+  // Appends up to kBuf accepted slots (the particle itself excluded) to the
+  // thread's FIFO column; returns how many were appended.  The NMAXPARTJ cap
+  // of CalcVarLength.f90:197-205 is applied on the accepted count.
+  __device__ __forceinline__ int fill(const SimDev& s, const Particles& P, const double4& xi, int self, int* col) {
+    constexpr int NR = (DIM == 3) ? 9 : 3;
+    int nb = 0;
+    while (!done && nb < kBuf) {
+      if (q >= qe) {
+        if (r >= NR) {
+          done = true;
+          break;
+        }
+        neighbour_run<DIM>(s, P.cell_start, ci, cj, ck, r, q, qe);
+        r++;
+        cand += qe - q;
+        continue;
+      }
+      if (nacc >= s.nmaxpartj) {
+        trunc = true;
+        done = true;
+        break;
+      }
+      double4 xj = P.X[q];
+      double r0 = xi.x - xj.x, r1 = xi.y - xj.y, r2 = xi.z - xj.z;
+      double rr = r0 * r0 + r1 * r1 + r2 * r2;
+      if (!(rr > s.square_doubleh)) {
+        nacc++;
+        if (q != self) {
+          col[nb * kBlock] = q;
+          nb++;
+        }
+      }
+      q++;
+    }
+    return nb;
+  }
+};
+
 template <int DIM, bool FUSED>
-__global__ void __launch_bounds__(kBlock) k_momentum(DevBatch b) {
+__global__ void __launch_bounds__(kBlock, 2) k_momentum(DevBatch b) {
   __shared__ SimDev s;
-  __shared__ double red[kBlock / 32];
+  __shared__ int sbuf[kBuf * kBlock];
   int cur = -1;
   const Particles& P = b.P;
   const double GI = (double)9.80665f;   // Static_allocation_module.f90:72, a default-REAL literal
+  int* col = sbuf + threadIdx.x;
   for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
     Tile tl = b.tiles[t];
     load_sim(s, b.sims, tl.sim, cur);
     SimDyn* dyn = b.dyn + tl.sim;
     int p = tl.start + threadIdx.x;
     bool active = threadIdx.x < tl.count && p < s.p_off + dyn->nag;
-    double dtc = 1.0e300;
-    int nneigh = 0;
-    int cnt_cand = 0, cnt_pairs = 0;
     if (FUSED && active && dyn->frozen) {
       // a finished simulation of a batch: carry the record through the sort
       double4 v4 = P.V[p];
@@ -980,87 +1040,94 @@ __global__ void __launch_bounds__(kBlock) k_momentum(DevBatch b) {
       P.L2[p] = P.L[p];
       active = false;
     }
+    double4 xi = make_double4(0.0, 0.0, 0.0, 0.0);
+    double vi[3] = {0.0, 0.0, 0.0};
+    double rhoi = 1.0, pi = 0.0;
+    int lam = 0, nb = 0, bstart = 0;
+    double tpres[3] = {0, 0, 0}, tdiss[3] = {0, 0, 0}, tvisc[3] = {0, 0, 0};
+    int ci = 0, cj = 0, ck = 0;
+    bool in_grid = false;
     if (active) {
-      double4 xi = P.X[p];
+      xi = P.X[p];
       double4 v4 = P.V[p];
       double2 rp = P.RP[p];
-      double vi[3] = {v4.x, v4.y, v4.z};
-      double rhoi = rp.x, pi = rp.y;
-      int lam = P.L[p];
-      double tpres[3] = {0, 0, 0}, tdiss[3] = {0, 0, 0}, tvisc[3] = {0, 0, 0};
-      int nb = P.bdt_count[p];
-      int bstart = nb > 0 ? P.bdt_start[p] : 0;
+      vi[0] = v4.x;
+      vi[1] = v4.y;
+      vi[2] = v4.z;
+      rhoi = rp.x;
+      pi = rp.y;
+      lam = P.L[p];
+      nb = P.bdt_count[p];
+      bstart = nb > 0 ? P.bdt_start[p] : 0;
       if (nb > 0) {
         if (DIM == 3) me_boundary3d(s, b, nb, bstart, vi, rhoi, pi, lam, tpres, tdiss, tvisc);
         else me_boundary2d(s, b, nb, bstart, vi, rhoi, pi, lam, tpres, tdiss, tvisc);
       }
-      int ci = 0, cj = 0, ck = 0;
-      bool in_grid = particle_cell(s, xi.x, xi.y, xi.z, ci, cj, ck);
+      in_grid = particle_cell(s, xi.x, xi.y, xi.z, ci, cj, ck);
       if (!in_grid) set_status(dyn, SPH_ERR_INVALID_ARGUMENT);   // state not re-sorted after a move
-      double tp0 = 0, tp1 = 0, tp2 = 0, al0 = 0, al1 = 0, al2 = 0;
-      double td0 = tdiss[0], td1 = tdiss[1], td2 = tdiss[2];
-      double tv0 = tvisc[0], tv1 = tvisc[1], tv2 = tvisc[2];
-      double rs0 = 0, rs1 = 0, rs2 = 0;
-      const double celt = s.celerita + s.celerita;
-      const bool morris = s.kin_visc > 1.0e-12;
-      const double nu = s.kin_visc;
-      bool trunc = false;
-      constexpr int NR = (DIM == 3) ? 9 : 3;
-      for (int r = 0; r < NR && !trunc && in_grid; ++r) {
-        int qb, qe;
-        neighbour_run<DIM>(s, P.cell_start, ci, cj, ck, r, qb, qe);
-        cnt_cand += qe - qb;
-        for (int q = qb; q < qe; ++q) {
-          if (nneigh >= s.nmaxpartj) { trunc = true; break; }
-          double4 xj = P.X[q];
-          double r0 = xi.x - xj.x, r1 = xi.y - xj.y, r2 = xi.z - xj.z;
-          double rr = r0 * r0 + r1 * r1 + r2 * r2;
-          if (rr > s.square_doubleh) continue;
-          nneigh++;
-          if (q == p) continue;
-          double PK1, PK2, PK3;
-          kernel_values(s, rr, PK1, PK2, PK3);
-          double4 vj = P.V[q];
-          double2 rpj = P.RP[q];
-          double rhoj = rpj.x, pj = rpj.y, amassj = xj.w;
-          double dv0 = vj.x - vi[0], dv1 = vj.y - vi[1], dv2 = vj.z - vi[2];
-          // pressure gradient and ALE1 terms, inter_EqMoto.f90:195-221
-          double alpha = (pj - pi) / (rhoi * rhoj);
-          tp0 = tp0 + -(amassj * alpha * r0 * PK3);
-          if (DIM == 3) tp1 = tp1 + -(amassj * alpha * r1 * PK3);
-          tp2 = tp2 + -(amassj * alpha * r2 * PK3);
-          double alpha2 = (pi * (rhoj / rhoi + 1.0) + pj * (rhoi / rhoj - 1.0)) / (rhoi * rhoj);
-          al0 = al0 - amassj * alpha2 * r0 * PK3;
-          if (DIM == 3) al1 = al1 - amassj * alpha2 * r1 * PK3;
-          al2 = al2 - amassj * alpha2 * r2 * PK3;
-          // viscomon.f90:54-73
-          double vrij = (DIM == 3) ? -(dv0 * r0) - dv1 * r1 - dv2 * r2 : -(dv0 * r0) - dv2 * r2;
-          double TermMon = s.alfa_mon * celt * s.h / (rhoi + rhoj);
-          double mtv = amassj * TermMon * vrij;
-          td0 = td0 + (mtv * r0 * PK2 + 0.0);
-          if (DIM == 3) td1 = td1 + (mtv * r1 * PK2 + 0.0);
-          td2 = td2 + (mtv * r2 * PK2 + 0.0);
-          // viscomorris.f90:60-71
-          if (morris) {
-            double rt = nu * rhoi + nu * rhoj + 1.0e-3;
-            double anuitilde = 4.0 * (nu * nu);
-            double factivis = amassj * anuitilde / rt;
-            double w0 = factivis * (-(dv0 * PK2 * rr));
-            double w2 = factivis * (-(dv2 * PK2 * rr));
-            tv0 = tv0 + w0;
-            rs0 = rs0 + w0;
-            if (DIM == 3) {
-              double w1 = factivis * (-(dv1 * PK2 * rr));
-              tv1 = tv1 + w1;
-              rs1 = rs1 + w1;
-            }
-            tv2 = tv2 + w2;
-            rs2 = rs2 + w2;
+    }
+    NeighbourScan<DIM> sc;
+    sc.init(active && in_grid, ci, cj, ck);
+    double tp0 = 0, tp1 = 0, tp2 = 0, al0 = 0, al1 = 0, al2 = 0;
+    double td0 = tdiss[0], td1 = tdiss[1], td2 = tdiss[2];
+    double tv0 = tvisc[0], tv1 = tvisc[1], tv2 = tvisc[2];
+    double rs0 = 0, rs1 = 0, rs2 = 0;
+    const double celt = s.celerita + s.celerita;
+    const bool morris = s.kin_visc > 1.0e-12;
+    const double nu = s.kin_visc;
+    while (__any_sync(0xffffffffu, !sc.done)) {
+      int nbuf = sc.fill(s, P, xi, p, col);
+      int nmax = __reduce_max_sync(0xffffffffu, (unsigned)nbuf);
+      for (int k = 0; k < nmax; ++k) {
+        if (k >= nbuf) continue;
+        int q = col[k * kBlock];
+        double4 xj = P.X[q];
+        double r0 = xi.x - xj.x, r1 = xi.y - xj.y, r2 = xi.z - xj.z;
+        double rr = r0 * r0 + r1 * r1 + r2 * r2;
+        double PK1, PK2, PK3;
+        kernel_values(s, rr, PK1, PK2, PK3);
+        double4 vj = P.V[q];
+        double2 rpj = P.RP[q];
+        double rhoj = rpj.x, pj = rpj.y, amassj = xj.w;
+        double dv0 = vj.x - vi[0], dv1 = vj.y - vi[1], dv2 = vj.z - vi[2];
+        // pressure gradient and ALE1 terms, inter_EqMoto.f90:195-221
+        double alpha = (pj - pi) / (rhoi * rhoj);
+        tp0 = tp0 + -(amassj * alpha * r0 * PK3);
+        if (DIM == 3) tp1 = tp1 + -(amassj * alpha * r1 * PK3);
+        tp2 = tp2 + -(amassj * alpha * r2 * PK3);
+        double alpha2 = (pi * (rhoj / rhoi + 1.0) + pj * (rhoi / rhoj - 1.0)) / (rhoi * rhoj);
+        al0 = al0 - amassj * alpha2 * r0 * PK3;
+        if (DIM == 3) al1 = al1 - amassj * alpha2 * r1 * PK3;
+        al2 = al2 - amassj * alpha2 * r2 * PK3;
+        // viscomon.f90:54-73
+        double vrij = (DIM == 3) ? -(dv0 * r0) - dv1 * r1 - dv2 * r2 : -(dv0 * r0) - dv2 * r2;
+        double TermMon = s.alfa_mon * celt * s.h / (rhoi + rhoj);
+        double mtv = amassj * TermMon * vrij;
+        td0 = td0 + (mtv * r0 * PK2 + 0.0);
+        if (DIM == 3) td1 = td1 + (mtv * r1 * PK2 + 0.0);
+        td2 = td2 + (mtv * r2 * PK2 + 0.0);
+        // viscomorris.f90:60-71
+        if (morris) {
+          double rt = nu * rhoi + nu * rhoj + 1.0e-3;
+          double anuitilde = 4.0 * (nu * nu);
+          double factivis = amassj * anuitilde / rt;
+          double w0 = factivis * (-(dv0 * PK2 * rr));
+          double w2 = factivis * (-(dv2 * PK2 * rr));
+          tv0 = tv0 + w0;
+          rs0 = rs0 + w0;
+          if (DIM == 3) {
+            double w1 = factivis * (-(dv1 * PK2 * rr));
+            tv1 = tv1 + w1;
+            rs1 = rs1 + w1;
           }
+          tv2 = tv2 + w2;
+          rs2 = rs2 + w2;
         }
       }
-      if (trunc) atomicOr(&dyn->warnings, SPH_WARN_NEIGHBOURS_TRUNCATED);
-      cnt_pairs = nneigh;
+    }
+    double dtc = 1.0e300;
+    if (active) {
+      if (sc.trunc) atomicOr(&dyn->warnings, SPH_WARN_NEIGHBOURS_TRUNCATED);
       tpres[0] = tpres[0] + tp0 + al0;
       tpres[1] = tpres[1] + tp1 + al1;
       tpres[2] = tpres[2] + tp2 + al2;
@@ -1101,18 +1168,11 @@ __global__ void __launch_bounds__(kBlock) k_momentum(DevBatch b) {
         P.L[p] = (uint8_t)lam_new;
       }
     }
-    block_count2(b.counters, cnt_cand, cnt_pairs);
+    block_count2(b.counters, sc.cand, sc.nacc);
     if (FUSED) {
       double m = warp_min(dtc);
-      int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-      if (lane == 0) red[wid] = m;
-      __syncthreads();
-      if (threadIdx.x == 0) {
-        double mm = red[0];
-        for (int w = 1; w < kBlock / 32; ++w) mm = fmin(mm, red[w]);
-        if (mm < 1.0e300) atomicMin(&dyn->dtmin_bits, (unsigned long long)__double_as_longlong(mm));
-      }
-      __syncthreads();
+      if ((threadIdx.x & 31) == 0 && m < 1.0e300)
+        atomicMin(&dyn->dtmin_bits, (unsigned long long)__double_as_longlong(m));
     }
   }
 }
@@ -1122,24 +1182,27 @@ __global__ void __launch_bounds__(kBlock) k_momentum(DevBatch b) {
 // Continuity_Equation, optionally fused with Leapfrog_continuity and the EoS.
 // ==========================================================================
 template <int DIM, bool FUSED>
-__global__ void __launch_bounds__(kBlock) k_continuity(DevBatch b) {
+__global__ void __launch_bounds__(kBlock, 2) k_continuity(DevBatch b) {
   __shared__ SimDev s;
-  __shared__ int redi[kBlock / 32];
+  __shared__ int sbuf[kBuf * kBlock];
   int cur = -1;
   const Particles& P = b.P;
+  int* col = sbuf + threadIdx.x;
   for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
     Tile tl = b.tiles[t];
     load_sim(s, b.sims, tl.sim, cur);
     SimDyn* dyn = b.dyn + tl.sim;
     int p = tl.start + threadIdx.x;
     bool active = threadIdx.x < tl.count && p < s.p_off + dyn->nag && !(FUSED && dyn->frozen);
-    int nneigh = 0;
-    int cnt_cand = 0;
+    double4 xi = make_double4(0.0, 0.0, 0.0, 0.0);
+    double4 vi = make_double4(0.0, 0.0, 0.0, 0.0);
+    double rhoi = 1.0, dden = 0.0;
+    int ci = 0, cj = 0, ck = 0;
+    bool in_grid = false;
     if (active) {
-      double4 xi = P.X[p];
-      double4 vi = P.V[p];
-      double rhoi = P.RP[p].x;
-      double dden = 0.0;
+      xi = P.X[p];
+      vi = P.V[p];
+      rhoi = P.RP[p].x;
       int nb = P.bdt_count[p];
       if (nb > 0) {
         int bstart = P.bdt_start[p];
@@ -1193,34 +1256,32 @@ __global__ void __launch_bounds__(kBlock) k_continuity(DevBatch b) {
         }
         dden = dden - rhoi * (gu0 + gv1 + gw2);
       }
-      int ci = 0, cj = 0, ck = 0;
-      bool in_grid = particle_cell(s, xi.x, xi.y, xi.z, ci, cj, ck);
+      in_grid = particle_cell(s, xi.x, xi.y, xi.z, ci, cj, ck);
       if (!in_grid) set_status(dyn, SPH_ERR_INVALID_ARGUMENT);   // state not re-sorted after a move
-      double a1 = 0.0, a2 = 0.0, a3 = 0.0;
-      bool trunc = false;
-      constexpr int NR = (DIM == 3) ? 9 : 3;
-      for (int r = 0; r < NR && !trunc && in_grid; ++r) {
-        int qb, qe;
-        neighbour_run<DIM>(s, P.cell_start, ci, cj, ck, r, qb, qe);
-        cnt_cand += qe - qb;
-        for (int q = qb; q < qe; ++q) {
-          if (nneigh >= s.nmaxpartj) { trunc = true; break; }
-          double4 xj = P.X[q];
-          double r0 = xi.x - xj.x, r1 = xi.y - xj.y, r2 = xi.z - xj.z;
-          double rr = r0 * r0 + r1 * r1 + r2 * r2;
-          if (rr > s.square_doubleh) continue;
-          nneigh++;
-          if (q == p) continue;   // dvar = 0 for the particle itself
-          double PK1, PK2, PK3;
-          kernel_values(s, rr, PK1, PK2, PK3);
-          double4 vj = P.V[q];
-          double c = rhoi * vj.w * PK1;     // rhoi * (amassj / rhoj) * PK1
-          a1 = a1 + c * (vj.x - vi.x) * r0;
-          if (DIM == 3) a2 = a2 + c * (vj.y - vi.y) * r1;
-          a3 = a3 + c * (vj.z - vi.z) * r2;
-        }
+    }
+    NeighbourScan<DIM> sc;
+    sc.init(active && in_grid, ci, cj, ck);
+    double a1 = 0.0, a2 = 0.0, a3 = 0.0;
+    while (__any_sync(0xffffffffu, !sc.done)) {
+      int nbuf = sc.fill(s, P, xi, p, col);   // the particle itself adds dvar = 0
+      int nmax = __reduce_max_sync(0xffffffffu, (unsigned)nbuf);
+      for (int k = 0; k < nmax; ++k) {
+        if (k >= nbuf) continue;
+        int q = col[k * kBlock];
+        double4 xj = P.X[q];
+        double r0 = xi.x - xj.x, r1 = xi.y - xj.y, r2 = xi.z - xj.z;
+        double rr = r0 * r0 + r1 * r1 + r2 * r2;
+        double PK1, PK2, PK3;
+        kernel_values(s, rr, PK1, PK2, PK3);
+        double4 vj = P.V[q];
+        double c = rhoi * vj.w * PK1;     // rhoi * (amassj / rhoj) * PK1
+        a1 = a1 + c * (vj.x - vi.x) * r0;
+        if (DIM == 3) a2 = a2 + c * (vj.y - vi.y) * r1;
+        a3 = a3 + c * (vj.z - vi.z) * r2;
       }
-      if (trunc) atomicOr(&dyn->warnings, SPH_WARN_NEIGHBOURS_TRUNCATED);
+    }
+    if (active) {
+      if (sc.trunc) atomicOr(&dyn->warnings, SPH_WARN_NEIGHBOURS_TRUNCATED);
       if (DIM == 3) dden = dden - (a1 + a2 + a3);
       else dden = dden - (a1 + a3);
       if (FUSED) {
@@ -1236,17 +1297,9 @@ __global__ void __launch_bounds__(kBlock) k_continuity(DevBatch b) {
         P.DDEN[p] = dden;
       }
     }
-    block_count2(b.counters + 2, cnt_cand, nneigh);
-    int m = warp_max(nneigh);
-    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    if (lane == 0) redi[wid] = m;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      int mm = redi[0];
-      for (int w = 1; w < kBlock / 32; ++w) mm = max(mm, redi[w]);
-      if (mm > 0) atomicMax(&dyn->max_neigh, mm);
-    }
-    __syncthreads();
+    block_count2(b.counters + 2, sc.cand, sc.nacc);
+    int m = warp_max(sc.nacc);
+    if ((threadIdx.x & 31) == 0 && m > 0) atomicMax(&dyn->max_neigh, m);
   }
 }
 
