@@ -184,6 +184,30 @@ int prepare_sim(const SphParams& prm, const SphGeometry& g, int cap, HostSim& hs
     s.dcd[d] = dextr / s.ncd[d];
   }
   if (s.dim == 2) s.ncd[1] = 1;
+  // FP32 screening copies x - center (k_rank_permute) and the band of r^2
+  // values whose FP32 evaluation cannot decide r^2 <= (2h)^2: with R the
+  // largest |x - center| inside the grid, a copy is within 2^-24 R of the
+  // exact offset, so each FP32 component difference is within
+  // eps = 2^-23 R + 2^-24 |d| of the exact one (|d| <= 2 dcd for a
+  // candidate of the 27-cell block); the squares and the two additions add
+  // a relative 3 * 2^-24.  The band is twice that bound.
+  {
+    double R2 = 0.0, dmax = 0.0;
+    for (int d = 0; d < 3; ++d) {
+      s.center[d] = 0.5 * (prm.domain_lo[d] + prm.domain_hi[d]);
+      double lo = s.extr_lo[d], hi = s.extr_lo[d] + s.dcd[d] * s.ncd[d];
+      double rr = std::max(std::fabs(lo - s.center[d]), std::fabs(hi - s.center[d]));
+      if (s.dim == 2 && d == 1) rr = 0.0;
+      R2 += rr * rr;
+      if (!(s.dim == 2 && d == 1)) dmax = std::max(dmax, 2.0 * s.dcd[d]);
+    }
+    double R = std::sqrt(R2);
+    double eps = std::ldexp(R, -23) + std::ldexp(dmax, -24);
+    double err = 3.0 * (2.0 * dmax * eps + eps * eps) + 3.0 * std::ldexp(s.square_doubleh, -24) * 1.01;
+    double band = 2.0 * err + 1e-12 * s.square_doubleh;
+    s.rr_lo = std::nextafter((float)(s.square_doubleh - band), 0.0f);
+    s.rr_hi = std::nextafter((float)(s.square_doubleh + band), 3.0e38f);
+  }
   long long ncells = (long long)s.ncd[0] * s.ncd[1] * s.ncd[2];
   if (ncells > (1LL << 30)) return SPH_ERR_INVALID_ARGUMENT;
   s.ncells = (int)ncells;
@@ -625,7 +649,7 @@ int create_batch(int nsims, const SphParams* params, const SphGeometry* geoms, c
   A(h->d_cf_start, C);
   A(h->d_cf_count, C);
   A(h->d_near, C);
-  A(P.X, N); A(P.V, N); A(P.RP, N); A(P.I, N); A(P.L, N);
+  A(P.X, N); A(P.XF, N); A(P.V, N); A(P.RP, N); A(P.I, N); A(P.L, N);
   A(P.X2, N); A(P.V2, N); A(P.P2, N); A(P.I2, N); A(P.L2, N);
   A(P.bdt_count, N); A(P.bdt_start, N); A(P.bdt, bdt_cap);
   A(P.key, N); A(P.slot, N); A(P.cell_count, C + 1); A(P.cell_start, C + 1);

@@ -53,6 +53,8 @@ struct SimDev {
   double cfl, vsc_coeff, pesodt;
   double zpmin;           // 0.05 h, ComputeBoundaryVolumeIntegrals_P0.f90
   double ktdelta;         // kernel-table step
+  double center[3];       // origin of the FP32 position copies
+  float rr_lo, rr_hi;     // FP32 screening band around (2h)^2 (see k_rank_permute)
   double kerneltab[kKtRows + 1][5];
 };
 
@@ -122,6 +124,7 @@ struct Tile {
 // Device view of the particle storage.
 struct Particles {
   double4* X;       // x, y, z, mass          (sorted)
+  float4* XF;       // x - center in FP32 (screening copy of X)
   double4* V;       // vx, vy, vz, rho (density entering the continuity pass)
   double2* RP;      // current rho, p
   int* I;           // caller index (1-based)

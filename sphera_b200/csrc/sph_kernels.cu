@@ -405,6 +405,7 @@ __global__ void k_rank_permute(DevBatch b) {
     double4 x = P.X2[src];
     double4 v = P.V2[src];
     P.X[fin] = x;
+    P.XF[fin] = make_float4((float)(x.x - s.center[0]), (float)(x.y - s.center[1]), (float)(x.z - s.center[2]), 0.f);
     P.V[fin] = make_double4(v.x, v.y, v.z, x.w / v.w);
     P.RP[fin] = make_double2(v.w, P.P2[src]);
     P.I[fin] = myid;
@@ -804,7 +805,7 @@ __global__ void __launch_bounds__(kBlock) k_boundary2d(DevBatch b) {
 // ==========================================================================
 
 // AddBoundaryContributions_to_ME3D.f90:105-336 (fixe/tapi, slip mode 1).
-__device__ void me_boundary3d(const SimDev& s, const DevBatch& b, int nb, int start, const double* vi, double rhoi,
+__device__ __forceinline__ void me_boundary3d(const SimDev& s, const DevBatch& b, int nb, int start, const double* vi, double rhoi,
                               double pres, int lam, double* tpres, double* tdiss, double* tvisc) {
   double ALEt[3] = {0, 0, 0}, gradpt[3] = {0, 0, 0}, VMon[3] = {0, 0, 0}, VShear[3] = {0, 0, 0};
   for (int u = 0; u < nb; ++u) {
@@ -861,7 +862,7 @@ __device__ void me_boundary3d(const SimDev& s, const DevBatch& b, int nb, int st
 }
 
 // AddBoundaryContributions_to_ME2D.f90:96-402 (fixe/tapi, slip mode 1).
-__device__ void me_boundary2d(const SimDev& s, const DevBatch& b, int nb, int start, const double* vi, double roi,
+__device__ __forceinline__ void me_boundary2d(const SimDev& s, const DevBatch& b, int nb, int start, const double* vi, double roi,
                               double pressi, int lam, double* tpres, double* tdiss, double* tvisc) {
   const double pibmink = 10.0;
   double ro0 = s.den0, distpimin = s.dx;
@@ -918,7 +919,7 @@ __device__ void me_boundary2d(const SimDev& s, const DevBatch& b, int nb, int st
 
 // AddElasticBoundaryReaction_3D.f90:67-154 (no convex edges) / _2D.f90:63-97.
 template <int DIM>
-__device__ void elastic_reaction(const SimDev& s, const DevBatch& b, int nb, int start, const double* vi, double* R) {
+__device__ __forceinline__ void elastic_reaction(const SimDev& s, const DevBatch& b, int nb, int start, const double* vi, double* R) {
   R[0] = R[1] = R[2] = 0.0;
   double zimin = 0.25 * s.dx;
   double celer02 = s.eps / s.den0;
@@ -980,7 +981,27 @@ struct NeighbourScan {
   // Appends up to kBuf accepted slots (the particle itself excluded) to the
   // thread's FIFO column; returns how many were appended.  The NMAXPARTJ cap
   // of CalcVarLength.f90:197-205 is applied on the accepted count.
-  __device__ __forceinline__ int fill(const SimDev& s, const Particles& P, const double4& xi, int self, int* col) {
+  //
+  // The distance test r^2 <= (2h)^2 of CalcVarLength.f90:223-228 is decided
+  // in FP32 on the screening copies when r^2 lies outside [rr_lo, rr_hi], a
+  // band the host derives from the rounding bounds of the copies, and in
+  // FP64 exactly as the reference does inside the band: the accepted set is
+  // the reference's, bit for bit.
+  __device__ __forceinline__ bool accept(const SimDev& s, const Particles& P, const double4& xi, const float4& xf,
+                                         int q) const {
+    float4 xj = P.XF[q];
+    float d0 = xf.x - xj.x, d1 = xf.y - xj.y, d2 = xf.z - xj.z;
+    float rf = d0 * d0 + d1 * d1 + d2 * d2;
+    if (rf < s.rr_lo) return true;
+    if (rf > s.rr_hi) return false;
+    double4 xd = P.X[q];
+    double r0 = xi.x - xd.x, r1 = xi.y - xd.y, r2 = xi.z - xd.z;
+    double rr = r0 * r0 + r1 * r1 + r2 * r2;
+    return !(rr > s.square_doubleh);
+  }
+
+  __device__ __forceinline__ int fill(const SimDev& s, const Particles& P, const double4& xi, const float4& xf,
+                                      int self, int* col) {
     constexpr int NR = (DIM == 3) ? 9 : 3;
     int nb = 0;
     while (!done && nb < kBuf) {
@@ -999,17 +1020,30 @@ struct NeighbourScan {
         done = true;
         break;
       }
-      double4 xj = P.X[q];
-      double r0 = xi.x - xj.x, r1 = xi.y - xj.y, r2 = xi.z - xj.z;
-      double rr = r0 * r0 + r1 * r1 + r2 * r2;
-      if (!(rr > s.square_doubleh)) {
-        nacc++;
-        if (q != self) {
-          col[nb * kBlock] = q;
-          nb++;
+      bool a0 = accept(s, P, xi, xf, q);
+      if (q + 1 < qe) {
+        // two candidates per iteration: independent loads in flight
+        bool a1 = accept(s, P, xi, xf, q + 1);
+        if (a0) {
+          nacc++;
+          if (q != self) col[(nb++) * kBlock] = q;
         }
+        if (nacc >= s.nmaxpartj) {
+          q++;
+          continue;
+        }
+        if (a1) {
+          nacc++;
+          if (q + 1 != self) col[(nb++) * kBlock] = q + 1;
+        }
+        q += 2;
+      } else {
+        if (a0) {
+          nacc++;
+          if (q != self) col[(nb++) * kBlock] = q;
+        }
+        q++;
       }
-      q++;
     }
     return nb;
   }
@@ -1018,7 +1052,7 @@ struct NeighbourScan {
 template <int DIM, bool FUSED>
 __global__ void __launch_bounds__(kBlock, 2) k_momentum(DevBatch b) {
   __shared__ SimDev s;
-  __shared__ int sbuf[kBuf * kBlock];
+  __shared__ int sbuf[(kBuf + 1) * kBlock];
   int cur = -1;
   const Particles& P = b.P;
   const double GI = (double)9.80665f;   // Static_allocation_module.f90:72, a default-REAL literal
@@ -1068,6 +1102,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_momentum(DevBatch b) {
     }
     NeighbourScan<DIM> sc;
     sc.init(active && in_grid, ci, cj, ck);
+    float4 xfi = active ? P.XF[p] : make_float4(0.f, 0.f, 0.f, 0.f);
     double tp0 = 0, tp1 = 0, tp2 = 0, al0 = 0, al1 = 0, al2 = 0;
     double td0 = tdiss[0], td1 = tdiss[1], td2 = tdiss[2];
     double tv0 = tvisc[0], tv1 = tvisc[1], tv2 = tvisc[2];
@@ -1076,7 +1111,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_momentum(DevBatch b) {
     const bool morris = s.kin_visc > 1.0e-12;
     const double nu = s.kin_visc;
     while (__any_sync(0xffffffffu, !sc.done)) {
-      int nbuf = sc.fill(s, P, xi, p, col);
+      int nbuf = sc.fill(s, P, xi, xfi, p, col);
       int nmax = __reduce_max_sync(0xffffffffu, (unsigned)nbuf);
       for (int k = 0; k < nmax; ++k) {
         if (k >= nbuf) continue;
@@ -1184,7 +1219,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_momentum(DevBatch b) {
 template <int DIM, bool FUSED>
 __global__ void __launch_bounds__(kBlock, 2) k_continuity(DevBatch b) {
   __shared__ SimDev s;
-  __shared__ int sbuf[kBuf * kBlock];
+  __shared__ int sbuf[(kBuf + 1) * kBlock];
   int cur = -1;
   const Particles& P = b.P;
   int* col = sbuf + threadIdx.x;
@@ -1261,9 +1296,10 @@ __global__ void __launch_bounds__(kBlock, 2) k_continuity(DevBatch b) {
     }
     NeighbourScan<DIM> sc;
     sc.init(active && in_grid, ci, cj, ck);
+    float4 xfi = active ? P.XF[p] : make_float4(0.f, 0.f, 0.f, 0.f);
     double a1 = 0.0, a2 = 0.0, a3 = 0.0;
     while (__any_sync(0xffffffffu, !sc.done)) {
-      int nbuf = sc.fill(s, P, xi, p, col);   // the particle itself adds dvar = 0
+      int nbuf = sc.fill(s, P, xi, xfi, p, col);   // the particle itself adds dvar = 0
       int nmax = __reduce_max_sync(0xffffffffu, (unsigned)nbuf);
       for (int k = 0; k < nmax; ++k) {
         if (k >= nbuf) continue;
@@ -1339,6 +1375,7 @@ __global__ void k_leapfrog_trajectories(DevBatch b) {
     x.y = x.y + dt * v.y;
     x.z = x.z + dt * v.z;
     b.P.X[p] = x;
+    b.P.XF[p] = make_float4((float)(x.x - s.center[0]), (float)(x.y - s.center[1]), (float)(x.z - s.center[2]), 0.f);
   }
 }
 
