@@ -254,6 +254,33 @@ int  sph_dump_boundary(SphHandle* h, int32_t max_per, int32_t* ncb,
                        int32_t* clobonum, double* values);
 
 /* ---------------------------------------------------------------------- */
+/* Allocation-free entry point                                             */
+/* ---------------------------------------------------------------------- */
+
+/* No counterpart in the reference.  The OrdGrid1 binning and counting sort
+ * (pg%cella, Icont, NPartOrd) for callers that cannot let a library
+ * allocate device memory -- a Fortran host whose device arrays come from its
+ * own pool (CUDA Fortran / OpenACC data regions), or a time loop that must
+ * not meet the implicit synchronisation of cudaMalloc/cudaFree.  It calls
+ * no cudaMalloc, cudaFree or allocating library routine: its working memory
+ * is a fixed device array of about 20 MB inside the library, held by every
+ * GPU that loads the library until the process exits.
+ *   d_x        [n][3] positions (device memory, caller order)
+ *   d_cella    [n]    out: 1-based cell of each particle, 0 outside the grid
+ *   d_icont    [n_cells+1] out: 1-based first NPartOrd slot of each cell
+ *   d_npartord [n]    out: 1-based particle indices sorted by cell, then index;
+ *                     particles outside the grid are not listed
+ *   stream     a cudaStream_t (NULL: the default stream); the call only
+ *              enqueues work on it.
+ * Limits: n <= 1048576 and Grid%nmax <= 1048576, else
+ * SPH_ERR_INVALID_ARGUMENT.  The first call on a device looks up the address
+ * of the device array (with that device current) and must come before any
+ * stream capture on that device.  Every call shares the one array: calls
+ * whose work overlaps on the GPU race and must be serialised.             */
+int  sph_ord_grid_static(const SphParams* params, int32_t n, const double* d_x, int32_t* d_cella,
+                         int32_t* d_icont, int32_t* d_npartord, void* stream);
+
+/* ---------------------------------------------------------------------- */
 /* Profiling (the counterpart of the reference's start_and_stop phase      */
 /* timers, src/Post_processing/elapsed_time/start_and_stop.f90:65-152)      */
 /* ---------------------------------------------------------------------- */

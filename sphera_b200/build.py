@@ -20,6 +20,7 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-ffp-contract=o
 UNITS = [
     ("sph_kernels.cu", ["--fmad=false"]),
     ("sph_api.cu", ["--fmad=false"]),
+    ("sph_static.cu", ["--fmad=false"]),
 ]
 
 
