@@ -184,29 +184,35 @@ int prepare_sim(const SphParams& prm, const SphGeometry& g, int cap, HostSim& hs
     s.dcd[d] = dextr / s.ncd[d];
   }
   if (s.dim == 2) s.ncd[1] = 1;
-  // FP32 screening copies x - center (k_rank_permute) and the band of r^2
-  // values whose FP32 evaluation cannot decide r^2 <= (2h)^2: with R the
-  // largest |x - center| inside the grid, a copy is within 2^-24 R of the
-  // exact offset, so each FP32 component difference is within
-  // eps = 2^-23 R + 2^-24 |d| of the exact one (|d| <= 2 dcd for a
-  // candidate of the 27-cell block); the squares and the two additions add
-  // a relative 3 * 2^-24.  The band is twice that bound.
+  // FP32 screening copies (k_rank_permute): the offset f of a particle from
+  // the origin o of its cell, in FP32.  A candidate difference is formed as
+  // D + (f_i - f_j) with D = (float)(cell index difference * dcd), which is
+  // 0 or +-(float)dcd inside the 27-cell block.  Each component is then
+  // within eps = 8 * 2^-24 dcd (+ 2^-50 R for the FP64 origins) of x_i - x_j,
+  // |x_i - x_j| < 2 dcd, and the FP32 sum of squares adds at most 5 roundings
+  // of 2^-24.  Outside twice that band the FP32 value decides the test
+  // r^2 <= (2h)^2 exactly as the FP64 one would; inside it the FP64 test runs.
   {
     double R2 = 0.0, dmax = 0.0;
     for (int d = 0; d < 3; ++d) {
-      s.center[d] = 0.5 * (prm.domain_lo[d] + prm.domain_hi[d]);
+      if (s.dim == 2 && d == 1) {
+        s.dcdf[d] = 0.0f;
+        continue;
+      }
       double lo = s.extr_lo[d], hi = s.extr_lo[d] + s.dcd[d] * s.ncd[d];
-      double rr = std::max(std::fabs(lo - s.center[d]), std::fabs(hi - s.center[d]));
-      if (s.dim == 2 && d == 1) rr = 0.0;
+      double rr = std::max(std::fabs(lo), std::fabs(hi));
       R2 += rr * rr;
-      if (!(s.dim == 2 && d == 1)) dmax = std::max(dmax, 2.0 * s.dcd[d]);
+      dmax = std::max(dmax, s.dcd[d]);
+      s.dcdf[d] = (float)s.dcd[d];
     }
     double R = std::sqrt(R2);
-    double eps = std::ldexp(R, -23) + std::ldexp(dmax, -24);
-    double err = 3.0 * (2.0 * dmax * eps + eps * eps) + 3.0 * std::ldexp(s.square_doubleh, -24) * 1.01;
-    double band = 2.0 * err + 1e-12 * s.square_doubleh;
+    double eps = 8.0 * std::ldexp(dmax, -24) + std::ldexp(R, -50);
+    double err = 3.0 * (2.0 * (2.0 * dmax) * eps + eps * eps) + 5.0 * std::ldexp(s.square_doubleh, -24) * 1.01 +
+                 1e-14 * s.square_doubleh;
+    double band = 2.0 * err;
     s.rr_lo = std::nextafter((float)(s.square_doubleh - band), 0.0f);
     s.rr_hi = std::nextafter((float)(s.square_doubleh + band), 3.0e38f);
+    s.pad_f = 0.0f;
   }
   long long ncells = (long long)s.ncd[0] * s.ncd[1] * s.ncd[2];
   if (ncells > (1LL << 30)) return SPH_ERR_INVALID_ARGUMENT;
@@ -559,11 +565,25 @@ void sort_sequence(SphHandle* h, cudaStream_t st) {
   launch_rank_permute(h->db, st);
 }
 
+void momentum_pass(SphHandle* h, bool fused, cudaStream_t st) {
+  if (h->precision == SPH_PREC_FP32C) launch_momentum_f32(h->db, fused, st);
+  else launch_momentum(h->db, fused, st);
+}
+
+void continuity_pass(SphHandle* h, bool fused, cudaStream_t st) {
+  if (h->precision == SPH_PREC_FP32C) launch_continuity_f32(h->db, fused, st);
+  else launch_continuity(h->db, fused, st);
+}
+
+void refresh_copies(SphHandle* h, cudaStream_t st) {
+  if (h->precision == SPH_PREC_FP32C) launch_refresh_f32(h->db, st);
+}
+
 void step_sequence(SphHandle* h, cudaStream_t st) {
-  launch_momentum(h->db, true, st);
+  momentum_pass(h, true, st);
   sort_sequence(h, st);
   launch_boundary(h->db, st);
-  launch_continuity(h->db, true, st);
+  continuity_pass(h, true, st);
   launch_finalize(h->db, 1, st);
 }
 
@@ -630,6 +650,7 @@ int create_batch(int nsims, const SphParams* params, const SphGeometry* geoms, c
     soff += (int)hs.sides.size();
     bdt_cap += hs.prm.bdt_capacity > 0 ? (size_t)hs.prm.bdt_capacity : (size_t)hs.cap;
   }
+  if (poff >= (1 << 28)) { delete h; return SPH_ERR_INVALID_ARGUMENT; }   // FIFO entries carry 28-bit slots
   h->total_slots = poff;
   h->total_cells = coff;
   h->total_faces = foff;
@@ -649,7 +670,7 @@ int create_batch(int nsims, const SphParams* params, const SphGeometry* geoms, c
   A(h->d_cf_start, C);
   A(h->d_cf_count, C);
   A(h->d_near, C);
-  A(P.X, N); A(P.XF, N); A(P.V, N); A(P.RP, N); A(P.I, N); A(P.L, N);
+  A(P.X, N); A(P.XF, N); A(P.VF, N); A(P.RF, N); A(P.V, N); A(P.RP, N); A(P.I, N); A(P.L, N);
   A(P.X2, N); A(P.V2, N); A(P.P2, N); A(P.I2, N); A(P.L2, N);
   A(P.bdt_count, N); A(P.bdt_start, N); A(P.bdt, bdt_cap);
   A(P.key, N); A(P.slot, N); A(P.cell_count, C + 1); A(P.cell_start, C + 1);
@@ -919,7 +940,7 @@ int sph_time_step_duration(SphHandle* h, double* dt_out) {
 
 int sph_rhs_momentum(SphHandle* h, double* acc_out) {
   if (!h || !h->uploaded) return SPH_ERR_INVALID_ARGUMENT;
-  launch_momentum(h->db, false, h->stream);
+  momentum_pass(h, false, h->stream);
   SPH_CUDA(cudaGetLastError());
   if (acc_out) return download_impl(h, 0, nullptr, acc_out, nullptr);
   return sync_dyn(h);
@@ -928,6 +949,7 @@ int sph_rhs_momentum(SphHandle* h, double* acc_out) {
 int sph_leapfrog_momentum(SphHandle* h) {
   if (!h || !h->uploaded) return SPH_ERR_INVALID_ARGUMENT;
   launch_leapfrog_momentum(h->db, h->stream);
+  refresh_copies(h, h->stream);
   SPH_CUDA(cudaGetLastError());
   return sync_dyn(h);
 }
@@ -956,7 +978,7 @@ int sph_boundary_data_tab(SphHandle* h) {
 
 int sph_continuity(SphHandle* h, double* dden_out) {
   if (!h || !h->uploaded) return SPH_ERR_INVALID_ARGUMENT;
-  launch_continuity(h->db, false, h->stream);
+  continuity_pass(h, false, h->stream);
   SPH_CUDA(cudaGetLastError());
   if (dden_out) return download_impl(h, 0, nullptr, nullptr, dden_out);
   return sync_dyn(h);
@@ -965,6 +987,7 @@ int sph_continuity(SphHandle* h, double* dden_out) {
 int sph_leapfrog_continuity(SphHandle* h) {
   if (!h || !h->uploaded) return SPH_ERR_INVALID_ARGUMENT;
   launch_leapfrog_continuity(h->db, h->stream);
+  refresh_copies(h, h->stream);
   SPH_CUDA(cudaGetLastError());
   return sync_dyn(h);
 }
@@ -972,6 +995,7 @@ int sph_leapfrog_continuity(SphHandle* h) {
 int sph_eos(SphHandle* h) {
   if (!h || !h->uploaded) return SPH_ERR_INVALID_ARGUMENT;
   launch_eos(h->db, h->stream);
+  refresh_copies(h, h->stream);
   launch_dt_reduce(h->db, h->stream);
   launch_finalize(h->db, 1, h->stream);
   SPH_CUDA(cudaGetLastError());
@@ -1064,13 +1088,13 @@ int sph_profile_phases(SphHandle* h, int32_t nsteps, double* ms) {
   cudaError_t e = cudaSuccess;
   for (int s = 0; s < nsteps && e == cudaSuccess; ++s) {
     cudaEventRecord(ev[0], q);
-    launch_momentum(h->db, true, q);
+    momentum_pass(h, true, q);
     cudaEventRecord(ev[1], q);
     sort_sequence(h, q);
     cudaEventRecord(ev[2], q);
     launch_boundary(h->db, q);
     cudaEventRecord(ev[3], q);
-    launch_continuity(h->db, true, q);
+    continuity_pass(h, true, q);
     cudaEventRecord(ev[4], q);
     launch_finalize(h->db, 1, q);
     cudaEventRecord(ev[5], q);

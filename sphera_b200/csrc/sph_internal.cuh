@@ -53,8 +53,9 @@ struct SimDev {
   double cfl, vsc_coeff, pesodt;
   double zpmin;           // 0.05 h, ComputeBoundaryVolumeIntegrals_P0.f90
   double ktdelta;         // kernel-table step
-  double center[3];       // origin of the FP32 position copies
-  float rr_lo, rr_hi;     // FP32 screening band around (2h)^2 (see k_rank_permute)
+  float dcdf[3];          // (float)dcd: cell origins differ by multiples of it
+  float rr_lo, rr_hi;     // FP32 screening band around (2h)^2 (see sph_api.cu)
+  float pad_f;
   double kerneltab[kKtRows + 1][5];
 };
 
@@ -124,7 +125,9 @@ struct Tile {
 // Device view of the particle storage.
 struct Particles {
   double4* X;       // x, y, z, mass          (sorted)
-  float4* XF;       // x - center in FP32 (screening copy of X)
+  float4* XF;       // offset from the cell origin in FP32, w = the cell's k index (int bits)
+  float4* VF;       // FP32 form: vx, vy, vz, m/rho
+  float4* RF;       // FP32 form: rho, p/rho^2, m, 0
   double4* V;       // vx, vy, vz, rho (density entering the continuity pass)
   double2* RP;      // current rho, p
   int* I;           // caller index (1-based)

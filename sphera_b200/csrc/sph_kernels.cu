@@ -55,6 +55,16 @@ __device__ __forceinline__ bool particle_cell(const SimDev& s, double x, double 
   return true;
 }
 
+// FP32 offset of a particle from the origin of its cell (w: the cell's k).
+__device__ __forceinline__ float4 screening_copy(const SimDev& s, const double4& x) {
+  int i, j, k;
+  if (!particle_cell(s, x.x, x.y, x.z, i, j, k)) return make_float4(0.f, 0.f, 0.f, __int_as_float(-8));
+  double ox = s.extr_lo[0] + s.dcd[0] * (i - 1);
+  double oy = (s.dim == 3) ? s.extr_lo[1] + s.dcd[1] * (j - 1) : 0.0;
+  double oz = s.extr_lo[2] + s.dcd[2] * (k - 1);
+  return make_float4((float)(x.x - ox), (float)(x.y - oy), (float)(x.z - oz), __int_as_float(k));
+}
+
 // Contiguous slot range of neighbour column r (reference order: y, then x).
 template <int DIM>
 __device__ __forceinline__ void neighbour_run(const SimDev& s, const int* __restrict__ cell_start, int ci, int cj,
@@ -405,9 +415,13 @@ __global__ void k_rank_permute(DevBatch b) {
     double4 x = P.X2[src];
     double4 v = P.V2[src];
     P.X[fin] = x;
-    P.XF[fin] = make_float4((float)(x.x - s.center[0]), (float)(x.y - s.center[1]), (float)(x.z - s.center[2]), 0.f);
-    P.V[fin] = make_double4(v.x, v.y, v.z, x.w / v.w);
-    P.RP[fin] = make_double2(v.w, P.P2[src]);
+    P.XF[fin] = screening_copy(s, x);
+    double vol = x.w / v.w;
+    double pr = P.P2[src];
+    P.V[fin] = make_double4(v.x, v.y, v.z, vol);
+    P.RP[fin] = make_double2(v.w, pr);
+    P.VF[fin] = make_float4((float)v.x, (float)v.y, (float)v.z, (float)vol);
+    P.RF[fin] = make_float4((float)v.w, (float)(pr / (v.w * v.w)), (float)x.w, 0.f);
     P.I[fin] = myid;
     P.L[fin] = P.L2[src];
   }
@@ -960,9 +974,14 @@ __device__ __forceinline__ void elastic_reaction(const SimDev& s, const DevBatch
 // lockstep, so the expensive FP64 work runs on (nearly) all lanes.
 constexpr int kBuf = 16;
 
+// FIFO entries: slot | (neighbour run << 28).
+constexpr int kSlotBits = 28;
+constexpr int kSlotMask = (1 << kSlotBits) - 1;
+
 template <int DIM>
 struct NeighbourScan {
   int r, q, qe, ci, cj, ck, nacc, cand;
+  float Dx, Dy;          // FP32 cell-origin difference of the current run
   bool done, trunc;
 
   __device__ __forceinline__ void init(bool on, int ci_, int cj_, int ck_) {
@@ -974,14 +993,12 @@ struct NeighbourScan {
     qe = 0;
     nacc = 0;
     cand = 0;
+    Dx = 0.f;
+    Dy = 0.f;
     trunc = false;
     done = !on;
   }
 
-  // Appends up to kBuf accepted slots (the particle itself excluded) to the
-  // thread's FIFO column; returns how many were appended.  The NMAXPARTJ cap
-  // of CalcVarLength.f90:197-205 is applied on the accepted count.
-  //
   // The distance test r^2 <= (2h)^2 of CalcVarLength.f90:223-228 is decided
   // in FP32 on the screening copies when r^2 lies outside [rr_lo, rr_hi], a
   // band the host derives from the rounding bounds of the copies, and in
@@ -990,7 +1007,8 @@ struct NeighbourScan {
   __device__ __forceinline__ bool accept(const SimDev& s, const Particles& P, const double4& xi, const float4& xf,
                                          int q) const {
     float4 xj = P.XF[q];
-    float d0 = xf.x - xj.x, d1 = xf.y - xj.y, d2 = xf.z - xj.z;
+    float Dz = (float)(ck - __float_as_int(xj.w)) * s.dcdf[2];
+    float d0 = Dx + (xf.x - xj.x), d1 = Dy + (xf.y - xj.y), d2 = Dz + (xf.z - xj.z);
     float rf = d0 * d0 + d1 * d1 + d2 * d2;
     if (rf < s.rr_lo) return true;
     if (rf > s.rr_hi) return false;
@@ -1000,6 +1018,9 @@ struct NeighbourScan {
     return !(rr > s.square_doubleh);
   }
 
+  // Appends up to kBuf(+1) accepted neighbours (the particle itself excluded)
+  // to the thread's FIFO column; returns how many were appended.  The
+  // NMAXPARTJ cap of CalcVarLength.f90:197-205 applies to the accepted count.
   __device__ __forceinline__ int fill(const SimDev& s, const Particles& P, const double4& xi, const float4& xf,
                                       int self, int* col) {
     constexpr int NR = (DIM == 3) ? 9 : 3;
@@ -1011,6 +1032,10 @@ struct NeighbourScan {
           break;
         }
         neighbour_run<DIM>(s, P.cell_start, ci, cj, ck, r, q, qe);
+        int jr = (DIM == 3) ? cj - 1 + r / 3 : cj;
+        int ir = ci - 1 + ((DIM == 3) ? r % 3 : r);
+        Dx = (float)(ci - ir) * s.dcdf[0];
+        Dy = (DIM == 3) ? (float)(cj - jr) * s.dcdf[1] : 0.f;
         r++;
         cand += qe - q;
         continue;
@@ -1020,13 +1045,14 @@ struct NeighbourScan {
         done = true;
         break;
       }
+      const int tag = (r - 1) << kSlotBits;
       bool a0 = accept(s, P, xi, xf, q);
       if (q + 1 < qe) {
         // two candidates per iteration: independent loads in flight
         bool a1 = accept(s, P, xi, xf, q + 1);
         if (a0) {
           nacc++;
-          if (q != self) col[(nb++) * kBlock] = q;
+          if (q != self) col[(nb++) * kBlock] = q | tag;
         }
         if (nacc >= s.nmaxpartj) {
           q++;
@@ -1034,13 +1060,13 @@ struct NeighbourScan {
         }
         if (a1) {
           nacc++;
-          if (q + 1 != self) col[(nb++) * kBlock] = q + 1;
+          if (q + 1 != self) col[(nb++) * kBlock] = (q + 1) | tag;
         }
         q += 2;
       } else {
         if (a0) {
           nacc++;
-          if (q != self) col[(nb++) * kBlock] = q;
+          if (q != self) col[(nb++) * kBlock] = q | tag;
         }
         q++;
       }
@@ -1115,7 +1141,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_momentum(DevBatch b) {
       int nmax = __reduce_max_sync(0xffffffffu, (unsigned)nbuf);
       for (int k = 0; k < nmax; ++k) {
         if (k >= nbuf) continue;
-        int q = col[k * kBlock];
+        int q = col[k * kBlock] & kSlotMask;
         double4 xj = P.X[q];
         double r0 = xi.x - xj.x, r1 = xi.y - xj.y, r2 = xi.z - xj.z;
         double rr = r0 * r0 + r1 * r1 + r2 * r2;
@@ -1303,7 +1329,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_continuity(DevBatch b) {
       int nmax = __reduce_max_sync(0xffffffffu, (unsigned)nbuf);
       for (int k = 0; k < nmax; ++k) {
         if (k >= nbuf) continue;
-        int q = col[k * kBlock];
+        int q = col[k * kBlock] & kSlotMask;
         double4 xj = P.X[q];
         double r0 = xi.x - xj.x, r1 = xi.y - xj.y, r2 = xi.z - xj.z;
         double rr = r0 * r0 + r1 * r1 + r2 * r2;
@@ -1336,6 +1362,362 @@ __global__ void __launch_bounds__(kBlock, 2) k_continuity(DevBatch b) {
     block_count2(b.counters + 2, sc.cand, sc.nacc);
     int m = warp_max(sc.nacc);
     if ((threadIdx.x & 31) == 0 && m > 0) atomicMax(&dyn->max_neigh, m);
+  }
+}
+
+// ==========================================================================
+// FP32-compensated form.  Pair arithmetic in FP32 on the screening copies
+// (FP64 cell origin + FP32 offset) with compensated (Kahan) per-particle
+// sums; the pressure term uses the symmetric form that the two accumulators
+// of inter_EqMoto.f90:195-221 add up to.  Boundary terms, the elastic
+// reaction, time integration and the time step stay in FP64.
+// ==========================================================================
+struct Kahan {
+  float s, c;
+  __device__ __forceinline__ void zero() {
+    s = 0.f;
+    c = 0.f;
+  }
+  // built without contraction (--fmad=false), as compensation requires
+  __device__ __forceinline__ void add(float x) {
+    float y = x - c;
+    float t = s + y;
+    c = (t - s) - y;
+    s = t;
+  }
+  __device__ __forceinline__ double val() const { return (double)s - (double)c; }
+};
+
+struct F32Const {
+  float hinv, h2inv, eta, eta2, ke, kacl, amon, nu, nu4, sq2h;
+  __device__ __forceinline__ void load(const SimDev& s) {
+    hinv = (float)(1.0 / s.h);
+    h2inv = (float)(1.0 / s.squareh);
+    eta = (float)s.eta;
+    eta2 = (float)s.eta2;
+    ke = (float)s.ke_coef;
+    kacl = (float)s.kacl_coef;
+    amon = (float)(s.alfa_mon * (s.celerita + s.celerita) * s.h);
+    nu = (float)s.kin_visc;
+    nu4 = (float)(4.0 * (s.kin_visc * s.kin_visc));
+    sq2h = (float)s.square_doubleh;
+  }
+};
+
+__device__ __forceinline__ void kernel_values_f32(const F32Const& c, float rr, float& PK1, float& PK2, float& PK3) {
+  float r = sqrtf(rr);
+  float q = r * c.hinv;
+  float q2 = rr * c.h2inv;
+  if (q >= 2.0f) {
+    PK1 = 0.f;
+    PK2 = 0.f;
+    PK3 = 0.f;
+    return;
+  }
+  float denom = __fdividef(1.0f, r + c.eta);
+  float g = (q < 1.0f) ? fmaf(1.5f, q2, -2.0f * q) : fmaf(-0.5f, q2, fmaf(2.0f, q, -2.0f));
+  float gw = fmaf(12.0f, q, fmaf(-3.0f, q2, -12.0f));
+  PK1 = g * c.ke * denom;
+  PK2 = __fdividef(PK1, rr + c.eta2);
+  PK3 = gw * c.kacl * denom;
+}
+
+// FP32 separation of FIFO entry e from particle (xfi, cell ci,cj,ck).
+template <int DIM>
+__device__ __forceinline__ int separation_f32(const SimDev& s, const Particles& P, int e, const float4& xfi, int ci,
+                                              int cj, int ck, float& d0, float& d1, float& d2) {
+  int q = e & kSlotMask;
+  int r = e >> kSlotBits;
+  int jr = (DIM == 3) ? cj - 1 + r / 3 : cj;
+  int ir = ci - 1 + ((DIM == 3) ? r % 3 : r);
+  float4 xj = P.XF[q];
+  float Dx = (float)(ci - ir) * s.dcdf[0];
+  float Dy = (DIM == 3) ? (float)(cj - jr) * s.dcdf[1] : 0.f;
+  float Dz = (float)(ck - __float_as_int(xj.w)) * s.dcdf[2];
+  d0 = Dx + (xfi.x - xj.x);
+  d1 = (DIM == 3) ? Dy + (xfi.y - xj.y) : 0.f;
+  d2 = Dz + (xfi.z - xj.z);
+  return q;
+}
+
+template <int DIM, bool FUSED>
+__global__ void __launch_bounds__(kBlock, 3) k_momentum_f32(DevBatch b) {
+  __shared__ SimDev s;
+  __shared__ int sbuf[(kBuf + 1) * kBlock];
+  int cur = -1;
+  const Particles& P = b.P;
+  const double GI = (double)9.80665f;   // Static_allocation_module.f90:72, a default-REAL literal
+  int* col = sbuf + threadIdx.x;
+  for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
+    Tile tl = b.tiles[t];
+    load_sim(s, b.sims, tl.sim, cur);
+    F32Const fc;
+    fc.load(s);
+    SimDyn* dyn = b.dyn + tl.sim;
+    int p = tl.start + threadIdx.x;
+    bool active = threadIdx.x < tl.count && p < s.p_off + dyn->nag;
+    if (FUSED && active && dyn->frozen) {
+      double4 v4 = P.V[p];
+      double2 rp = P.RP[p];
+      P.X2[p] = P.X[p];
+      P.V2[p] = make_double4(v4.x, v4.y, v4.z, rp.x);
+      P.P2[p] = rp.y;
+      P.I2[p] = P.I[p];
+      P.L2[p] = P.L[p];
+      active = false;
+    }
+    double4 xi = make_double4(0.0, 0.0, 0.0, 0.0);
+    double vi[3] = {0.0, 0.0, 0.0};
+    double rhoi = 1.0, pi = 0.0;
+    int lam = 0, nb = 0, bstart = 0;
+    double tpres[3] = {0, 0, 0}, tdiss[3] = {0, 0, 0}, tvisc[3] = {0, 0, 0};
+    int ci = 0, cj = 0, ck = 0;
+    bool in_grid = false;
+    if (active) {
+      xi = P.X[p];
+      double4 v4 = P.V[p];
+      double2 rp = P.RP[p];
+      vi[0] = v4.x;
+      vi[1] = v4.y;
+      vi[2] = v4.z;
+      rhoi = rp.x;
+      pi = rp.y;
+      lam = P.L[p];
+      nb = P.bdt_count[p];
+      bstart = nb > 0 ? P.bdt_start[p] : 0;
+      if (nb > 0) {
+        if (DIM == 3) me_boundary3d(s, b, nb, bstart, vi, rhoi, pi, lam, tpres, tdiss, tvisc);
+        else me_boundary2d(s, b, nb, bstart, vi, rhoi, pi, lam, tpres, tdiss, tvisc);
+      }
+      in_grid = particle_cell(s, xi.x, xi.y, xi.z, ci, cj, ck);
+      if (!in_grid) set_status(dyn, SPH_ERR_INVALID_ARGUMENT);
+    }
+    NeighbourScan<DIM> sc;
+    sc.init(active && in_grid, ci, cj, ck);
+    float4 xfi = active ? P.XF[p] : make_float4(0.f, 0.f, 0.f, 0.f);
+    const float vix = (float)vi[0], viy = (float)vi[1], viz = (float)vi[2];
+    const float rhof = (float)rhoi;
+    const float Pi = (float)(pi / (rhoi * rhoi));
+    const bool morris = s.kin_visc > 1.0e-12;
+    Kahan tp0, tp1, tp2, td0, td1, td2, tv0, tv1, tv2;
+    tp0.zero(); tp1.zero(); tp2.zero(); td0.zero(); td1.zero(); td2.zero(); tv0.zero(); tv1.zero(); tv2.zero();
+    while (__any_sync(0xffffffffu, !sc.done)) {
+      int nbuf = sc.fill(s, P, xi, xfi, p, col);
+      int nmax = __reduce_max_sync(0xffffffffu, (unsigned)nbuf);
+      for (int k = 0; k < nmax; ++k) {
+        if (k >= nbuf) continue;
+        float d0, d1, d2;
+        int q = separation_f32<DIM>(s, P, col[k * kBlock], xfi, ci, cj, ck, d0, d1, d2);
+        float rr = d0 * d0 + d1 * d1 + d2 * d2;
+        float PK1, PK2, PK3;
+        kernel_values_f32(fc, rr, PK1, PK2, PK3);
+        float4 vj = P.VF[q];
+        float4 rfj = P.RF[q];
+        float mj = rfj.z;
+        // pressure (both accumulators of inter_EqMoto together)
+        float pf = -(mj * (Pi + rfj.y) * PK3);
+        tp0.add(pf * d0);
+        if (DIM == 3) tp1.add(pf * d1);
+        tp2.add(pf * d2);
+        float dv0 = vj.x - vix, dv1 = vj.y - viy, dv2 = vj.z - viz;
+        float rsum = rhof + rfj.x;
+        // viscomon
+        float vr = -(dv0 * d0 + dv1 * d1 + dv2 * d2);
+        float df = mj * __fdividef(fc.amon, rsum) * vr * PK2;
+        td0.add(df * d0);
+        if (DIM == 3) td1.add(df * d1);
+        td2.add(df * d2);
+        // viscomorris
+        if (morris) {
+          float vf = -(__fdividef(mj * fc.nu4, fmaf(fc.nu, rsum, 1.0e-3f)) * PK2 * rr);
+          tv0.add(vf * dv0);
+          if (DIM == 3) tv1.add(vf * dv1);
+          tv2.add(vf * dv2);
+        }
+      }
+    }
+    double dtc = 1.0e300;
+    if (active) {
+      if (sc.trunc) atomicOr(&dyn->warnings, SPH_WARN_NEIGHBOURS_TRUNCATED);
+      double rs0 = tv0.val(), rs1 = tv1.val(), rs2 = tv2.val();
+      tpres[0] = tpres[0] + tp0.val();
+      tpres[1] = tpres[1] + tp1.val();
+      tpres[2] = tpres[2] + tp2.val();
+      int lam_new = 0;
+      if (s.kin_visc > 0.0) {
+        double absv_pres = sqrt(tpres[0] * tpres[0] + tpres[1] * tpres[1] + tpres[2] * tpres[2]) + GI;
+        double absv_morris = sqrt(rs0 * rs0 + rs1 * rs1 + rs2 * rs2);
+        double weight = 0.0;
+        if (absv_pres != 0.0) weight = absv_morris / absv_pres * 100.0;
+        lam_new = (weight > 5.0 || absv_pres == 0.0) ? 1 : 0;
+      }
+      double acc[3];
+      acc[0] = tpres[0] + (tdiss[0] + td0.val()) + (tvisc[0] + rs0) + s.grav[0];
+      acc[1] = tpres[1] + (tdiss[1] + td1.val()) + (tvisc[1] + rs1) + s.grav[1];
+      acc[2] = tpres[2] + (tdiss[2] + td2.val()) + (tvisc[2] + rs2) + s.grav[2];
+      if (nb > 0) {
+        double R[3];
+        elastic_reaction<DIM>(s, b, nb, bstart, vi, R);
+        for (int d = 0; d < 3; ++d) acc[d] = acc[d] + R[d];
+      }
+      if (FUSED) {
+        double dtvel = dyn->dtvel, dt = dyn->dt;
+        double vn[3];
+        for (int d = 0; d < 3; ++d) vn[d] = vi[d] + dtvel * acc[d];
+        P.X2[p] = make_double4(xi.x + dt * vn[0], xi.y + dt * vn[1], xi.z + dt * vn[2], xi.w);
+        P.V2[p] = make_double4(vn[0], vn[1], vn[2], rhoi);
+        P.P2[p] = pi;
+        P.I2[p] = P.I[p];
+        P.L2[p] = (uint8_t)lam_new;
+        double U = sqrt(vn[0] * vn[0] + vn[1] * vn[1] + vn[2] * vn[2]);
+        dtc = s.cfl * 2.0 * s.h / (s.celerita + U);
+      } else {
+        P.ACC[p] = make_double4(acc[0], acc[1], acc[2], 0.0);
+        P.L[p] = (uint8_t)lam_new;
+      }
+    }
+    block_count2(b.counters, sc.cand, sc.nacc);
+    if (FUSED) {
+      double m = warp_min(dtc);
+      if ((threadIdx.x & 31) == 0 && m < 1.0e300)
+        atomicMin(&dyn->dtmin_bits, (unsigned long long)__double_as_longlong(m));
+    }
+  }
+}
+
+template <int DIM, bool FUSED>
+__global__ void __launch_bounds__(kBlock, 3) k_continuity_f32(DevBatch b) {
+  __shared__ SimDev s;
+  __shared__ int sbuf[(kBuf + 1) * kBlock];
+  int cur = -1;
+  const Particles& P = b.P;
+  int* col = sbuf + threadIdx.x;
+  for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
+    Tile tl = b.tiles[t];
+    load_sim(s, b.sims, tl.sim, cur);
+    F32Const fc;
+    fc.load(s);
+    SimDyn* dyn = b.dyn + tl.sim;
+    int p = tl.start + threadIdx.x;
+    bool active = threadIdx.x < tl.count && p < s.p_off + dyn->nag && !(FUSED && dyn->frozen);
+    double4 xi = make_double4(0.0, 0.0, 0.0, 0.0);
+    double4 vi = make_double4(0.0, 0.0, 0.0, 0.0);
+    double rhoi = 1.0, dden = 0.0;
+    int ci = 0, cj = 0, ck = 0;
+    bool in_grid = false;
+    if (active) {
+      xi = P.X[p];
+      vi = P.V[p];
+      rhoi = P.RP[p].x;
+      int nb = P.bdt_count[p];
+      if (nb > 0) {
+        int bstart = P.bdt_start[p];
+        double gu0 = 0, gv1 = 0, gw2 = 0;
+        if (DIM == 3) {
+          double gu[3] = {0, 0, 0}, gv[3] = {0, 0, 0}, gw[3] = {0, 0, 0};
+          const double var[3] = {vi.x, vi.y, vi.z};
+          for (int u = 0; u < nb; ++u) {
+            const BdtEntry& e = P.bdt[bstart + u];
+            const FaceDev& f = b.faces[s.face_off + e.clobonum - 1];
+            if (!(e.loc[2] > 0.0)) continue;
+            double dp = 0.0;
+            for (int d = 0; d < 3; ++d) dp = dp + (2.0 * (f.velocity[d] - var[d])) * f.T[d][2];
+            double dvel[3] = {dp * f.T[0][2], dp * f.T[1][2], dp * f.T[2][2]};
+            for (int i = 0; i < 3; ++i) {
+              double a = 0.0;
+              for (int k = 0; k < 3; ++k) a = a + f.T[i][k] * e.bi[3 + k];
+              gu[i] = gu[i] - dvel[0] * a;
+              gv[i] = gv[i] - dvel[1] * a;
+              gw[i] = gw[i] - dvel[2] * a;
+            }
+          }
+          gu0 = gu[0];
+          gv1 = gv[1];
+          gw2 = gw[2];
+          atomicMax(&dyn->ncbf_max, nb);
+        } else {
+          double gu_x = 0.0, gw_z = 0.0;
+          for (int u = 0; u < nb; ++u) {
+            const BdtEntry& e = P.bdt[bstart + u];
+            const SideDev& S = b.sides[s.side_off + e.clobonum - 1];
+            double dvel0, dvel1;
+            if (S.zone_type == SPH_ZONE_TAPI) {
+              dvel0 = 2.0 * (S.velocity[0] - vi.x);
+              dvel1 = 2.0 * (S.velocity[2] - vi.z);
+            } else {
+              dvel0 = 2.0 * (-vi.x);
+              dvel1 = 2.0 * (-vi.z);
+            }
+            gu_x = gu_x - dvel0 * S.nnn[0] * e.bi[0];
+            gw_z = gw_z - dvel1 * S.nnn[1] * e.bi[0];
+          }
+          gu0 = gu_x;
+          gw2 = gw_z;
+        }
+        dden = dden - rhoi * (gu0 + gv1 + gw2);
+      }
+      in_grid = particle_cell(s, xi.x, xi.y, xi.z, ci, cj, ck);
+      if (!in_grid) set_status(dyn, SPH_ERR_INVALID_ARGUMENT);
+    }
+    NeighbourScan<DIM> sc;
+    sc.init(active && in_grid, ci, cj, ck);
+    float4 xfi = active ? P.XF[p] : make_float4(0.f, 0.f, 0.f, 0.f);
+    const float vix = (float)vi.x, viy = (float)vi.y, viz = (float)vi.z;
+    const float rhof = (float)rhoi;
+    Kahan sum;
+    sum.zero();
+    while (__any_sync(0xffffffffu, !sc.done)) {
+      int nbuf = sc.fill(s, P, xi, xfi, p, col);
+      int nmax = __reduce_max_sync(0xffffffffu, (unsigned)nbuf);
+      for (int k = 0; k < nmax; ++k) {
+        if (k >= nbuf) continue;
+        float d0, d1, d2;
+        int q = separation_f32<DIM>(s, P, col[k * kBlock], xfi, ci, cj, ck, d0, d1, d2);
+        float rr = d0 * d0 + d1 * d1 + d2 * d2;
+        float PK1, PK2, PK3;
+        kernel_values_f32(fc, rr, PK1, PK2, PK3);
+        float4 vj = P.VF[q];
+        float c = rhof * vj.w * PK1;    // rho_i (m_j / rho_j) PK1
+        sum.add(c * ((vj.x - vix) * d0 + (vj.y - viy) * d1 + (vj.z - viz) * d2));
+      }
+    }
+    if (active) {
+      if (sc.trunc) atomicOr(&dyn->warnings, SPH_WARN_NEIGHBOURS_TRUNCATED);
+      dden = dden - sum.val();
+      if (FUSED) {
+        double rho = rhoi + dyn->dt * dden;
+        if (s.density_thresholds == 1) {
+          if (rho < 0.9 * s.den0) rho = 0.9 * s.den0;
+          if (rho > 1.1 * s.den0) rho = 1.1 * s.den0;
+        }
+        double pr = s.k_over_rho0 * (rho - s.den0) + s.p_ref;
+        P.RP[p] = make_double2(rho, pr);
+        P.RF[p] = make_float4((float)rho, (float)(pr / (rho * rho)), (float)xi.w, 0.f);
+      } else {
+        P.DDEN[p] = dden;
+      }
+    }
+    block_count2(b.counters + 2, sc.cand, sc.nacc);
+    int m = warp_max(sc.nacc);
+    if ((threadIdx.x & 31) == 0 && m > 0) atomicMax(&dyn->max_neigh, m);
+  }
+}
+
+// FP32 copies of velocity, density and pressure after an in-place update
+// of the FP64 state by the per-call ABI.
+__global__ void k_refresh_f32(DevBatch b) {
+  __shared__ SimDev s;
+  int cur = -1;
+  for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
+    Tile tl = b.tiles[t];
+    load_sim(s, b.sims, tl.sim, cur);
+    int p = tl.start + threadIdx.x;
+    if (threadIdx.x >= tl.count || p >= s.p_off + b.dyn[tl.sim].nag) continue;
+    double4 x = b.P.X[p];
+    double4 v = b.P.V[p];
+    double2 rp = b.P.RP[p];
+    b.P.VF[p] = make_float4((float)v.x, (float)v.y, (float)v.z, (float)v.w);
+    b.P.RF[p] = make_float4((float)rp.x, (float)(rp.y / (rp.x * rp.x)), (float)x.w, 0.f);
   }
 }
 
@@ -1374,8 +1756,7 @@ __global__ void k_leapfrog_trajectories(DevBatch b) {
     x.x = x.x + dt * v.x;
     x.y = x.y + dt * v.y;
     x.z = x.z + dt * v.z;
-    b.P.X[p] = x;
-    b.P.XF[p] = make_float4((float)(x.x - s.center[0]), (float)(x.y - s.center[1]), (float)(x.z - s.center[2]), 0.f);
+    b.P.X[p] = x;   // the screening copies are rebuilt by the next sph_ord_grid
   }
 }
 
@@ -1722,6 +2103,30 @@ void launch_momentum(const DevBatch& b, bool fused, cudaStream_t st) {
     else k_momentum<2, false><<<g, kBlock, 0, st>>>(b);
   }
 }
+
+void launch_momentum_f32(const DevBatch& b, bool fused, cudaStream_t st) {
+  int g = blocks_for(b);
+  if (b.dim == 3) {
+    if (fused) k_momentum_f32<3, true><<<g, kBlock, 0, st>>>(b);
+    else k_momentum_f32<3, false><<<g, kBlock, 0, st>>>(b);
+  } else {
+    if (fused) k_momentum_f32<2, true><<<g, kBlock, 0, st>>>(b);
+    else k_momentum_f32<2, false><<<g, kBlock, 0, st>>>(b);
+  }
+}
+
+void launch_continuity_f32(const DevBatch& b, bool fused, cudaStream_t st) {
+  int g = blocks_for(b);
+  if (b.dim == 3) {
+    if (fused) k_continuity_f32<3, true><<<g, kBlock, 0, st>>>(b);
+    else k_continuity_f32<3, false><<<g, kBlock, 0, st>>>(b);
+  } else {
+    if (fused) k_continuity_f32<2, true><<<g, kBlock, 0, st>>>(b);
+    else k_continuity_f32<2, false><<<g, kBlock, 0, st>>>(b);
+  }
+}
+
+void launch_refresh_f32(const DevBatch& b, cudaStream_t st) { k_refresh_f32<<<blocks_for(b), kBlock, 0, st>>>(b); }
 
 void launch_continuity(const DevBatch& b, bool fused, cudaStream_t st) {
   int g = blocks_for(b);

@@ -43,6 +43,10 @@ void launch_rank_reference(const DevBatch& b, const int* cell_start_ref, int* np
 void launch_boundary(const DevBatch& b, cudaStream_t st);
 void launch_momentum(const DevBatch& b, bool fused, cudaStream_t st);
 void launch_continuity(const DevBatch& b, bool fused, cudaStream_t st);
+// physics (FP32-compensated form)
+void launch_momentum_f32(const DevBatch& b, bool fused, cudaStream_t st);
+void launch_continuity_f32(const DevBatch& b, bool fused, cudaStream_t st);
+void launch_refresh_f32(const DevBatch& b, cudaStream_t st);
 void launch_leapfrog_momentum(const DevBatch& b, cudaStream_t st);
 void launch_leapfrog_trajectories(const DevBatch& b, cudaStream_t st);
 void launch_leapfrog_continuity(const DevBatch& b, cudaStream_t st);
