@@ -213,51 +213,65 @@ def main():
 
     import torch
     torch.cuda.set_device(local)
-    from sphera_b200 import Simulation, cases, measure_fp64_peak
+    from sphera_b200 import Simulation, abi, cases, measure_fp32_peak, measure_fp64_peak
 
-    case = cases.dam_break_3d()
-    n = case.n
-    sim = Simulation(case)
-    sim.upload(case.state)
-    sim.step(args.warmup)
-    stream = torch.cuda.ExternalStream(sim.stream)
     fp64_peak = measure_fp64_peak()
-
+    fp32_peak = measure_fp32_peak()
     try:
         gpu_id = "GPU-" + str(torch.cuda.get_device_properties(local).uuid)
     except Exception:
         gpu_id = str(local)
-    sampler = ClockSampler(gpu_id)
-    _barrier(ws)
-    torch.cuda.synchronize()
-    sim.sync()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    sim.step_async(args.steps)
-    e1.record(stream)
-    e1.synchronize()
-    sim.sync()
-    torch.cuda.synchronize()
-    _barrier(ws)
-    ms = e0.elapsed_time(e1)
-    clocks = sampler.stop()
-    ms_max = _max_over_ranks(ws, ms)
-    value = ws * n * args.steps / (ms_max * 1e-3)
 
-    # phase times and counters of the same workload (un-graphed steps)
-    sim.counters(reset=True)
-    nprof = 10
-    phases = sim.profile_phases(nprof)
-    cnt = sim.counters(reset=True)
-    diag = sim.diagnostics()
-    mom_ms = phases["momentum"] / nprof
+    def run_form(precision):
+        case = cases.dam_break_3d(precision=precision)
+        n = case.n
+        sim = Simulation(case)
+        sim.upload(case.state)
+        sim.step(args.warmup)
+        stream = torch.cuda.ExternalStream(sim.stream)
+        sampler = ClockSampler(gpu_id)
+        _barrier(ws)
+        torch.cuda.synchronize()
+        sim.sync()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        sim.step_async(args.steps)
+        e1.record(stream)
+        e1.synchronize()
+        sim.sync()
+        torch.cuda.synchronize()
+        _barrier(ws)
+        ms = e0.elapsed_time(e1)
+        clocks = sampler.stop()
+        ms_max = _max_over_ranks(ws, ms)
+        value = ws * n * args.steps / (ms_max * 1e-3)
+        # phase times and counters of the same workload (un-graphed steps)
+        sim.counters(reset=True)
+        nprof = 10
+        phases = sim.profile_phases(nprof)
+        cnt = sim.counters(reset=True)
+        diag = sim.diagnostics()
+        return dict(case=case, n=n, sim=sim, stream=stream, value=value, ms=ms_max, clocks=clocks,
+                    phases={k: v / nprof for k, v in phases.items()}, nprof=nprof, cnt=cnt, diag=diag,
+                    e0=e0, e1=e1)
+
+    r64 = run_form(abi.SPH_PREC_FP64)
+    r64["sim"].close()
+    r32 = run_form(abi.SPH_PREC_FP32C)
+    case, n, sim, stream = r32["case"], r32["n"], r32["sim"], r32["stream"]
+    e0, e1 = r32["e0"], r32["e1"]
+    value, ms_max, clocks, cnt, diag = r32["value"], r32["ms"], r32["clocks"], r32["cnt"], r32["diag"]
+    nprof = r32["nprof"]
+    mom_ms = r32["phases"]["momentum"]
     alg_bytes = n * MOM_BYTES_PER_PARTICLE + diag.bdt_entries * BDT_ENTRY_BYTES
     hbm_peak, peak_kind = _peaks()
     achieved_gbs = alg_bytes / (mom_ms * 1e-3) / 1e9
     mom_flops = (cnt["mom_candidates"] * FLOP_CAND + (cnt["mom_pairs"] - n * nprof) * FLOP_MOM_PAIR) / nprof
-    cont_flops = (cnt["cont_candidates"] * FLOP_CAND + (cnt["cont_pairs"] - n * nprof) * FLOP_CONT_PAIR) / nprof
     mom_tflops = mom_flops / (mom_ms * 1e-3) / 1e12
+    mom64_ms = r64["phases"]["momentum"]
+    c64 = r64["cnt"]
+    mom64_flops = (c64["mom_candidates"] * FLOP_CAND + (c64["mom_pairs"] - n * nprof) * FLOP_MOM_PAIR) / nprof
     workload = "dam_break_3d"
     traffic = _traffic(workload)
 
@@ -305,26 +319,31 @@ def main():
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": "fp32c (f32 pair sums, compensated; f64 positions/integration/boundary terms)",
         "data": "synthetic (seeded 3D dam break generated in-repo)",
         "config": {"workload": "dam_break_3d: tank 1.6x0.6x0.6 m, block 0.6x0.3x0.6 m, dx 0.005 m, "
-                               "864000 particles per GPU, SA-SPH walls, FP64 form",
-                   "particles_per_gpu": n, "form": "fp64",
+                               "864000 particles per GPU, SA-SPH walls",
+                   "particles_per_gpu": n, "form": "fp32c",
                    "l2": "state and scratch (~250 MB per step) exceed the 126 MB L2; no flush",
                    "parallelism": f"replicas x{ws} (independent simulations, no collective)"},
+        "fp64": {"value": r64["value"], "ms_per_step": r64["ms"] / args.steps,
+                 "phases_ms_per_step": r64["phases"], "clocks": r64["clocks"],
+                 "momentum_fp64_tflops": mom64_flops / (mom64_ms * 1e-3) / 1e12,
+                 "fp64_peak_tflops": fp64_peak},
+        "speedup_fp32c_vs_fp64": value / r64["value"],
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": state_bytes,
                 "d2h_bytes_per_step": state_bytes, "steps": args.e2e_steps,
-                "path": "sph_upload + sph_step_async(1) + sph_download per step, pinned host buffers"},
+                "path": "sph_upload + sph_step_async(1) + sph_download per step, pinned host buffers, fp32c form"},
         "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": hbm_peak, "unit": "GB/s",
                      "frac": achieved_gbs / hbm_peak, "traffic": traffic,
-                     "kernel": "k_momentum<3,true> (fused momentum + leapfrog)",
+                     "kernel": "k_momentum_f32<3,true> (fused momentum + leapfrog)",
                      "peak_kind": f"{peak_kind} HBM copy bandwidth",
-                     "fp64": {"achieved_tflops": mom_tflops, "peak_tflops": fp64_peak,
-                              "frac": mom_tflops / fp64_peak, "peak_kind": "measured FP64 FMA rate (in-run)"}},
-        "phases_ms_per_step": {k: v / nprof for k, v in phases.items()},
+                     "fp": {"achieved_tflops": mom_tflops, "peak_tflops": fp32_peak,
+                            "frac": mom_tflops / fp32_peak, "peak_kind": "measured FP32 FMA rate (in-run)"}},
+        "phases_ms_per_step": r32["phases"],
         "pairs_per_particle": cnt["mom_pairs"] / nprof / n,
         "candidates_per_particle": cnt["mom_candidates"] / nprof / n,
-        "continuity_tflops": cont_flops / (phases["continuity"] / nprof * 1e-3) / 1e12,
         "gpu_launches": KERNELS_PER_STEP * args.steps,
         "clocks": clocks,
         "cpu_baseline": cpu,

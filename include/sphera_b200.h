@@ -293,8 +293,10 @@ int  sph_profile_phases(SphHandle* h, int32_t nsteps, double* ms);
 /* Neighbour candidates and accepted pairs (incl. self) counted by the pair
  * passes: c[0..1] momentum, c[2..3] continuity; reset != 0 zeroes them.   */
 int  sph_get_counters(SphHandle* h, uint64_t* c, int32_t reset);
-/* Measured dense FP64 FMA throughput of the current device in TFLOP/s.    */
+/* Measured dense FMA throughput of the current device in TFLOP/s: FP64,
+ * or FP32 when fp32 != 0.                                                 */
 int  sph_measure_fp64_peak(double* tflops);
+int  sph_measure_fma_peak(int32_t fp32, double* tflops);
 
 #ifdef __cplusplus
 }

@@ -74,6 +74,7 @@ def lib():
         "sph_profile_phases": ([vp, C.c_int32, dp], C.c_int),
         "sph_get_counters": ([vp, C.POINTER(C.c_uint64), C.c_int32], C.c_int),
         "sph_measure_fp64_peak": ([dp], C.c_int),
+        "sph_measure_fma_peak": ([C.c_int32, dp], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -234,6 +235,13 @@ def measure_fp64_peak():
     """Dense FP64 FMA throughput of the current device, TFLOP/s."""
     t = C.c_double()
     _chk(lib().sph_measure_fp64_peak(C.byref(t)), "sph_measure_fp64_peak")
+    return t.value
+
+
+def measure_fp32_peak():
+    """Dense FP32 FMA throughput of the current device, TFLOP/s."""
+    t = C.c_double()
+    _chk(lib().sph_measure_fma_peak(1, C.byref(t)), "sph_measure_fma_peak")
     return t.value
 
 

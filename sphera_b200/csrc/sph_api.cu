@@ -1123,9 +1123,9 @@ int sph_get_counters(SphHandle* h, uint64_t* c, int32_t reset) {
   return SPH_OK;
 }
 
-// Dense FP64 FMA throughput of the current device (TFLOP/s), the FP64
-// roofline of the pair passes.
-int sph_measure_fp64_peak(double* tflops) {
+// Dense FP64 (fp32 = 0) or FP32 (fp32 = 1) FMA throughput of the current
+// device (TFLOP/s): the arithmetic roofline of the pair passes.
+int sph_measure_fma_peak(int32_t fp32, double* tflops) {
   if (!tflops) return SPH_ERR_INVALID_ARGUMENT;
   int dev = 0, sms = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
@@ -1141,9 +1141,12 @@ int sph_measure_fp64_peak(double* tflops) {
   cudaEventCreate(&a);
   cudaEventCreate(&b);
   double flops = 0.0;
-  for (int w = 0; w < 3; ++w) launch_fp64_probe(sink, blocks, q);
+  for (int w = 0; w < 3; ++w) {
+    if (fp32) launch_fp32_probe((float*)sink, blocks, q);
+    else launch_fp64_probe(sink, blocks, q);
+  }
   cudaEventRecord(a, q);
-  for (int r = 0; r < 10; ++r) flops += launch_fp64_probe(sink, blocks, q);
+  for (int r = 0; r < 10; ++r) flops += fp32 ? launch_fp32_probe((float*)sink, blocks, q) : launch_fp64_probe(sink, blocks, q);
   cudaEventRecord(b, q);
   cudaError_t e = cudaEventSynchronize(b);
   float ms = 0.f;
@@ -1156,5 +1159,7 @@ int sph_measure_fp64_peak(double* tflops) {
   *tflops = flops / (ms * 1e-3) / 1e12;
   return SPH_OK;
 }
+
+int sph_measure_fp64_peak(double* tflops) { return sph_measure_fma_peak(0, tflops); }
 
 }  // extern "C"

@@ -1427,7 +1427,7 @@ template <int DIM>
 __device__ __forceinline__ int separation_f32(const SimDev& s, const Particles& P, int e, const float4& xfi, int ci,
                                               int cj, int ck, float& d0, float& d1, float& d2) {
   int q = e & kSlotMask;
-  int r = e >> kSlotBits;
+  int r = (int)((unsigned)e >> kSlotBits);   // run 8 sets the top bit
   int jr = (DIM == 3) ? cj - 1 + r / 3 : cj;
   int ir = ci - 1 + ((DIM == 3) ? r % 3 : r);
   float4 xj = P.XF[q];
@@ -2036,6 +2036,25 @@ __global__ void __launch_bounds__(256) k_fp64_probe(double* sink, int iters) {
   }
   double r = a0 + a1 + a2 + a3 + a4 + a5 + a6 + a7;
   if (r == 12345.0) sink[blockIdx.x] = r;
+}
+
+// FP32 fused multiply-add throughput probe.
+__global__ void __launch_bounds__(256) k_fp32_probe(float* sink, int iters) {
+  float a0 = threadIdx.x * 1e-6f, a1 = a0 + 1e-6f, a2 = a0 + 2e-6f, a3 = a0 + 3e-6f;
+  float a4 = a0 + 4e-6f, a5 = a0 + 5e-6f, a6 = a0 + 6e-6f, a7 = a0 + 7e-6f;
+  const float m = 0.9999f, c = 1e-7f;
+  for (int i = 0; i < iters; ++i) {
+    a0 = fmaf(a0, m, c); a1 = fmaf(a1, m, c); a2 = fmaf(a2, m, c); a3 = fmaf(a3, m, c);
+    a4 = fmaf(a4, m, c); a5 = fmaf(a5, m, c); a6 = fmaf(a6, m, c); a7 = fmaf(a7, m, c);
+  }
+  float r = a0 + a1 + a2 + a3 + a4 + a5 + a6 + a7;
+  if (r == 12345.0f) sink[blockIdx.x] = r;
+}
+
+double launch_fp32_probe(float* sink, int blocks, cudaStream_t st) {
+  const int iters = 8192;
+  k_fp32_probe<<<blocks, 256, 0, st>>>(sink, iters);
+  return 2.0 * 8.0 * iters * 256.0 * blocks;
 }
 
 double launch_fp64_probe(double* sink, int blocks, cudaStream_t st) {

@@ -64,5 +64,6 @@ void launch_dump_boundary(const DevBatch& b, int max_per, int* ncb, int* clob, d
 void launch_dump_cella(const DevBatch& b, int* cella, cudaStream_t st);
 // FP64 FMA throughput probe: returns flops per launch
 double launch_fp64_probe(double* sink, int blocks, cudaStream_t st);
+double launch_fp32_probe(float* sink, int blocks, cudaStream_t st);
 
 }  // namespace sph
