@@ -36,14 +36,14 @@ import numpy as np  # noqa: E402
 
 METRIC = "particle-steps/s FP32c vs FP64 at ≤1e-3 rel L2; ensemble p50/p99 time-to-result"
 UNIT = "particle-steps/s"
-KERNELS_PER_STEP = 13          # momentum, 7 sort, 2 boundary, continuity, finalize... counted in step_sequence
+KERNELS_PER_STEP = 14          # sph_api.cu step_sequence: momentum, 8 sort, 2 boundary, lists, continuity, finalize
 # algorithmic bytes of the fused momentum kernel per particle: reads X 32,
 # V 32, RP 16, L 1, bdt_count 4, I 4; writes X2 32, V2 32, P2 8, I2 4, L2 1
 MOM_BYTES_PER_PARTICLE = 166
 BDT_ENTRY_BYTES = 168
-# FP64 operations: 9 per candidate distance test, 107 per accepted non-self
-# pair in the momentum pass, 34 in the continuity pass (sqrt and divide
-# counted as one)
+# Operations per accepted non-self pair: 107 in the momentum pass, 34 in the
+# continuity pass (sqrt and divide counted as one); 9 per candidate test of
+# the neighbour-list pass
 FLOP_CAND, FLOP_MOM_PAIR, FLOP_CONT_PAIR = 9, 107, 34
 
 
@@ -267,11 +267,11 @@ def main():
     alg_bytes = n * MOM_BYTES_PER_PARTICLE + diag.bdt_entries * BDT_ENTRY_BYTES
     hbm_peak, peak_kind = _peaks()
     achieved_gbs = alg_bytes / (mom_ms * 1e-3) / 1e9
-    mom_flops = (cnt["mom_candidates"] * FLOP_CAND + (cnt["mom_pairs"] - n * nprof) * FLOP_MOM_PAIR) / nprof
+    mom_flops = (cnt["pairs"] - n * nprof) * FLOP_MOM_PAIR / nprof
     mom_tflops = mom_flops / (mom_ms * 1e-3) / 1e12
     mom64_ms = r64["phases"]["momentum"]
     c64 = r64["cnt"]
-    mom64_flops = (c64["mom_candidates"] * FLOP_CAND + (c64["mom_pairs"] - n * nprof) * FLOP_MOM_PAIR) / nprof
+    mom64_flops = (c64["pairs"] - n * nprof) * FLOP_MOM_PAIR / nprof
     workload = "dam_break_3d"
     traffic = _traffic(workload)
 
@@ -342,8 +342,8 @@ def main():
                      "fp": {"achieved_tflops": mom_tflops, "peak_tflops": fp32_peak,
                             "frac": mom_tflops / fp32_peak, "peak_kind": "measured FP32 FMA rate (in-run)"}},
         "phases_ms_per_step": r32["phases"],
-        "pairs_per_particle": cnt["mom_pairs"] / nprof / n,
-        "candidates_per_particle": cnt["mom_candidates"] / nprof / n,
+        "pairs_per_particle": cnt["pairs"] / nprof / n,
+        "candidates_per_particle": cnt["candidates"] / nprof / n,
         "gpu_launches": KERNELS_PER_STEP * args.steps,
         "clocks": clocks,
         "cpu_baseline": cpu,

@@ -286,12 +286,14 @@ int  sph_ord_grid_static(const SphParams* params, int32_t n, const double* d_x, 
 /* ---------------------------------------------------------------------- */
 
 /* Runs nsteps whole steps without the graph, timing each phase with CUDA
- * events on the handle's stream; ms[0..4] receive the summed milliseconds of
+ * events on the handle's stream; ms[0..5] receive the summed milliseconds of
  * momentum (+leapfrog, trajectories), OrdGrid1, ComputeBoundaryDataTab,
- * continuity (+Leapfrog_continuity, EoS) and the time-step closing.       */
+ * the neighbour lists (CalcVarLength), continuity (+Leapfrog_continuity,
+ * EoS) and the time-step closing.                                         */
 int  sph_profile_phases(SphHandle* h, int32_t nsteps, double* ms);
-/* Neighbour candidates and accepted pairs (incl. self) counted by the pair
- * passes: c[0..1] momentum, c[2..3] continuity; reset != 0 zeroes them.   */
+/* Neighbour candidates tested (c[0]) and pairs accepted incl. the particle
+ * itself (c[1]) by the neighbour-list pass; c[2..3] reserved.  reset != 0
+ * zeroes them.                                                            */
 int  sph_get_counters(SphHandle* h, uint64_t* c, int32_t reset);
 /* Measured dense FMA throughput of the current device in TFLOP/s: FP64,
  * or FP32 when fp32 != 0.                                                 */

@@ -194,17 +194,17 @@ class Simulation:
         _chk(lib().sph_eos(self._h), "sph_eos")
 
     # ------------------------------------------------------------ profiling
-    PHASES = ("momentum", "ord_grid", "boundary_data_tab", "continuity", "time_step")
+    PHASES = ("momentum", "ord_grid", "boundary_data_tab", "neighbour_lists", "continuity", "time_step")
 
     def profile_phases(self, nsteps):
-        ms = np.zeros(5)
+        ms = np.zeros(6)
         _chk(lib().sph_profile_phases(self._h, int(nsteps), abi.dptr(ms)), "sph_profile_phases")
         return dict(zip(self.PHASES, ms))
 
     def counters(self, reset=False):
         c = (C.c_uint64 * 4)()
         _chk(lib().sph_get_counters(self._h, c, int(bool(reset))), "sph_get_counters")
-        return dict(mom_candidates=c[0], mom_pairs=c[1], cont_candidates=c[2], cont_pairs=c[3])
+        return dict(candidates=c[0], pairs=c[1])
 
     # --------------------------------------------------------- verification
     def dump_grid(self):

@@ -510,6 +510,9 @@ struct SphHandle {
   int *d_cf_start = nullptr, *d_cf_count = nullptr, *d_cf_list = nullptr;
   uint8_t* d_near = nullptr;
   int* d_scan = nullptr;
+  int* d_nlist = nullptr;
+  int* d_ncount = nullptr;
+  int list_cap = 0;
   unsigned long long* d_counters = nullptr;
   Particles P{};
   std::vector<void*> owned;
@@ -583,6 +586,7 @@ void step_sequence(SphHandle* h, cudaStream_t st) {
   momentum_pass(h, true, st);
   sort_sequence(h, st);
   launch_boundary(h->db, st);
+  launch_neighbour_lists(h->db, st);
   continuity_pass(h, true, st);
   launch_finalize(h->db, 1, st);
 }
@@ -683,6 +687,9 @@ int create_batch(int nsims, const SphParams* params, const SphGeometry* geoms, c
   int nb = (int)((C + 4095) / 4096) + 1;
   A(h->d_scan, nb);
   A(h->d_counters, 4);
+  for (int s = 0; s < nsims; ++s) h->list_cap = std::max(h->list_cap, h->sims[s].dev.nmaxpartj);
+  A(h->d_nlist, N * (size_t)h->list_cap);
+  A(h->d_ncount, N);
 #undef A
   if (st != SPH_OK) { sph_destroy(h); return st; }
   P.bdt_cap = (int)std::min(bdt_cap, (size_t)0x7fffffff);
@@ -735,6 +742,7 @@ int create_batch(int nsims, const SphParams* params, const SphGeometry* geoms, c
   if (e == cudaSuccess) e = cudaMemsetAsync(P.ACC, 0, sizeof(double4) * N, q);
   if (e == cudaSuccess) e = cudaMemsetAsync(P.DDEN, 0, sizeof(double) * N, q);
   if (e == cudaSuccess) e = cudaMemsetAsync(h->d_counters, 0, sizeof(unsigned long long) * 4, q);
+  if (e == cudaSuccess) e = cudaMemsetAsync(h->d_ncount, 0, sizeof(int) * N, q);
   if (e == cudaSuccess) upload_bit2d(&bit2d[0][0], q);
   if (e == cudaSuccess) e = cudaStreamSynchronize(q);
   if (e != cudaSuccess) { sph_destroy(h); return cuda_status(e); }
@@ -755,6 +763,9 @@ int create_batch(int nsims, const SphParams* params, const SphGeometry* geoms, c
   b.cell_near = h->d_near;
   b.scan_block_sums = h->d_scan;
   b.counters = h->d_counters;
+  b.nlist = h->d_nlist;
+  b.ncount = h->d_ncount;
+  b.list_cap = h->list_cap;
   b.scan_nblocks = nb;
   b.grid_blocks = prop.multiProcessorCount * 8;
   *out = h;
@@ -790,6 +801,7 @@ int initialise(SphHandle* h) {
   launch_init_from_caller(h->db, h->d_cx, h->d_cv, h->d_crho, h->d_cp, h->d_cm, q);
   sort_sequence(h, q);
   launch_boundary(h->db, q);
+  launch_neighbour_lists(h->db, q);
   launch_dt_reduce(h->db, q);
   launch_finalize(h->db, 0, q);
   SPH_CUDA(cudaGetLastError());
@@ -965,6 +977,7 @@ int sph_ord_grid(SphHandle* h) {
   if (!h || !h->uploaded) return SPH_ERR_INVALID_ARGUMENT;
   launch_stage(h->db, h->stream);
   sort_sequence(h, h->stream);
+  launch_neighbour_lists(h->db, h->stream);
   SPH_CUDA(cudaGetLastError());
   return sync_dyn(h);
 }
@@ -1076,14 +1089,15 @@ int sph_dump_boundary(SphHandle* h, int32_t max_per, int32_t* ncb, int32_t* clob
 //   ms[0] momentum (RHS_momentum_equation + leapfrog + trajectories)
 //   ms[1] OrdGrid1 (bin, removals, scan, place, rank/permute)
 //   ms[2] ComputeBoundaryDataTab
-//   ms[3] continuity + Leapfrog_continuity + EoS
-//   ms[4] time_step_duration closing
+//   ms[3] neighbour lists (CalcVarLength)
+//   ms[4] continuity + Leapfrog_continuity + EoS
+//   ms[5] time_step_duration closing
 int sph_profile_phases(SphHandle* h, int32_t nsteps, double* ms) {
   if (!h || !h->uploaded || nsteps <= 0 || !ms) return SPH_ERR_INVALID_ARGUMENT;
-  cudaEvent_t ev[6];
-  for (int i = 0; i < 6; ++i)
+  cudaEvent_t ev[7];
+  for (int i = 0; i < 7; ++i)
     if (cudaEventCreate(&ev[i]) != cudaSuccess) { cudaGetLastError(); return SPH_ERR_CUDA; }
-  for (int i = 0; i < 5; ++i) ms[i] = 0.0;
+  for (int i = 0; i < 6; ++i) ms[i] = 0.0;
   cudaStream_t q = h->stream;
   cudaError_t e = cudaSuccess;
   for (int s = 0; s < nsteps && e == cudaSuccess; ++s) {
@@ -1094,25 +1108,26 @@ int sph_profile_phases(SphHandle* h, int32_t nsteps, double* ms) {
     cudaEventRecord(ev[2], q);
     launch_boundary(h->db, q);
     cudaEventRecord(ev[3], q);
-    continuity_pass(h, true, q);
+    launch_neighbour_lists(h->db, q);
     cudaEventRecord(ev[4], q);
-    launch_finalize(h->db, 1, q);
+    continuity_pass(h, true, q);
     cudaEventRecord(ev[5], q);
-    e = cudaEventSynchronize(ev[5]);
-    for (int i = 0; i < 5 && e == cudaSuccess; ++i) {
+    launch_finalize(h->db, 1, q);
+    cudaEventRecord(ev[6], q);
+    e = cudaEventSynchronize(ev[6]);
+    for (int i = 0; i < 6 && e == cudaSuccess; ++i) {
       float t = 0.f;
       e = cudaEventElapsedTime(&t, ev[i], ev[i + 1]);
       ms[i] += t;
     }
   }
-  for (int i = 0; i < 6; ++i) cudaEventDestroy(ev[i]);
+  for (int i = 0; i < 7; ++i) cudaEventDestroy(ev[i]);
   if (e != cudaSuccess) return cuda_status(e);
   return sync_dyn(h);
 }
 
-// Candidate and accepted-pair counts accumulated by the pair passes:
-// c[0] momentum candidates, c[1] momentum pairs (incl. the particle
-// itself), c[2] continuity candidates, c[3] continuity pairs.
+// Candidates tested and pairs accepted (incl. the particle itself) by the
+// neighbour-list pass: c[0], c[1]; c[2..3] are reserved (zero).
 int sph_get_counters(SphHandle* h, uint64_t* c, int32_t reset) {
   if (!h || !c) return SPH_ERR_INVALID_ARGUMENT;
   unsigned long long t[4];

@@ -968,121 +968,159 @@ __device__ __forceinline__ void elastic_reaction(const SimDev& s, const DevBatch
   }
 }
 
-// Accepted-neighbour FIFO per thread.  The candidate scan (cheap, divergent:
-// about one candidate in six lies within 2h) fills it in the reference's
-// visiting order; the pair arithmetic then drains it with the whole warp in
-// lockstep, so the expensive FP64 work runs on (nearly) all lanes.
-constexpr int kBuf = 16;
-
-// FIFO entries: slot | (neighbour run << 28).
+// ==========================================================================
+// Neighbour lists (the list-free-kernel-values replacement of
+// CalcVarLength.f90:133-269).  One pass after the sort stores, per particle,
+// the slots of its accepted neighbours (the particle itself excluded, its
+// acceptance still counted for the NMAXPARTJ cap) in the reference's
+// visiting order: runs in (y, x) order, slots increasing inside a run.  Only
+// 4-byte slot indices are kept, never kernel values or separations (the
+// reference keeps 60 B per slot); every pass recomputes those.  The list of a
+// step serves its continuity pass and the next step's momentum pass, which
+// see the same positions.
+//
+// Layout: entry k of particle p at ((p / 32) * cap + k) * 32 + p % 32, so a
+// warp reads one 128-byte line per k.  An entry is slot | (run << 28); the
+// run gives the FP32 form the cell-origin difference of the pair.
+//
+// The scan is warp-cooperative: the lanes of a warp that share a (y, x) cell
+// column (nearly always all of them, particles being sorted z-fastest) stage
+// the union of their 3-cell runs through shared memory 32 candidates at a
+// time and test them in lockstep; each lane keeps the candidates of its own
+// k-1..k+1 window, so its accepted sequence is exactly its reference order.
+// ==========================================================================
 constexpr int kSlotBits = 28;
 constexpr int kSlotMask = (1 << kSlotBits) - 1;
 
+__device__ __forceinline__ size_t list_base(int p, int cap) {
+  return (size_t)(p >> 5) * (size_t)cap * 32 + (size_t)(p & 31);
+}
+
+// r^2 <= (2h)^2 (CalcVarLength.f90:223-228) decided on the FP32 screening
+// copies outside [rr_lo, rr_hi] (a band the host derives from the copies'
+// rounding bounds) and in FP64, exactly as the reference, inside it.
+__device__ __forceinline__ bool accept_pair(const SimDev& s, const Particles& P, const double4& xi, float d0,
+                                            float d1, float d2, int q) {
+  float rf = d0 * d0 + d1 * d1 + d2 * d2;
+  if (rf < s.rr_lo) return true;
+  if (rf > s.rr_hi) return false;
+  double4 xd = P.X[q];
+  double r0 = xi.x - xd.x, r1 = xi.y - xd.y, r2 = xi.z - xd.z;
+  double rr = r0 * r0 + r1 * r1 + r2 * r2;
+  return !(rr > s.square_doubleh);
+}
+
 template <int DIM>
-struct NeighbourScan {
-  int r, q, qe, ci, cj, ck, nacc, cand;
-  float Dx, Dy;          // FP32 cell-origin difference of the current run
-  bool done, trunc;
-
-  __device__ __forceinline__ void init(bool on, int ci_, int cj_, int ck_) {
-    ci = ci_;
-    cj = cj_;
-    ck = ck_;
-    r = 0;
-    q = 0;
-    qe = 0;
-    nacc = 0;
-    cand = 0;
-    Dx = 0.f;
-    Dy = 0.f;
-    trunc = false;
-    done = !on;
-  }
-
-  // The distance test r^2 <= (2h)^2 of CalcVarLength.f90:223-228 is decided
-  // in FP32 on the screening copies when r^2 lies outside [rr_lo, rr_hi], a
-  // band the host derives from the rounding bounds of the copies, and in
-  // FP64 exactly as the reference does inside the band: the accepted set is
-  // the reference's, bit for bit.
-  __device__ __forceinline__ bool accept(const SimDev& s, const Particles& P, const double4& xi, const float4& xf,
-                                         int q) const {
-    float4 xj = P.XF[q];
-    float Dz = (float)(ck - __float_as_int(xj.w)) * s.dcdf[2];
-    float d0 = Dx + (xf.x - xj.x), d1 = Dy + (xf.y - xj.y), d2 = Dz + (xf.z - xj.z);
-    float rf = d0 * d0 + d1 * d1 + d2 * d2;
-    if (rf < s.rr_lo) return true;
-    if (rf > s.rr_hi) return false;
-    double4 xd = P.X[q];
-    double r0 = xi.x - xd.x, r1 = xi.y - xd.y, r2 = xi.z - xd.z;
-    double rr = r0 * r0 + r1 * r1 + r2 * r2;
-    return !(rr > s.square_doubleh);
-  }
-
-  // Appends up to kBuf(+1) accepted neighbours (the particle itself excluded)
-  // to the thread's FIFO column; returns how many were appended.  The
-  // NMAXPARTJ cap of CalcVarLength.f90:197-205 applies to the accepted count.
-  __device__ __forceinline__ int fill(const SimDev& s, const Particles& P, const double4& xi, const float4& xf,
-                                      int self, int* col) {
-    constexpr int NR = (DIM == 3) ? 9 : 3;
-    int nb = 0;
-    while (!done && nb < kBuf) {
-      if (q >= qe) {
-        if (r >= NR) {
-          done = true;
-          break;
+__global__ void __launch_bounds__(kBlock) k_neighbour_lists(DevBatch b) {
+  __shared__ SimDev s;
+  __shared__ float4 cbuf[kBlock];
+  int cur = -1;
+  const Particles& P = b.P;
+  const int lane = threadIdx.x & 31;
+  float4* wbuf = cbuf + (threadIdx.x & ~31);
+  constexpr int NR = (DIM == 3) ? 9 : 3;
+  const unsigned FULL = 0xffffffffu;
+  for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
+    Tile tl = b.tiles[t];
+    load_sim(s, b.sims, tl.sim, cur);
+    SimDyn* dyn = b.dyn + tl.sim;
+    int p = tl.start + threadIdx.x;
+    bool active = threadIdx.x < tl.count && p < s.p_off + dyn->nag && !dyn->frozen;
+    double4 xd = make_double4(0.0, 0.0, 0.0, 0.0);
+    float4 xf = make_float4(0.f, 0.f, 0.f, 0.f);
+    int ci = 0, cj = 0, ck = 0;
+    bool on = false;
+    if (active) {
+      xd = P.X[p];
+      xf = P.XF[p];
+      on = particle_cell(s, xd.x, xd.y, xd.z, ci, cj, ck);
+      if (!on) set_status(dyn, SPH_ERR_INVALID_ARGUMENT);   // state not re-sorted after a move
+    }
+    int colkey = on ? (cj * s.ncd[0] + ci) : -1;
+    unsigned remaining = __ballot_sync(FULL, on);
+    int cnt = 0, nacc = 0, cand = 0;
+    bool trunc = false, done = !on;
+    const int cap = s.nmaxpartj;
+    size_t lb = list_base(p, b.list_cap);
+    while (remaining) {
+      int leader = __ffs(remaining) - 1;
+      int key = __shfl_sync(FULL, colkey, leader);
+      unsigned group = __ballot_sync(FULL, on && colkey == key) & remaining;
+      remaining &= ~group;
+      bool mine = (group >> lane) & 1u;
+      int kmin = __reduce_min_sync(FULL, mine ? ck : 0x7fffffff);
+      int kmax = __reduce_max_sync(FULL, mine ? ck : -0x7fffffff);
+      int gci = __shfl_sync(FULL, ci, leader);
+      int gcj = __shfl_sync(FULL, cj, leader);
+      for (int r = 0; r < NR; ++r) {
+        int jr = (DIM == 3) ? gcj - 1 + r / 3 : gcj;
+        int ir = gci - 1 + ((DIM == 3) ? r % 3 : r);
+        if (ir < 1 || ir > s.ncd[0] || jr < 1 || jr > s.ncd[1]) continue;
+        int klo = kmin > 1 ? kmin - 1 : 1;
+        int khi = kmax < s.ncd[2] ? kmax + 1 : s.ncd[2];
+        int base = s.cell_off + ((jr - 1) * s.ncd[0] + (ir - 1)) * s.ncd[2];
+        int ub = __ldg(P.cell_start + base + klo - 1);
+        int ue = __ldg(P.cell_start + base + khi);
+        float Dx = (float)(gci - ir) * s.dcdf[0];
+        float Dy = (DIM == 3) ? (float)(gcj - jr) * s.dcdf[1] : 0.f;
+        const int tag = r << kSlotBits;
+        for (int c0 = ub; c0 < ue; c0 += 32) {
+          int cidx = c0 + lane;
+          __syncwarp();
+          wbuf[lane] = (cidx < ue) ? P.XF[cidx] : make_float4(0.f, 0.f, 0.f, __int_as_float(-0x3fffffff));
+          __syncwarp();
+          int nt = ue - c0 < 32 ? ue - c0 : 32;
+          if (mine && !done) {
+            for (int u = 0; u < nt; ++u) {
+              float4 xj = wbuf[u];
+              int kj = __float_as_int(xj.w);
+              if (kj < ck - 1 || kj > ck + 1) continue;
+              cand++;
+              if (nacc >= cap) {
+                trunc = true;
+                done = true;
+                break;
+              }
+              float Dz = (float)(ck - kj) * s.dcdf[2];
+              float d0 = Dx + (xf.x - xj.x);
+              float d1 = (DIM == 3) ? Dy + (xf.y - xj.y) : 0.f;
+              float d2 = Dz + (xf.z - xj.z);
+              int q = c0 + u;
+              if (accept_pair(s, P, xd, d0, d1, d2, q)) {
+                nacc++;
+                if (q != p) {
+                  b.nlist[lb + (size_t)cnt * 32] = q | tag;
+                  cnt++;
+                }
+              }
+            }
+          }
         }
-        neighbour_run<DIM>(s, P.cell_start, ci, cj, ck, r, q, qe);
-        int jr = (DIM == 3) ? cj - 1 + r / 3 : cj;
-        int ir = ci - 1 + ((DIM == 3) ? r % 3 : r);
-        Dx = (float)(ci - ir) * s.dcdf[0];
-        Dy = (DIM == 3) ? (float)(cj - jr) * s.dcdf[1] : 0.f;
-        r++;
-        cand += qe - q;
-        continue;
-      }
-      if (nacc >= s.nmaxpartj) {
-        trunc = true;
-        done = true;
-        break;
-      }
-      const int tag = (r - 1) << kSlotBits;
-      bool a0 = accept(s, P, xi, xf, q);
-      if (q + 1 < qe) {
-        // two candidates per iteration: independent loads in flight
-        bool a1 = accept(s, P, xi, xf, q + 1);
-        if (a0) {
-          nacc++;
-          if (q != self) col[(nb++) * kBlock] = q | tag;
-        }
-        if (nacc >= s.nmaxpartj) {
-          q++;
-          continue;
-        }
-        if (a1) {
-          nacc++;
-          if (q + 1 != self) col[(nb++) * kBlock] = (q + 1) | tag;
-        }
-        q += 2;
-      } else {
-        if (a0) {
-          nacc++;
-          if (q != self) col[(nb++) * kBlock] = q | tag;
-        }
-        q++;
       }
     }
-    return nb;
+    if (active) {
+      b.ncount[p] = cnt;
+      if (trunc) atomicOr(&dyn->warnings, SPH_WARN_NEIGHBOURS_TRUNCATED);
+    }
+    block_count2(b.counters, cand, nacc);
+    int m = warp_max(nacc);
+    if (lane == 0 && m > 0) atomicMax(&dyn->max_neigh, m);
   }
-};
+}
 
+// ==========================================================================
+// Momentum, FP64 form: RHS_momentum_equation + inter_EqMoto + viscomon +
+// viscomorris + AddBoundaryContributions_to_ME3D/2D +
+// AddElasticBoundaryReaction_3D/2D, optionally fused with Leapfrog_momentum,
+// velocity_smoothing_2 (TetaV = 0), Leapfrog_trajectories and the CFL part of
+// time_step_duration.  The list is drained in warp lockstep.
+// ==========================================================================
 template <int DIM, bool FUSED>
 __global__ void __launch_bounds__(kBlock, 2) k_momentum(DevBatch b) {
   __shared__ SimDev s;
-  __shared__ int sbuf[(kBuf + 1) * kBlock];
   int cur = -1;
   const Particles& P = b.P;
   const double GI = (double)9.80665f;   // Static_allocation_module.f90:72, a default-REAL literal
-  int* col = sbuf + threadIdx.x;
   for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
     Tile tl = b.tiles[t];
     load_sim(s, b.sims, tl.sim, cur);
@@ -1103,10 +1141,8 @@ __global__ void __launch_bounds__(kBlock, 2) k_momentum(DevBatch b) {
     double4 xi = make_double4(0.0, 0.0, 0.0, 0.0);
     double vi[3] = {0.0, 0.0, 0.0};
     double rhoi = 1.0, pi = 0.0;
-    int lam = 0, nb = 0, bstart = 0;
+    int lam = 0, nb = 0, bstart = 0, cnt = 0;
     double tpres[3] = {0, 0, 0}, tdiss[3] = {0, 0, 0}, tvisc[3] = {0, 0, 0};
-    int ci = 0, cj = 0, ck = 0;
-    bool in_grid = false;
     if (active) {
       xi = P.X[p];
       double4 v4 = P.V[p];
@@ -1117,18 +1153,14 @@ __global__ void __launch_bounds__(kBlock, 2) k_momentum(DevBatch b) {
       rhoi = rp.x;
       pi = rp.y;
       lam = P.L[p];
+      cnt = b.ncount[p];
       nb = P.bdt_count[p];
       bstart = nb > 0 ? P.bdt_start[p] : 0;
       if (nb > 0) {
         if (DIM == 3) me_boundary3d(s, b, nb, bstart, vi, rhoi, pi, lam, tpres, tdiss, tvisc);
         else me_boundary2d(s, b, nb, bstart, vi, rhoi, pi, lam, tpres, tdiss, tvisc);
       }
-      in_grid = particle_cell(s, xi.x, xi.y, xi.z, ci, cj, ck);
-      if (!in_grid) set_status(dyn, SPH_ERR_INVALID_ARGUMENT);   // state not re-sorted after a move
     }
-    NeighbourScan<DIM> sc;
-    sc.init(active && in_grid, ci, cj, ck);
-    float4 xfi = active ? P.XF[p] : make_float4(0.f, 0.f, 0.f, 0.f);
     double tp0 = 0, tp1 = 0, tp2 = 0, al0 = 0, al1 = 0, al2 = 0;
     double td0 = tdiss[0], td1 = tdiss[1], td2 = tdiss[2];
     double tv0 = tvisc[0], tv1 = tvisc[1], tv2 = tvisc[2];
@@ -1136,59 +1168,56 @@ __global__ void __launch_bounds__(kBlock, 2) k_momentum(DevBatch b) {
     const double celt = s.celerita + s.celerita;
     const bool morris = s.kin_visc > 1.0e-12;
     const double nu = s.kin_visc;
-    while (__any_sync(0xffffffffu, !sc.done)) {
-      int nbuf = sc.fill(s, P, xi, xfi, p, col);
-      int nmax = __reduce_max_sync(0xffffffffu, (unsigned)nbuf);
-      for (int k = 0; k < nmax; ++k) {
-        if (k >= nbuf) continue;
-        int q = col[k * kBlock] & kSlotMask;
-        double4 xj = P.X[q];
-        double r0 = xi.x - xj.x, r1 = xi.y - xj.y, r2 = xi.z - xj.z;
-        double rr = r0 * r0 + r1 * r1 + r2 * r2;
-        double PK1, PK2, PK3;
-        kernel_values(s, rr, PK1, PK2, PK3);
-        double4 vj = P.V[q];
-        double2 rpj = P.RP[q];
-        double rhoj = rpj.x, pj = rpj.y, amassj = xj.w;
-        double dv0 = vj.x - vi[0], dv1 = vj.y - vi[1], dv2 = vj.z - vi[2];
-        // pressure gradient and ALE1 terms, inter_EqMoto.f90:195-221
-        double alpha = (pj - pi) / (rhoi * rhoj);
-        tp0 = tp0 + -(amassj * alpha * r0 * PK3);
-        if (DIM == 3) tp1 = tp1 + -(amassj * alpha * r1 * PK3);
-        tp2 = tp2 + -(amassj * alpha * r2 * PK3);
-        double alpha2 = (pi * (rhoj / rhoi + 1.0) + pj * (rhoi / rhoj - 1.0)) / (rhoi * rhoj);
-        al0 = al0 - amassj * alpha2 * r0 * PK3;
-        if (DIM == 3) al1 = al1 - amassj * alpha2 * r1 * PK3;
-        al2 = al2 - amassj * alpha2 * r2 * PK3;
-        // viscomon.f90:54-73
-        double vrij = (DIM == 3) ? -(dv0 * r0) - dv1 * r1 - dv2 * r2 : -(dv0 * r0) - dv2 * r2;
-        double TermMon = s.alfa_mon * celt * s.h / (rhoi + rhoj);
-        double mtv = amassj * TermMon * vrij;
-        td0 = td0 + (mtv * r0 * PK2 + 0.0);
-        if (DIM == 3) td1 = td1 + (mtv * r1 * PK2 + 0.0);
-        td2 = td2 + (mtv * r2 * PK2 + 0.0);
-        // viscomorris.f90:60-71
-        if (morris) {
-          double rt = nu * rhoi + nu * rhoj + 1.0e-3;
-          double anuitilde = 4.0 * (nu * nu);
-          double factivis = amassj * anuitilde / rt;
-          double w0 = factivis * (-(dv0 * PK2 * rr));
-          double w2 = factivis * (-(dv2 * PK2 * rr));
-          tv0 = tv0 + w0;
-          rs0 = rs0 + w0;
-          if (DIM == 3) {
-            double w1 = factivis * (-(dv1 * PK2 * rr));
-            tv1 = tv1 + w1;
-            rs1 = rs1 + w1;
-          }
-          tv2 = tv2 + w2;
-          rs2 = rs2 + w2;
+    const size_t lb = list_base(p, b.list_cap);
+    const int nmax = __reduce_max_sync(0xffffffffu, (unsigned)cnt);
+    for (int k = 0; k < nmax; ++k) {
+      if (k >= cnt) continue;
+      int q = b.nlist[lb + (size_t)k * 32] & kSlotMask;
+      double4 xj = P.X[q];
+      double r0 = xi.x - xj.x, r1 = xi.y - xj.y, r2 = xi.z - xj.z;
+      double rr = r0 * r0 + r1 * r1 + r2 * r2;
+      double PK1, PK2, PK3;
+      kernel_values(s, rr, PK1, PK2, PK3);
+      double4 vj = P.V[q];
+      double2 rpj = P.RP[q];
+      double rhoj = rpj.x, pj = rpj.y, amassj = xj.w;
+      double dv0 = vj.x - vi[0], dv1 = vj.y - vi[1], dv2 = vj.z - vi[2];
+      // pressure gradient and ALE1 terms, inter_EqMoto.f90:195-221
+      double alpha = (pj - pi) / (rhoi * rhoj);
+      tp0 = tp0 + -(amassj * alpha * r0 * PK3);
+      if (DIM == 3) tp1 = tp1 + -(amassj * alpha * r1 * PK3);
+      tp2 = tp2 + -(amassj * alpha * r2 * PK3);
+      double alpha2 = (pi * (rhoj / rhoi + 1.0) + pj * (rhoi / rhoj - 1.0)) / (rhoi * rhoj);
+      al0 = al0 - amassj * alpha2 * r0 * PK3;
+      if (DIM == 3) al1 = al1 - amassj * alpha2 * r1 * PK3;
+      al2 = al2 - amassj * alpha2 * r2 * PK3;
+      // viscomon.f90:54-73
+      double vrij = (DIM == 3) ? -(dv0 * r0) - dv1 * r1 - dv2 * r2 : -(dv0 * r0) - dv2 * r2;
+      double TermMon = s.alfa_mon * celt * s.h / (rhoi + rhoj);
+      double mtv = amassj * TermMon * vrij;
+      td0 = td0 + (mtv * r0 * PK2 + 0.0);
+      if (DIM == 3) td1 = td1 + (mtv * r1 * PK2 + 0.0);
+      td2 = td2 + (mtv * r2 * PK2 + 0.0);
+      // viscomorris.f90:60-71
+      if (morris) {
+        double rt = nu * rhoi + nu * rhoj + 1.0e-3;
+        double anuitilde = 4.0 * (nu * nu);
+        double factivis = amassj * anuitilde / rt;
+        double w0 = factivis * (-(dv0 * PK2 * rr));
+        double w2 = factivis * (-(dv2 * PK2 * rr));
+        tv0 = tv0 + w0;
+        rs0 = rs0 + w0;
+        if (DIM == 3) {
+          double w1 = factivis * (-(dv1 * PK2 * rr));
+          tv1 = tv1 + w1;
+          rs1 = rs1 + w1;
         }
+        tv2 = tv2 + w2;
+        rs2 = rs2 + w2;
       }
     }
     double dtc = 1.0e300;
     if (active) {
-      if (sc.trunc) atomicOr(&dyn->warnings, SPH_WARN_NEIGHBOURS_TRUNCATED);
       tpres[0] = tpres[0] + tp0 + al0;
       tpres[1] = tpres[1] + tp1 + al1;
       tpres[2] = tpres[2] + tp2 + al2;
@@ -1229,7 +1258,6 @@ __global__ void __launch_bounds__(kBlock, 2) k_momentum(DevBatch b) {
         P.L[p] = (uint8_t)lam_new;
       }
     }
-    block_count2(b.counters, sc.cand, sc.nacc);
     if (FUSED) {
       double m = warp_min(dtc);
       if ((threadIdx.x & 31) == 0 && m < 1.0e300)
@@ -1238,17 +1266,70 @@ __global__ void __launch_bounds__(kBlock, 2) k_momentum(DevBatch b) {
   }
 }
 
-// ==========================================================================
-// Continuity: SASPH_continuity + AddBoundaryContribution_to_CE3D/2D +
-// Continuity_Equation, optionally fused with Leapfrog_continuity and the EoS.
-// ==========================================================================
+// SASPH_continuity.f90:89-169 with AddBoundaryContribution_to_CE3D/2D: the
+// wall term of drho/dt, starting value of the continuity sum (FP64).
+template <int DIM>
+__device__ __forceinline__ double continuity_boundary(const SimDev& s, const DevBatch& b, SimDyn* dyn, int nb,
+                                                      int bstart, const double4& vi, double rhoi) {
+  const Particles& P = b.P;
+  double gu0 = 0, gv1 = 0, gw2 = 0;
+  if (DIM == 3) {
+    double gu[3] = {0, 0, 0}, gv[3] = {0, 0, 0}, gw[3] = {0, 0, 0};
+    const double var[3] = {vi.x, vi.y, vi.z};
+    for (int u = 0; u < nb; ++u) {
+      const BdtEntry& e = P.bdt[bstart + u];
+      const FaceDev& f = b.faces[s.face_off + e.clobonum - 1];
+      if (!(e.loc[2] > 0.0)) continue;
+      double dp = 0.0;
+      for (int d = 0; d < 3; ++d) dp = dp + (2.0 * (f.velocity[d] - var[d])) * f.T[d][2];
+      double dvel[3] = {dp * f.T[0][2], dp * f.T[1][2], dp * f.T[2][2]};
+      double av[3];
+      for (int i = 0; i < 3; ++i) {
+        double a = 0.0;
+        for (int k = 0; k < 3; ++k) a = a + f.T[i][k] * e.bi[3 + k];
+        av[i] = a;
+      }
+      for (int d = 0; d < 3; ++d) {
+        gu[d] = gu[d] - dvel[0] * av[d];
+        gv[d] = gv[d] - dvel[1] * av[d];
+        gw[d] = gw[d] - dvel[2] * av[d];
+      }
+    }
+    gu0 = gu[0];
+    gv1 = gv[1];
+    gw2 = gw[2];
+    atomicMax(&dyn->ncbf_max, nb);
+  } else {
+    const double var2[2] = {vi.x, vi.z};
+    double gu_x = 0.0, gw_z = 0.0;
+    for (int u = 0; u < nb; ++u) {
+      const BdtEntry& e = P.bdt[bstart + u];
+      const SideDev& S = b.sides[s.side_off + e.clobonum - 1];
+      double IntWdS = e.bi[0];
+      double dvel0, dvel1;
+      if (S.zone_type == SPH_ZONE_TAPI) {
+        dvel0 = 2.0 * (S.velocity[0] - var2[0]);
+        dvel1 = 2.0 * (S.velocity[2] - var2[1]);
+      } else {
+        dvel0 = 2.0 * (-var2[0]);
+        dvel1 = 2.0 * (-var2[1]);
+      }
+      gu_x = gu_x - dvel0 * S.nnn[0] * IntWdS;
+      gw_z = gw_z - dvel1 * S.nnn[1] * IntWdS;
+    }
+    gu0 = gu_x;
+    gw2 = gw_z;
+  }
+  return 0.0 - rhoi * (gu0 + gv1 + gw2);
+}
+
+// Continuity, FP64 form: SASPH_continuity + Continuity_Equation, optionally
+// fused with Leapfrog_continuity and the EoS.
 template <int DIM, bool FUSED>
 __global__ void __launch_bounds__(kBlock, 2) k_continuity(DevBatch b) {
   __shared__ SimDev s;
-  __shared__ int sbuf[(kBuf + 1) * kBlock];
   int cur = -1;
   const Particles& P = b.P;
-  int* col = sbuf + threadIdx.x;
   for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
     Tile tl = b.tiles[t];
     load_sim(s, b.sims, tl.sim, cur);
@@ -1258,92 +1339,33 @@ __global__ void __launch_bounds__(kBlock, 2) k_continuity(DevBatch b) {
     double4 xi = make_double4(0.0, 0.0, 0.0, 0.0);
     double4 vi = make_double4(0.0, 0.0, 0.0, 0.0);
     double rhoi = 1.0, dden = 0.0;
-    int ci = 0, cj = 0, ck = 0;
-    bool in_grid = false;
+    int cnt = 0;
     if (active) {
       xi = P.X[p];
       vi = P.V[p];
       rhoi = P.RP[p].x;
+      cnt = b.ncount[p];
       int nb = P.bdt_count[p];
-      if (nb > 0) {
-        int bstart = P.bdt_start[p];
-        double gu0 = 0, gv1 = 0, gw2 = 0;
-        if (DIM == 3) {
-          double gu[3] = {0, 0, 0}, gv[3] = {0, 0, 0}, gw[3] = {0, 0, 0};
-          const double var[3] = {vi.x, vi.y, vi.z};
-          for (int u = 0; u < nb; ++u) {
-            const BdtEntry& e = P.bdt[bstart + u];
-            const FaceDev& f = b.faces[s.face_off + e.clobonum - 1];
-            if (!(e.loc[2] > 0.0)) continue;
-            double dp = 0.0;
-            for (int d = 0; d < 3; ++d) dp = dp + (2.0 * (f.velocity[d] - var[d])) * f.T[d][2];
-            double dvel[3] = {dp * f.T[0][2], dp * f.T[1][2], dp * f.T[2][2]};
-            double av[3];
-            for (int i = 0; i < 3; ++i) {
-              double a = 0.0;
-              for (int k = 0; k < 3; ++k) a = a + f.T[i][k] * e.bi[3 + k];
-              av[i] = a;
-            }
-            for (int d = 0; d < 3; ++d) {
-              gu[d] = gu[d] - dvel[0] * av[d];
-              gv[d] = gv[d] - dvel[1] * av[d];
-              gw[d] = gw[d] - dvel[2] * av[d];
-            }
-          }
-          gu0 = gu[0];
-          gv1 = gv[1];
-          gw2 = gw[2];
-          atomicMax(&dyn->ncbf_max, nb);
-        } else {
-          const double var2[2] = {vi.x, vi.z};
-          double gu_x = 0.0, gw_z = 0.0;
-          for (int u = 0; u < nb; ++u) {
-            const BdtEntry& e = P.bdt[bstart + u];
-            const SideDev& S = b.sides[s.side_off + e.clobonum - 1];
-            double IntWdS = e.bi[0];
-            double dvel0, dvel1;
-            if (S.zone_type == SPH_ZONE_TAPI) {
-              dvel0 = 2.0 * (S.velocity[0] - var2[0]);
-              dvel1 = 2.0 * (S.velocity[2] - var2[1]);
-            } else {
-              dvel0 = 2.0 * (-var2[0]);
-              dvel1 = 2.0 * (-var2[1]);
-            }
-            gu_x = gu_x - dvel0 * S.nnn[0] * IntWdS;
-            gw_z = gw_z - dvel1 * S.nnn[1] * IntWdS;
-          }
-          gu0 = gu_x;
-          gw2 = gw_z;
-        }
-        dden = dden - rhoi * (gu0 + gv1 + gw2);
-      }
-      in_grid = particle_cell(s, xi.x, xi.y, xi.z, ci, cj, ck);
-      if (!in_grid) set_status(dyn, SPH_ERR_INVALID_ARGUMENT);   // state not re-sorted after a move
+      if (nb > 0) dden = continuity_boundary<DIM>(s, b, dyn, nb, P.bdt_start[p], vi, rhoi);
     }
-    NeighbourScan<DIM> sc;
-    sc.init(active && in_grid, ci, cj, ck);
-    float4 xfi = active ? P.XF[p] : make_float4(0.f, 0.f, 0.f, 0.f);
     double a1 = 0.0, a2 = 0.0, a3 = 0.0;
-    while (__any_sync(0xffffffffu, !sc.done)) {
-      int nbuf = sc.fill(s, P, xi, xfi, p, col);   // the particle itself adds dvar = 0
-      int nmax = __reduce_max_sync(0xffffffffu, (unsigned)nbuf);
-      for (int k = 0; k < nmax; ++k) {
-        if (k >= nbuf) continue;
-        int q = col[k * kBlock] & kSlotMask;
-        double4 xj = P.X[q];
-        double r0 = xi.x - xj.x, r1 = xi.y - xj.y, r2 = xi.z - xj.z;
-        double rr = r0 * r0 + r1 * r1 + r2 * r2;
-        double PK1, PK2, PK3;
-        kernel_values(s, rr, PK1, PK2, PK3);
-        double4 vj = P.V[q];
-        double c = rhoi * vj.w * PK1;     // rhoi * (amassj / rhoj) * PK1
-        a1 = a1 + c * (vj.x - vi.x) * r0;
-        if (DIM == 3) a2 = a2 + c * (vj.y - vi.y) * r1;
-        a3 = a3 + c * (vj.z - vi.z) * r2;
-      }
+    const size_t lb = list_base(p, b.list_cap);
+    const int nmax = __reduce_max_sync(0xffffffffu, (unsigned)cnt);
+    for (int k = 0; k < nmax; ++k) {
+      if (k >= cnt) continue;
+      int q = b.nlist[lb + (size_t)k * 32] & kSlotMask;
+      double4 xj = P.X[q];
+      double r0 = xi.x - xj.x, r1 = xi.y - xj.y, r2 = xi.z - xj.z;
+      double rr = r0 * r0 + r1 * r1 + r2 * r2;
+      double PK1, PK2, PK3;
+      kernel_values(s, rr, PK1, PK2, PK3);
+      double4 vj = P.V[q];
+      double c = rhoi * vj.w * PK1;     // rhoi * (amassj / rhoj) * PK1
+      a1 = a1 + c * (vj.x - vi.x) * r0;
+      if (DIM == 3) a2 = a2 + c * (vj.y - vi.y) * r1;
+      a3 = a3 + c * (vj.z - vi.z) * r2;
     }
     if (active) {
-      if (sc.trunc) atomicOr(&dyn->warnings, SPH_WARN_NEIGHBOURS_TRUNCATED);
       if (DIM == 3) dden = dden - (a1 + a2 + a3);
       else dden = dden - (a1 + a3);
       if (FUSED) {
@@ -1359,9 +1381,6 @@ __global__ void __launch_bounds__(kBlock, 2) k_continuity(DevBatch b) {
         P.DDEN[p] = dden;
       }
     }
-    block_count2(b.counters + 2, sc.cand, sc.nacc);
-    int m = warp_max(sc.nacc);
-    if ((threadIdx.x & 31) == 0 && m > 0) atomicMax(&dyn->max_neigh, m);
   }
 }
 
@@ -1389,7 +1408,7 @@ struct Kahan {
 };
 
 struct F32Const {
-  float hinv, h2inv, eta, eta2, ke, kacl, amon, nu, nu4, sq2h;
+  float hinv, h2inv, eta, eta2, ke, kacl, amon, nu, nu4;
   __device__ __forceinline__ void load(const SimDev& s) {
     hinv = (float)(1.0 / s.h);
     h2inv = (float)(1.0 / s.squareh);
@@ -1400,7 +1419,6 @@ struct F32Const {
     amon = (float)(s.alfa_mon * (s.celerita + s.celerita) * s.h);
     nu = (float)s.kin_visc;
     nu4 = (float)(4.0 * (s.kin_visc * s.kin_visc));
-    sq2h = (float)s.square_doubleh;
   }
 };
 
@@ -1422,7 +1440,7 @@ __device__ __forceinline__ void kernel_values_f32(const F32Const& c, float rr, f
   PK3 = gw * c.kacl * denom;
 }
 
-// FP32 separation of FIFO entry e from particle (xfi, cell ci,cj,ck).
+// FP32 separation of list entry e from particle (xfi, cell ci, cj, ck).
 template <int DIM>
 __device__ __forceinline__ int separation_f32(const SimDev& s, const Particles& P, int e, const float4& xfi, int ci,
                                               int cj, int ck, float& d0, float& d1, float& d2) {
@@ -1443,11 +1461,9 @@ __device__ __forceinline__ int separation_f32(const SimDev& s, const Particles& 
 template <int DIM, bool FUSED>
 __global__ void __launch_bounds__(kBlock, 3) k_momentum_f32(DevBatch b) {
   __shared__ SimDev s;
-  __shared__ int sbuf[(kBuf + 1) * kBlock];
   int cur = -1;
   const Particles& P = b.P;
   const double GI = (double)9.80665f;   // Static_allocation_module.f90:72, a default-REAL literal
-  int* col = sbuf + threadIdx.x;
   for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
     Tile tl = b.tiles[t];
     load_sim(s, b.sims, tl.sim, cur);
@@ -1469,10 +1485,9 @@ __global__ void __launch_bounds__(kBlock, 3) k_momentum_f32(DevBatch b) {
     double4 xi = make_double4(0.0, 0.0, 0.0, 0.0);
     double vi[3] = {0.0, 0.0, 0.0};
     double rhoi = 1.0, pi = 0.0;
-    int lam = 0, nb = 0, bstart = 0;
+    int lam = 0, nb = 0, bstart = 0, cnt = 0;
     double tpres[3] = {0, 0, 0}, tdiss[3] = {0, 0, 0}, tvisc[3] = {0, 0, 0};
     int ci = 0, cj = 0, ck = 0;
-    bool in_grid = false;
     if (active) {
       xi = P.X[p];
       double4 v4 = P.V[p];
@@ -1483,17 +1498,15 @@ __global__ void __launch_bounds__(kBlock, 3) k_momentum_f32(DevBatch b) {
       rhoi = rp.x;
       pi = rp.y;
       lam = P.L[p];
+      cnt = b.ncount[p];
       nb = P.bdt_count[p];
       bstart = nb > 0 ? P.bdt_start[p] : 0;
       if (nb > 0) {
         if (DIM == 3) me_boundary3d(s, b, nb, bstart, vi, rhoi, pi, lam, tpres, tdiss, tvisc);
         else me_boundary2d(s, b, nb, bstart, vi, rhoi, pi, lam, tpres, tdiss, tvisc);
       }
-      in_grid = particle_cell(s, xi.x, xi.y, xi.z, ci, cj, ck);
-      if (!in_grid) set_status(dyn, SPH_ERR_INVALID_ARGUMENT);
+      particle_cell(s, xi.x, xi.y, xi.z, ci, cj, ck);
     }
-    NeighbourScan<DIM> sc;
-    sc.init(active && in_grid, ci, cj, ck);
     float4 xfi = active ? P.XF[p] : make_float4(0.f, 0.f, 0.f, 0.f);
     const float vix = (float)vi[0], viy = (float)vi[1], viz = (float)vi[2];
     const float rhof = (float)rhoi;
@@ -1501,44 +1514,41 @@ __global__ void __launch_bounds__(kBlock, 3) k_momentum_f32(DevBatch b) {
     const bool morris = s.kin_visc > 1.0e-12;
     Kahan tp0, tp1, tp2, td0, td1, td2, tv0, tv1, tv2;
     tp0.zero(); tp1.zero(); tp2.zero(); td0.zero(); td1.zero(); td2.zero(); tv0.zero(); tv1.zero(); tv2.zero();
-    while (__any_sync(0xffffffffu, !sc.done)) {
-      int nbuf = sc.fill(s, P, xi, xfi, p, col);
-      int nmax = __reduce_max_sync(0xffffffffu, (unsigned)nbuf);
-      for (int k = 0; k < nmax; ++k) {
-        if (k >= nbuf) continue;
-        float d0, d1, d2;
-        int q = separation_f32<DIM>(s, P, col[k * kBlock], xfi, ci, cj, ck, d0, d1, d2);
-        float rr = d0 * d0 + d1 * d1 + d2 * d2;
-        float PK1, PK2, PK3;
-        kernel_values_f32(fc, rr, PK1, PK2, PK3);
-        float4 vj = P.VF[q];
-        float4 rfj = P.RF[q];
-        float mj = rfj.z;
-        // pressure (both accumulators of inter_EqMoto together)
-        float pf = -(mj * (Pi + rfj.y) * PK3);
-        tp0.add(pf * d0);
-        if (DIM == 3) tp1.add(pf * d1);
-        tp2.add(pf * d2);
-        float dv0 = vj.x - vix, dv1 = vj.y - viy, dv2 = vj.z - viz;
-        float rsum = rhof + rfj.x;
-        // viscomon
-        float vr = -(dv0 * d0 + dv1 * d1 + dv2 * d2);
-        float df = mj * __fdividef(fc.amon, rsum) * vr * PK2;
-        td0.add(df * d0);
-        if (DIM == 3) td1.add(df * d1);
-        td2.add(df * d2);
-        // viscomorris
-        if (morris) {
-          float vf = -(__fdividef(mj * fc.nu4, fmaf(fc.nu, rsum, 1.0e-3f)) * PK2 * rr);
-          tv0.add(vf * dv0);
-          if (DIM == 3) tv1.add(vf * dv1);
-          tv2.add(vf * dv2);
-        }
+    const size_t lb = list_base(p, b.list_cap);
+    const int nmax = __reduce_max_sync(0xffffffffu, (unsigned)cnt);
+    for (int k = 0; k < nmax; ++k) {
+      if (k >= cnt) continue;
+      float d0, d1, d2;
+      int q = separation_f32<DIM>(s, P, b.nlist[lb + (size_t)k * 32], xfi, ci, cj, ck, d0, d1, d2);
+      float rr = d0 * d0 + d1 * d1 + d2 * d2;
+      float PK1, PK2, PK3;
+      kernel_values_f32(fc, rr, PK1, PK2, PK3);
+      float4 vj = P.VF[q];
+      float4 rfj = P.RF[q];
+      float mj = rfj.z;
+      // pressure (both accumulators of inter_EqMoto together)
+      float pf = -(mj * (Pi + rfj.y) * PK3);
+      tp0.add(pf * d0);
+      if (DIM == 3) tp1.add(pf * d1);
+      tp2.add(pf * d2);
+      float dv0 = vj.x - vix, dv1 = vj.y - viy, dv2 = vj.z - viz;
+      float rsum = rhof + rfj.x;
+      // viscomon
+      float vr = -(dv0 * d0 + dv1 * d1 + dv2 * d2);
+      float df = mj * __fdividef(fc.amon, rsum) * vr * PK2;
+      td0.add(df * d0);
+      if (DIM == 3) td1.add(df * d1);
+      td2.add(df * d2);
+      // viscomorris
+      if (morris) {
+        float vf = -(__fdividef(mj * fc.nu4, fmaf(fc.nu, rsum, 1.0e-3f)) * PK2 * rr);
+        tv0.add(vf * dv0);
+        if (DIM == 3) tv1.add(vf * dv1);
+        tv2.add(vf * dv2);
       }
     }
     double dtc = 1.0e300;
     if (active) {
-      if (sc.trunc) atomicOr(&dyn->warnings, SPH_WARN_NEIGHBOURS_TRUNCATED);
       double rs0 = tv0.val(), rs1 = tv1.val(), rs2 = tv2.val();
       tpres[0] = tpres[0] + tp0.val();
       tpres[1] = tpres[1] + tp1.val();
@@ -1576,7 +1586,6 @@ __global__ void __launch_bounds__(kBlock, 3) k_momentum_f32(DevBatch b) {
         P.L[p] = (uint8_t)lam_new;
       }
     }
-    block_count2(b.counters, sc.cand, sc.nacc);
     if (FUSED) {
       double m = warp_min(dtc);
       if ((threadIdx.x & 31) == 0 && m < 1.0e300)
@@ -1588,10 +1597,8 @@ __global__ void __launch_bounds__(kBlock, 3) k_momentum_f32(DevBatch b) {
 template <int DIM, bool FUSED>
 __global__ void __launch_bounds__(kBlock, 3) k_continuity_f32(DevBatch b) {
   __shared__ SimDev s;
-  __shared__ int sbuf[(kBuf + 1) * kBlock];
   int cur = -1;
   const Particles& P = b.P;
-  int* col = sbuf + threadIdx.x;
   for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
     Tile tl = b.tiles[t];
     load_sim(s, b.sims, tl.sim, cur);
@@ -1603,86 +1610,35 @@ __global__ void __launch_bounds__(kBlock, 3) k_continuity_f32(DevBatch b) {
     double4 xi = make_double4(0.0, 0.0, 0.0, 0.0);
     double4 vi = make_double4(0.0, 0.0, 0.0, 0.0);
     double rhoi = 1.0, dden = 0.0;
-    int ci = 0, cj = 0, ck = 0;
-    bool in_grid = false;
+    int ci = 0, cj = 0, ck = 0, cnt = 0;
     if (active) {
       xi = P.X[p];
       vi = P.V[p];
       rhoi = P.RP[p].x;
+      cnt = b.ncount[p];
       int nb = P.bdt_count[p];
-      if (nb > 0) {
-        int bstart = P.bdt_start[p];
-        double gu0 = 0, gv1 = 0, gw2 = 0;
-        if (DIM == 3) {
-          double gu[3] = {0, 0, 0}, gv[3] = {0, 0, 0}, gw[3] = {0, 0, 0};
-          const double var[3] = {vi.x, vi.y, vi.z};
-          for (int u = 0; u < nb; ++u) {
-            const BdtEntry& e = P.bdt[bstart + u];
-            const FaceDev& f = b.faces[s.face_off + e.clobonum - 1];
-            if (!(e.loc[2] > 0.0)) continue;
-            double dp = 0.0;
-            for (int d = 0; d < 3; ++d) dp = dp + (2.0 * (f.velocity[d] - var[d])) * f.T[d][2];
-            double dvel[3] = {dp * f.T[0][2], dp * f.T[1][2], dp * f.T[2][2]};
-            for (int i = 0; i < 3; ++i) {
-              double a = 0.0;
-              for (int k = 0; k < 3; ++k) a = a + f.T[i][k] * e.bi[3 + k];
-              gu[i] = gu[i] - dvel[0] * a;
-              gv[i] = gv[i] - dvel[1] * a;
-              gw[i] = gw[i] - dvel[2] * a;
-            }
-          }
-          gu0 = gu[0];
-          gv1 = gv[1];
-          gw2 = gw[2];
-          atomicMax(&dyn->ncbf_max, nb);
-        } else {
-          double gu_x = 0.0, gw_z = 0.0;
-          for (int u = 0; u < nb; ++u) {
-            const BdtEntry& e = P.bdt[bstart + u];
-            const SideDev& S = b.sides[s.side_off + e.clobonum - 1];
-            double dvel0, dvel1;
-            if (S.zone_type == SPH_ZONE_TAPI) {
-              dvel0 = 2.0 * (S.velocity[0] - vi.x);
-              dvel1 = 2.0 * (S.velocity[2] - vi.z);
-            } else {
-              dvel0 = 2.0 * (-vi.x);
-              dvel1 = 2.0 * (-vi.z);
-            }
-            gu_x = gu_x - dvel0 * S.nnn[0] * e.bi[0];
-            gw_z = gw_z - dvel1 * S.nnn[1] * e.bi[0];
-          }
-          gu0 = gu_x;
-          gw2 = gw_z;
-        }
-        dden = dden - rhoi * (gu0 + gv1 + gw2);
-      }
-      in_grid = particle_cell(s, xi.x, xi.y, xi.z, ci, cj, ck);
-      if (!in_grid) set_status(dyn, SPH_ERR_INVALID_ARGUMENT);
+      if (nb > 0) dden = continuity_boundary<DIM>(s, b, dyn, nb, P.bdt_start[p], vi, rhoi);
+      particle_cell(s, xi.x, xi.y, xi.z, ci, cj, ck);
     }
-    NeighbourScan<DIM> sc;
-    sc.init(active && in_grid, ci, cj, ck);
     float4 xfi = active ? P.XF[p] : make_float4(0.f, 0.f, 0.f, 0.f);
     const float vix = (float)vi.x, viy = (float)vi.y, viz = (float)vi.z;
     const float rhof = (float)rhoi;
     Kahan sum;
     sum.zero();
-    while (__any_sync(0xffffffffu, !sc.done)) {
-      int nbuf = sc.fill(s, P, xi, xfi, p, col);
-      int nmax = __reduce_max_sync(0xffffffffu, (unsigned)nbuf);
-      for (int k = 0; k < nmax; ++k) {
-        if (k >= nbuf) continue;
-        float d0, d1, d2;
-        int q = separation_f32<DIM>(s, P, col[k * kBlock], xfi, ci, cj, ck, d0, d1, d2);
-        float rr = d0 * d0 + d1 * d1 + d2 * d2;
-        float PK1, PK2, PK3;
-        kernel_values_f32(fc, rr, PK1, PK2, PK3);
-        float4 vj = P.VF[q];
-        float c = rhof * vj.w * PK1;    // rho_i (m_j / rho_j) PK1
-        sum.add(c * ((vj.x - vix) * d0 + (vj.y - viy) * d1 + (vj.z - viz) * d2));
-      }
+    const size_t lb = list_base(p, b.list_cap);
+    const int nmax = __reduce_max_sync(0xffffffffu, (unsigned)cnt);
+    for (int k = 0; k < nmax; ++k) {
+      if (k >= cnt) continue;
+      float d0, d1, d2;
+      int q = separation_f32<DIM>(s, P, b.nlist[lb + (size_t)k * 32], xfi, ci, cj, ck, d0, d1, d2);
+      float rr = d0 * d0 + d1 * d1 + d2 * d2;
+      float PK1, PK2, PK3;
+      kernel_values_f32(fc, rr, PK1, PK2, PK3);
+      float4 vj = P.VF[q];
+      float c = rhof * vj.w * PK1;    // rho_i (m_j / rho_j) PK1
+      sum.add(c * ((vj.x - vix) * d0 + (vj.y - viy) * d1 + (vj.z - viz) * d2));
     }
     if (active) {
-      if (sc.trunc) atomicOr(&dyn->warnings, SPH_WARN_NEIGHBOURS_TRUNCATED);
       dden = dden - sum.val();
       if (FUSED) {
         double rho = rhoi + dyn->dt * dden;
@@ -1697,9 +1653,6 @@ __global__ void __launch_bounds__(kBlock, 3) k_continuity_f32(DevBatch b) {
         P.DDEN[p] = dden;
       }
     }
-    block_count2(b.counters + 2, sc.cand, sc.nacc);
-    int m = warp_max(sc.nacc);
-    if ((threadIdx.x & 31) == 0 && m > 0) atomicMax(&dyn->max_neigh, m);
   }
 }
 
@@ -2121,6 +2074,11 @@ void launch_momentum(const DevBatch& b, bool fused, cudaStream_t st) {
     if (fused) k_momentum<2, true><<<g, kBlock, 0, st>>>(b);
     else k_momentum<2, false><<<g, kBlock, 0, st>>>(b);
   }
+}
+
+void launch_neighbour_lists(const DevBatch& b, cudaStream_t st) {
+  if (b.dim == 3) k_neighbour_lists<3><<<blocks_for(b), kBlock, 0, st>>>(b);
+  else k_neighbour_lists<2><<<blocks_for(b), kBlock, 0, st>>>(b);
 }
 
 void launch_momentum_f32(const DevBatch& b, bool fused, cudaStream_t st) {

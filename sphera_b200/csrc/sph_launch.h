@@ -20,6 +20,9 @@ struct DevBatch {
   const int* cf_count;     // per global cell: faces cutting the cell
   const int* cf_list;      // face ids (1-based within the simulation)
   const uint8_t* cell_near;  // per global cell: faces cut the 27-cell block
+  int* nlist;              // neighbour lists (see k_neighbour_lists)
+  int* ncount;             // entries per particle
+  int list_cap;            // entries reserved per particle (max NMAXPARTJ)
   unsigned long long* counters;  // [0] momentum candidates, [1] momentum pairs,
                                  // [2] continuity candidates, [3] continuity pairs
   int* scan_block_sums;    // scan scratch
@@ -39,6 +42,8 @@ void upload_bit2d(const double* tab, cudaStream_t st);
 void launch_place(const DevBatch& b, cudaStream_t st);
 void launch_rank_permute(const DevBatch& b, cudaStream_t st);
 void launch_rank_reference(const DevBatch& b, const int* cell_start_ref, int* npartord, cudaStream_t st);
+// neighbour lists (CalcVarLength replacement)
+void launch_neighbour_lists(const DevBatch& b, cudaStream_t st);
 // physics (FP64)
 void launch_boundary(const DevBatch& b, cudaStream_t st);
 void launch_momentum(const DevBatch& b, bool fused, cudaStream_t st);
