@@ -688,6 +688,7 @@ int create_batch(int nsims, const SphParams* params, const SphGeometry* geoms, c
   A(h->d_scan, nb);
   A(h->d_counters, 4);
   for (int s = 0; s < nsims; ++s) h->list_cap = std::max(h->list_cap, h->sims[s].dev.nmaxpartj);
+  h->list_cap = (h->list_cap + 3) / 4 * 4;
   A(h->d_nlist, N * (size_t)h->list_cap);
   A(h->d_ncount, N);
 #undef A
@@ -765,7 +766,7 @@ int create_batch(int nsims, const SphParams* params, const SphGeometry* geoms, c
   b.counters = h->d_counters;
   b.nlist = h->d_nlist;
   b.ncount = h->d_ncount;
-  b.list_cap = h->list_cap;
+  b.list_cap4 = h->list_cap / 4;
   b.scan_nblocks = nb;
   b.grid_blocks = prop.multiProcessorCount * 8;
   *out = h;

@@ -992,9 +992,29 @@ __device__ __forceinline__ void elastic_reaction(const SimDev& s, const DevBatch
 constexpr int kSlotBits = 28;
 constexpr int kSlotMask = (1 << kSlotBits) - 1;
 
-__device__ __forceinline__ size_t list_base(int p, int cap) {
-  return (size_t)(p >> 5) * (size_t)cap * 32 + (size_t)(p & 31);
+// Entries are stored as 16-byte chunks of 4: chunk c of particle p sits at
+// int4 index ((p / 32) * cap4 + c) * 32 + p % 32, so a warp reading chunk c
+// of its 32 particles reads 512 contiguous bytes.
+__device__ __forceinline__ size_t list_base4(int p, int cap4) {
+  return (size_t)(p >> 5) * (size_t)cap4 * 32 + (size_t)(p & 31);
 }
+
+// Sequential reader of one particle's list.
+struct ListReader {
+  const int4* base;
+  int4 cur;
+  __device__ __forceinline__ void init(const int* nlist, int p, int cap4) {
+    base = reinterpret_cast<const int4*>(nlist) + list_base4(p, cap4);
+  }
+  __device__ __forceinline__ int get(int k) {
+    if ((k & 3) == 0) cur = __ldg(base + (size_t)(k >> 2) * 32);
+    int e = cur.x;
+    cur.x = cur.y;
+    cur.y = cur.z;
+    cur.z = cur.w;
+    return e;
+  }
+};
 
 // r^2 <= (2h)^2 (CalcVarLength.f90:223-228) decided on the FP32 screening
 // copies outside [rr_lo, rr_hi] (a band the host derives from the copies'
@@ -1039,9 +1059,10 @@ __global__ void __launch_bounds__(kBlock) k_neighbour_lists(DevBatch b) {
     int colkey = on ? (cj * s.ncd[0] + ci) : -1;
     unsigned remaining = __ballot_sync(FULL, on);
     int cnt = 0, nacc = 0, cand = 0;
-    bool trunc = false, done = !on;
+    bool trunc = false;
     const int cap = s.nmaxpartj;
-    size_t lb = list_base(p, b.list_cap);
+    int4* out = reinterpret_cast<int4*>(b.nlist) + list_base4(p, b.list_cap4);
+    int4 pend = make_int4(0, 0, 0, 0);   // entries not yet written, oldest in x
     while (remaining) {
       int leader = __ffs(remaining) - 1;
       int key = __shfl_sync(FULL, colkey, leader);
@@ -1063,40 +1084,65 @@ __global__ void __launch_bounds__(kBlock) k_neighbour_lists(DevBatch b) {
         int ue = __ldg(P.cell_start + base + khi);
         float Dx = (float)(gci - ir) * s.dcdf[0];
         float Dy = (DIM == 3) ? (float)(gcj - jr) * s.dcdf[1] : 0.f;
+        float ax = Dx + xf.x, ay = Dy + xf.y;
         const int tag = r << kSlotBits;
         for (int c0 = ub; c0 < ue; c0 += 32) {
           int cidx = c0 + lane;
           __syncwarp();
           wbuf[lane] = (cidx < ue) ? P.XF[cidx] : make_float4(0.f, 0.f, 0.f, __int_as_float(-0x3fffffff));
           __syncwarp();
+          if (!mine) continue;
           int nt = ue - c0 < 32 ? ue - c0 : 32;
-          if (mine && !done) {
-            for (int u = 0; u < nt; ++u) {
-              float4 xj = wbuf[u];
-              int kj = __float_as_int(xj.w);
-              if (kj < ck - 1 || kj > ck + 1) continue;
-              cand++;
-              if (nacc >= cap) {
-                trunc = true;
-                done = true;
-                break;
-              }
-              float Dz = (float)(ck - kj) * s.dcdf[2];
-              float d0 = Dx + (xf.x - xj.x);
-              float d1 = (DIM == 3) ? Dy + (xf.y - xj.y) : 0.f;
-              float d2 = Dz + (xf.z - xj.z);
-              int q = c0 + u;
-              if (accept_pair(s, P, xd, d0, d1, d2, q)) {
-                nacc++;
-                if (q != p) {
-                  b.nlist[lb + (size_t)cnt * 32] = q | tag;
-                  cnt++;
-                }
+          for (int u = 0; u < nt; ++u) {
+            float4 xj = wbuf[u];
+            int kj = __float_as_int(xj.w);
+            float Dz = (float)(ck - kj) * s.dcdf[2];
+            float d0 = ax - xj.x;
+            float d1 = (DIM == 3) ? ay - xj.y : 0.f;
+            float d2 = (Dz + xf.z) - xj.z;
+            float rf = d0 * d0 + d1 * d1 + d2 * d2;
+            bool inwin = (unsigned)(kj - (ck - 1)) <= 2u;
+            if (!inwin || rf > s.rr_hi) {
+              cand += inwin ? 1 : 0;
+              if (inwin && nacc >= cap) trunc = true;
+              continue;
+            }
+            cand++;
+            if (nacc >= cap) {
+              trunc = true;
+              continue;
+            }
+            int q = c0 + u;
+            bool acc = rf < s.rr_lo;
+            if (!acc) {
+              double4 xq = P.X[q];
+              double r0 = xd.x - xq.x, r1 = xd.y - xq.y, r2 = xd.z - xq.z;
+              double rr = r0 * r0 + r1 * r1 + r2 * r2;
+              acc = !(rr > s.square_doubleh);
+            }
+            if (acc) {
+              nacc++;
+              if (q != p) {
+                pend.x = pend.y;
+                pend.y = pend.z;
+                pend.z = pend.w;
+                pend.w = q | tag;
+                cnt++;
+                if ((cnt & 3) == 0) out[(size_t)((cnt >> 2) - 1) * 32] = pend;
               }
             }
           }
         }
       }
+    }
+    if (cnt & 3) {
+      // flush the last partial chunk, entries moved to its front
+      int rem = cnt & 3;
+      int4 w = pend;
+      if (rem == 1) w = make_int4(pend.w, 0, 0, 0);
+      else if (rem == 2) w = make_int4(pend.z, pend.w, 0, 0);
+      else w = make_int4(pend.y, pend.z, pend.w, 0);
+      out[(size_t)(cnt >> 2) * 32] = w;
     }
     if (active) {
       b.ncount[p] = cnt;
@@ -1168,11 +1214,13 @@ __global__ void __launch_bounds__(kBlock, 2) k_momentum(DevBatch b) {
     const double celt = s.celerita + s.celerita;
     const bool morris = s.kin_visc > 1.0e-12;
     const double nu = s.kin_visc;
-    const size_t lb = list_base(p, b.list_cap);
+    ListReader lr;
+    lr.init(b.nlist, p, b.list_cap4);
     const int nmax = __reduce_max_sync(0xffffffffu, (unsigned)cnt);
     for (int k = 0; k < nmax; ++k) {
+      int e = lr.get(k);
       if (k >= cnt) continue;
-      int q = b.nlist[lb + (size_t)k * 32] & kSlotMask;
+      int q = e & kSlotMask;
       double4 xj = P.X[q];
       double r0 = xi.x - xj.x, r1 = xi.y - xj.y, r2 = xi.z - xj.z;
       double rr = r0 * r0 + r1 * r1 + r2 * r2;
@@ -1349,11 +1397,13 @@ __global__ void __launch_bounds__(kBlock, 2) k_continuity(DevBatch b) {
       if (nb > 0) dden = continuity_boundary<DIM>(s, b, dyn, nb, P.bdt_start[p], vi, rhoi);
     }
     double a1 = 0.0, a2 = 0.0, a3 = 0.0;
-    const size_t lb = list_base(p, b.list_cap);
+    ListReader lr;
+    lr.init(b.nlist, p, b.list_cap4);
     const int nmax = __reduce_max_sync(0xffffffffu, (unsigned)cnt);
     for (int k = 0; k < nmax; ++k) {
+      int e = lr.get(k);
       if (k >= cnt) continue;
-      int q = b.nlist[lb + (size_t)k * 32] & kSlotMask;
+      int q = e & kSlotMask;
       double4 xj = P.X[q];
       double r0 = xi.x - xj.x, r1 = xi.y - xj.y, r2 = xi.z - xj.z;
       double rr = r0 * r0 + r1 * r1 + r2 * r2;
@@ -1514,12 +1564,14 @@ __global__ void __launch_bounds__(kBlock, 3) k_momentum_f32(DevBatch b) {
     const bool morris = s.kin_visc > 1.0e-12;
     Kahan tp0, tp1, tp2, td0, td1, td2, tv0, tv1, tv2;
     tp0.zero(); tp1.zero(); tp2.zero(); td0.zero(); td1.zero(); td2.zero(); tv0.zero(); tv1.zero(); tv2.zero();
-    const size_t lb = list_base(p, b.list_cap);
+    ListReader lr;
+    lr.init(b.nlist, p, b.list_cap4);
     const int nmax = __reduce_max_sync(0xffffffffu, (unsigned)cnt);
     for (int k = 0; k < nmax; ++k) {
+      int e = lr.get(k);
       if (k >= cnt) continue;
       float d0, d1, d2;
-      int q = separation_f32<DIM>(s, P, b.nlist[lb + (size_t)k * 32], xfi, ci, cj, ck, d0, d1, d2);
+      int q = separation_f32<DIM>(s, P, e, xfi, ci, cj, ck, d0, d1, d2);
       float rr = d0 * d0 + d1 * d1 + d2 * d2;
       float PK1, PK2, PK3;
       kernel_values_f32(fc, rr, PK1, PK2, PK3);
@@ -1625,12 +1677,14 @@ __global__ void __launch_bounds__(kBlock, 3) k_continuity_f32(DevBatch b) {
     const float rhof = (float)rhoi;
     Kahan sum;
     sum.zero();
-    const size_t lb = list_base(p, b.list_cap);
+    ListReader lr;
+    lr.init(b.nlist, p, b.list_cap4);
     const int nmax = __reduce_max_sync(0xffffffffu, (unsigned)cnt);
     for (int k = 0; k < nmax; ++k) {
+      int e = lr.get(k);
       if (k >= cnt) continue;
       float d0, d1, d2;
-      int q = separation_f32<DIM>(s, P, b.nlist[lb + (size_t)k * 32], xfi, ci, cj, ck, d0, d1, d2);
+      int q = separation_f32<DIM>(s, P, e, xfi, ci, cj, ck, d0, d1, d2);
       float rr = d0 * d0 + d1 * d1 + d2 * d2;
       float PK1, PK2, PK3;
       kernel_values_f32(fc, rr, PK1, PK2, PK3);

@@ -22,7 +22,7 @@ struct DevBatch {
   const uint8_t* cell_near;  // per global cell: faces cut the 27-cell block
   int* nlist;              // neighbour lists (see k_neighbour_lists)
   int* ncount;             // entries per particle
-  int list_cap;            // entries reserved per particle (max NMAXPARTJ)
+  int list_cap4;           // 4-entry chunks reserved per particle (max NMAXPARTJ / 4)
   unsigned long long* counters;  // [0] momentum candidates, [1] momentum pairs,
                                  // [2] continuity candidates, [3] continuity pairs
   int* scan_block_sums;    // scan scratch
