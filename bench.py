@@ -36,7 +36,7 @@ import numpy as np  # noqa: E402
 
 METRIC = "particle-steps/s FP32c vs FP64 at ≤1e-3 rel L2; ensemble p50/p99 time-to-result"
 UNIT = "particle-steps/s"
-KERNELS_PER_STEP = 14          # sph_api.cu step_sequence: momentum, 8 sort, 2 boundary, lists, continuity, finalize
+KERNELS_PER_STEP = 15          # sph_api.cu step_sequence (3D): momentum, 8 sort, 3 boundary, lists, continuity, finalize
 # algorithmic bytes of the fused momentum kernel per particle: reads X 32,
 # V 32, RP 16, L 1, bdt_count 4, I 4; writes X2 32, V2 32, P2 8, I2 4, L2 1
 MOM_BYTES_PER_PARTICLE = 166

@@ -581,7 +581,6 @@ __global__ void __launch_bounds__(kBlock) k_boundary3d(DevBatch b) {
     atomicMax(&dyn->ncbf_max, ncbf);
     P.bdt_count[p] = ncbf;
     P.bdt_start[p] = gbase;
-    const double* bit = b.bit + (size_t)tl.sim * kBitRows * 7;
     for (int u = 0; u < ncbf; ++u) {
       const FaceDev& f = b.faces[s.face_off + clob[u] - 1];
       double locx[3];
@@ -593,15 +592,32 @@ __global__ void __launch_bounds__(kBlock) k_boundary3d(DevBatch b) {
         locx[sdi] = acc;
       }
       locx[2] = pin[u];
-      BdtEntry e;
-      face_integrals(s, bit, f, locx, e);
+      BdtEntry& e = P.bdt[gbase + u];
       e.loc[0] = locx[0];
       e.loc[1] = locx[1];
       e.loc[2] = locx[2];
       e.clobonum = clob[u];
-      e.pad = 0;
-      P.bdt[gbase + u] = e;
+      e.pad = tl.sim;            // the integrals pass needs the simulation
     }
+  }
+}
+
+// ComputeBoundaryVolumeIntegrals_P0.f90:81-155 for every entry the find
+// pass allocated, one (particle, face) per thread: the quadrature costs are
+// balanced across the GPU whatever the particles' distribution over tiles.
+__global__ void __launch_bounds__(128) k_boundary3d_integrals(DevBatch b) {
+  int used = b.dyn[b.nsims].bdt_used;
+  if (used > b.P.bdt_cap) used = b.P.bdt_cap;
+  for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < used; idx += gridDim.x * blockDim.x) {
+    BdtEntry& e = b.P.bdt[idx];
+    int sim = e.pad;
+    const SimDev& s = b.sims[sim];
+    const FaceDev& f = b.faces[s.face_off + e.clobonum - 1];
+    double locx[3] = {e.loc[0], e.loc[1], e.loc[2]};
+    BdtEntry r;
+    face_integrals(s, b.bit + (size_t)sim * kBitRows * 7, f, locx, r);
+    for (int q = 0; q < 8; ++q) e.bi[q] = r.bi[q];
+    for (int q = 0; q < 9; ++q) e.ig[q] = r.ig[q];
   }
 }
 
@@ -2115,8 +2131,12 @@ void launch_rank_reference(const DevBatch& b, const int* cell_start_ref, int* np
 
 void launch_boundary(const DevBatch& b, cudaStream_t st) {
   k_bdt_reset<<<(b.nsims + 127) / 128, 128, 0, st>>>(b);
-  if (b.dim == 3) k_boundary3d<<<blocks_for(b), kBlock, 0, st>>>(b);
-  else k_boundary2d<<<blocks_for(b), kBlock, 0, st>>>(b);
+  if (b.dim == 3) {
+    k_boundary3d<<<blocks_for(b), kBlock, 0, st>>>(b);
+    k_boundary3d_integrals<<<b.grid_blocks * 2, 128, 0, st>>>(b);
+  } else {
+    k_boundary2d<<<blocks_for(b), kBlock, 0, st>>>(b);
+  }
 }
 
 void launch_momentum(const DevBatch& b, bool fused, cudaStream_t st) {
