@@ -1525,7 +1525,7 @@ __device__ __forceinline__ int separation_f32(const SimDev& s, const Particles& 
 }
 
 template <int DIM, bool FUSED>
-__global__ void __launch_bounds__(kBlock, 3) k_momentum_f32(DevBatch b) {
+__global__ void __launch_bounds__(kBlock, 2) k_momentum_f32(DevBatch b) {
   __shared__ SimDev s;
   int cur = -1;
   const Particles& P = b.P;
@@ -1578,8 +1578,10 @@ __global__ void __launch_bounds__(kBlock, 3) k_momentum_f32(DevBatch b) {
     const float rhof = (float)rhoi;
     const float Pi = (float)(pi / (rhoi * rhoi));
     const bool morris = s.kin_visc > 1.0e-12;
+    // compensated sums of 4-entry partial sums (one list chunk each)
     Kahan tp0, tp1, tp2, td0, td1, td2, tv0, tv1, tv2;
     tp0.zero(); tp1.zero(); tp2.zero(); td0.zero(); td1.zero(); td2.zero(); tv0.zero(); tv1.zero(); tv2.zero();
+    float cp0 = 0.f, cp1 = 0.f, cp2 = 0.f, cd0 = 0.f, cd1 = 0.f, cd2 = 0.f, cv0 = 0.f, cv1 = 0.f, cv2 = 0.f;
     ListReader lr;
     lr.init(b.nlist, p, b.list_cap4);
     const int nmax = __reduce_max_sync(0xffffffffu, (unsigned)cnt);
@@ -1596,23 +1598,29 @@ __global__ void __launch_bounds__(kBlock, 3) k_momentum_f32(DevBatch b) {
       float mj = rfj.z;
       // pressure (both accumulators of inter_EqMoto together)
       float pf = -(mj * (Pi + rfj.y) * PK3);
-      tp0.add(pf * d0);
-      if (DIM == 3) tp1.add(pf * d1);
-      tp2.add(pf * d2);
+      cp0 += pf * d0;
+      if (DIM == 3) cp1 += pf * d1;
+      cp2 += pf * d2;
       float dv0 = vj.x - vix, dv1 = vj.y - viy, dv2 = vj.z - viz;
       float rsum = rhof + rfj.x;
       // viscomon
       float vr = -(dv0 * d0 + dv1 * d1 + dv2 * d2);
       float df = mj * __fdividef(fc.amon, rsum) * vr * PK2;
-      td0.add(df * d0);
-      if (DIM == 3) td1.add(df * d1);
-      td2.add(df * d2);
+      cd0 += df * d0;
+      if (DIM == 3) cd1 += df * d1;
+      cd2 += df * d2;
       // viscomorris
       if (morris) {
         float vf = -(__fdividef(mj * fc.nu4, fmaf(fc.nu, rsum, 1.0e-3f)) * PK2 * rr);
-        tv0.add(vf * dv0);
-        if (DIM == 3) tv1.add(vf * dv1);
-        tv2.add(vf * dv2);
+        cv0 += vf * dv0;
+        if (DIM == 3) cv1 += vf * dv1;
+        cv2 += vf * dv2;
+      }
+      if ((k & 3) == 3 || k == cnt - 1) {
+        tp0.add(cp0); tp1.add(cp1); tp2.add(cp2);
+        td0.add(cd0); td1.add(cd1); td2.add(cd2);
+        tv0.add(cv0); tv1.add(cv1); tv2.add(cv2);
+        cp0 = cp1 = cp2 = cd0 = cd1 = cd2 = cv0 = cv1 = cv2 = 0.f;
       }
     }
     double dtc = 1.0e300;
@@ -1693,6 +1701,7 @@ __global__ void __launch_bounds__(kBlock, 3) k_continuity_f32(DevBatch b) {
     const float rhof = (float)rhoi;
     Kahan sum;
     sum.zero();
+    float part = 0.f;   // 4-entry partial sum, compensated into sum per chunk
     ListReader lr;
     lr.init(b.nlist, p, b.list_cap4);
     const int nmax = __reduce_max_sync(0xffffffffu, (unsigned)cnt);
@@ -1706,7 +1715,11 @@ __global__ void __launch_bounds__(kBlock, 3) k_continuity_f32(DevBatch b) {
       kernel_values_f32(fc, rr, PK1, PK2, PK3);
       float4 vj = P.VF[q];
       float c = rhof * vj.w * PK1;    // rho_i (m_j / rho_j) PK1
-      sum.add(c * ((vj.x - vix) * d0 + (vj.y - viy) * d1 + (vj.z - viz) * d2));
+      part += c * ((vj.x - vix) * d0 + (vj.y - viy) * d1 + (vj.z - viz) * d2);
+      if ((k & 3) == 3 || k == cnt - 1) {
+        sum.add(part);
+        part = 0.f;
+      }
     }
     if (active) {
       dden = dden - sum.val();
