@@ -198,6 +198,16 @@ int  sph_batch_download(SphHandle* h, int32_t sim, SphState* state);
  * stays on the device for download while the others continue.             */
 int  sph_batch_set_end_time(SphHandle* h, int32_t sim, double t_end);
 int  sph_batch_info(SphHandle* h, int32_t sim, SphStepInfo* info, int32_t* frozen);
+/* Every simulation's frozen flag, time and completed steps ([nsims] each,
+ * any may be NULL) from one read-back of the device state.                */
+int  sph_batch_status(SphHandle* h, int32_t* frozen, double* time, int32_t* steps);
+
+/* Autotuner (no reference counterpart): sizes the persistent grid of the
+ * neighbour-list, momentum, continuity and boundary kernels on the live
+ * state by timing `reps` launches of each candidate (1 to 32 blocks per
+ * SM) of variants that leave the state unchanged, then rebuilds the step
+ * graph.  grid_out[0..4] (may be NULL) receives the chosen blocks.        */
+int  sph_autotune(SphHandle* h, int32_t reps, int32_t* grid_out);
 
 /* ---------------------------------------------------------------------- */
 /* Fine-grained calls, one per replaced Fortran call site                  */

@@ -75,6 +75,8 @@ def lib():
         "sph_get_counters": ([vp, C.POINTER(C.c_uint64), C.c_int32], C.c_int),
         "sph_measure_fp64_peak": ([dp], C.c_int),
         "sph_measure_fma_peak": ([C.c_int32, dp], C.c_int),
+        "sph_autotune": ([vp, C.c_int32, ip], C.c_int),
+        "sph_batch_status": ([vp, ip, dp, ip], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -193,6 +195,13 @@ class Simulation:
     def eos(self):
         _chk(lib().sph_eos(self._h), "sph_eos")
 
+    # ------------------------------------------------------------ autotuner
+    def autotune(self, reps=3):
+        """Sizes the persistent grids of the pair, list and boundary kernels."""
+        g = np.zeros(5, np.int32)
+        _chk(lib().sph_autotune(self._h, int(reps), abi.iptr(g)), "sph_autotune")
+        return dict(zip(("lists", "momentum", "continuity", "boundary", "integrals"), g.tolist()))
+
     # ------------------------------------------------------------ profiling
     PHASES = ("momentum", "ord_grid", "boundary_data_tab", "neighbour_lists", "continuity", "time_step")
 
@@ -287,11 +296,25 @@ class Batch:
     def sync(self):
         _chk(lib().sph_sync(self._h), "sph_sync")
 
+    def autotune(self, reps=3):
+        g = np.zeros(5, np.int32)
+        _chk(lib().sph_autotune(self._h, int(reps), abi.iptr(g)), "sph_autotune")
+        return dict(zip(("lists", "momentum", "continuity", "boundary", "integrals"), g.tolist()))
+
     def info(self, sim):
         info = abi.SphStepInfo()
         fr = C.c_int32()
         _chk(lib().sph_batch_info(self._h, int(sim), C.byref(info), C.byref(fr)), "sph_batch_info")
         return info, bool(fr.value)
+
+    def status(self):
+        """(frozen, time, steps) arrays of all simulations, one read-back."""
+        n = len(self.cases)
+        fr = np.zeros(n, np.int32)
+        t = np.zeros(n)
+        st = np.zeros(n, np.int32)
+        _chk(lib().sph_batch_status(self._h, abi.iptr(fr), abi.dptr(t), abi.iptr(st)), "sph_batch_status")
+        return fr.astype(bool), t, st
 
     def download(self, sim):
         n = self.cases[sim].n

@@ -769,6 +769,8 @@ int create_batch(int nsims, const SphParams* params, const SphGeometry* geoms, c
   b.list_cap4 = h->list_cap / 4;
   b.scan_nblocks = nb;
   b.grid_blocks = prop.multiProcessorCount * 8;
+  b.sms = prop.multiProcessorCount;
+  for (int c = 0; c < kGridClasses; ++c) b.grid[c] = 0;
   *out = h;
   return SPH_OK;
 }
@@ -927,6 +929,18 @@ int sph_batch_info(SphHandle* h, int32_t sim, SphStepInfo* info, int32_t* frozen
 
 void* sph_stream(SphHandle* h) { return h ? (void*)h->stream : nullptr; }
 
+// All simulations' progress in one read-back: frozen flag, time and steps.
+int sph_batch_status(SphHandle* h, int32_t* frozen, double* time, int32_t* steps) {
+  if (!h) return SPH_ERR_INVALID_ARGUMENT;
+  SPH_TRY(sync_dyn(h));
+  for (int s = 0; s < h->nsims; ++s) {
+    if (frozen) frozen[s] = h->h_dyn[s].frozen;
+    if (time) time[s] = h->h_dyn[s].time;
+    if (steps) steps[s] = h->h_dyn[s].step;
+  }
+  return SPH_OK;
+}
+
 int sph_get_diagnostics(SphHandle* h, SphDiagnostics* diag) {
   if (!h || !diag) return SPH_ERR_INVALID_ARGUMENT;
   int st = sync_dyn(h);
@@ -1081,6 +1095,67 @@ int sph_dump_boundary(SphHandle* h, int32_t max_per, int32_t* ncb, int32_t* clob
   cudaFree(dc);
   cudaFree(dv);
   return cuda_status(e);
+}
+
+// ---------------------------------------------------------------- autotuner
+// Sizes the persistent grid of each kernel class on the live state: every
+// candidate (1 to 32 blocks per SM) is timed over `reps` launches of a
+// variant that leaves the state unchanged -- the rate-only momentum and
+// continuity passes (their laminar-flag write is saved and restored), the
+// neighbour-list and boundary passes (idempotent) -- and the fastest kept.
+// The step graph is rebuilt with the choice.  grid_out[0..4] receives the
+// chosen blocks of lists, momentum, continuity, boundary find, integrals.
+int sph_autotune(SphHandle* h, int32_t reps, int32_t* grid_out) {
+  if (!h || !h->uploaded || reps <= 0) return SPH_ERR_INVALID_ARGUMENT;
+  cudaStream_t q = h->stream;
+  DevBatch& b = h->db;
+  const int mult[] = {1, 2, 4, 8, 16, 32};
+  cudaEvent_t e0, e1;
+  if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) { cudaGetLastError(); return SPH_ERR_CUDA; }
+  // the rate-only momentum pass rewrites the laminar flags: keep them
+  SPH_CUDA(cudaMemcpyAsync(b.P.L2, b.P.L, (size_t)h->total_slots, cudaMemcpyDeviceToDevice, q));
+  cudaError_t e = cudaSuccess;
+  for (int cls = 0; cls < kGridClasses && e == cudaSuccess; ++cls) {
+    if (cls == kGridIntegrals && h->dim != 3) continue;
+    float best = 1e30f;
+    int best_g = 0;
+    for (int m : mult) {
+      int g = b.sms * m;
+      b.grid[cls] = g;
+      auto run = [&]() {
+        switch (cls) {
+          case kGridLists: launch_neighbour_lists(b, q); break;
+          case kGridMomentum: momentum_pass(h, false, q); break;
+          case kGridContinuity: continuity_pass(h, false, q); break;
+          default: launch_boundary(b, q); break;
+        }
+      };
+      run();   // warm-up
+      cudaEventRecord(e0, q);
+      for (int r = 0; r < reps; ++r) run();
+      cudaEventRecord(e1, q);
+      e = cudaEventSynchronize(e1);
+      float ms = 0.f;
+      if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+      if (e != cudaSuccess) break;
+      if (ms < best) {
+        best = ms;
+        best_g = g;
+      }
+    }
+    b.grid[cls] = best_g;
+    if (grid_out) grid_out[cls] = best_g;
+  }
+  if (e == cudaSuccess) e = cudaMemcpyAsync(b.P.L, b.P.L2, (size_t)h->total_slots, cudaMemcpyDeviceToDevice, q);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (e != cudaSuccess) return cuda_status(e);
+  if (h->graph) {
+    cudaGraphExecDestroy(h->graph);
+    h->graph = nullptr;
+  }
+  SPH_TRY(sync_dyn(h));
+  return build_graph(h);
 }
 
 // ---------------------------------------------------------------- profiling

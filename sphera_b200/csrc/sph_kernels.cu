@@ -2103,6 +2103,10 @@ double launch_fp64_probe(double* sink, int blocks, cudaStream_t st) {
 // launch wrappers
 // ==========================================================================
 static inline int blocks_for(const DevBatch& b) { return b.ntiles < b.grid_blocks ? b.ntiles : b.grid_blocks; }
+static inline int blocks_for(const DevBatch& b, int cls) {
+  int g = b.grid[cls] > 0 ? b.grid[cls] : b.grid_blocks;
+  return b.ntiles < g ? b.ntiles : g;
+}
 
 void launch_stage(const DevBatch& b, cudaStream_t st) { k_stage<<<blocks_for(b), kBlock, 0, st>>>(b); }
 
@@ -2145,15 +2149,15 @@ void launch_rank_reference(const DevBatch& b, const int* cell_start_ref, int* np
 void launch_boundary(const DevBatch& b, cudaStream_t st) {
   k_bdt_reset<<<(b.nsims + 127) / 128, 128, 0, st>>>(b);
   if (b.dim == 3) {
-    k_boundary3d<<<blocks_for(b), kBlock, 0, st>>>(b);
-    k_boundary3d_integrals<<<b.grid_blocks * 2, 128, 0, st>>>(b);
+    k_boundary3d<<<blocks_for(b, kGridBoundary), kBlock, 0, st>>>(b);
+    k_boundary3d_integrals<<<b.grid[kGridIntegrals] > 0 ? b.grid[kGridIntegrals] : b.grid_blocks * 2, 128, 0, st>>>(b);
   } else {
-    k_boundary2d<<<blocks_for(b), kBlock, 0, st>>>(b);
+    k_boundary2d<<<blocks_for(b, kGridBoundary), kBlock, 0, st>>>(b);
   }
 }
 
 void launch_momentum(const DevBatch& b, bool fused, cudaStream_t st) {
-  int g = blocks_for(b);
+  int g = blocks_for(b, kGridMomentum);
   if (b.dim == 3) {
     if (fused) k_momentum<3, true><<<g, kBlock, 0, st>>>(b);
     else k_momentum<3, false><<<g, kBlock, 0, st>>>(b);
@@ -2164,12 +2168,13 @@ void launch_momentum(const DevBatch& b, bool fused, cudaStream_t st) {
 }
 
 void launch_neighbour_lists(const DevBatch& b, cudaStream_t st) {
-  if (b.dim == 3) k_neighbour_lists<3><<<blocks_for(b), kBlock, 0, st>>>(b);
-  else k_neighbour_lists<2><<<blocks_for(b), kBlock, 0, st>>>(b);
+  int g = blocks_for(b, kGridLists);
+  if (b.dim == 3) k_neighbour_lists<3><<<g, kBlock, 0, st>>>(b);
+  else k_neighbour_lists<2><<<g, kBlock, 0, st>>>(b);
 }
 
 void launch_momentum_f32(const DevBatch& b, bool fused, cudaStream_t st) {
-  int g = blocks_for(b);
+  int g = blocks_for(b, kGridMomentum);
   if (b.dim == 3) {
     if (fused) k_momentum_f32<3, true><<<g, kBlock, 0, st>>>(b);
     else k_momentum_f32<3, false><<<g, kBlock, 0, st>>>(b);
@@ -2180,7 +2185,7 @@ void launch_momentum_f32(const DevBatch& b, bool fused, cudaStream_t st) {
 }
 
 void launch_continuity_f32(const DevBatch& b, bool fused, cudaStream_t st) {
-  int g = blocks_for(b);
+  int g = blocks_for(b, kGridContinuity);
   if (b.dim == 3) {
     if (fused) k_continuity_f32<3, true><<<g, kBlock, 0, st>>>(b);
     else k_continuity_f32<3, false><<<g, kBlock, 0, st>>>(b);
@@ -2193,7 +2198,7 @@ void launch_continuity_f32(const DevBatch& b, bool fused, cudaStream_t st) {
 void launch_refresh_f32(const DevBatch& b, cudaStream_t st) { k_refresh_f32<<<blocks_for(b), kBlock, 0, st>>>(b); }
 
 void launch_continuity(const DevBatch& b, bool fused, cudaStream_t st) {
-  int g = blocks_for(b);
+  int g = blocks_for(b, kGridContinuity);
   if (b.dim == 3) {
     if (fused) k_continuity<3, true><<<g, kBlock, 0, st>>>(b);
     else k_continuity<3, false><<<g, kBlock, 0, st>>>(b);

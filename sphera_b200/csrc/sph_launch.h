@@ -5,6 +5,10 @@
 
 namespace sph {
 
+// Kernel classes whose persistent grid the autotuner sizes.
+enum GridClass { kGridLists = 0, kGridMomentum = 1, kGridContinuity = 2, kGridBoundary = 3, kGridIntegrals = 4,
+                 kGridClasses = 5 };
+
 struct DevBatch {
   const SimDev* sims;      // [nsims]
   SimDyn* dyn;             // [nsims]
@@ -27,7 +31,9 @@ struct DevBatch {
                                  // [2] continuity candidates, [3] continuity pairs
   int* scan_block_sums;    // scan scratch
   int scan_nblocks;
-  int grid_blocks;         // blocks of the persistent particle kernels
+  int grid_blocks;         // blocks of the persistent particle kernels (default)
+  int sms;                 // streaming multiprocessors of the device
+  int grid[kGridClasses];  // autotuned blocks per kernel class (0 = grid_blocks)
 };
 
 enum class KeyKind { Sort = 0, Reference = 1 };
