@@ -639,11 +639,13 @@ int create_batch(int nsims, const SphParams* params, const SphGeometry* geoms, c
     hs.dev.cell_off = coff;
     hs.dev.face_off = foff;
     hs.dev.side_off = soff;
+    // tiles cover the padded segment: every slot, padding included, takes
+    // part in the sort, so each simulation's segment stays in place
     for (int t = 0; t < hs.cap; t += kBlock) {
       Tile tl;
       tl.sim = s;
       tl.start = poff + t;
-      tl.count = std::min(kBlock, hs.cap - t);
+      tl.count = kBlock;
       tl.pad = 0;
       tiles.push_back(tl);
     }
