@@ -73,6 +73,16 @@ def _max_over_ranks(ws, v):
     return float(t.item())
 
 
+def _sum_over_ranks(ws, v):
+    if ws == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons during the timed region."""
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
@@ -242,6 +252,48 @@ def run_ensemble(args, ws, rank):
     return 0
 
 
+def run_serving(args, ws, rank):
+    """A seeded Poisson stream (mean 20 requests/s) of 3D dam-break and
+    sloshing-tank requests (dx log-uniform in [0.005, 0.0125] m, 55k-1M
+    particles, FP32-compensated form, each run to t = 0.3 s) served in real
+    time: admission by HBM budget, grouped batches on their own streams,
+    state resident on the device, each result downloaded when its request
+    finishes.  Reports p50/p99 time-to-result (arrival to result on the
+    host) and the aggregate particle-steps/s over the run's wall time."""
+    import torch
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    from sphera_b200 import abi, cases
+    from sphera_b200.serve import Server, summarize
+    reqs = cases.serving_requests(n_requests=args.requests, rate=20.0, seed=0xC4 + rank, t_end=args.t_end,
+                                  precision=abi.SPH_PREC_FP32C)
+    budget = int(args.hbm_budget_gib * (1 << 30))
+    srv = Server(budget, chunk=32)
+    _barrier(ws)
+    res = srv.run(reqs)
+    summ = summarize(res, srv.wall)
+    wall = _max_over_ranks(ws, srv.wall)
+    total_work = _sum_over_ranks(ws, summ["particle_steps"])
+    d2h = sum(r.n * (3 + 3 + 1 + 1 + 1) * 8 for r in res.values() if not r.rejected)
+    line = {
+        "metric": METRIC, "workload": "serving", "value": total_work / wall, "unit": UNIT,
+        "n_gpus": ws, "higher_is_better": True, "scaling": "weak", "dtype": "fp32c",
+        "config": {"workload": f"{len(reqs)} requests, Poisson 20/s, 3D dam break and sloshing tank "
+                               "(1.0x0.5x0.5 m half filled, A 0.02 m, T U[0.8,1.6] s), dx log-uniform "
+                               f"[0.005,0.0125] m, each to t = {args.t_end} s, FP32c",
+                   "hbm_budget_bytes": budget, "particles": [r.case.n for r in reqs],
+                   "kinds": [r.case.name for r in reqs]},
+        "time_to_result_s": {"p50": summ["p50_s"], "p99": summ["p99_s"],
+                             "mean_queue": summ["mean_queue_s"]},
+        "completed": summ["completed"], "rejected": summ["rejected"],
+        "peak_resident_bytes": srv.peak_used, "groups": srv.groups_formed,
+        "max_concurrent_requests": srv.max_concurrent, "result_d2h_bytes": d2h,
+        "elapsed_s": wall,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -251,14 +303,18 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--cpu-steps", type=int, default=3)
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--workload", default="dam_break_3d", choices=["dam_break_3d", "ensemble"])
+    ap.add_argument("--workload", default="dam_break_3d", choices=["dam_break_3d", "ensemble", "serving"])
     ap.add_argument("--n-sims", type=int, default=256)
-    ap.add_argument("--t-end", type=float, default=0.5)
+    ap.add_argument("--t-end", type=float, default=None)
+    ap.add_argument("--requests", type=int, default=8)
+    ap.add_argument("--hbm-budget-gib", type=float, default=4.0)
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
+    if args.t_end is None:
+        args.t_end = 0.3 if args.workload == "serving" else 0.5
     ws, rank, local = _dist()
-    if args.workload == "ensemble" and args.impl == "ours":
-        rc = run_ensemble(args, ws, rank)
+    if args.workload in ("ensemble", "serving") and args.impl == "ours":
+        rc = (run_ensemble if args.workload == "ensemble" else run_serving)(args, ws, rank)
         if ws > 1:
             import torch.distributed as dist
             dist.destroy_process_group()

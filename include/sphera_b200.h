@@ -86,9 +86,18 @@ typedef struct SphParams {
     double  vsc_coeff;              /* input_any_t%vsc_coeff                          */
     double  pesodt;                 /* pesodt                                         */
     int32_t density_thresholds;     /* input_any_t%density_thresholds (0/1)           */
-    int32_t bdt_capacity;           /* BoundaryDataTab entries to reserve, 0 = n      */
+    int32_t bdt_capacity;           /* BoundaryDataTab entries to reserve,            */
+                                    /* 0 = 3 n (3D) or 2 n (2D)                       */
     double  teta_p;                 /* input_any_t%TetaP (must be 0 on this path)     */
     double  teta_v;                 /* input_any_t%TetaV (must be 0 on this path)     */
+    /* Lateral tank forcing, no reference counterpart: the tank moves as
+     * x = A sin(2 pi t / T) and the fluid, computed in the tank frame, feels
+     * the body force grav + A (2 pi / T)^2 sin(2 pi t / T) along x, with
+     * t the end time of the step being computed (the simulation time when
+     * time_step_loop.f90 calls RHS_momentum_equation).  amplitude 0
+     * disables it.                                                        */
+    double  forcing_amplitude;      /* A [m]                                          */
+    double  forcing_period;         /* T [s]                                          */
 } SphParams;
 
 /* One boundary zone (Tratto). */
@@ -201,6 +210,16 @@ int  sph_batch_info(SphHandle* h, int32_t sim, SphStepInfo* info, int32_t* froze
 /* Every simulation's frozen flag, time and completed steps ([nsims] each,
  * any may be NULL) from one read-back of the device state.                */
 int  sph_batch_status(SphHandle* h, int32_t* frozen, double* time, int32_t* steps);
+
+/* Device memory, in bytes, that sph_batch_create would allocate for these
+ * arguments (sph_create: nsims = 1), computed on the host without touching
+ * the device; the admission test of a server that packs simulations into
+ * an HBM budget (no reference counterpart).                               */
+int  sph_memory_required(int32_t nsims, const SphParams* params, const SphGeometry* geometries,
+                         const int32_t* n_capacity, uint64_t* bytes);
+/* *idle = 1 when all work enqueued on the handle's stream has finished,
+ * 0 while some is still running; never waits.                             */
+int  sph_idle(SphHandle* h, int32_t* idle);
 
 /* Autotuner (no reference counterpart): sizes the persistent grid of the
  * neighbour-list, momentum, continuity and boundary kernels on the live

@@ -62,8 +62,15 @@ def lib():
         L.ora_WIntegr.restype = C.c_double
         L.ora_w.argtypes = [C.c_double, C.c_double, C.c_double]
         L.ora_w.restype = C.c_double
+        L.ora_forcing_sin.argtypes = [C.c_double]
+        L.ora_forcing_sin.restype = C.c_double
         _lib = L
     return _lib
+
+
+def forcing_sin(x):
+    """The sine used by the tank forcing (an extension, not in the reference)."""
+    return lib().ora_forcing_sin(float(x))
 
 
 class Oracle:

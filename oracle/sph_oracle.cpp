@@ -164,7 +164,36 @@ struct Oracle {
   double dt = 0, dt_average = 0, simulation_time = 0, dtvel = 0;
   int on_going_time_step = -999;
   int nthreads = 1;
+  // body force used by RHS_momentum_equation: prm.grav plus the lateral tank
+  // forcing (an extension of the library, absent from the reference)
+  double geff[3] = {0, 0, 0};
 };
+
+// Sine of the forcing phase, the same sequence of IEEE operations as the
+// library's device function: reduction by the nearest multiple of 2 pi,
+// folding into [-pi/2, pi/2], Taylor series to r^23 in nested form.
+static double forcing_sin(double x) {
+  const double two_pi = 6.283185307179586, pi = 3.141592653589793, half_pi = 1.5707963267948966;
+  double k = std::nearbyint(x / two_pi);
+  double r = x - k * two_pi;
+  if (r > half_pi) r = pi - r;
+  else if (r < -half_pi) r = -pi - r;
+  double r2 = r * r;
+  double t = 1.0;
+  for (int n = 22; n >= 2; n -= 2) t = 1.0 - r2 / (double)(n * (n + 1)) * t;
+  return r * t;
+}
+
+// geff at simulation time t: grav + A w^2 sin(w t) along x, w = 2 pi / T,
+// for a tank moving as x = A sin(w t); equal to grav when A = 0.
+static void set_body_force(Oracle& o, double t) {
+  for (int d = 0; d < 3; ++d) o.geff[d] = o.prm.grav[d];
+  if (o.prm.forcing_amplitude != 0.0) {
+    double w = 6.283185307179586 / o.prm.forcing_period;
+    double aw2 = o.prm.forcing_amplitude * w * w;
+    o.geff[0] = o.prm.grav[0] + aw2 * forcing_sin(w * t);
+  }
+}
 
 inline double sq3(double a) { return (a * a) * a; }
 
@@ -1205,7 +1234,7 @@ void AddBoundaryContributions_to_ME3D(const Oracle& o, int npi, int Ncbf, double
     double gl[3];
     for (int SD = 0; SD < 3; ++SD) {
       gl[SD] = 0.0;
-      for (int sdj = 0; sdj < 3; ++sdj) gl[SD] = gl[SD] + f.T[sdj][SD] * o.prm.grav[sdj];
+      for (int sdj = 0; sdj < 3; ++sdj) gl[SD] = gl[SD] + f.T[sdj][SD] * o.geff[sdj];
     }
     double loc[3], glob[3];
     for (int i = 0; i < 3; ++i) {
@@ -1276,8 +1305,8 @@ void AddBoundaryContributions_to_ME2D(const Oracle& o, int npi, int IntNcbs, dou
     double GravN = 0.0, nnlocal[2], gradbPsuro[2];
     for (int i = 0; i < 2; ++i) {
       nnlocal[i] = s.T[acix[i]][2];
-      gradbPsuro[i] = o.prm.grav[acix[i]];
-      GravN = GravN + o.prm.grav[acix[i]] * nnlocal[i];
+      gradbPsuro[i] = o.geff[acix[i]];
+      GravN = GravN + o.geff[acix[i]] * nnlocal[i];
     }
     double sidevel[2];
     for (int i = 0; i < 2; ++i) sidevel[i] = (z.type == SPH_ZONE_TAPI) ? s.velocity[acix[i]] : 0.0;
@@ -1447,9 +1476,9 @@ void RHS_momentum_equation(Oracle& o) {
       double R[3];
       if (o.dim == 3) AddElasticBoundaryReaction_3D(o, npi, ncb, R);
       else AddElasticBoundaryReaction_2D(o, npi, intn, R);
-      for (int d = 0; d < 3; ++d) p.acc[d] = tpres[d] + tdiss[d] + tvisc[d] + o.prm.grav[d] + R[d];
+      for (int d = 0; d < 3; ++d) p.acc[d] = tpres[d] + tdiss[d] + tvisc[d] + o.geff[d] + R[d];
     } else {
-      for (int d = 0; d < 3; ++d) p.acc[d] = tpres[d] + tdiss[d] + tvisc[d] + o.prm.grav[d];
+      for (int d = 0; d < 3; ++d) p.acc[d] = tpres[d] + tdiss[d] + tvisc[d] + o.geff[d];
     }
   }
 }
@@ -1573,6 +1602,7 @@ void* ora_create(const SphParams* prm, const SphGeometry* g, int n, const double
                  const double* rho, const double* p, const double* m, int nthreads) {
   Oracle* o = new Oracle();
   o->prm = *prm;
+  set_body_force(*o, 0.0);
   o->dim = prm->dim;
   o->ncord = prm->dim;
   o->nthreads = nthreads > 0 ? nthreads : omp_get_max_threads();
@@ -1658,6 +1688,7 @@ int ora_truncated(void* h) { return static_cast<Oracle*>(h)->truncated; }
 int ora_removed(void* h) { return static_cast<Oracle*>(h)->EpOrdGrid; }
 int ora_ncbf_max(void* h) { return static_cast<Oracle*>(h)->Ncbf_Max; }
 double ora_dt(void* h) { return static_cast<Oracle*>(h)->dt; }
+double ora_forcing_sin(double x) { return forcing_sin(x); }
 double ora_time(void* h) { return static_cast<Oracle*>(h)->simulation_time; }
 int ora_step_index(void* h) { return static_cast<Oracle*>(h)->on_going_time_step; }
 void ora_grid_info(void* h, int* ncd, double* extr_lo, double* dcd) {
@@ -1674,6 +1705,7 @@ int ora_prepare(void* h) {
   if (st) return check(o, st);
   o.on_going_time_step = -999;
   time_step_duration(o);
+  set_body_force(o, o.simulation_time + o.dt);
   return 0;
 }
 
@@ -1698,6 +1730,7 @@ int ora_step(void* h, int nsteps) {
     double dt_previous_step = o.dt;
     time_step_duration(o);
     o.simulation_time = o.simulation_time + o.dt;
+    set_body_force(o, o.simulation_time);
     RHS_momentum_equation(o);
     Leapfrog_momentum(o, dt_previous_step);
     Leapfrog_trajectories(o);

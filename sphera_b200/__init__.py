@@ -77,6 +77,9 @@ def lib():
         "sph_measure_fma_peak": ([C.c_int32, dp], C.c_int),
         "sph_autotune": ([vp, C.c_int32, ip], C.c_int),
         "sph_batch_status": ([vp, ip, dp, ip], C.c_int),
+        "sph_memory_required": ([C.c_int32, C.POINTER(abi.SphParams), C.POINTER(abi.SphGeometry), ip,
+                                 C.POINTER(C.c_uint64)], C.c_int),
+        "sph_idle": ([vp, ip], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -151,6 +154,12 @@ class Simulation:
 
     def sync(self):
         _chk(lib().sph_sync(self._h), "sph_sync")
+
+    def idle(self):
+        """True when the work enqueued by step_async has finished (never waits)."""
+        v = C.c_int32()
+        _chk(lib().sph_idle(self._h, C.byref(v)), "sph_idle")
+        return bool(v.value)
 
     @property
     def stream(self):
@@ -240,6 +249,19 @@ class Simulation:
         return ncb, clob, vals
 
 
+def memory_required(cases):
+    """Device bytes a batch of these cases would allocate (one case: a
+    Simulation), computed on the host; no device is needed."""
+    cases = list(cases)
+    n = len(cases)
+    prm = (abi.SphParams * n)(*[c.params for c in cases])
+    geo = (abi.SphGeometry * n)(*[c.geometry.struct for c in cases])
+    caps = np.array([c.n for c in cases], np.int32)
+    b = C.c_uint64()
+    _chk(lib().sph_memory_required(n, prm, geo, abi.iptr(caps), C.byref(b)), "sph_memory_required")
+    return int(b.value)
+
+
 def measure_fp64_peak():
     """Dense FP64 FMA throughput of the current device, TFLOP/s."""
     t = C.c_double()
@@ -295,6 +317,12 @@ class Batch:
 
     def sync(self):
         _chk(lib().sph_sync(self._h), "sph_sync")
+
+    def idle(self):
+        """True when the work enqueued by step_async has finished (never waits)."""
+        v = C.c_int32()
+        _chk(lib().sph_idle(self._h, C.byref(v)), "sph_idle")
+        return bool(v.value)
 
     def autotune(self, reps=3):
         g = np.zeros(5, np.int32)

@@ -71,6 +71,8 @@ class SphParams(C.Structure):
         ("bdt_capacity", C.c_int32),
         ("teta_p", C.c_double),
         ("teta_v", C.c_double),
+        ("forcing_amplitude", C.c_double),
+        ("forcing_period", C.c_double),
     ]
 
 

@@ -16,6 +16,12 @@ Workloads (all synthetic, no external dataset):
                    rho = 1000 (1 + N(0, 1e-3)), v ~ N(0, 0.1), no walls
   * ensemble_2d:   dam breaks with column width U[0.5, 2.0] and height
                    U[0.5, 2.5] in the 2D tank at dx 0.01
+  * sloshing_3d:   1.0 x 0.5 x 0.5 m tank, half filled, moved sideways as
+                   x = A sin(2 pi t / T) (A = 0.02 m); the fluid is computed
+                   in the tank frame with the body force
+                   g + A (2 pi / T)^2 sin(2 pi t / T) along x
+  * serving_requests: a seeded Poisson stream of dam-break and sloshing
+                   requests, each run to t_end = 0.3 s
 """
 from dataclasses import dataclass, field
 
@@ -156,4 +162,54 @@ def ensemble_2d(n_sims=256, dx=0.01, seed=0xC3, precision=abi.SPH_PREC_FP32C):
         hgt = round(hgt / dx) * dx
         out.append(dam_break_2d(dx=dx, column=(w, hgt), seed=int(rng.integers(1 << 31)),
                                 precision=precision))
+    return out
+
+
+def sloshing_3d(dx=0.01, tank=(1.0, 0.5, 0.5), fill=0.5, amplitude=0.02, period=1.2, jitter=0.01, seed=0xC5,
+                precision=abi.SPH_PREC_FP64, cfl=0.1):
+    rng = np.random.Generator(np.random.PCG64(seed))
+    nx, ny, nz = (int(round(v / dx)) for v in (tank[0], tank[1], tank[2] * fill))
+    i, j, k = np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing="ij")
+    x = np.stack([(i.ravel() + 0.5) * dx, (j.ravel() + 0.5) * dx, (k.ravel() + 0.5) * dx], axis=1)
+    x += _jitter(rng, x.shape, dx, jitter)
+    prm = _params(3, dx, (0.0, 0.0, 0.0), tank, cfl=cfl, precision=precision,
+                  forcing_amplitude=amplitude, forcing_period=period)
+    p, rho = _hydrostatic(x[:, 2], dx, prm.den0, prm.eps, prm.p_ref)
+    m = np.full(len(p), dx ** 3 * prm.den0)
+    st = abi.State(x, np.zeros_like(x), rho, p, m)
+    return Case("sloshing_3d", prm, tank_3d(*tank), st,
+                dict(dx=dx, tank=tank, fill=fill, amplitude=amplitude, period=period, seed=seed, t_end=0.3))
+
+
+@dataclass
+class Request:
+    """One simulation request of a serving stream: run `case` to `t_end`."""
+    rid: int
+    arrival: float          # seconds after the stream starts
+    case: Case
+    t_end: float
+
+
+def serving_requests(n_requests=16, rate=20.0, seed=0xC4, t_end=0.3, dx_range=(0.005, 0.0125),
+                     period_range=(0.8, 1.6), amplitude=0.02, precision=abi.SPH_PREC_FP32C):
+    """Seeded Poisson arrivals (mean `rate` per second) of 3D dam-break and
+    sloshing-tank requests, half of each on average.  dx is drawn
+    log-uniformly from `dx_range`; at the default range the dam break holds
+    55k-864k particles and the half-filled sloshing tank 64k-1M (a larger
+    dx would fall under 50k particles with these geometries).  Sloshing
+    periods are uniform in `period_range`."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    out = []
+    t = 0.0
+    lo, hi = np.log(dx_range[0]), np.log(dx_range[1])
+    for r in range(n_requests):
+        t += rng.exponential(1.0 / rate)
+        dx = float(np.exp(rng.uniform(lo, hi)))
+        sub = int(rng.integers(1 << 31))
+        if rng.random() < 0.5:
+            case = dam_break_3d(dx=dx, seed=sub, precision=precision)
+        else:
+            case = sloshing_3d(dx=dx, amplitude=amplitude, period=float(rng.uniform(*period_range)),
+                               seed=sub, precision=precision)
+        out.append(Request(r, t, case, t_end))
     return out

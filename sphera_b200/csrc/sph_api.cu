@@ -169,6 +169,10 @@ int prepare_sim(const SphParams& prm, const SphGeometry& g, int cap, HostSim& hs
   s.cfl = prm.cfl;
   s.vsc_coeff = prm.vsc_coeff;
   s.pesodt = prm.pesodt;
+  if (prm.forcing_period < 0.0 || (prm.forcing_amplitude != 0.0 && !(prm.forcing_period > 0.0)))
+    return SPH_ERR_INVALID_ARGUMENT;
+  s.forcing_w = prm.forcing_period > 0.0 ? 6.283185307179586 / prm.forcing_period : 0.0;
+  s.forcing_aw2 = prm.forcing_amplitude * s.forcing_w * s.forcing_w;
   s.dt_alfa_mon = prm.dt_alfa_mon;
   s.density_thresholds = prm.density_thresholds;
   s.zpmin = 0.05 * s.h;
@@ -526,6 +530,8 @@ struct SphHandle {
   cudaGraphExec_t graph = nullptr;
   bool uploaded = false;
   std::vector<SimDyn> h_dyn;
+  size_t device_bytes = 0;          // bytes of the arrays below `owned`
+  bool dry = false;                 // size the arrays only (sph_memory_required)
 };
 
 namespace {
@@ -543,11 +549,23 @@ int cuda_status(cudaError_t e) {
   } while (0)
 #define SPH_CUDA(x) SPH_TRY(cuda_status(x))
 
+// Handle arrays come from the stream-ordered allocator on the handle's own
+// stream, so creating and destroying a handle does not wait for the work
+// other handles have queued on the device.
 template <class T>
 int halloc(SphHandle* h, T** p, size_t n) {
-  int st = dalloc(p, n);
-  if (st == SPH_OK) h->owned.push_back((void*)*p);
-  return st;
+  *p = nullptr;
+  size_t bytes = (n == 0 ? 1 : n) * sizeof(T);
+  h->device_bytes += bytes;
+  if (h->dry) return SPH_OK;
+  cudaError_t e = cudaMallocAsync((void**)p, bytes, h->stream);
+  if (e != cudaSuccess) {
+    *p = nullptr;
+    cudaGetLastError();
+    return SPH_ERR_ALLOC;
+  }
+  h->owned.push_back((void*)*p);
+  return SPH_OK;
 }
 
 int sync_dyn(SphHandle* h) {
@@ -603,17 +621,23 @@ int build_graph(SphHandle* h) {
   return cuda_status(e);
 }
 
+// With bytes_out set, nothing touches the device: the arrays are sized,
+// their total goes to *bytes_out and no handle is returned.
 int create_batch(int nsims, const SphParams* params, const SphGeometry* geoms, const int32_t* caps,
-                 SphHandle** out) {
-  if (!out || nsims <= 0 || !params || !geoms || !caps) return SPH_ERR_INVALID_ARGUMENT;
-  *out = nullptr;
+                 SphHandle** out, uint64_t* bytes_out = nullptr) {
+  const bool dry = bytes_out != nullptr;
+  if ((!out && !dry) || nsims <= 0 || !params || !geoms || !caps) return SPH_ERR_INVALID_ARGUMENT;
+  if (out) *out = nullptr;
   int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess) { cudaGetLastError(); return SPH_ERR_NO_DEVICE; }
-  cudaDeviceProp prop;
-  if (cudaGetDeviceProperties(&prop, dev) != cudaSuccess) { cudaGetLastError(); return SPH_ERR_NO_DEVICE; }
-  if (prop.major != 10) return SPH_ERR_NO_DEVICE;
+  cudaDeviceProp prop{};
+  if (!dry) {
+    if (cudaGetDevice(&dev) != cudaSuccess) { cudaGetLastError(); return SPH_ERR_NO_DEVICE; }
+    if (cudaGetDeviceProperties(&prop, dev) != cudaSuccess) { cudaGetLastError(); return SPH_ERR_NO_DEVICE; }
+    if (prop.major != 10) return SPH_ERR_NO_DEVICE;
+  }
   SphHandle* h = new (std::nothrow) SphHandle();
   if (!h) return SPH_ERR_ALLOC;
+  h->dry = dry;
   h->device = dev;
   h->nsims = nsims;
   h->dim = params[0].dim;
@@ -654,7 +678,10 @@ int create_batch(int nsims, const SphParams* params, const SphGeometry* geoms, c
     coff += hs.dev.ncells + 1;
     foff += (int)hs.faces.size();
     soff += (int)hs.sides.size();
-    bdt_cap += hs.prm.bdt_capacity > 0 ? (size_t)hs.prm.bdt_capacity : (size_t)hs.cap;
+    // default: room for three close faces (two close sides) per particle,
+    // a box corner's worth; the reference reserves MAXCLOSEBOUNDFACES per
+    // particle (Gest_Trans.f90:90), far more than a flow uses
+    bdt_cap += hs.prm.bdt_capacity > 0 ? (size_t)hs.prm.bdt_capacity : (size_t)hs.cap * (h->dim == 3 ? 3 : 2);
   }
   if (poff >= (1 << 28)) { delete h; return SPH_ERR_INVALID_ARGUMENT; }   // FIFO entries carry 28-bit slots
   h->total_slots = poff;
@@ -662,8 +689,11 @@ int create_batch(int nsims, const SphParams* params, const SphGeometry* geoms, c
   h->total_faces = foff;
   h->total_sides = soff;
   int st = SPH_OK;
-  cudaError_t e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
-  if (e != cudaSuccess) { delete h; return cuda_status(e); }
+  cudaError_t e = cudaSuccess;
+  if (!dry) {
+    e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) { delete h; return cuda_status(e); }
+  }
   size_t N = poff, C = coff;
   Particles& P = h->P;
 #define A(ptr, n) if (st == SPH_OK) st = halloc(h, &(ptr), (n))
@@ -720,6 +750,11 @@ int create_batch(int nsims, const SphParams* params, const SphGeometry* geoms, c
     cfl.insert(cfl.end(), hs.cf_list.begin(), hs.cf_list.end());
   }
   if (st == SPH_OK) st = halloc(h, &h->d_cf_list, cfl.size());
+  if (dry) {
+    *bytes_out = h->device_bytes;
+    delete h;
+    return SPH_OK;
+  }
   if (st != SPH_OK) { sph_destroy(h); return st; }
   cudaStream_t q = h->stream;
   std::vector<SimDyn> dyn0(nsims + 1);
@@ -835,10 +870,31 @@ void sph_destroy(SphHandle* h) {
   if (!h) return;
   if (h->stream) cudaStreamSynchronize(h->stream);
   if (h->graph) cudaGraphExecDestroy(h->graph);
-  for (void* p : h->owned) cudaFree(p);
-  if (h->stream) cudaStreamDestroy(h->stream);
+  for (void* p : h->owned) cudaFreeAsync(p, h->stream);
+  if (h->stream) {
+    cudaStreamSynchronize(h->stream);
+    cudaStreamDestroy(h->stream);
+  }
   cudaGetLastError();
   delete h;
+}
+
+int sph_memory_required(int32_t nsims, const SphParams* params, const SphGeometry* geometries,
+                        const int32_t* n_capacity, uint64_t* bytes) {
+  if (!bytes) return SPH_ERR_INVALID_ARGUMENT;
+  *bytes = 0;
+  return create_batch(nsims, params, geometries, n_capacity, nullptr, bytes);
+}
+
+int sph_idle(SphHandle* h, int32_t* idle) {
+  if (!h || !idle) return SPH_ERR_INVALID_ARGUMENT;
+  cudaError_t e = cudaStreamQuery(h->stream);
+  if (e == cudaErrorNotReady) {
+    *idle = 0;
+    return SPH_OK;
+  }
+  *idle = 1;
+  return cuda_status(e);
 }
 
 int sph_upload(SphHandle* h, const SphState* state) {

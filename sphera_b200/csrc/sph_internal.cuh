@@ -51,6 +51,8 @@ struct SimDev {
   double dx, den0, eps, k_over_rho0, celerita, alfa_mon, kin_visc, p_ref;
   double grav[3];
   double cfl, vsc_coeff, pesodt;
+  double forcing_aw2;     // A (2 pi / T)^2 of the lateral tank forcing (0: none)
+  double forcing_w;       // 2 pi / T
   double zpmin;           // 0.05 h, ComputeBoundaryVolumeIntegrals_P0.f90
   double ktdelta;         // kernel-table step
   float dcdf[3];          // (float)dcd: cell origins differ by multiples of it
@@ -74,6 +76,7 @@ struct SimDyn {
   int bdt_used;
   int frozen;                      // reached t_end: state kept, no longer advanced
   double t_end;                    // 0 = run without end
+  double geff[3];                  // body force of the next step: grav (+ tank forcing)
 };
 
 // Solid face (TyBoundaryFace) prepared on the host.

@@ -836,7 +836,7 @@ __global__ void __launch_bounds__(kBlock) k_boundary2d(DevBatch b) {
 
 // AddBoundaryContributions_to_ME3D.f90:105-336 (fixe/tapi, slip mode 1).
 __device__ __forceinline__ void me_boundary3d(const SimDev& s, const DevBatch& b, int nb, int start, const double* vi, double rhoi,
-                              double pres, int lam, double* tpres, double* tdiss, double* tvisc) {
+                              double pres, int lam, const double* grav, double* tpres, double* tdiss, double* tvisc) {
   double ALEt[3] = {0, 0, 0}, gradpt[3] = {0, 0, 0}, VMon[3] = {0, 0, 0}, VShear[3] = {0, 0, 0};
   for (int u = 0; u < nb; ++u) {
     const BdtEntry& e = b.P.bdt[start + u];
@@ -850,7 +850,7 @@ __device__ __forceinline__ void me_boundary3d(const SimDev& s, const DevBatch& b
     double gl[3];
     for (int SD = 0; SD < 3; ++SD) {
       double a = 0.0;
-      for (int sdj = 0; sdj < 3; ++sdj) a = a + f.T[sdj][SD] * s.grav[sdj];
+      for (int sdj = 0; sdj < 3; ++sdj) a = a + f.T[sdj][SD] * grav[sdj];
       gl[SD] = a;
     }
     double loc[3];
@@ -893,11 +893,11 @@ __device__ __forceinline__ void me_boundary3d(const SimDev& s, const DevBatch& b
 
 // AddBoundaryContributions_to_ME2D.f90:96-402 (fixe/tapi, slip mode 1).
 __device__ __forceinline__ void me_boundary2d(const SimDev& s, const DevBatch& b, int nb, int start, const double* vi, double roi,
-                              double pressi, int lam, double* tpres, double* tdiss, double* tvisc) {
+                              double pressi, int lam, const double* grav, double* tpres, double* tdiss, double* tvisc) {
   const double pibmink = 10.0;
   double ro0 = s.den0, distpimin = s.dx;
   double VMon[2] = {0, 0}, VShear[2] = {0, 0}, RG_sum[2] = {0, 0}, ALEt[2] = {0, 0};
-  const double g2[2] = {s.grav[0], s.grav[2]};
+  const double g2[2] = {grav[0], grav[2]};
   const double v2[2] = {vi[0], vi[2]};
   for (int u = 0; u < nb; ++u) {
     const BdtEntry& e = b.P.bdt[start + u];
@@ -1187,6 +1187,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_momentum(DevBatch b) {
     Tile tl = b.tiles[t];
     load_sim(s, b.sims, tl.sim, cur);
     SimDyn* dyn = b.dyn + tl.sim;
+    const double* geff = dyn->geff;
     int p = tl.start + threadIdx.x;
     bool active = threadIdx.x < tl.count && p < s.p_off + dyn->nag;
     if (FUSED && active && dyn->frozen) {
@@ -1219,8 +1220,8 @@ __global__ void __launch_bounds__(kBlock, 2) k_momentum(DevBatch b) {
       nb = P.bdt_count[p];
       bstart = nb > 0 ? P.bdt_start[p] : 0;
       if (nb > 0) {
-        if (DIM == 3) me_boundary3d(s, b, nb, bstart, vi, rhoi, pi, lam, tpres, tdiss, tvisc);
-        else me_boundary2d(s, b, nb, bstart, vi, rhoi, pi, lam, tpres, tdiss, tvisc);
+        if (DIM == 3) me_boundary3d(s, b, nb, bstart, vi, rhoi, pi, lam, geff, tpres, tdiss, tvisc);
+        else me_boundary2d(s, b, nb, bstart, vi, rhoi, pi, lam, geff, tpres, tdiss, tvisc);
       }
     }
     double tp0 = 0, tp1 = 0, tp2 = 0, al0 = 0, al1 = 0, al2 = 0;
@@ -1295,9 +1296,9 @@ __global__ void __launch_bounds__(kBlock, 2) k_momentum(DevBatch b) {
         lam_new = (weight > 5.0 || absv_pres == 0.0) ? 1 : 0;
       }
       double acc[3];
-      acc[0] = tpres[0] + td0 + tv0 + s.grav[0];
-      acc[1] = tpres[1] + td1 + tv1 + s.grav[1];
-      acc[2] = tpres[2] + td2 + tv2 + s.grav[2];
+      acc[0] = tpres[0] + td0 + tv0 + geff[0];
+      acc[1] = tpres[1] + td1 + tv1 + geff[1];
+      acc[2] = tpres[2] + td2 + tv2 + geff[2];
       if (nb > 0) {
         double R[3];
         elastic_reaction<DIM>(s, b, nb, bstart, vi, R);
@@ -1536,6 +1537,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_momentum_f32(DevBatch b) {
     F32Const fc;
     fc.load(s);
     SimDyn* dyn = b.dyn + tl.sim;
+    const double* geff = dyn->geff;
     int p = tl.start + threadIdx.x;
     bool active = threadIdx.x < tl.count && p < s.p_off + dyn->nag;
     if (FUSED && active && dyn->frozen) {
@@ -1568,8 +1570,8 @@ __global__ void __launch_bounds__(kBlock, 2) k_momentum_f32(DevBatch b) {
       nb = P.bdt_count[p];
       bstart = nb > 0 ? P.bdt_start[p] : 0;
       if (nb > 0) {
-        if (DIM == 3) me_boundary3d(s, b, nb, bstart, vi, rhoi, pi, lam, tpres, tdiss, tvisc);
-        else me_boundary2d(s, b, nb, bstart, vi, rhoi, pi, lam, tpres, tdiss, tvisc);
+        if (DIM == 3) me_boundary3d(s, b, nb, bstart, vi, rhoi, pi, lam, geff, tpres, tdiss, tvisc);
+        else me_boundary2d(s, b, nb, bstart, vi, rhoi, pi, lam, geff, tpres, tdiss, tvisc);
       }
       particle_cell(s, xi.x, xi.y, xi.z, ci, cj, ck);
     }
@@ -1638,9 +1640,9 @@ __global__ void __launch_bounds__(kBlock, 2) k_momentum_f32(DevBatch b) {
         lam_new = (weight > 5.0 || absv_pres == 0.0) ? 1 : 0;
       }
       double acc[3];
-      acc[0] = tpres[0] + (tdiss[0] + td0.val()) + (tvisc[0] + rs0) + s.grav[0];
-      acc[1] = tpres[1] + (tdiss[1] + td1.val()) + (tvisc[1] + rs1) + s.grav[1];
-      acc[2] = tpres[2] + (tdiss[2] + td2.val()) + (tvisc[2] + rs2) + s.grav[2];
+      acc[0] = tpres[0] + (tdiss[0] + td0.val()) + (tvisc[0] + rs0) + geff[0];
+      acc[1] = tpres[1] + (tdiss[1] + td1.val()) + (tvisc[1] + rs1) + geff[1];
+      acc[2] = tpres[2] + (tdiss[2] + td2.val()) + (tvisc[2] + rs2) + geff[2];
       if (nb > 0) {
         double R[3];
         elastic_reaction<DIM>(s, b, nb, bstart, vi, R);
@@ -1893,6 +1895,24 @@ __device__ void tsd_close(const SimDev& s, SimDyn& d, double dtmin_cfl, int on_g
 //         this step left).
 // Between steps the state keeps: step = completed steps, time = sum of their
 // dt, dt = dt of the next step, dt_prev = dt of the last step.
+// Sine of the tank forcing phase, written out so that host and device give
+// the same bits: x is reduced by the nearest multiple of 2 pi into
+// [-pi, pi], folded into [-pi/2, pi/2] by sin(r) = sin(+-pi - r), and the
+// Taylor series of sin is summed to the r^23 term in nested form,
+// r (1 - r^2/(2*3) (1 - r^2/(4*5) (...))), truncation below 1e-20 there.
+// Every operation is a correctly rounded IEEE operation.
+__device__ __forceinline__ double forcing_sin(double x) {
+  const double two_pi = 6.283185307179586, pi = 3.141592653589793, half_pi = 1.5707963267948966;
+  double k = rint(x / two_pi);
+  double r = x - k * two_pi;
+  if (r > half_pi) r = pi - r;
+  else if (r < -half_pi) r = -pi - r;
+  double r2 = r * r;
+  double t = 1.0;
+  for (int n = 22; n >= 2; n -= 2) t = 1.0 - r2 / (double)(n * (n + 1)) * t;
+  return r * t;
+}
+
 __global__ void k_finalize(DevBatch b, int mode) {
   int sim = blockIdx.x * blockDim.x + threadIdx.x;
   if (sim >= b.nsims) return;
@@ -1920,6 +1940,15 @@ __global__ void k_finalize(DevBatch b, int mode) {
     if (d.t_end > 0.0 && d.time >= d.t_end) d.frozen = 1;
   }
   d.dtvel = 0.5 * (d.dt + d.dt_prev);
+  // body force of the next step, taken at that step's end time d.time + d.dt
+  // (the simulation time when its momentum equation is evaluated): gravity,
+  // plus the lateral forcing of a tank moving as x = A sin(w t) seen in the
+  // tank frame, A w^2 sin(w t) along x (no reference counterpart; zero
+  // amplitude leaves grav unchanged)
+  d.geff[0] = s.forcing_aw2 != 0.0 ? s.grav[0] + s.forcing_aw2 * forcing_sin(s.forcing_w * (d.time + d.dt))
+                                   : s.grav[0];
+  d.geff[1] = s.grav[1];
+  d.geff[2] = s.grav[2];
 }
 
 __global__ void k_sort_reset(DevBatch b) {

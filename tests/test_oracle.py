@@ -146,3 +146,37 @@ def test_steps_advance_time(oracle_lib):
     s = o.get()
     assert np.all(np.isfinite(s["x"]))
     assert s["v"][:, 0].max() > 0.0
+
+
+def test_tank_forcing_is_a_lateral_body_force(oracle_lib):
+    """The sloshing tank's forcing adds A w^2 sin(w t) to the x acceleration
+    of every particle (t: the end time of the step being computed, here the
+    first step's) and leaves y and z untouched; zero amplitude is plain
+    gravity."""
+    A, T = 0.02, 0.8
+    base = _small_box(grav=(0.0, 0.0, -9.81))
+    forced = _small_box(grav=(0.0, 0.0, -9.81))
+    forced.params.forcing_amplitude = A
+    forced.params.forcing_period = T
+    out = []
+    for c in (base, forced):
+        o = oracle_lib.Oracle(c)
+        o.prepare()
+        o.rhs_momentum()
+        out.append((o.get()["acc"], o.dt))
+    (a0, dt0), (a1, dt1) = out
+    assert dt0 == dt1
+    w = 2.0 * np.pi / T
+    expect = A * w * w * np.sin(w * dt0)
+    scale = np.abs(a0).max()
+    assert np.all(np.abs((a1[:, 0] - a0[:, 0]) - expect) <= 1e-13 * scale)
+    assert np.array_equal(a1[:, 1:], a0[:, 1:])
+
+
+def test_forcing_sine_matches_libm(oracle_lib):
+    """The forcing's own sine (range reduction by the nearest multiple of
+    2 pi, Taylor series; the same IEEE sequence on host and device) against
+    libm over phases well beyond what a run reaches."""
+    x = np.concatenate([np.linspace(-200.0, 200.0, 40001), np.pi * np.arange(-64, 65) / 4.0])
+    got = np.array([oracle_lib.forcing_sin(v) for v in x])
+    assert np.all(np.abs(got - np.sin(x)) <= 1e-15 * (1.0 + np.abs(x)))
