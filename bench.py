@@ -294,6 +294,18 @@ def run_serving(args, ws, rank):
     return 0
 
 
+def _fp64_summary(r64, n, steps, fp64_peak):
+    if r64 is None:
+        return None
+    c64, nprof = r64["cnt"], r64["nprof"]
+    mom64_ms = r64["phases"]["momentum"]
+    mom64_flops = (c64["pairs"] - n * nprof) * FLOP_MOM_PAIR / nprof
+    return {"value": r64["value"], "ms_per_step": r64["ms"] / steps,
+            "phases_ms_per_step": r64["phases"], "clocks": r64["clocks"],
+            "momentum_fp64_tflops": mom64_flops / (mom64_ms * 1e-3) / 1e12,
+            "fp64_peak_tflops": fp64_peak}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -308,6 +320,9 @@ def main():
     ap.add_argument("--t-end", type=float, default=None)
     ap.add_argument("--requests", type=int, default=8)
     ap.add_argument("--hbm-budget-gib", type=float, default=4.0)
+    ap.add_argument("--dx", type=float, default=0.005,
+                    help="lattice spacing of the 3D dam break (0.005: the 864000-particle workload)")
+    ap.add_argument("--forms", default="both", choices=["both", "fp32c", "fp64"])
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     if args.t_end is None:
@@ -338,7 +353,7 @@ def main():
         gpu_id = str(local)
 
     def run_form(precision):
-        case = cases.dam_break_3d(precision=precision)
+        case = cases.dam_break_3d(dx=args.dx, precision=precision)
         n = case.n
         sim = Simulation(case)
         sim.upload(case.state)
@@ -371,9 +386,17 @@ def main():
                     phases={k: v / nprof for k, v in phases.items()}, nprof=nprof, cnt=cnt, diag=diag,
                     e0=e0, e1=e1)
 
-    r64 = run_form(abi.SPH_PREC_FP64)
-    r64["sim"].close()
-    r32 = run_form(abi.SPH_PREC_FP32C)
+    r64 = r32 = None
+    if args.forms in ("both", "fp64"):
+        r64 = run_form(abi.SPH_PREC_FP64)
+        r64["sim"].close()
+    if args.forms in ("both", "fp32c"):
+        r32 = run_form(abi.SPH_PREC_FP32C)
+    else:
+        r32 = r64
+        r32["sim"] = Simulation(r64["case"])
+        r32["sim"].upload(r64["case"].state)
+        r32["stream"] = torch.cuda.ExternalStream(r32["sim"].stream)
     case, n, sim, stream = r32["case"], r32["n"], r32["sim"], r32["stream"]
     e0, e1 = r32["e0"], r32["e1"]
     value, ms_max, clocks, cnt, diag = r32["value"], r32["ms"], r32["clocks"], r32["cnt"], r32["diag"]
@@ -384,10 +407,7 @@ def main():
     achieved_gbs = alg_bytes / (mom_ms * 1e-3) / 1e9
     mom_flops = (cnt["pairs"] - n * nprof) * FLOP_MOM_PAIR / nprof
     mom_tflops = mom_flops / (mom_ms * 1e-3) / 1e12
-    mom64_ms = r64["phases"]["momentum"]
-    c64 = r64["cnt"]
-    mom64_flops = (c64["pairs"] - n * nprof) * FLOP_MOM_PAIR / nprof
-    workload = "dam_break_3d"
+    workload = "dam_break_3d" if args.dx == 0.005 else f"dam_break_3d_dx{args.dx:g}"
     traffic = _traffic(workload)
 
     # end to end through the C ABI with pinned host buffers
@@ -428,7 +448,7 @@ def main():
         threads = os.cpu_count() or 1
         rate, el = cpu_oracle_rate(case, args.cpu_steps, threads)
         cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
-               "sample": f"{args.cpu_steps} leapfrog steps of the full 864000-particle 3D dam break after "
+               "sample": f"{args.cpu_steps} leapfrog steps of the full {n}-particle 3D dam break after "
                          f"its IC ({el:.1f} s), FP64 oracle, OpenMP on all host threads"}
 
     line = {
@@ -437,16 +457,13 @@ def main():
         "scaling": "weak", "vs_baseline": None,
         "dtype": "fp32c (f32 pair sums, compensated; f64 positions/integration/boundary terms)",
         "data": "synthetic (seeded 3D dam break generated in-repo)",
-        "config": {"workload": "dam_break_3d: tank 1.6x0.6x0.6 m, block 0.6x0.3x0.6 m, dx 0.005 m, "
-                               "864000 particles per GPU, SA-SPH walls",
-                   "particles_per_gpu": n, "form": "fp32c",
+        "config": {"workload": f"dam_break_3d: tank 1.6x0.6x0.6 m, block 0.6x0.3x0.6 m, dx {args.dx:g} m, "
+                               f"{n} particles per GPU, SA-SPH walls",
+                   "particles_per_gpu": n, "form": "fp32c" if args.forms != "fp64" else "fp64",
                    "l2": "state and scratch (~250 MB per step) exceed the 126 MB L2; no flush",
                    "parallelism": f"replicas x{ws} (independent simulations, no collective)"},
-        "fp64": {"value": r64["value"], "ms_per_step": r64["ms"] / args.steps,
-                 "phases_ms_per_step": r64["phases"], "clocks": r64["clocks"],
-                 "momentum_fp64_tflops": mom64_flops / (mom64_ms * 1e-3) / 1e12,
-                 "fp64_peak_tflops": fp64_peak},
-        "speedup_fp32c_vs_fp64": value / r64["value"],
+        "fp64": _fp64_summary(r64, n, args.steps, fp64_peak),
+        "speedup_fp32c_vs_fp64": value / r64["value"] if r64 else None,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": state_bytes,
                 "d2h_bytes_per_step": state_bytes, "steps": args.e2e_steps,
                 "path": "sph_upload + sph_step_async(1) + sph_download per step, pinned host buffers, fp32c form"},

@@ -191,11 +191,15 @@ int prepare_sim(const SphParams& prm, const SphGeometry& g, int cap, HostSim& hs
   // FP32 screening copies (k_rank_permute): the offset f of a particle from
   // the origin o of its cell, in FP32.  A candidate difference is formed as
   // D + (f_i - f_j) with D = (float)(cell index difference * dcd), which is
-  // 0 or +-(float)dcd inside the 27-cell block.  Each component is then
-  // within eps = 8 * 2^-24 dcd (+ 2^-50 R for the FP64 origins) of x_i - x_j,
-  // |x_i - x_j| < 2 dcd, and the FP32 sum of squares adds at most 5 roundings
-  // of 2^-24.  Outside twice that band the FP32 value decides the test
-  // r^2 <= (2h)^2 exactly as the FP64 one would; inside it the FP64 test runs.
+  // 0 or +-(float)dcd inside the 27-cell block; in z the neighbour-list
+  // kernel may instead subtract (A dcdf + f_i) - (B dcdf + f_j), A and B the
+  // cell indices less the warp's lowest (|A| <= 6, |B| <= 7), whose rounding
+  // is at most (2|A| + 2|B| + 7) 2^-24 dcd <= 33 2^-24 dcd.  Each component
+  // is then within eps = 40 * 2^-24 dcd (+ 2^-50 R for the FP64 origins) of
+  // x_i - x_j, |x_i - x_j| < 2 dcd, and the FP32 sum of squares adds at most
+  // 5 roundings of 2^-24.  Outside twice that band the FP32 value decides
+  // the test r^2 <= (2h)^2 exactly as the FP64 one would; inside it the FP64
+  // test runs.
   {
     double R2 = 0.0, dmax = 0.0;
     for (int d = 0; d < 3; ++d) {
@@ -210,7 +214,7 @@ int prepare_sim(const SphParams& prm, const SphGeometry& g, int cap, HostSim& hs
       s.dcdf[d] = (float)s.dcd[d];
     }
     double R = std::sqrt(R2);
-    double eps = 8.0 * std::ldexp(dmax, -24) + std::ldexp(R, -50);
+    double eps = 40.0 * std::ldexp(dmax, -24) + std::ldexp(R, -50);
     double err = 3.0 * (2.0 * (2.0 * dmax) * eps + eps * eps) + 5.0 * std::ldexp(s.square_doubleh, -24) * 1.01 +
                  1e-14 * s.square_doubleh;
     double band = 2.0 * err;

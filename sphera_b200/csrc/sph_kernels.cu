@@ -1032,22 +1032,64 @@ struct ListReader {
   }
 };
 
-// r^2 <= (2h)^2 (CalcVarLength.f90:223-228) decided on the FP32 screening
-// copies outside [rr_lo, rr_hi] (a band the host derives from the copies'
-// rounding bounds) and in FP64, exactly as the reference, inside it.
-__device__ __forceinline__ bool accept_pair(const SimDev& s, const Particles& P, const double4& xi, float d0,
-                                            float d1, float d2, int q) {
-  float rf = d0 * d0 + d1 * d1 + d2 * d2;
-  if (rf < s.rr_lo) return true;
-  if (rf > s.rr_hi) return false;
-  double4 xd = P.X[q];
-  double r0 = xi.x - xd.x, r1 = xi.y - xd.y, r2 = xi.z - xd.z;
-  double rr = r0 * r0 + r1 * r1 + r2 * r2;
-  return !(rr > s.square_doubleh);
+// r^2 <= (2h)^2 (CalcVarLength.f90:223-228) is decided on the FP32
+// screening copies outside [rr_lo, rr_hi], a band the host derives from the
+// copies' rounding bounds, and in FP64, exactly as the reference, inside it.
+// A group of lanes whose z cells span at most kRebaseSpan stages candidate z
+// values re-based on the group's lowest cell, (kj - kmin) dcd + f_j, so the
+// z difference costs one subtraction; the band covers that form's rounding
+// too.  Candidates are rejected on the FP32 value alone; the window test
+// (the candidate's z cell within one of the lane's), the NMAXPARTJ cap and
+// the acceptance run only for the few that pass.
+constexpr int kRebaseSpan = 6;
+
+// FP32 r^2 of the lane and staged candidate xj.  REBASE: staged z values
+// are (kj - kmin) dcdf + f_j and zi the lane's own; otherwise the raw
+// offsets f_j with the cell difference formed here.
+template <int DIM, bool REBASE>
+__device__ __forceinline__ float screen_rf(const float4& xj, float ax, float ay, float zi, float fz, int ck, float dz) {
+  float d0 = ax - xj.x;
+  float d1 = (DIM == 3) ? ay - xj.y : 0.f;
+  float d2 = REBASE ? zi - xj.z : ((float)(ck - __float_as_int(xj.w)) * dz + fz) - xj.z;
+  return __fmaf_rn(d2, d2, __fmaf_rn(d1, d1, __fmul_rn(d0, d0)));
+}
+
+// Screens the staged tile of nt candidates for one lane, branch-free: bit u
+// of hitm is set unless candidate u's FP32 r^2 exceeds rr_hi (a certain
+// rejection), bit u of lom when it is below rr_lo (a certain acceptance:
+// such a pair is closer than 2h <= dcd, so the candidate lies in the lane's
+// 3-cell window).  Hits are about one candidate in nine; the band cases
+// (hit, not low) are left to the caller.  Entries past nt are staged far
+// away and never hit, so the tile is screened in blocks of 8.
+template <int DIM, bool REBASE>
+__device__ __forceinline__ void screen_tile(const float4* wbuf, int nt, float ax, float ay, float zi, float fz, int ck,
+                                            float dz, float rr_lo, float rr_hi, unsigned& hitm, unsigned& lom) {
+  unsigned hm = 0u, lm = 0u;
+  for (int u0 = 0; u0 < nt; u0 += 8) {
+    unsigned h8 = 0u, l8 = 0u;
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+      float rf = screen_rf<DIM, REBASE>(wbuf[u0 + c], ax, ay, zi, fz, ck, dz);
+      if (!(rf > rr_hi)) h8 |= 1u << c;
+      if (rf < rr_lo) l8 |= 1u << c;
+    }
+    hm |= h8 << u0;
+    lm |= l8 << u0;
+  }
+  hitm = hm;
+  lom = lm;
+}
+
+// Whether any staged candidate u0 <= u < nt lies in the lane's 3-cell z
+// window (the truncation test once NMAXPARTJ is reached; rare).
+__device__ __forceinline__ bool window_candidate(const float4* wbuf, int u0, int nt, int ck) {
+  for (int u = u0; u < nt; ++u)
+    if ((unsigned)(__float_as_int(wbuf[u].w) - (ck - 1)) <= 2u) return true;
+  return false;
 }
 
 template <int DIM>
-__global__ void __launch_bounds__(kBlock) k_neighbour_lists(DevBatch b) {
+__global__ void __launch_bounds__(kBlock, 3) k_neighbour_lists(DevBatch b) {
   __shared__ SimDev s;
   __shared__ float4 cbuf[kBlock];
   int cur = -1;
@@ -1079,6 +1121,8 @@ __global__ void __launch_bounds__(kBlock) k_neighbour_lists(DevBatch b) {
     const int cap = s.nmaxpartj;
     int4* out = reinterpret_cast<int4*>(b.nlist) + list_base4(p, b.list_cap4);
     int4 pend = make_int4(0, 0, 0, 0);   // entries not yet written, oldest in x
+    const float rr_lo = s.rr_lo, rr_hi = s.rr_hi, dz = s.dcdf[2];
+    bool full = cap <= 0;                            // NMAXPARTJ reached
     while (remaining) {
       int leader = __ffs(remaining) - 1;
       int key = __shfl_sync(FULL, colkey, leader);
@@ -1089,6 +1133,8 @@ __global__ void __launch_bounds__(kBlock) k_neighbour_lists(DevBatch b) {
       int kmax = __reduce_max_sync(FULL, mine ? ck : -0x7fffffff);
       int gci = __shfl_sync(FULL, ci, leader);
       int gcj = __shfl_sync(FULL, cj, leader);
+      const bool rebase = kmax - kmin <= kRebaseSpan;          // uniform over the warp
+      const float zi = rebase ? (float)(ck - kmin) * dz + xf.z : 0.f;
       for (int r = 0; r < NR; ++r) {
         int jr = (DIM == 3) ? gcj - 1 + r / 3 : gcj;
         int ir = gci - 1 + ((DIM == 3) ? r % 3 : r);
@@ -1098,46 +1144,57 @@ __global__ void __launch_bounds__(kBlock) k_neighbour_lists(DevBatch b) {
         int base = s.cell_off + ((jr - 1) * s.ncd[0] + (ir - 1)) * s.ncd[2];
         int ub = __ldg(P.cell_start + base + klo - 1);
         int ue = __ldg(P.cell_start + base + khi);
+        if (mine) {
+          // candidates of this lane's own window (the reference's loop count)
+          int ml = ck > 1 ? ck - 1 : 1, mh = ck < s.ncd[2] ? ck + 1 : s.ncd[2];
+          cand += __ldg(P.cell_start + base + mh) - __ldg(P.cell_start + base + ml - 1);
+        }
         float Dx = (float)(gci - ir) * s.dcdf[0];
         float Dy = (DIM == 3) ? (float)(gcj - jr) * s.dcdf[1] : 0.f;
         float ax = Dx + xf.x, ay = Dy + xf.y;
         const int tag = r << kSlotBits;
         for (int c0 = ub; c0 < ue; c0 += 32) {
           int cidx = c0 + lane;
+          float4 st = (cidx < ue) ? P.XF[cidx] : make_float4(3.0e18f, 3.0e18f, 3.0e18f, __int_as_float(-0x3fffffff));
+          if (rebase && cidx < ue) st.z = (float)(__float_as_int(st.w) - kmin) * dz + st.z;
           __syncwarp();
-          wbuf[lane] = (cidx < ue) ? P.XF[cidx] : make_float4(0.f, 0.f, 0.f, __int_as_float(-0x3fffffff));
+          wbuf[lane] = st;
           __syncwarp();
           if (!mine) continue;
           int nt = ue - c0 < 32 ? ue - c0 : 32;
-          for (int u = 0; u < nt; ++u) {
-            float4 xj = wbuf[u];
-            int kj = __float_as_int(xj.w);
-            float Dz = (float)(ck - kj) * s.dcdf[2];
-            float d0 = ax - xj.x;
-            float d1 = (DIM == 3) ? ay - xj.y : 0.f;
-            float d2 = (Dz + xf.z) - xj.z;
-            float rf = d0 * d0 + d1 * d1 + d2 * d2;
-            bool inwin = (unsigned)(kj - (ck - 1)) <= 2u;
-            if (!inwin || rf > s.rr_hi) {
-              cand += inwin ? 1 : 0;
-              if (inwin && nacc >= cap) trunc = true;
-              continue;
-            }
-            cand++;
-            if (nacc >= cap) {
-              trunc = true;
-              continue;
-            }
-            int q = c0 + u;
-            bool acc = rf < s.rr_lo;
-            if (!acc) {
-              double4 xq = P.X[q];
-              double r0 = xd.x - xq.x, r1 = xd.y - xq.y, r2 = xd.z - xq.z;
+          // phase 1: screening masks of the tile
+          unsigned hitm, lom;
+          if (rebase) screen_tile<DIM, true>(wbuf, nt, ax, ay, zi, xf.z, ck, dz, rr_lo, rr_hi, hitm, lom);
+          else screen_tile<DIM, false>(wbuf, nt, ax, ay, zi, xf.z, ck, dz, rr_lo, rr_hi, hitm, lom);
+          if (full) {
+            // NMAXPARTJ reached: every later candidate of the window is refused
+            if (!trunc && window_candidate(wbuf, 0, nt, ck)) trunc = true;
+            continue;
+          }
+          // phase 2a (rare): resolve band hits -- outside the lane's window
+          // (the reference never visits those) or failing the FP64 test
+          // they are dropped; hitm then holds exactly the accepted ones
+          unsigned band = hitm & ~lom;
+          while (band) {
+            int u = __ffs(band) - 1;
+            band &= band - 1;
+            bool keep = (unsigned)(__float_as_int(wbuf[u].w) - (ck - 1)) <= 2u;
+            if (keep) {
+              double4 xq = P.X[c0 + u], xi = P.X[p];
+              double r0 = xi.x - xq.x, r1 = xi.y - xq.y, r2 = xi.z - xq.z;
               double rr = r0 * r0 + r1 * r1 + r2 * r2;
-              acc = !(rr > s.square_doubleh);
+              keep = !(rr > s.square_doubleh);
             }
-            if (acc) {
+            if (!keep) hitm &= ~(1u << u);
+          }
+          if (nacc + __popc(hitm) >= cap) {
+            // reaching NMAXPARTJ in this tile (rare): accepted ones in
+            // visiting order up to the cap, then the truncation test
+            while (hitm) {
+              int u = __ffs(hitm) - 1;
+              hitm &= hitm - 1;
               nacc++;
+              int q = c0 + u;
               if (q != p) {
                 pend.x = pend.y;
                 pend.y = pend.z;
@@ -1146,7 +1203,29 @@ __global__ void __launch_bounds__(kBlock) k_neighbour_lists(DevBatch b) {
                 cnt++;
                 if ((cnt & 3) == 0) out[(size_t)((cnt >> 2) - 1) * 32] = pend;
               }
+              if (nacc >= cap) {
+                full = true;
+                if (window_candidate(wbuf, u + 1, nt, ck)) trunc = true;   // window candidates follow
+                break;
+              }
             }
+            continue;
+          }
+          // phase 2b: append the accepted ones in visiting order (the lane
+          // itself counted, not stored)
+          nacc += __popc(hitm);
+          unsigned self = (unsigned)(p - c0) < (unsigned)nt ? 1u << (p - c0) : 0u;
+          hitm &= ~self;
+          const int qbase = c0 | tag;                 // c0 + u < 2^28: no carry into the run bits
+          while (hitm) {
+            int u = __ffs(hitm) - 1;
+            hitm &= hitm - 1;
+            pend.x = pend.y;
+            pend.y = pend.z;
+            pend.z = pend.w;
+            pend.w = qbase + u;
+            cnt++;
+            if ((cnt & 3) == 0) out[(size_t)((cnt >> 2) - 1) * 32] = pend;
           }
         }
       }
