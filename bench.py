@@ -37,9 +37,13 @@ import numpy as np  # noqa: E402
 METRIC = "particle-steps/s FP32c vs FP64 at ≤1e-3 rel L2; ensemble p50/p99 time-to-result"
 UNIT = "particle-steps/s"
 KERNELS_PER_STEP = 15          # sph_api.cu step_sequence (3D): momentum, 8 sort, 3 boundary, lists, continuity, finalize
-# algorithmic bytes of the fused momentum kernel per particle: reads X 32,
-# V 32, RP 16, L 1, bdt_count 4, I 4; writes X2 32, V2 32, P2 8, I2 4, L2 1
-MOM_BYTES_PER_PARTICLE = 166
+# algorithmic bytes of the fused FP32c momentum kernel (k_momentum_f32):
+# per particle, each record read once -- X 32, V 32, RP 16, XF 16, VF 16,
+# RF 16 (the neighbours' XF/VF/RF are these same records), L 1, I 4,
+# ncount 4, bdt_count 4 -- and written once -- X2 32, V2 32, P2 8, I2 4,
+# L2 1; plus 4 B per neighbour-list entry and 168 B per boundary entry
+MOM_BYTES_PER_PARTICLE = 218
+LIST_ENTRY_BYTES = 4
 BDT_ENTRY_BYTES = 168
 # Operations per accepted non-self pair: 107 in the momentum pass, 34 in the
 # continuity pass (sqrt and divide counted as one); 9 per candidate test of
@@ -402,7 +406,8 @@ def main():
     value, ms_max, clocks, cnt, diag = r32["value"], r32["ms"], r32["clocks"], r32["cnt"], r32["diag"]
     nprof = r32["nprof"]
     mom_ms = r32["phases"]["momentum"]
-    alg_bytes = n * MOM_BYTES_PER_PARTICLE + diag.bdt_entries * BDT_ENTRY_BYTES
+    list_entries = cnt["pairs"] / nprof - n          # accepted pairs less the particle itself
+    alg_bytes = n * MOM_BYTES_PER_PARTICLE + list_entries * LIST_ENTRY_BYTES + diag.bdt_entries * BDT_ENTRY_BYTES
     hbm_peak, peak_kind = _peaks()
     achieved_gbs = alg_bytes / (mom_ms * 1e-3) / 1e9
     mom_flops = (cnt["pairs"] - n * nprof) * FLOP_MOM_PAIR / nprof

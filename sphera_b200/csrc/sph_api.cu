@@ -500,6 +500,8 @@ using namespace sph;
 struct SphHandle {
   int device = 0;
   cudaStream_t stream = nullptr;
+  cudaStream_t stream2 = nullptr;   // the boundary pass beside the lists (step graph)
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   int nsims = 0;
   int dim = 3;
   int precision = SPH_PREC_FP64;
@@ -604,11 +606,20 @@ void refresh_copies(SphHandle* h, cudaStream_t st) {
   if (h->precision == SPH_PREC_FP32C) launch_refresh_f32(h->db, st);
 }
 
+// One whole step.  The boundary data (SA-SPH, FP64, latency-bound) and the
+// neighbour lists (FP32 screening, issue-bound) both read the freshly sorted
+// state and nothing the other writes, so the boundary pass runs on a second
+// stream beside the lists and the continuity pass waits for both; captured
+// into the step graph this is a fork and a join.
 void step_sequence(SphHandle* h, cudaStream_t st) {
   momentum_pass(h, true, st);
   sort_sequence(h, st);
-  launch_boundary(h->db, st);
+  cudaEventRecord(h->ev_fork, st);
+  cudaStreamWaitEvent(h->stream2, h->ev_fork, 0);
+  launch_boundary(h->db, h->stream2);
+  cudaEventRecord(h->ev_join, h->stream2);
   launch_neighbour_lists(h->db, st);
+  cudaStreamWaitEvent(st, h->ev_join, 0);
   continuity_pass(h, true, st);
   launch_finalize(h->db, 1, st);
 }
@@ -696,7 +707,10 @@ int create_batch(int nsims, const SphParams* params, const SphGeometry* geoms, c
   cudaError_t e = cudaSuccess;
   if (!dry) {
     e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
-    if (e != cudaSuccess) { delete h; return cuda_status(e); }
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->stream2, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming);
+    if (e != cudaSuccess) { sph_destroy(h); return cuda_status(e); }
   }
   size_t N = poff, C = coff;
   Particles& P = h->P;
@@ -879,6 +893,9 @@ void sph_destroy(SphHandle* h) {
     cudaStreamSynchronize(h->stream);
     cudaStreamDestroy(h->stream);
   }
+  if (h->stream2) cudaStreamDestroy(h->stream2);
+  if (h->ev_fork) cudaEventDestroy(h->ev_fork);
+  if (h->ev_join) cudaEventDestroy(h->ev_join);
   cudaGetLastError();
   delete h;
 }

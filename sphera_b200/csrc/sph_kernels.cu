@@ -1032,6 +1032,31 @@ struct ListReader {
   }
 };
 
+// Sequential reader that loads chunk c + 1 while chunk c is consumed, so
+// the list's HBM latency overlaps four pairs' work.
+struct ListPrefetcher {
+  const int4* base;
+  int4 cur, nxt;
+  int nchunks;
+  __device__ __forceinline__ void init(const int* nlist, int p, int cap4, int cnt) {
+    base = reinterpret_cast<const int4*>(nlist) + list_base4(p, cap4);
+    nchunks = (cnt + 3) >> 2;
+    nxt = nchunks > 0 ? __ldg(base) : make_int4(0, 0, 0, 0);
+  }
+  __device__ __forceinline__ int get(int k) {
+    if ((k & 3) == 0) {
+      cur = nxt;
+      int c = (k >> 2) + 1;
+      if (c < nchunks) nxt = __ldg(base + (size_t)c * 32);
+    }
+    int e = cur.x;
+    cur.x = cur.y;
+    cur.y = cur.z;
+    cur.z = cur.w;
+    return e;
+  }
+};
+
 // r^2 <= (2h)^2 (CalcVarLength.f90:223-228) is decided on the FP32
 // screening copies outside [rr_lo, rr_hi], a band the host derives from the
 // copies' rounding bounds, and in FP64, exactly as the reference, inside it.
@@ -1663,8 +1688,8 @@ __global__ void __launch_bounds__(kBlock, 2) k_momentum_f32(DevBatch b) {
     Kahan tp0, tp1, tp2, td0, td1, td2, tv0, tv1, tv2;
     tp0.zero(); tp1.zero(); tp2.zero(); td0.zero(); td1.zero(); td2.zero(); tv0.zero(); tv1.zero(); tv2.zero();
     float cp0 = 0.f, cp1 = 0.f, cp2 = 0.f, cd0 = 0.f, cd1 = 0.f, cd2 = 0.f, cv0 = 0.f, cv1 = 0.f, cv2 = 0.f;
-    ListReader lr;
-    lr.init(b.nlist, p, b.list_cap4);
+    ListPrefetcher lr;
+    lr.init(b.nlist, p, b.list_cap4, cnt);
     const int nmax = __reduce_max_sync(0xffffffffu, (unsigned)cnt);
     for (int k = 0; k < nmax; ++k) {
       int e = lr.get(k);
@@ -1783,8 +1808,8 @@ __global__ void __launch_bounds__(kBlock, 3) k_continuity_f32(DevBatch b) {
     Kahan sum;
     sum.zero();
     float part = 0.f;   // 4-entry partial sum, compensated into sum per chunk
-    ListReader lr;
-    lr.init(b.nlist, p, b.list_cap4);
+    ListPrefetcher lr;
+    lr.init(b.nlist, p, b.list_cap4, cnt);
     const int nmax = __reduce_max_sync(0xffffffffu, (unsigned)cnt);
     for (int k = 0; k < nmax; ++k) {
       int e = lr.get(k);
