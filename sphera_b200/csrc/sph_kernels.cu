@@ -1611,24 +1611,25 @@ __device__ __forceinline__ void kernel_values_f32(const F32Const& c, float rr, f
   PK3 = gw * c.kacl * denom;
 }
 
-// FP32 separation of list entry e from particle (xfi, cell ci, cj, ck).
+// FP32 separation from a neighbour's XF record xj reached through run r.
 template <int DIM>
-__device__ __forceinline__ int separation_f32(const SimDev& s, const Particles& P, int e, const float4& xfi, int ci,
-                                              int cj, int ck, float& d0, float& d1, float& d2) {
-  int q = e & kSlotMask;
-  int r = (int)((unsigned)e >> kSlotBits);   // run 8 sets the top bit
+__device__ __forceinline__ void separation_rec(const SimDev& s, int r, const float4& xj, const float4& xfi, int ci,
+                                               int cj, int ck, float& d0, float& d1, float& d2) {
   int jr = (DIM == 3) ? cj - 1 + r / 3 : cj;
   int ir = ci - 1 + ((DIM == 3) ? r % 3 : r);
-  float4 xj = P.XF[q];
   float Dx = (float)(ci - ir) * s.dcdf[0];
   float Dy = (DIM == 3) ? (float)(cj - jr) * s.dcdf[1] : 0.f;
   float Dz = (float)(ck - __float_as_int(xj.w)) * s.dcdf[2];
   d0 = Dx + (xfi.x - xj.x);
   d1 = (DIM == 3) ? Dy + (xfi.y - xj.y) : 0.f;
   d2 = Dz + (xfi.z - xj.z);
-  return q;
 }
 
+// The pair loop holds only what it needs in registers -- the particle's
+// FP32 values, the compensated sums and the next pair's neighbour records,
+// loaded one pair ahead so their latency overlaps the current pair's
+// arithmetic.  The FP64 boundary terms (an independent sum) and the update
+// run after the loop from a second read of the particle's record.
 template <int DIM, bool FUSED>
 __global__ void __launch_bounds__(kBlock, 2) k_momentum_f32(DevBatch b) {
   __shared__ SimDev s;
@@ -1641,10 +1642,10 @@ __global__ void __launch_bounds__(kBlock, 2) k_momentum_f32(DevBatch b) {
     F32Const fc;
     fc.load(s);
     SimDyn* dyn = b.dyn + tl.sim;
-    const double* geff = dyn->geff;
     int p = tl.start + threadIdx.x;
     bool active = threadIdx.x < tl.count && p < s.p_off + dyn->nag;
     if (FUSED && active && dyn->frozen) {
+      // a finished simulation of a batch: carry the record through the sort
       double4 v4 = P.V[p];
       double2 rp = P.RP[p];
       P.X2[p] = P.X[p];
@@ -1654,35 +1655,22 @@ __global__ void __launch_bounds__(kBlock, 2) k_momentum_f32(DevBatch b) {
       P.L2[p] = P.L[p];
       active = false;
     }
-    double4 xi = make_double4(0.0, 0.0, 0.0, 0.0);
-    double vi[3] = {0.0, 0.0, 0.0};
-    double rhoi = 1.0, pi = 0.0;
-    int lam = 0, nb = 0, bstart = 0, cnt = 0;
-    double tpres[3] = {0, 0, 0}, tdiss[3] = {0, 0, 0}, tvisc[3] = {0, 0, 0};
-    int ci = 0, cj = 0, ck = 0;
+    int ci = 0, cj = 0, ck = 0, cnt = 0;
+    float4 xfi = make_float4(0.f, 0.f, 0.f, 0.f);
+    float vix = 0.f, viy = 0.f, viz = 0.f, rhof = 1.f, Pi = 0.f;
     if (active) {
-      xi = P.X[p];
+      double4 xi = P.X[p];
       double4 v4 = P.V[p];
       double2 rp = P.RP[p];
-      vi[0] = v4.x;
-      vi[1] = v4.y;
-      vi[2] = v4.z;
-      rhoi = rp.x;
-      pi = rp.y;
-      lam = P.L[p];
-      cnt = b.ncount[p];
-      nb = P.bdt_count[p];
-      bstart = nb > 0 ? P.bdt_start[p] : 0;
-      if (nb > 0) {
-        if (DIM == 3) me_boundary3d(s, b, nb, bstart, vi, rhoi, pi, lam, geff, tpres, tdiss, tvisc);
-        else me_boundary2d(s, b, nb, bstart, vi, rhoi, pi, lam, geff, tpres, tdiss, tvisc);
-      }
       particle_cell(s, xi.x, xi.y, xi.z, ci, cj, ck);
+      xfi = P.XF[p];
+      vix = (float)v4.x;
+      viy = (float)v4.y;
+      viz = (float)v4.z;
+      rhof = (float)rp.x;
+      Pi = (float)(rp.y / (rp.x * rp.x));
+      cnt = b.ncount[p];
     }
-    float4 xfi = active ? P.XF[p] : make_float4(0.f, 0.f, 0.f, 0.f);
-    const float vix = (float)vi[0], viy = (float)vi[1], viz = (float)vi[2];
-    const float rhof = (float)rhoi;
-    const float Pi = (float)(pi / (rhoi * rhoi));
     const bool morris = s.kin_visc > 1.0e-12;
     // compensated sums of 4-entry partial sums (one list chunk each)
     Kahan tp0, tp1, tp2, td0, td1, td2, tv0, tv1, tv2;
@@ -1691,16 +1679,31 @@ __global__ void __launch_bounds__(kBlock, 2) k_momentum_f32(DevBatch b) {
     ListPrefetcher lr;
     lr.init(b.nlist, p, b.list_cap4, cnt);
     const int nmax = __reduce_max_sync(0xffffffffu, (unsigned)cnt);
+    int ne = 0;
+    float4 nx = make_float4(0.f, 0.f, 0.f, 0.f), nv = nx, nr = nx;
+    if (cnt > 0) {
+      ne = lr.get(0);
+      int q = ne & kSlotMask;
+      nx = P.XF[q];
+      nv = P.VF[q];
+      nr = P.RF[q];
+    }
     for (int k = 0; k < nmax; ++k) {
-      int e = lr.get(k);
+      const int e = ne;
+      const float4 xj = nx, vj = nv, rfj = nr;
+      if (k + 1 < cnt) {
+        ne = lr.get(k + 1);
+        int q = ne & kSlotMask;
+        nx = P.XF[q];
+        nv = P.VF[q];
+        nr = P.RF[q];
+      }
       if (k >= cnt) continue;
       float d0, d1, d2;
-      int q = separation_f32<DIM>(s, P, e, xfi, ci, cj, ck, d0, d1, d2);
+      separation_rec<DIM>(s, (int)((unsigned)e >> kSlotBits), xj, xfi, ci, cj, ck, d0, d1, d2);
       float rr = d0 * d0 + d1 * d1 + d2 * d2;
       float PK1, PK2, PK3;
       kernel_values_f32(fc, rr, PK1, PK2, PK3);
-      float4 vj = P.VF[q];
-      float4 rfj = P.RF[q];
       float mj = rfj.z;
       // pressure (both accumulators of inter_EqMoto together)
       float pf = -(mj * (Pi + rfj.y) * PK3);
@@ -1731,6 +1734,19 @@ __global__ void __launch_bounds__(kBlock, 2) k_momentum_f32(DevBatch b) {
     }
     double dtc = 1.0e300;
     if (active) {
+      double4 v4 = P.V[p];
+      double2 rp = P.RP[p];
+      const double vi[3] = {v4.x, v4.y, v4.z};
+      const double rhoi = rp.x, pi = rp.y;
+      const int nb = P.bdt_count[p];
+      const int bstart = nb > 0 ? P.bdt_start[p] : 0;
+      double tpres[3] = {0, 0, 0}, tdiss[3] = {0, 0, 0}, tvisc[3] = {0, 0, 0};
+      const double* geff = dyn->geff;
+      if (nb > 0) {
+        const int lam = P.L[p];
+        if (DIM == 3) me_boundary3d(s, b, nb, bstart, vi, rhoi, pi, lam, geff, tpres, tdiss, tvisc);
+        else me_boundary2d(s, b, nb, bstart, vi, rhoi, pi, lam, geff, tpres, tdiss, tvisc);
+      }
       double rs0 = tv0.val(), rs1 = tv1.val(), rs2 = tv2.val();
       tpres[0] = tpres[0] + tp0.val();
       tpres[1] = tpres[1] + tp1.val();
@@ -1753,6 +1769,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_momentum_f32(DevBatch b) {
         for (int d = 0; d < 3; ++d) acc[d] = acc[d] + R[d];
       }
       if (FUSED) {
+        double4 xi = P.X[p];
         double dtvel = dyn->dtvel, dt = dyn->dt;
         double vn[3];
         for (int d = 0; d < 3; ++d) vn[d] = vi[d] + dtvel * acc[d];
@@ -1789,37 +1806,48 @@ __global__ void __launch_bounds__(kBlock, 3) k_continuity_f32(DevBatch b) {
     SimDyn* dyn = b.dyn + tl.sim;
     int p = tl.start + threadIdx.x;
     bool active = threadIdx.x < tl.count && p < s.p_off + dyn->nag && !(FUSED && dyn->frozen);
-    double4 xi = make_double4(0.0, 0.0, 0.0, 0.0);
-    double4 vi = make_double4(0.0, 0.0, 0.0, 0.0);
-    double rhoi = 1.0, dden = 0.0;
     int ci = 0, cj = 0, ck = 0, cnt = 0;
+    float4 xfi = make_float4(0.f, 0.f, 0.f, 0.f);
+    float vix = 0.f, viy = 0.f, viz = 0.f, rhof = 1.f;
     if (active) {
-      xi = P.X[p];
-      vi = P.V[p];
-      rhoi = P.RP[p].x;
-      cnt = b.ncount[p];
-      int nb = P.bdt_count[p];
-      if (nb > 0) dden = continuity_boundary<DIM>(s, b, dyn, nb, P.bdt_start[p], vi, rhoi);
+      double4 xi = P.X[p];
+      double4 vi = P.V[p];
       particle_cell(s, xi.x, xi.y, xi.z, ci, cj, ck);
+      xfi = P.XF[p];
+      vix = (float)vi.x;
+      viy = (float)vi.y;
+      viz = (float)vi.z;
+      rhof = (float)P.RP[p].x;
+      cnt = b.ncount[p];
     }
-    float4 xfi = active ? P.XF[p] : make_float4(0.f, 0.f, 0.f, 0.f);
-    const float vix = (float)vi.x, viy = (float)vi.y, viz = (float)vi.z;
-    const float rhof = (float)rhoi;
     Kahan sum;
     sum.zero();
     float part = 0.f;   // 4-entry partial sum, compensated into sum per chunk
     ListPrefetcher lr;
     lr.init(b.nlist, p, b.list_cap4, cnt);
     const int nmax = __reduce_max_sync(0xffffffffu, (unsigned)cnt);
+    // the next pair's records, loaded one pair ahead
+    int ne = 0;
+    float4 nx = make_float4(0.f, 0.f, 0.f, 0.f), nv = nx;
+    if (cnt > 0) {
+      ne = lr.get(0);
+      nx = P.XF[ne & kSlotMask];
+      nv = P.VF[ne & kSlotMask];
+    }
     for (int k = 0; k < nmax; ++k) {
-      int e = lr.get(k);
+      const int e = ne;
+      const float4 xj = nx, vj = nv;
+      if (k + 1 < cnt) {
+        ne = lr.get(k + 1);
+        nx = P.XF[ne & kSlotMask];
+        nv = P.VF[ne & kSlotMask];
+      }
       if (k >= cnt) continue;
       float d0, d1, d2;
-      int q = separation_f32<DIM>(s, P, e, xfi, ci, cj, ck, d0, d1, d2);
+      separation_rec<DIM>(s, (int)((unsigned)e >> kSlotBits), xj, xfi, ci, cj, ck, d0, d1, d2);
       float rr = d0 * d0 + d1 * d1 + d2 * d2;
       float PK1, PK2, PK3;
       kernel_values_f32(fc, rr, PK1, PK2, PK3);
-      float4 vj = P.VF[q];
       float c = rhof * vj.w * PK1;    // rho_i (m_j / rho_j) PK1
       part += c * ((vj.x - vix) * d0 + (vj.y - viy) * d1 + (vj.z - viz) * d2);
       if ((k & 3) == 3 || k == cnt - 1) {
@@ -1828,6 +1856,12 @@ __global__ void __launch_bounds__(kBlock, 3) k_continuity_f32(DevBatch b) {
       }
     }
     if (active) {
+      // the FP64 boundary term (an independent sum) after the pair loop
+      const double4 vi = P.V[p];
+      const double rhoi = P.RP[p].x;
+      double dden = 0.0;
+      const int nb = P.bdt_count[p];
+      if (nb > 0) dden = continuity_boundary<DIM>(s, b, dyn, nb, P.bdt_start[p], vi, rhoi);
       dden = dden - sum.val();
       if (FUSED) {
         double rho = rhoi + dyn->dt * dden;
@@ -1837,7 +1871,7 @@ __global__ void __launch_bounds__(kBlock, 3) k_continuity_f32(DevBatch b) {
         }
         double pr = s.k_over_rho0 * (rho - s.den0) + s.p_ref;
         P.RP[p] = make_double2(rho, pr);
-        P.RF[p] = make_float4((float)rho, (float)(pr / (rho * rho)), (float)xi.w, 0.f);
+        P.RF[p] = make_float4((float)rho, (float)(pr / (rho * rho)), (float)P.X[p].w, 0.f);
       } else {
         P.DDEN[p] = dden;
       }
