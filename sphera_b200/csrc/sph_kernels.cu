@@ -452,8 +452,37 @@ __global__ void k_rank_reference(DevBatch b, const int* __restrict__ cstart, int
 // ==========================================================================
 
 // ComputeBoundaryVolumeIntegrals_P0.f90:81-155 for one (particle, face).
+// The point-in-face test of one face held in registers (the same arithmetic
+// as point_internal).
+struct FaceTest {
+  double a0, a1, b0, b1, c0, c1, u;
+  int fkod;
+  __device__ __forceinline__ void load(const FaceDev& f) {
+    a0 = f.AA[0];
+    a1 = f.AA[1];
+    b0 = f.BB[0];
+    b1 = f.BB[1];
+    c0 = f.CC[0];
+    c1 = f.CC[1];
+    u = f.usu_due_area;
+    fkod = f.fkod;
+  }
+  __device__ __forceinline__ bool inside(double px, double py) const {
+    double k0 = (a0 + b0 * px + c0 * py) * u;
+    double k1 = (a1 + b1 * px + c1 * py) * u;
+    if (fkod == 2) return !(k0 < 0.0 || k0 > 1.0 || k1 < 0.0 || k1 > 1.0);
+    if (fkod == 1) {
+      double k2 = 1.0 - (k0 + k1);
+      return !(k0 < 0.0 || k0 > 1.0 || k1 < 0.0 || k1 > 1.0 || k2 < 0.0 || k2 > 1.0);
+    }
+    return false;
+  }
+};
+
 __device__ void face_integrals(const SimDev& s, const double* __restrict__ bit, const FaceDev& f,
                                const double* locx, BdtEntry& e) {
+  FaceTest ft;
+  ft.load(f);
   double IntWdV = 0.0, IntdWrm1dV = 0.0, IntGWZrm1dV = 0.0;
   double G0 = 0.0, G1 = 0.0, G2 = 0.0;
   double R00 = 0.0, R01 = 0.0, R02 = 0.0, R11 = 0.0, R12 = 0.0, R22 = 0.0;
@@ -474,7 +503,7 @@ __device__ void face_integrals(const SimDev& s, const double* __restrict__ bit, 
         double lpj1 = L1 + row[1];
         double px0 = L0 + (lpj0 - L0) * tsegnato;
         double px1 = L1 + (lpj1 - L1) * tsegnato;
-        if (!point_internal(f, px0, px1)) continue;
+        if (!ft.inside(px0, px1)) continue;
         double d0 = px0 - L0, d1 = px1 - L1, d2 = 0.0 - L2;
         double dist = sqrt(d0 * d0 + d1 * d1 + d2 * d2);
         double rob = dist / s.h;
@@ -606,16 +635,33 @@ __global__ void __launch_bounds__(kBlock) k_boundary3d(DevBatch b) {
 // pass allocated, one (particle, face) per thread: the quadrature costs are
 // balanced across the GPU whatever the particles' distribution over tiles.
 __global__ void __launch_bounds__(128) k_boundary3d_integrals(DevBatch b) {
+  // the simulation constants and hemisphere table of the chunk's first
+  // entry, staged in shared memory (a batch chunk can mix simulations:
+  // entries of another one read theirs from global memory)
+  __shared__ SimDev ssim;
+  __shared__ double sbit[kBitRows * 7];
+  int loaded = -1;
   int used = b.dyn[b.nsims].bdt_used;
   if (used > b.P.bdt_cap) used = b.P.bdt_cap;
-  for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < used; idx += gridDim.x * blockDim.x) {
+  for (int base = blockIdx.x * blockDim.x; base < used; base += gridDim.x * blockDim.x) {
+    const int first = b.P.bdt[base].pad;
+    if (first != loaded) {
+      load_sim(ssim, b.sims, first, loaded);
+      const double* src = b.bit + (size_t)first * kBitRows * 7;
+      for (int i = threadIdx.x; i < kBitRows * 7; i += blockDim.x) sbit[i] = src[i];
+      __syncthreads();
+    }
+    const int idx = base + threadIdx.x;
+    if (idx >= used) continue;
     BdtEntry& e = b.P.bdt[idx];
-    int sim = e.pad;
-    const SimDev& s = b.sims[sim];
+    const int sim = e.pad;
+    const bool mine = sim == loaded;
+    const SimDev& s = mine ? ssim : b.sims[sim];
+    const double* bit = mine ? sbit : b.bit + (size_t)sim * kBitRows * 7;
     const FaceDev& f = b.faces[s.face_off + e.clobonum - 1];
     double locx[3] = {e.loc[0], e.loc[1], e.loc[2]};
     BdtEntry r;
-    face_integrals(s, b.bit + (size_t)sim * kBitRows * 7, f, locx, r);
+    face_integrals(s, bit, f, locx, r);
     for (int q = 0; q < 8; ++q) e.bi[q] = r.bi[q];
     for (int q = 0; q < 9; ++q) e.ig[q] = r.ig[q];
   }
