@@ -1061,22 +1061,6 @@ __device__ __forceinline__ size_t list_base4(int p, int cap4) {
   return (size_t)(p >> 5) * (size_t)cap4 * 32 + (size_t)(p & 31);
 }
 
-// Sequential reader of one particle's list.
-struct ListReader {
-  const int4* base;
-  int4 cur;
-  __device__ __forceinline__ void init(const int* nlist, int p, int cap4) {
-    base = reinterpret_cast<const int4*>(nlist) + list_base4(p, cap4);
-  }
-  __device__ __forceinline__ int get(int k) {
-    if ((k & 3) == 0) cur = __ldg(base + (size_t)(k >> 2) * 32);
-    int e = cur.x;
-    cur.x = cur.y;
-    cur.y = cur.z;
-    cur.z = cur.w;
-    return e;
-  }
-};
 
 // Sequential reader that loads chunk c + 1 while chunk c is consumed, so
 // the list's HBM latency overlaps four pairs' work.
@@ -1330,6 +1314,7 @@ __global__ void __launch_bounds__(kBlock, 3) k_neighbour_lists(DevBatch b) {
 template <int DIM, bool FUSED>
 __global__ void __launch_bounds__(kBlock, 2) k_momentum(DevBatch b) {
   __shared__ SimDev s;
+  __shared__ double stpres[3][kBlock];   // the wall pressure term, kept out of the pair loop's registers
   int cur = -1;
   const Particles& P = b.P;
   const double GI = (double)9.80665f;   // Static_allocation_module.f90:72, a default-REAL literal
@@ -1354,8 +1339,8 @@ __global__ void __launch_bounds__(kBlock, 2) k_momentum(DevBatch b) {
     double4 xi = make_double4(0.0, 0.0, 0.0, 0.0);
     double vi[3] = {0.0, 0.0, 0.0};
     double rhoi = 1.0, pi = 0.0;
-    int lam = 0, nb = 0, bstart = 0, cnt = 0;
-    double tpres[3] = {0, 0, 0}, tdiss[3] = {0, 0, 0}, tvisc[3] = {0, 0, 0};
+    int cnt = 0;
+    double tdiss[3] = {0, 0, 0}, tvisc[3] = {0, 0, 0};
     if (active) {
       xi = P.X[p];
       double4 v4 = P.V[p];
@@ -1365,14 +1350,16 @@ __global__ void __launch_bounds__(kBlock, 2) k_momentum(DevBatch b) {
       vi[2] = v4.z;
       rhoi = rp.x;
       pi = rp.y;
-      lam = P.L[p];
       cnt = b.ncount[p];
-      nb = P.bdt_count[p];
-      bstart = nb > 0 ? P.bdt_start[p] : 0;
+      const int nb = P.bdt_count[p];
+      double tpres[3] = {0, 0, 0};
       if (nb > 0) {
+        const int lam = P.L[p];
+        const int bstart = P.bdt_start[p];
         if (DIM == 3) me_boundary3d(s, b, nb, bstart, vi, rhoi, pi, lam, geff, tpres, tdiss, tvisc);
         else me_boundary2d(s, b, nb, bstart, vi, rhoi, pi, lam, geff, tpres, tdiss, tvisc);
       }
+      for (int d = 0; d < 3; ++d) stpres[d][threadIdx.x] = tpres[d];
     }
     double tp0 = 0, tp1 = 0, tp2 = 0, al0 = 0, al1 = 0, al2 = 0;
     double td0 = tdiss[0], td1 = tdiss[1], td2 = tdiss[2];
@@ -1381,8 +1368,8 @@ __global__ void __launch_bounds__(kBlock, 2) k_momentum(DevBatch b) {
     const double celt = s.celerita + s.celerita;
     const bool morris = s.kin_visc > 1.0e-12;
     const double nu = s.kin_visc;
-    ListReader lr;
-    lr.init(b.nlist, p, b.list_cap4);
+    ListPrefetcher lr;
+    lr.init(b.nlist, p, b.list_cap4, cnt);
     const int nmax = __reduce_max_sync(0xffffffffu, (unsigned)cnt);
     for (int k = 0; k < nmax; ++k) {
       int e = lr.get(k);
@@ -1433,9 +1420,12 @@ __global__ void __launch_bounds__(kBlock, 2) k_momentum(DevBatch b) {
     }
     double dtc = 1.0e300;
     if (active) {
-      tpres[0] = tpres[0] + tp0 + al0;
-      tpres[1] = tpres[1] + tp1 + al1;
-      tpres[2] = tpres[2] + tp2 + al2;
+      double tpres[3];
+      tpres[0] = stpres[0][threadIdx.x] + tp0 + al0;
+      tpres[1] = stpres[1][threadIdx.x] + tp1 + al1;
+      tpres[2] = stpres[2][threadIdx.x] + tp2 + al2;
+      const int nb = P.bdt_count[p];
+      const int bstart = nb > 0 ? P.bdt_start[p] : 0;
       // laminar_flag, inter_EqMoto.f90:269-283
       int lam_new = 0;
       if (s.kin_visc > 0.0) {
@@ -1564,8 +1554,8 @@ __global__ void __launch_bounds__(kBlock, 2) k_continuity(DevBatch b) {
       if (nb > 0) dden = continuity_boundary<DIM>(s, b, dyn, nb, P.bdt_start[p], vi, rhoi);
     }
     double a1 = 0.0, a2 = 0.0, a3 = 0.0;
-    ListReader lr;
-    lr.init(b.nlist, p, b.list_cap4);
+    ListPrefetcher lr;
+    lr.init(b.nlist, p, b.list_cap4, cnt);
     const int nmax = __reduce_max_sync(0xffffffffu, (unsigned)cnt);
     for (int k = 0; k < nmax; ++k) {
       int e = lr.get(k);
