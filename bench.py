@@ -36,7 +36,9 @@ import numpy as np  # noqa: E402
 
 METRIC = "particle-steps/s FP32c vs FP64 at ≤1e-3 rel L2; ensemble p50/p99 time-to-result"
 UNIT = "particle-steps/s"
-KERNELS_PER_STEP = 15          # sph_api.cu step_sequence (3D): momentum, 8 sort, 3 boundary, lists, continuity, finalize
+# launches of one FP32c step graph (3D, sph_api.cu step_sequence): momentum,
+# 8 sort, 3 boundary, lists, continuity pair sums, continuity finish, finalize
+KERNELS_PER_STEP = 16
 # algorithmic bytes of the fused FP32c momentum kernel (k_momentum_f32):
 # per particle, each record read once -- X 32, V 32, RP 16, XF 16, VF 16,
 # RF 16 (the neighbours' XF/VF/RF are these same records), L 1, I 4,

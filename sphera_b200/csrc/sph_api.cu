@@ -609,8 +609,10 @@ void refresh_copies(SphHandle* h, cudaStream_t st) {
 // One whole step.  The boundary data (SA-SPH, FP64, latency-bound) and the
 // neighbour lists (FP32 screening, issue-bound) both read the freshly sorted
 // state and nothing the other writes, so the boundary pass runs on a second
-// stream beside the lists and the continuity pass waits for both; captured
-// into the step graph this is a fork and a join.
+// stream beside the lists; captured into the step graph this is a fork and
+// a join.  The FP64 continuity pass starts its sum from the wall term (the
+// reference's order) and waits for both; the FP32c pass sums the pairs
+// beside the boundary pass too and adds the wall term after the join.
 void step_sequence(SphHandle* h, cudaStream_t st) {
   momentum_pass(h, true, st);
   sort_sequence(h, st);
@@ -619,8 +621,14 @@ void step_sequence(SphHandle* h, cudaStream_t st) {
   launch_boundary(h->db, h->stream2);
   cudaEventRecord(h->ev_join, h->stream2);
   launch_neighbour_lists(h->db, st);
-  cudaStreamWaitEvent(st, h->ev_join, 0);
-  continuity_pass(h, true, st);
+  if (h->precision == SPH_PREC_FP32C) {
+    launch_continuity_f32_pairs(h->db, st);
+    cudaStreamWaitEvent(st, h->ev_join, 0);
+    launch_continuity_f32_finish(h->db, true, st);
+  } else {
+    cudaStreamWaitEvent(st, h->ev_join, 0);
+    continuity_pass(h, true, st);
+  }
   launch_finalize(h->db, 1, st);
 }
 

@@ -1829,7 +1829,12 @@ __global__ void __launch_bounds__(kBlock, 2) k_momentum_f32(DevBatch b) {
   }
 }
 
-template <int DIM, bool FUSED>
+// Continuity, FP32c form, in two launches so that the pair sum need not
+// wait for the boundary data: k_continuity_f32 writes the compensated pair
+// sum of each particle to DDEN, and k_continuity_f32_finish, once the
+// boundary data exist, forms dden = (SA-SPH wall term) - (pair sum) and, in
+// the fused step, Leapfrog_continuity and the EoS.
+template <int DIM>
 __global__ void __launch_bounds__(kBlock, 3) k_continuity_f32(DevBatch b) {
   __shared__ SimDev s;
   int cur = -1;
@@ -1841,7 +1846,7 @@ __global__ void __launch_bounds__(kBlock, 3) k_continuity_f32(DevBatch b) {
     fc.load(s);
     SimDyn* dyn = b.dyn + tl.sim;
     int p = tl.start + threadIdx.x;
-    bool active = threadIdx.x < tl.count && p < s.p_off + dyn->nag && !(FUSED && dyn->frozen);
+    bool active = threadIdx.x < tl.count && p < s.p_off + dyn->nag && !dyn->frozen;
     int ci = 0, cj = 0, ck = 0, cnt = 0;
     float4 xfi = make_float4(0.f, 0.f, 0.f, 0.f);
     float vix = 0.f, viy = 0.f, viz = 0.f, rhof = 1.f;
@@ -1891,26 +1896,38 @@ __global__ void __launch_bounds__(kBlock, 3) k_continuity_f32(DevBatch b) {
         part = 0.f;
       }
     }
-    if (active) {
-      // the FP64 boundary term (an independent sum) after the pair loop
-      const double4 vi = P.V[p];
-      const double rhoi = P.RP[p].x;
-      double dden = 0.0;
-      const int nb = P.bdt_count[p];
-      if (nb > 0) dden = continuity_boundary<DIM>(s, b, dyn, nb, P.bdt_start[p], vi, rhoi);
-      dden = dden - sum.val();
-      if (FUSED) {
-        double rho = rhoi + dyn->dt * dden;
-        if (s.density_thresholds == 1) {
-          if (rho < 0.9 * s.den0) rho = 0.9 * s.den0;
-          if (rho > 1.1 * s.den0) rho = 1.1 * s.den0;
-        }
-        double pr = s.k_over_rho0 * (rho - s.den0) + s.p_ref;
-        P.RP[p] = make_double2(rho, pr);
-        P.RF[p] = make_float4((float)rho, (float)(pr / (rho * rho)), (float)P.X[p].w, 0.f);
-      } else {
-        P.DDEN[p] = dden;
+    if (active) P.DDEN[p] = sum.val();
+  }
+}
+
+template <int DIM, bool FUSED>
+__global__ void __launch_bounds__(kBlock) k_continuity_f32_finish(DevBatch b) {
+  __shared__ SimDev s;
+  int cur = -1;
+  const Particles& P = b.P;
+  for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
+    Tile tl = b.tiles[t];
+    load_sim(s, b.sims, tl.sim, cur);
+    SimDyn* dyn = b.dyn + tl.sim;
+    int p = tl.start + threadIdx.x;
+    if (!(threadIdx.x < tl.count && p < s.p_off + dyn->nag && !dyn->frozen)) continue;
+    const double4 vi = P.V[p];
+    const double rhoi = P.RP[p].x;
+    double dden = 0.0;
+    const int nb = P.bdt_count[p];
+    if (nb > 0) dden = continuity_boundary<DIM>(s, b, dyn, nb, P.bdt_start[p], vi, rhoi);
+    dden = dden - P.DDEN[p];
+    if (FUSED) {
+      double rho = rhoi + dyn->dt * dden;
+      if (s.density_thresholds == 1) {
+        if (rho < 0.9 * s.den0) rho = 0.9 * s.den0;
+        if (rho > 1.1 * s.den0) rho = 1.1 * s.den0;
       }
+      double pr = s.k_over_rho0 * (rho - s.den0) + s.p_ref;
+      P.RP[p] = make_double2(rho, pr);
+      P.RF[p] = make_float4((float)rho, (float)(pr / (rho * rho)), (float)P.X[p].w, 0.f);
+    } else {
+      P.DDEN[p] = dden;
     }
   }
 }
@@ -2387,15 +2404,26 @@ void launch_momentum_f32(const DevBatch& b, bool fused, cudaStream_t st) {
   }
 }
 
-void launch_continuity_f32(const DevBatch& b, bool fused, cudaStream_t st) {
+void launch_continuity_f32_pairs(const DevBatch& b, cudaStream_t st) {
   int g = blocks_for(b, kGridContinuity);
+  if (b.dim == 3) k_continuity_f32<3><<<g, kBlock, 0, st>>>(b);
+  else k_continuity_f32<2><<<g, kBlock, 0, st>>>(b);
+}
+
+void launch_continuity_f32_finish(const DevBatch& b, bool fused, cudaStream_t st) {
+  int g = blocks_for(b);
   if (b.dim == 3) {
-    if (fused) k_continuity_f32<3, true><<<g, kBlock, 0, st>>>(b);
-    else k_continuity_f32<3, false><<<g, kBlock, 0, st>>>(b);
+    if (fused) k_continuity_f32_finish<3, true><<<g, kBlock, 0, st>>>(b);
+    else k_continuity_f32_finish<3, false><<<g, kBlock, 0, st>>>(b);
   } else {
-    if (fused) k_continuity_f32<2, true><<<g, kBlock, 0, st>>>(b);
-    else k_continuity_f32<2, false><<<g, kBlock, 0, st>>>(b);
+    if (fused) k_continuity_f32_finish<2, true><<<g, kBlock, 0, st>>>(b);
+    else k_continuity_f32_finish<2, false><<<g, kBlock, 0, st>>>(b);
   }
+}
+
+void launch_continuity_f32(const DevBatch& b, bool fused, cudaStream_t st) {
+  launch_continuity_f32_pairs(b, st);
+  launch_continuity_f32_finish(b, fused, st);
 }
 
 void launch_refresh_f32(const DevBatch& b, cudaStream_t st) { k_refresh_f32<<<blocks_for(b), kBlock, 0, st>>>(b); }

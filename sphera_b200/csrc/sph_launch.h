@@ -56,7 +56,9 @@ void launch_momentum(const DevBatch& b, bool fused, cudaStream_t st);
 void launch_continuity(const DevBatch& b, bool fused, cudaStream_t st);
 // physics (FP32-compensated form)
 void launch_momentum_f32(const DevBatch& b, bool fused, cudaStream_t st);
-void launch_continuity_f32(const DevBatch& b, bool fused, cudaStream_t st);
+void launch_continuity_f32(const DevBatch& b, bool fused, cudaStream_t st);   // pairs + finish
+void launch_continuity_f32_pairs(const DevBatch& b, cudaStream_t st);
+void launch_continuity_f32_finish(const DevBatch& b, bool fused, cudaStream_t st);
 void launch_refresh_f32(const DevBatch& b, cudaStream_t st);
 void launch_leapfrog_momentum(const DevBatch& b, cudaStream_t st);
 void launch_leapfrog_trajectories(const DevBatch& b, cudaStream_t st);
