@@ -1835,7 +1835,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_momentum_f32(DevBatch b) {
 // boundary data exist, forms dden = (SA-SPH wall term) - (pair sum) and, in
 // the fused step, Leapfrog_continuity and the EoS.
 template <int DIM>
-__global__ void __launch_bounds__(kBlock, 3) k_continuity_f32(DevBatch b) {
+__global__ void __launch_bounds__(kBlock, 4) k_continuity_f32(DevBatch b) {
   __shared__ SimDev s;
   int cur = -1;
   const Particles& P = b.P;
