@@ -36,15 +36,18 @@ import numpy as np  # noqa: E402
 
 METRIC = "particle-steps/s FP32c vs FP64 at ≤1e-3 rel L2; ensemble p50/p99 time-to-result"
 UNIT = "particle-steps/s"
-# launches of one FP32c step graph (3D, sph_api.cu step_sequence): momentum,
-# 8 sort, 3 boundary, lists, continuity pair sums, continuity finish, finalize
-KERNELS_PER_STEP = 16
-# algorithmic bytes of the fused FP32c momentum kernel (k_momentum_f32):
-# per particle, each record read once -- X 32, V 32, RP 16, XF 16, VF 16,
-# RF 16 (the neighbours' XF/VF/RF are these same records), L 1, I 4,
-# ncount 4, bdt_count 4 -- and written once -- X2 32, V2 32, P2 8, I2 4,
-# L2 1; plus 4 B per neighbour-list entry and 168 B per boundary entry
-MOM_BYTES_PER_PARTICLE = 218
+# launches of one FP32c step graph (3D, sph_api.cu step_sequence): momentum
+# pair sums and finish, 8 sort, 3 boundary, lists, continuity pair sums and
+# finish, finalize
+KERNELS_PER_STEP = 17
+# algorithmic bytes of the fused FP32c momentum pass (k_momentum_f32 pair
+# sums + k_momentum_f32_finish): per particle, each record read once -- X 32,
+# V 32, RP 16, XF 16, VF 16, RF 16 (the neighbours' XF/VF/RF are these same
+# records), L 1, I 4, ncount 4, bdt_count 4 -- and written once -- X2 32,
+# V2 32, P2 8, I2 4, L2 1 -- plus the nine pair sums passed between the two
+# launches (72 B written, 72 B read); 4 B per neighbour-list entry and 168 B
+# per boundary entry
+MOM_BYTES_PER_PARTICLE = 362
 LIST_ENTRY_BYTES = 4
 BDT_ENTRY_BYTES = 168
 # Operations per accepted non-self pair: 107 in the momentum pass, 34 in the
@@ -476,7 +479,7 @@ def main():
                 "path": "sph_upload + sph_step_async(1) + sph_download per step, pinned host buffers, fp32c form"},
         "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": hbm_peak, "unit": "GB/s",
                      "frac": achieved_gbs / hbm_peak, "traffic": traffic,
-                     "kernel": "k_momentum_f32<3,true> (fused momentum + leapfrog)",
+                     "kernel": "k_momentum_f32<3> + k_momentum_f32_finish<3,true> (momentum pair sums; wall terms, leapfrog)",
                      "peak_kind": f"{peak_kind} HBM copy bandwidth",
                      "fp": {"achieved_tflops": mom_tflops, "peak_tflops": fp32_peak,
                             "frac": mom_tflops / fp32_peak, "peak_kind": "measured FP32 FMA rate (in-run)"}},

@@ -157,6 +157,7 @@ struct Particles {
   // outputs of the fine-grained calls
   double4* ACC;     // dv/dt
   double* DDEN;     // drho/dt
+  double* MSUM;     // FP32c momentum pair sums of a slot: 9 values (pressure, Monaghan, Morris x 3)
   // removal replay
   uint8_t* out_flag;   // by caller index
   int* id_remap;       // by caller index

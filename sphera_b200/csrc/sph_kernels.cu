@@ -1661,17 +1661,20 @@ __device__ __forceinline__ void separation_rec(const SimDev& s, int r, const flo
   d2 = Dz + (xfi.z - xj.z);
 }
 
-// The pair loop holds only what it needs in registers -- the particle's
-// FP32 values, the compensated sums and the next pair's neighbour records,
-// loaded one pair ahead so their latency overlaps the current pair's
-// arithmetic.  The FP64 boundary terms (an independent sum) and the update
-// run after the loop from a second read of the particle's record.
-template <int DIM, bool FUSED>
-__global__ void __launch_bounds__(kBlock, 2) k_momentum_f32(DevBatch b) {
+// Momentum, FP32c form, in two launches.  k_momentum_f32 holds only what
+// the pair loop needs -- the particle's FP32 values, the compensated sums,
+// the list chunk being read and the next one -- so that it runs at 3 blocks
+// of 256 per SM without spilling (gathers are latency-bound: occupancy pays
+// more than loading the next pair's records ahead), and writes the nine
+// compensated sums of each particle to MSUM.
+// k_momentum_f32_finish adds the FP64 wall terms (an independent sum), the
+// laminar flag, gravity and the elastic reaction and, in the fused step,
+// the leapfrog update and the CFL minimum.
+template <int DIM>
+__global__ void __launch_bounds__(kBlock, 3) k_momentum_f32(DevBatch b) {
   __shared__ SimDev s;
   int cur = -1;
   const Particles& P = b.P;
-  const double GI = (double)9.80665f;   // Static_allocation_module.f90:72, a default-REAL literal
   for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
     Tile tl = b.tiles[t];
     load_sim(s, b.sims, tl.sim, cur);
@@ -1679,18 +1682,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_momentum_f32(DevBatch b) {
     fc.load(s);
     SimDyn* dyn = b.dyn + tl.sim;
     int p = tl.start + threadIdx.x;
-    bool active = threadIdx.x < tl.count && p < s.p_off + dyn->nag;
-    if (FUSED && active && dyn->frozen) {
-      // a finished simulation of a batch: carry the record through the sort
-      double4 v4 = P.V[p];
-      double2 rp = P.RP[p];
-      P.X2[p] = P.X[p];
-      P.V2[p] = make_double4(v4.x, v4.y, v4.z, rp.x);
-      P.P2[p] = rp.y;
-      P.I2[p] = P.I[p];
-      P.L2[p] = P.L[p];
-      active = false;
-    }
+    const bool active = threadIdx.x < tl.count && p < s.p_off + dyn->nag && !dyn->frozen;
     int ci = 0, cj = 0, ck = 0, cnt = 0;
     float4 xfi = make_float4(0.f, 0.f, 0.f, 0.f);
     float vix = 0.f, viy = 0.f, viz = 0.f, rhof = 1.f, Pi = 0.f;
@@ -1715,26 +1707,11 @@ __global__ void __launch_bounds__(kBlock, 2) k_momentum_f32(DevBatch b) {
     ListPrefetcher lr;
     lr.init(b.nlist, p, b.list_cap4, cnt);
     const int nmax = __reduce_max_sync(0xffffffffu, (unsigned)cnt);
-    int ne = 0;
-    float4 nx = make_float4(0.f, 0.f, 0.f, 0.f), nv = nx, nr = nx;
-    if (cnt > 0) {
-      ne = lr.get(0);
-      int q = ne & kSlotMask;
-      nx = P.XF[q];
-      nv = P.VF[q];
-      nr = P.RF[q];
-    }
     for (int k = 0; k < nmax; ++k) {
-      const int e = ne;
-      const float4 xj = nx, vj = nv, rfj = nr;
-      if (k + 1 < cnt) {
-        ne = lr.get(k + 1);
-        int q = ne & kSlotMask;
-        nx = P.XF[q];
-        nv = P.VF[q];
-        nr = P.RF[q];
-      }
+      const int e = lr.get(k);
       if (k >= cnt) continue;
+      const int q = e & kSlotMask;
+      const float4 xj = P.XF[q], vj = P.VF[q], rfj = P.RF[q];
       float d0, d1, d2;
       separation_rec<DIM>(s, (int)((unsigned)e >> kSlotBits), xj, xfi, ci, cj, ck, d0, d1, d2);
       float rr = d0 * d0 + d1 * d1 + d2 * d2;
@@ -1768,8 +1745,49 @@ __global__ void __launch_bounds__(kBlock, 2) k_momentum_f32(DevBatch b) {
         cp0 = cp1 = cp2 = cd0 = cd1 = cd2 = cv0 = cv1 = cv2 = 0.f;
       }
     }
+    if (active) {
+      double* o = P.MSUM + p;
+      const size_t st = (size_t)P.total_slots;   // component-major: coalesced
+      o[0] = tp0.val();
+      o[st] = tp1.val();
+      o[2 * st] = tp2.val();
+      o[3 * st] = td0.val();
+      o[4 * st] = td1.val();
+      o[5 * st] = td2.val();
+      o[6 * st] = tv0.val();
+      o[7 * st] = tv1.val();
+      o[8 * st] = tv2.val();
+    }
+  }
+}
+
+template <int DIM, bool FUSED>
+__global__ void __launch_bounds__(kBlock) k_momentum_f32_finish(DevBatch b) {
+  __shared__ SimDev s;
+  int cur = -1;
+  const Particles& P = b.P;
+  const double GI = (double)9.80665f;   // Static_allocation_module.f90:72, a default-REAL literal
+  for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
+    Tile tl = b.tiles[t];
+    load_sim(s, b.sims, tl.sim, cur);
+    SimDyn* dyn = b.dyn + tl.sim;
+    int p = tl.start + threadIdx.x;
+    bool active = threadIdx.x < tl.count && p < s.p_off + dyn->nag;
+    if (FUSED && active && dyn->frozen) {
+      // a finished simulation of a batch: carry the record through the sort
+      double4 v4 = P.V[p];
+      double2 rp = P.RP[p];
+      P.X2[p] = P.X[p];
+      P.V2[p] = make_double4(v4.x, v4.y, v4.z, rp.x);
+      P.P2[p] = rp.y;
+      P.I2[p] = P.I[p];
+      P.L2[p] = P.L[p];
+      active = false;
+    }
     double dtc = 1.0e300;
     if (active) {
+      double ms[9];
+      for (int c = 0; c < 9; ++c) ms[c] = P.MSUM[(size_t)c * P.total_slots + p];
       double4 v4 = P.V[p];
       double2 rp = P.RP[p];
       const double vi[3] = {v4.x, v4.y, v4.z};
@@ -1783,10 +1801,10 @@ __global__ void __launch_bounds__(kBlock, 2) k_momentum_f32(DevBatch b) {
         if (DIM == 3) me_boundary3d(s, b, nb, bstart, vi, rhoi, pi, lam, geff, tpres, tdiss, tvisc);
         else me_boundary2d(s, b, nb, bstart, vi, rhoi, pi, lam, geff, tpres, tdiss, tvisc);
       }
-      double rs0 = tv0.val(), rs1 = tv1.val(), rs2 = tv2.val();
-      tpres[0] = tpres[0] + tp0.val();
-      tpres[1] = tpres[1] + tp1.val();
-      tpres[2] = tpres[2] + tp2.val();
+      double rs0 = ms[6], rs1 = ms[7], rs2 = ms[8];
+      tpres[0] = tpres[0] + ms[0];
+      tpres[1] = tpres[1] + ms[1];
+      tpres[2] = tpres[2] + ms[2];
       int lam_new = 0;
       if (s.kin_visc > 0.0) {
         double absv_pres = sqrt(tpres[0] * tpres[0] + tpres[1] * tpres[1] + tpres[2] * tpres[2]) + GI;
@@ -1796,9 +1814,9 @@ __global__ void __launch_bounds__(kBlock, 2) k_momentum_f32(DevBatch b) {
         lam_new = (weight > 5.0 || absv_pres == 0.0) ? 1 : 0;
       }
       double acc[3];
-      acc[0] = tpres[0] + (tdiss[0] + td0.val()) + (tvisc[0] + rs0) + geff[0];
-      acc[1] = tpres[1] + (tdiss[1] + td1.val()) + (tvisc[1] + rs1) + geff[1];
-      acc[2] = tpres[2] + (tdiss[2] + td2.val()) + (tvisc[2] + rs2) + geff[2];
+      acc[0] = tpres[0] + (tdiss[0] + ms[3]) + (tvisc[0] + rs0) + geff[0];
+      acc[1] = tpres[1] + (tdiss[1] + ms[4]) + (tvisc[1] + rs1) + geff[1];
+      acc[2] = tpres[2] + (tdiss[2] + ms[5]) + (tvisc[2] + rs2) + geff[2];
       if (nb > 0) {
         double R[3];
         elastic_reaction<DIM>(s, b, nb, bstart, vi, R);
@@ -2395,12 +2413,15 @@ void launch_neighbour_lists(const DevBatch& b, cudaStream_t st) {
 
 void launch_momentum_f32(const DevBatch& b, bool fused, cudaStream_t st) {
   int g = blocks_for(b, kGridMomentum);
+  int gf = blocks_for(b);
   if (b.dim == 3) {
-    if (fused) k_momentum_f32<3, true><<<g, kBlock, 0, st>>>(b);
-    else k_momentum_f32<3, false><<<g, kBlock, 0, st>>>(b);
+    k_momentum_f32<3><<<g, kBlock, 0, st>>>(b);
+    if (fused) k_momentum_f32_finish<3, true><<<gf, kBlock, 0, st>>>(b);
+    else k_momentum_f32_finish<3, false><<<gf, kBlock, 0, st>>>(b);
   } else {
-    if (fused) k_momentum_f32<2, true><<<g, kBlock, 0, st>>>(b);
-    else k_momentum_f32<2, false><<<g, kBlock, 0, st>>>(b);
+    k_momentum_f32<2><<<g, kBlock, 0, st>>>(b);
+    if (fused) k_momentum_f32_finish<2, true><<<gf, kBlock, 0, st>>>(b);
+    else k_momentum_f32_finish<2, false><<<gf, kBlock, 0, st>>>(b);
   }
 }
 
