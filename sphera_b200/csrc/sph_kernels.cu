@@ -1853,7 +1853,7 @@ __global__ void __launch_bounds__(kBlock) k_momentum_f32_finish(DevBatch b) {
 // boundary data exist, forms dden = (SA-SPH wall term) - (pair sum) and, in
 // the fused step, Leapfrog_continuity and the EoS.
 template <int DIM>
-__global__ void __launch_bounds__(kBlock, 4) k_continuity_f32(DevBatch b) {
+__global__ void __launch_bounds__(kBlock, 5) k_continuity_f32(DevBatch b) {
   __shared__ SimDev s;
   int cur = -1;
   const Particles& P = b.P;
@@ -1885,23 +1885,10 @@ __global__ void __launch_bounds__(kBlock, 4) k_continuity_f32(DevBatch b) {
     ListPrefetcher lr;
     lr.init(b.nlist, p, b.list_cap4, cnt);
     const int nmax = __reduce_max_sync(0xffffffffu, (unsigned)cnt);
-    // the next pair's records, loaded one pair ahead
-    int ne = 0;
-    float4 nx = make_float4(0.f, 0.f, 0.f, 0.f), nv = nx;
-    if (cnt > 0) {
-      ne = lr.get(0);
-      nx = P.XF[ne & kSlotMask];
-      nv = P.VF[ne & kSlotMask];
-    }
     for (int k = 0; k < nmax; ++k) {
-      const int e = ne;
-      const float4 xj = nx, vj = nv;
-      if (k + 1 < cnt) {
-        ne = lr.get(k + 1);
-        nx = P.XF[ne & kSlotMask];
-        nv = P.VF[ne & kSlotMask];
-      }
+      const int e = lr.get(k);
       if (k >= cnt) continue;
+      const float4 xj = P.XF[e & kSlotMask], vj = P.VF[e & kSlotMask];
       float d0, d1, d2;
       separation_rec<DIM>(s, (int)((unsigned)e >> kSlotBits), xj, xfi, ci, cj, ck, d0, d1, d2);
       float rr = d0 * d0 + d1 * d1 + d2 * d2;
