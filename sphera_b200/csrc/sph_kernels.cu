@@ -1144,7 +1144,7 @@ __device__ __forceinline__ bool window_candidate(const float4* wbuf, int u0, int
 }
 
 template <int DIM>
-__global__ void __launch_bounds__(kBlock, 3) k_neighbour_lists(DevBatch b) {
+__global__ void __launch_bounds__(kBlock, 4) k_neighbour_lists(DevBatch b) {
   __shared__ SimDev s;
   __shared__ float4 cbuf[kBlock];
   int cur = -1;
