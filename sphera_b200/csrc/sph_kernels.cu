@@ -1741,29 +1741,29 @@ __global__ void __launch_bounds__(kBlock, 3) k_momentum_f32(DevBatch b) {
       const float4 xj = P.XF[q], vj = P.VF[q], rfj = P.RF[q];
       float d0, d1, d2;
       separation_cols<DIM>(s, (int)((unsigned)e >> kSlotBits), xj, xfi, ci, cj, ck, d0, d1, d2);
-      float rr = d0 * d0 + d1 * d1 + d2 * d2;
+      float rr = fmaf(d2, d2, fmaf(d1, d1, d0 * d0));
       float PK1, PK2, PK3;
       kernel_values_f32<false>(fc, rr, PK1, PK2, PK3);
       float mj = rfj.z;
       // pressure (both accumulators of inter_EqMoto together)
       float pf = -(mj * (Pi + rfj.y) * PK3);
-      cp0 += pf * d0;
-      if (DIM == 3) cp1 += pf * d1;
-      cp2 += pf * d2;
+      cp0 = fmaf(pf, d0, cp0);
+      if (DIM == 3) cp1 = fmaf(pf, d1, cp1);
+      cp2 = fmaf(pf, d2, cp2);
       float dv0 = vj.x - vix, dv1 = vj.y - viy, dv2 = vj.z - viz;
       float rsum = rhof + rfj.x;
       // viscomon
-      float vr = -(dv0 * d0 + dv1 * d1 + dv2 * d2);
+      float vr = -fmaf(dv2, d2, fmaf(dv1, d1, dv0 * d0));
       float df = mj * __fdividef(fc.amon, rsum) * vr * PK2;
-      cd0 += df * d0;
-      if (DIM == 3) cd1 += df * d1;
-      cd2 += df * d2;
+      cd0 = fmaf(df, d0, cd0);
+      if (DIM == 3) cd1 = fmaf(df, d1, cd1);
+      cd2 = fmaf(df, d2, cd2);
       // viscomorris
       if (morris) {
         float vf = -(__fdividef(mj * fc.nu4, fmaf(fc.nu, rsum, 1.0e-3f)) * PK2 * rr);
-        cv0 += vf * dv0;
-        if (DIM == 3) cv1 += vf * dv1;
-        cv2 += vf * dv2;
+        cv0 = fmaf(vf, dv0, cv0);
+        if (DIM == 3) cv1 = fmaf(vf, dv1, cv1);
+        cv2 = fmaf(vf, dv2, cv2);
       }
       if ((k & 3) == 3 || k == cnt - 1) {
         tp0.add(cp0); tp1.add(cp1); tp2.add(cp2);
