@@ -1743,7 +1743,7 @@ __global__ void __launch_bounds__(kBlock, 3) k_momentum_f32(DevBatch b) {
       separation_cols<DIM>(s, (int)((unsigned)e >> kSlotBits), xj, xfi, ci, cj, ck, d0, d1, d2);
       float rr = fmaf(d2, d2, fmaf(d1, d1, d0 * d0));
       float PK1, PK2, PK3;
-      kernel_values_f32<false>(fc, rr, PK1, PK2, PK3);
+      kernel_values_f32<true>(fc, rr, PK1, PK2, PK3);
       float mj = rfj.z;
       // pressure (both accumulators of inter_EqMoto together)
       float pf = -(mj * (Pi + rfj.y) * PK3);
