@@ -1650,18 +1650,6 @@ __device__ __forceinline__ void kernel_values_f32(const F32Const& c, float rr, f
   PK3 = gw * c.kacl * denom;
 }
 
-// Cell-origin offsets of the 9 (3D) / 3 (2D) neighbour runs: run r lies in
-// column (ci - 1 + r % 3, cj - 1 + r / 3), so the offset (ci - ir) dcd,
-// (cj - jr) dcd depends on r alone.  Filled per simulation in shared memory.
-template <int DIM>
-__device__ __forceinline__ void fill_run_offsets(const SimDev& s, float2* runoff) {
-  if (threadIdx.x < 9) {
-    int r = threadIdx.x;
-    runoff[r] = make_float2((float)(1 - r % 3) * s.dcdf[0], (DIM == 3) ? (float)(1 - r / 3) * s.dcdf[1] : 0.f);
-  }
-  __syncthreads();
-}
-
 // FP32 separation from a neighbour's XF record xj reached through run r,
 // the run's cell-origin offset formed from the particle's column.
 template <int DIM>
@@ -1674,17 +1662,6 @@ __device__ __forceinline__ void separation_cols(const SimDev& s, int r, const fl
   float Dz = (float)(ck - __float_as_int(xj.w)) * s.dcdf[2];
   d0 = Dx + (xfi.x - xj.x);
   d1 = (DIM == 3) ? Dy + (xfi.y - xj.y) : 0.f;
-  d2 = Dz + (xfi.z - xj.z);
-}
-
-// FP32 separation from a neighbour's XF record xj reached through run r.
-template <int DIM>
-__device__ __forceinline__ void separation_rec(const float2* runoff, float dz, int r, const float4& xj,
-                                               const float4& xfi, int ck, float& d0, float& d1, float& d2) {
-  const float2 D = runoff[r];
-  float Dz = (float)(ck - __float_as_int(xj.w)) * dz;
-  d0 = D.x + (xfi.x - xj.x);
-  d1 = (DIM == 3) ? D.y + (xfi.y - xj.y) : 0.f;
   d2 = Dz + (xfi.z - xj.z);
 }
 
@@ -1882,15 +1859,11 @@ __global__ void __launch_bounds__(kBlock) k_momentum_f32_finish(DevBatch b) {
 template <int DIM>
 __global__ void __launch_bounds__(kBlock, 5) k_continuity_f32(DevBatch b) {
   __shared__ SimDev s;
-  __shared__ float2 runoff[9];
   int cur = -1;
   const Particles& P = b.P;
   for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
     Tile tl = b.tiles[t];
-    if (tl.sim != cur) {
-      load_sim(s, b.sims, tl.sim, cur);
-      fill_run_offsets<DIM>(s, runoff);
-    }
+    load_sim(s, b.sims, tl.sim, cur);
     F32Const fc;
     fc.load(s);
     SimDyn* dyn = b.dyn + tl.sim;
@@ -1921,7 +1894,7 @@ __global__ void __launch_bounds__(kBlock, 5) k_continuity_f32(DevBatch b) {
       if (k >= cnt) continue;
       const float4 xj = P.XF[e & kSlotMask], vj = P.VF[e & kSlotMask];
       float d0, d1, d2;
-      separation_rec<DIM>(runoff, s.dcdf[2], (int)((unsigned)e >> kSlotBits), xj, xfi, ck, d0, d1, d2);
+      separation_cols<DIM>(s, (int)((unsigned)e >> kSlotBits), xj, xfi, ci, cj, ck, d0, d1, d2);
       float rr = fmaf(d2, d2, fmaf(d1, d1, d0 * d0));
       float PK1, PK2, PK3;
       kernel_values_f32<true>(fc, rr, PK1, PK2, PK3);
