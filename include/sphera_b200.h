@@ -88,8 +88,8 @@ typedef struct SphParams {
     int32_t density_thresholds;     /* input_any_t%density_thresholds (0/1)           */
     int32_t bdt_capacity;           /* BoundaryDataTab entries to reserve,            */
                                     /* 0 = 3 n (3D) or 2 n (2D)                       */
-    double  teta_p;                 /* input_any_t%TetaP (must be 0 on this path)     */
-    double  teta_v;                 /* input_any_t%TetaV (must be 0 on this path)     */
+    double  teta_p;                 /* input_any_t%TetaP, partial pressure smoothing  */
+    double  teta_v;                 /* input_any_t%TetaV, partial velocity smoothing  */
     /* Lateral tank forcing, no reference counterpart: the tank moves as
      * x = A sin(2 pi t / T) and the fluid, computed in the tank frame, feels
      * the body force grav + A (2 pi / T)^2 sin(2 pi t / T) along x, with
@@ -241,8 +241,10 @@ int  sph_time_step_duration(SphHandle* h, double* dt_out);
  * (time_step_loop.f90:222).  acc_out ([n][3], caller order) may be NULL.  */
 int  sph_rhs_momentum(SphHandle* h, double* acc_out);
 /* Leapfrog_momentum.f90:66-99 (time_step_loop.f90:241) using the
- * accelerations of the last sph_rhs_momentum, then velocity_smoothing_2
- * with TetaV = 0 (var = vel).                                             */
+ * accelerations of the last sph_rhs_momentum, then (TetaV > 1e-9)
+ * velocity_smoothing.f90:85-132 with velocity_smoothing_SA_SPH_3D/2D and
+ * velocity_smoothing_2.f90:68-102 (time_step_loop.f90:249-259); with
+ * TetaV = 0, var = vel.                                                   */
 int  sph_leapfrog_momentum(SphHandle* h);
 /* Leapfrog_trajectories.f90:52-66 (time_step_loop.f90:262). */
 int  sph_leapfrog_trajectories(SphHandle* h);
@@ -259,7 +261,8 @@ int  sph_continuity(SphHandle* h, double* dden_out);
 /* Leapfrog_continuity.f90:54-68 (time_step_loop.f90:382). */
 int  sph_leapfrog_continuity(SphHandle* h);
 /* EoS_fluid_loop.f90:59-69 with EoS_barotropic_linear.f90:49-55
- * (time_step_loop.f90:386).                                               */
+ * (time_step_loop.f90:386), then (TetaP > 0) PressureSmoothing_3D.f90:88-160
+ * / _2D.f90:102-235 (time_step_loop.f90:397-404); closes the step.        */
 int  sph_eos(SphHandle* h);
 
 /* ---------------------------------------------------------------------- */

@@ -24,7 +24,7 @@
 //
 // Scope: Domain%tipo = "semi" (SA-SPH), time_split = 1 (leapfrog), one
 // liquid medium, all particles vel_type = "std", state = "flu"; ALE3,
-// C1_BE, KTGF, DB-SPH, bodies off; TetaP = TetaV = 0; wall zones "fixe" and
+// C1_BE, KTGF, DB-SPH, bodies off; wall zones "fixe" and
 // "tapi" with slip_coefficient_mode = 1.
 #include <cmath>
 #include <cstdint>
@@ -1567,6 +1567,154 @@ void EoS_fluid_loop(Oracle& o) {
   }
 }
 
+// velocity_smoothing.f90:85-132 with velocity_smoothing_SA_SPH_3D.f90:61-125 /
+// _2D.f90:66-117 (wall zones fixe/tapi, slip mode 1), then
+// velocity_smoothing_2.f90:68-102 for TetaV > 1e-9 (time_step_loop.f90:249-259)
+void velocity_smoothing(Oracle& o) {
+  const int NM = o.NMAXPARTJ;
+#pragma omp parallel for schedule(static) num_threads(o.nthreads)
+  for (int npi = 1; npi <= o.nag; ++npi) {
+    Particle& p = o.pg[npi];
+    for (int d = 0; d < 3; ++d) p.var[d] = 0.0;
+    for (int contj = 1; contj <= o.nPartIntorno[npi]; ++contj) {
+      long npartint = (long)(npi - 1) * NM + contj;
+      const Particle& q = o.pg[o.PartIntorno[npartint]];
+      double rhoj = q.dens, amassj = q.mass;
+      double dervel[3];
+      for (int d = 0; d < 3; ++d) dervel[d] = q.vel[d] - p.vel[d];
+      double pesoj = amassj * o.PartKernel[npartint * 4 + 3] / rhoj;
+      for (int d = 0; d < 3; ++d) p.var[d] = p.var[d] + dervel[d] * pesoj;
+    }
+    int ibdt = o.BDP[3 * (npi - 1) + 2];
+    if (o.dim == 3) {
+      int Ncbf = o.BDP[3 * (npi - 1)];
+      for (int icbf = 1; icbf <= Ncbf; ++icbf) {
+        const BDT& e = o.BDTab[ibdt + icbf - 2];
+        const Face& f = o.faces[e.CloBoNum - 1];
+        const SphZone& z = o.zones[f.stretch - 1];
+        double DVGlo[3], DVLoc[3], BCLoc[3];
+        for (int i = 0; i < 3; ++i) DVGlo[i] = 2.0 * (f.velocity[i] - p.vel[i]);   // Tratto%velocity (0 for fixe)
+        for (int i = 0; i < 3; ++i) {
+          DVLoc[i] = 0.0;
+          for (int j = 0; j < 3; ++j) DVLoc[i] = DVLoc[i] + f.T[j][i] * DVGlo[j];
+        }
+        double IntWdV = e.BoundaryIntegral[1];
+        double slip = z.bc_shear_stress_input;
+        BCLoc[0] = DVLoc[0] * IntWdV * slip;
+        BCLoc[1] = DVLoc[1] * IntWdV * slip;
+        BCLoc[2] = DVLoc[2] * IntWdV;
+        for (int i = 0; i < 3; ++i) {
+          double g = 0.0;
+          for (int j = 0; j < 3; ++j) g = g + f.T[i][j] * BCLoc[j];
+          p.var[i] = p.var[i] + g;
+        }
+      }
+    } else {
+      int IntNcbs = o.BDP[3 * (npi - 1) + 1];
+      const int acix[2] = {0, 2};
+      for (int icbs = 1; icbs <= IntNcbs; ++icbs) {
+        const BDT& e = o.BDTab[ibdt + icbs - 2];
+        const Side& sd = o.sides[e.CloBoNum - 1];
+        const SphZone& z = o.zones[sd.stretch - 1];
+        double sss[2], nnn[2], DVGlo[2], DVLoc[2], BCLoc[2], BCGlo[2];
+        for (int i = 0; i < 2; ++i) {
+          sss[i] = sd.T[acix[i]][0];
+          nnn[i] = sd.T[acix[i]][2];
+          DVGlo[i] = 2.0 * (sd.velocity[acix[i]] - p.vel[acix[i]]);   // Tratto%velocity (0 for fixe)
+        }
+        DVLoc[0] = sss[0] * DVGlo[0] + sss[1] * DVGlo[1];
+        DVLoc[1] = nnn[0] * DVGlo[0] + nnn[1] * DVGlo[1];
+        double IntWdV = e.BoundaryIntegral[2];
+        double slip = z.bc_shear_stress_input;
+        BCLoc[0] = DVLoc[0] * IntWdV * slip;
+        BCLoc[1] = DVLoc[1] * IntWdV;
+        BCGlo[0] = sss[0] * BCLoc[0] + nnn[0] * BCLoc[1];
+        BCGlo[1] = sss[1] * BCLoc[0] + nnn[1] * BCLoc[1];
+        p.var[0] = p.var[0] + BCGlo[0];
+        p.var[2] = p.var[2] + BCGlo[1];
+      }
+    }
+  }
+  const double TetaV1 = o.prm.teta_v * o.celerita * o.dt / o.h;
+#pragma omp parallel for schedule(static) num_threads(o.nthreads)
+  for (int npi = 1; npi <= o.nag; ++npi) {
+    Particle& p = o.pg[npi];
+    if (p.kodvel == 0) {
+      for (int d = 0; d < 3; ++d) p.var[d] = p.vel[d] + TetaV1 * p.var[d];
+      for (int d = 0; d < 3; ++d) p.vel[d] = p.var[d];
+    } else {
+      for (int d = 0; d < 3; ++d) p.var[d] = p.vel[d];
+    }
+  }
+}
+
+// PressureSmoothing_3D.f90:88-160 / PressureSmoothing_2D.f90:102-235
+// (SmoothVersion "b"; wall zones fixe/tapi), time_step_loop.f90:397-404
+void PressureSmoothing(Oracle& o) {
+  const int NM = o.NMAXPARTJ;
+  std::vector<double> vpres(o.nag + 1, 0.0);
+  const double TetaP1 = o.prm.teta_p * o.celerita * o.dt / o.h;
+  const double p0i = o.prm.p_ref, ro0i = o.prm.den0;
+#pragma omp parallel for schedule(static) num_threads(o.nthreads)
+  for (int npi = 1; npi <= o.nag; ++npi) {
+    Particle& p = o.pg[npi];
+    if (p.koddens != 0) continue;
+    int Nsp = o.nPartIntorno[npi];
+    double pi = p.pres, sompW = 0.0, AppUnity = 0.0;
+    for (int j = 1; j <= Nsp; ++j) {
+      long npartint = (long)(npi - 1) * NM + j;
+      const Particle& q = o.pg[o.PartIntorno[npartint]];
+      double pesoj = q.mass * o.PartKernel[npartint * 4 + 3] / q.dens;
+      AppUnity = AppUnity + pesoj;
+      sompW = sompW + (q.pres - pi) * pesoj;
+    }
+    int ibdt = o.BDP[3 * (npi - 1) + 2];
+    if (o.dim == 3) {
+      double DiffP = 0.0;
+      if (Nsp > 0) {
+        int Ncbf = o.BDP[3 * (npi - 1)];
+        for (int icbf = 1; icbf <= Ncbf; ++icbf) {
+          const BDT& e = o.BDTab[ibdt + icbf - 2];
+          if (e.LocXYZ[2] > 0.0) AppUnity = AppUnity + e.BoundaryIntegral[1];
+        }
+        if (AppUnity < 0.95) DiffP = sompW + (p0i - pi) * (1.0 - AppUnity);
+        else DiffP = sompW / AppUnity;
+      }
+      vpres[npi] = pi + TetaP1 * DiffP;
+    } else {
+      if (Nsp <= 0) {
+        vpres[npi] = pi;
+        continue;
+      }
+      const int acix[2] = {0, 2};
+      double VIntWdV_FT = 0.0;
+      int IntNcbs = o.BDP[3 * (npi - 1) + 1];
+      for (int icbs = 1; icbs <= IntNcbs; ++icbs) {
+        const BDT& e = o.BDTab[ibdt + icbs - 2];
+        const Side& sd = o.sides[e.CloBoNum - 1];
+        double sss[2], nnn[2], mf[2];
+        for (int i = 0; i < 2; ++i) {
+          sss[i] = sd.T[acix[i]][0];
+          nnn[i] = sd.T[acix[i]][2];
+        }
+        mf[0] = sss[0] * o.geff[acix[0]] + sss[1] * o.geff[acix[1]];
+        mf[1] = nnn[0] * o.geff[acix[0]] + nnn[1] * o.geff[acix[1]];
+        VIntWdV_FT = VIntWdV_FT + e.BoundaryIntegral[1];
+        sompW = sompW + ro0i * (mf[0] * e.BoundaryIntegral[3] + mf[1] * e.BoundaryIntegral[4]);
+      }
+      AppUnity = AppUnity + VIntWdV_FT + 0.0 + 0.0 + 0.0;
+      vpres[npi] = pi + TetaP1 * (sompW + (pi - pi) * 0.0 + (pi - pi) * 0.0 + (p0i - pi) * (1.0 - AppUnity));
+    }
+  }
+#pragma omp parallel for schedule(static) num_threads(o.nthreads)
+  for (int npi = 1; npi <= o.nag; ++npi) {
+    Particle& p = o.pg[npi];
+    if (p.koddens != 0) continue;
+    p.pres = vpres[npi];
+    p.dens = o.prm.den0 * (1.0 + (p.pres - o.prm.p_ref) / o.prm.eps);   // EoS_barotropic_linear.f90:54
+  }
+}
+
 // time_step_loop.f90:338-360
 int continuity_block(Oracle& o) {
   int ncbfmax = 0;
@@ -1733,6 +1881,7 @@ int ora_step(void* h, int nsteps) {
     set_body_force(o, o.simulation_time);
     RHS_momentum_equation(o);
     Leapfrog_momentum(o, dt_previous_step);
+    if (o.prm.teta_v > 1.0e-9) velocity_smoothing(o);
     Leapfrog_trajectories(o);
     OrdGrid1(o);
     CalcVarLength(o);
@@ -1742,6 +1891,7 @@ int ora_step(void* h, int nsteps) {
     if (st) return check(o, st);
     Leapfrog_continuity(o);
     EoS_fluid_loop(o);
+    if (o.prm.teta_p > 0.0) PressureSmoothing(o);
   }
   return 0;
 }

@@ -126,7 +126,7 @@ int cell_indices(const SimDev& s, int nc, int& i, int& j, int& k) {   // CellInd
 int prepare_sim(const SphParams& prm, const SphGeometry& g, int cap, HostSim& hs) {
   if (prm.dim != 2 && prm.dim != 3) return SPH_ERR_INVALID_ARGUMENT;
   if (!(prm.dx > 0.0) || !(prm.trunc > 0.0) || !(prm.den0 > 0.0) || !(prm.eps > 0.0)) return SPH_ERR_INVALID_ARGUMENT;
-  if (prm.teta_p != 0.0 || prm.teta_v != 0.0) return SPH_ERR_UNSUPPORTED;
+  if (!(prm.teta_p >= 0.0) || !(prm.teta_v >= 0.0)) return SPH_ERR_INVALID_ARGUMENT;
   if (prm.precision != SPH_PREC_FP64 && prm.precision != SPH_PREC_FP32C) return SPH_ERR_INVALID_ARGUMENT;
   if (g.n_zones < 0 || (g.n_zones > 0 && !g.zones)) return SPH_ERR_INVALID_ARGUMENT;
   for (int z = 0; z < g.n_zones; ++z) {
@@ -173,6 +173,8 @@ int prepare_sim(const SphParams& prm, const SphGeometry& g, int cap, HostSim& hs
     return SPH_ERR_INVALID_ARGUMENT;
   s.forcing_w = prm.forcing_period > 0.0 ? 6.283185307179586 / prm.forcing_period : 0.0;
   s.forcing_aw2 = prm.forcing_amplitude * s.forcing_w * s.forcing_w;
+  s.teta_p = prm.teta_p;
+  s.teta_v = prm.teta_v;
   s.dt_alfa_mon = prm.dt_alfa_mon;
   s.density_thresholds = prm.density_thresholds;
   s.zpmin = 0.05 * s.h;
@@ -536,6 +538,8 @@ struct SphHandle {
   cudaGraphExec_t graph = nullptr;
   bool uploaded = false;
   std::vector<SimDyn> h_dyn;
+  bool any_teta_v = false;          // some simulation smooths velocities / pressures
+  bool any_teta_p = false;
   size_t device_bytes = 0;          // bytes of the arrays below `owned`
   bool dry = false;                 // size the arrays only (sph_memory_required)
 };
@@ -615,6 +619,7 @@ void refresh_copies(SphHandle* h, cudaStream_t st) {
 // beside the boundary pass too and adds the wall term after the join.
 void step_sequence(SphHandle* h, cudaStream_t st) {
   momentum_pass(h, true, st);
+  if (h->any_teta_v) launch_velocity_smoothing(h->db, true, st);
   sort_sequence(h, st);
   cudaEventRecord(h->ev_fork, st);
   cudaStreamWaitEvent(h->stream2, h->ev_fork, 0);
@@ -629,6 +634,7 @@ void step_sequence(SphHandle* h, cudaStream_t st) {
     cudaStreamWaitEvent(st, h->ev_join, 0);
     continuity_pass(h, true, st);
   }
+  if (h->any_teta_p) launch_pressure_smoothing(h->db, h->precision == SPH_PREC_FP32C, st);
   launch_finalize(h->db, 1, st);
 }
 
@@ -674,6 +680,8 @@ int create_batch(int nsims, const SphParams* params, const SphGeometry* geoms, c
     }
     int st = prepare_sim(params[s], geoms[s], caps[s], h->sims[s]);
     if (st != SPH_OK) { delete h; return st; }
+    if (params[s].teta_v > 1.0e-9) h->any_teta_v = true;
+    if (params[s].teta_p > 0.0) h->any_teta_p = true;
   }
   // layout of the concatenated arrays; simulations start on tile boundaries
   std::vector<Tile> tiles;
@@ -1064,6 +1072,7 @@ int sph_rhs_momentum(SphHandle* h, double* acc_out) {
 int sph_leapfrog_momentum(SphHandle* h) {
   if (!h || !h->uploaded) return SPH_ERR_INVALID_ARGUMENT;
   launch_leapfrog_momentum(h->db, h->stream);
+  if (h->any_teta_v) launch_velocity_smoothing(h->db, false, h->stream);
   refresh_copies(h, h->stream);
   SPH_CUDA(cudaGetLastError());
   return sync_dyn(h);
@@ -1111,6 +1120,7 @@ int sph_leapfrog_continuity(SphHandle* h) {
 int sph_eos(SphHandle* h) {
   if (!h || !h->uploaded) return SPH_ERR_INVALID_ARGUMENT;
   launch_eos(h->db, h->stream);
+  if (h->any_teta_p) launch_pressure_smoothing(h->db, false, h->stream);
   refresh_copies(h, h->stream);
   launch_dt_reduce(h->db, h->stream);
   launch_finalize(h->db, 1, h->stream);
@@ -1267,6 +1277,7 @@ int sph_profile_phases(SphHandle* h, int32_t nsteps, double* ms) {
   for (int s = 0; s < nsteps && e == cudaSuccess; ++s) {
     cudaEventRecord(ev[0], q);
     momentum_pass(h, true, q);
+    if (h->any_teta_v) launch_velocity_smoothing(h->db, true, q);
     cudaEventRecord(ev[1], q);
     sort_sequence(h, q);
     cudaEventRecord(ev[2], q);
@@ -1275,6 +1286,7 @@ int sph_profile_phases(SphHandle* h, int32_t nsteps, double* ms) {
     launch_neighbour_lists(h->db, q);
     cudaEventRecord(ev[4], q);
     continuity_pass(h, true, q);
+    if (h->any_teta_p) launch_pressure_smoothing(h->db, h->precision == SPH_PREC_FP32C, q);
     cudaEventRecord(ev[5], q);
     launch_finalize(h->db, 1, q);
     cudaEventRecord(ev[6], q);

@@ -53,6 +53,7 @@ struct SimDev {
   double cfl, vsc_coeff, pesodt;
   double forcing_aw2;     // A (2 pi / T)^2 of the lateral tank forcing (0: none)
   double forcing_w;       // 2 pi / T
+  double teta_p, teta_v;  // input_any_t%TetaP, TetaV (partial smoothing)
   double zpmin;           // 0.05 h, ComputeBoundaryVolumeIntegrals_P0.f90
   double ktdelta;         // kernel-table step
   float dcdf[3];          // (float)dcd: cell origins differ by multiples of it

@@ -1457,7 +1457,9 @@ __global__ void __launch_bounds__(kBlock, 2) k_momentum(DevBatch b) {
         P.I2[p] = P.I[p];
         P.L2[p] = (uint8_t)lam_new;
         double U = sqrt(vn[0] * vn[0] + vn[1] * vn[1] + vn[2] * vn[2]);
-        dtc = s.cfl * 2.0 * s.h / (s.celerita + U);
+        // with velocity smoothing the CFL minimum is taken on the smoothed
+        // velocities (k_velocity_smoothing_apply), which also moves X2
+        if (!(s.teta_v > 1.0e-9)) dtc = s.cfl * 2.0 * s.h / (s.celerita + U);
       } else {
         P.ACC[p] = make_double4(acc[0], acc[1], acc[2], 0.0);
         P.L[p] = (uint8_t)lam_new;
@@ -1837,7 +1839,9 @@ __global__ void __launch_bounds__(kBlock) k_momentum_f32_finish(DevBatch b) {
         P.I2[p] = P.I[p];
         P.L2[p] = (uint8_t)lam_new;
         double U = sqrt(vn[0] * vn[0] + vn[1] * vn[1] + vn[2] * vn[2]);
-        dtc = s.cfl * 2.0 * s.h / (s.celerita + U);
+        // with velocity smoothing the CFL minimum is taken on the smoothed
+        // velocities (k_velocity_smoothing_apply), which also moves X2
+        if (!(s.teta_v > 1.0e-9)) dtc = s.cfl * 2.0 * s.h / (s.celerita + U);
       } else {
         P.ACC[p] = make_double4(acc[0], acc[1], acc[2], 0.0);
         P.L[p] = (uint8_t)lam_new;
@@ -1956,6 +1960,261 @@ __global__ void k_refresh_f32(DevBatch b) {
     double2 rp = b.P.RP[p];
     b.P.VF[p] = make_float4((float)v.x, (float)v.y, (float)v.z, (float)v.w);
     b.P.RF[p] = make_float4((float)rp.x, (float)(rp.y / (rp.x * rp.x)), (float)x.w, 0.f);
+  }
+}
+
+// ==========================================================================
+// Partial smoothing (input_any_t%TetaV, %TetaP > 0), FP64 in both forms.
+// The reference's neighbour list includes the particle itself; the lists
+// here leave it out, so its term is added where the reference's order puts
+// it: before the first entry past (centre run, own slot).
+// ==========================================================================
+
+// PartKernel(4) of CalcVarLength.f90:241-268: the kernel value W = wu coefke.
+__device__ __forceinline__ double kernel_w(const SimDev& s, double rr) {
+  double r = sqrt(rr);
+  double q = r / s.h;
+  double q2 = rr / s.squareh;
+  int idx = (int)q;
+  if (idx >= 2) return 0.0;
+  double wu = 0.666666667 + q2 * (q * 0.5 - 1.0);
+  if (idx > 0) wu = (2.0 - q) * (2.0 - q) * (2.0 - q) * 0.166666666667;
+  return wu * s.coefke;
+}
+
+// velocity_smoothing.f90:85-132 with velocity_smoothing_SA_SPH_3D.f90:61-125
+// / _2D.f90:66-117 (fixe/tapi walls, slip mode 1): ACC = var, the smoothing
+// increment, from the velocities `vel` (the step's leapfrog velocities).
+template <int DIM>
+__global__ void __launch_bounds__(kBlock) k_velocity_smoothing(DevBatch b, const double4* __restrict__ vel) {
+  __shared__ SimDev s;
+  int cur = -1;
+  const Particles& P = b.P;
+  constexpr int RC = (DIM == 3) ? 4 : 1;   // the particle's own column run
+  for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
+    Tile tl = b.tiles[t];
+    load_sim(s, b.sims, tl.sim, cur);
+    SimDyn* dyn = b.dyn + tl.sim;
+    int p = tl.start + threadIdx.x;
+    const bool active = threadIdx.x < tl.count && p < s.p_off + dyn->nag && !dyn->frozen && s.teta_v > 1.0e-9;
+    const int cnt = active ? b.ncount[p] : 0;
+    double var[3] = {0.0, 0.0, 0.0};
+    double4 xi = make_double4(0.0, 0.0, 0.0, 0.0), vi = xi;
+    double self_w = 0.0;
+    if (active) {
+      xi = P.X[p];
+      vi = vel[p];
+      self_w = xi.w * kernel_w(s, 0.0) / P.RP[p].x;
+    }
+    bool self_done = !active;
+    ListPrefetcher lr;
+    lr.init(b.nlist, p, b.list_cap4, cnt);
+    const int nmax = __reduce_max_sync(0xffffffffu, (unsigned)cnt);
+    for (int k = 0; k < nmax; ++k) {
+      int e = lr.get(k);
+      if (k >= cnt) continue;
+      int q = e & kSlotMask;
+      int r = (int)((unsigned)e >> kSlotBits);
+      if (!self_done && (r > RC || (r == RC && q > p))) {
+        var[0] = var[0] + (vi.x - vi.x) * self_w;
+        var[1] = var[1] + (vi.y - vi.y) * self_w;
+        var[2] = var[2] + (vi.z - vi.z) * self_w;
+        self_done = true;
+      }
+      double4 xj = P.X[q];
+      double r0 = xi.x - xj.x, r1 = xi.y - xj.y, r2 = xi.z - xj.z;
+      double rr = r0 * r0 + r1 * r1 + r2 * r2;
+      double pesoj = xj.w * kernel_w(s, rr) / P.RP[q].x;
+      double4 vj = vel[q];
+      var[0] = var[0] + (vj.x - vi.x) * pesoj;
+      var[1] = var[1] + (vj.y - vi.y) * pesoj;
+      var[2] = var[2] + (vj.z - vi.z) * pesoj;
+    }
+    if (!active) continue;
+    if (!self_done) {
+      var[0] = var[0] + (vi.x - vi.x) * self_w;
+      var[1] = var[1] + (vi.y - vi.y) * self_w;
+      var[2] = var[2] + (vi.z - vi.z) * self_w;
+    }
+    const int nb = P.bdt_count[p];
+    const int bstart = nb > 0 ? P.bdt_start[p] : 0;
+    for (int u = 0; u < nb; ++u) {
+      const BdtEntry& e = P.bdt[bstart + u];
+      if (DIM == 3) {
+        const FaceDev& f = b.faces[s.face_off + e.clobonum - 1];
+        const double vv[3] = {vi.x, vi.y, vi.z};
+        double DVGlo[3], DVLoc[3], BCLoc[3];
+        for (int i = 0; i < 3; ++i) DVGlo[i] = 2.0 * (f.velocity[i] - vv[i]);
+        for (int i = 0; i < 3; ++i) {
+          double a = 0.0;
+          for (int j = 0; j < 3; ++j) a = a + f.T[j][i] * DVGlo[j];
+          DVLoc[i] = a;
+        }
+        double IntWdV = e.bi[1];
+        BCLoc[0] = DVLoc[0] * IntWdV * f.slip;
+        BCLoc[1] = DVLoc[1] * IntWdV * f.slip;
+        BCLoc[2] = DVLoc[2] * IntWdV;
+        for (int i = 0; i < 3; ++i) {
+          double g = 0.0;
+          for (int j = 0; j < 3; ++j) g = g + f.T[i][j] * BCLoc[j];
+          var[i] = var[i] + g;
+        }
+      } else {
+        const SideDev& S = b.sides[s.side_off + e.clobonum - 1];
+        double DVGlo0 = 2.0 * (S.velocity[0] - vi.x), DVGlo1 = 2.0 * (S.velocity[2] - vi.z);
+        double DVLoc0 = S.sss[0] * DVGlo0 + S.sss[1] * DVGlo1;
+        double DVLoc1 = S.nnn[0] * DVGlo0 + S.nnn[1] * DVGlo1;
+        double IntWdV = e.bi[2];
+        double BCLoc0 = DVLoc0 * IntWdV * S.slip;
+        double BCLoc1 = DVLoc1 * IntWdV;
+        var[0] = var[0] + (S.sss[0] * BCLoc0 + S.nnn[0] * BCLoc1);
+        var[2] = var[2] + (S.sss[1] * BCLoc0 + S.nnn[1] * BCLoc1);
+      }
+    }
+    P.ACC[p] = make_double4(var[0], var[1], var[2], 0.0);
+  }
+}
+
+// velocity_smoothing_2.f90:87-101 with TetaV > 1e-9: vel = vel + TetaV1 var.
+// FUSED (the step graph): on the momentum pass's record V2, then
+// Leapfrog_trajectories into X2 and the CFL minimum of the smoothed
+// velocities; otherwise in place on V (the per-call ABI).
+template <bool FUSED>
+__global__ void __launch_bounds__(kBlock) k_velocity_smoothing_apply(DevBatch b) {
+  __shared__ SimDev s;
+  int cur = -1;
+  const Particles& P = b.P;
+  for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
+    Tile tl = b.tiles[t];
+    load_sim(s, b.sims, tl.sim, cur);
+    SimDyn* dyn = b.dyn + tl.sim;
+    int p = tl.start + threadIdx.x;
+    const bool active = threadIdx.x < tl.count && p < s.p_off + dyn->nag && !dyn->frozen && s.teta_v > 1.0e-9;
+    double dtc = 1.0e300;
+    if (active) {
+      const double TetaV1 = s.teta_v * s.celerita * dyn->dt / s.h;
+      const double4 var = P.ACC[p];
+      double4 v = FUSED ? P.V2[p] : P.V[p];
+      v.x = v.x + TetaV1 * var.x;
+      v.y = v.y + TetaV1 * var.y;
+      v.z = v.z + TetaV1 * var.z;
+      if (FUSED) {
+        P.V2[p] = v;
+        const double4 x = P.X[p];
+        const double dt = dyn->dt;
+        P.X2[p] = make_double4(x.x + dt * v.x, x.y + dt * v.y, x.z + dt * v.z, x.w);
+        double U = sqrt(v.x * v.x + v.y * v.y + v.z * v.z);
+        dtc = s.cfl * 2.0 * s.h / (s.celerita + U);
+      } else {
+        P.V[p] = v;
+      }
+    }
+    if (FUSED) {
+      double m = warp_min(dtc);
+      if ((threadIdx.x & 31) == 0 && m < 1.0e300)
+        atomicMin(&dyn->dtmin_bits, (unsigned long long)__double_as_longlong(m));
+    }
+  }
+}
+
+// PressureSmoothing_3D.f90:88-134 / PressureSmoothing_2D.f90:102-212
+// (SmoothVersion "b", fixe/tapi walls): DDEN = the smoothed pressure, from
+// the pressures and densities after the step's EoS.
+template <int DIM>
+__global__ void __launch_bounds__(kBlock) k_pressure_smoothing(DevBatch b) {
+  __shared__ SimDev s;
+  int cur = -1;
+  const Particles& P = b.P;
+  constexpr int RC = (DIM == 3) ? 4 : 1;
+  for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
+    Tile tl = b.tiles[t];
+    load_sim(s, b.sims, tl.sim, cur);
+    SimDyn* dyn = b.dyn + tl.sim;
+    int p = tl.start + threadIdx.x;
+    const bool active = threadIdx.x < tl.count && p < s.p_off + dyn->nag && !dyn->frozen && s.teta_p > 0.0;
+    const int cnt = active ? b.ncount[p] : 0;
+    double4 xi = make_double4(0.0, 0.0, 0.0, 0.0);
+    double pi = 0.0, self_w = 0.0, sompW = 0.0, AppUnity = 0.0;
+    if (active) {
+      xi = P.X[p];
+      double2 rp = P.RP[p];
+      pi = rp.y;
+      self_w = xi.w * kernel_w(s, 0.0) / rp.x;
+    }
+    bool self_done = !active;
+    ListPrefetcher lr;
+    lr.init(b.nlist, p, b.list_cap4, cnt);
+    const int nmax = __reduce_max_sync(0xffffffffu, (unsigned)cnt);
+    for (int k = 0; k < nmax; ++k) {
+      int e = lr.get(k);
+      if (k >= cnt) continue;
+      int q = e & kSlotMask;
+      int r = (int)((unsigned)e >> kSlotBits);
+      if (!self_done && (r > RC || (r == RC && q > p))) {
+        AppUnity = AppUnity + self_w;
+        sompW = sompW + (pi - pi) * self_w;
+        self_done = true;
+      }
+      double4 xj = P.X[q];
+      double r0 = xi.x - xj.x, r1 = xi.y - xj.y, r2 = xi.z - xj.z;
+      double rr = r0 * r0 + r1 * r1 + r2 * r2;
+      double2 rpj = P.RP[q];
+      double pesoj = xj.w * kernel_w(s, rr) / rpj.x;
+      AppUnity = AppUnity + pesoj;
+      sompW = sompW + (rpj.y - pi) * pesoj;
+    }
+    if (!active) continue;
+    if (!self_done) {
+      AppUnity = AppUnity + self_w;
+      sompW = sompW + (pi - pi) * self_w;
+    }
+    const double TetaP1 = s.teta_p * s.celerita * dyn->dt / s.h;
+    const double p0i = s.p_ref;
+    const int nb = P.bdt_count[p];
+    const int bstart = nb > 0 ? P.bdt_start[p] : 0;
+    double vpres;
+    if (DIM == 3) {
+      for (int u = 0; u < nb; ++u) {
+        const BdtEntry& e = P.bdt[bstart + u];
+        if (e.loc[2] > 0.0) AppUnity = AppUnity + e.bi[1];
+      }
+      double DiffP = (AppUnity < 0.95) ? sompW + (p0i - pi) * (1.0 - AppUnity) : sompW / AppUnity;
+      vpres = pi + TetaP1 * DiffP;
+    } else {
+      const double* g = dyn->geff;
+      double VIntWdV_FT = 0.0;
+      for (int u = 0; u < nb; ++u) {
+        const BdtEntry& e = P.bdt[bstart + u];
+        const SideDev& S = b.sides[s.side_off + e.clobonum - 1];
+        double mf0 = S.sss[0] * g[0] + S.sss[1] * g[2];
+        double mf1 = S.nnn[0] * g[0] + S.nnn[1] * g[2];
+        VIntWdV_FT = VIntWdV_FT + e.bi[1];
+        sompW = sompW + s.den0 * (mf0 * e.bi[3] + mf1 * e.bi[4]);
+      }
+      AppUnity = AppUnity + VIntWdV_FT + 0.0 + 0.0 + 0.0;
+      vpres = pi + TetaP1 * (sompW + (pi - pi) * 0.0 + (pi - pi) * 0.0 + (p0i - pi) * (1.0 - AppUnity));
+    }
+    P.DDEN[p] = vpres;
+  }
+}
+
+// PressureSmoothing_3D.f90:137-158 / _2D.f90:216-233: p = the smoothed
+// pressure, density from the inverse EoS (EoS_barotropic_linear.f90:54),
+// and the FP32 record of the FP32c form.
+__global__ void __launch_bounds__(kBlock) k_pressure_smoothing_apply(DevBatch b, int refresh_f32) {
+  __shared__ SimDev s;
+  int cur = -1;
+  const Particles& P = b.P;
+  for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
+    Tile tl = b.tiles[t];
+    load_sim(s, b.sims, tl.sim, cur);
+    SimDyn* dyn = b.dyn + tl.sim;
+    int p = tl.start + threadIdx.x;
+    if (!(threadIdx.x < tl.count && p < s.p_off + dyn->nag && !dyn->frozen && s.teta_p > 0.0)) continue;
+    double pr = P.DDEN[p];
+    double rho = s.den0 * (1.0 + (pr - s.p_ref) / s.eps);
+    P.RP[p] = make_double2(rho, pr);
+    if (refresh_f32) P.RF[p] = make_float4((float)rho, (float)(pr / (rho * rho)), (float)P.X[p].w, 0.f);
   }
 }
 
@@ -2461,6 +2720,20 @@ void launch_leapfrog_continuity(const DevBatch& b, cudaStream_t st) {
   k_leapfrog_continuity<<<blocks_for(b), kBlock, 0, st>>>(b);
 }
 void launch_eos(const DevBatch& b, cudaStream_t st) { k_eos<<<blocks_for(b), kBlock, 0, st>>>(b); }
+
+void launch_velocity_smoothing(const DevBatch& b, bool fused, cudaStream_t st) {
+  const double4* vel = fused ? b.P.V2 : b.P.V;
+  if (b.dim == 3) k_velocity_smoothing<3><<<blocks_for(b), kBlock, 0, st>>>(b, vel);
+  else k_velocity_smoothing<2><<<blocks_for(b), kBlock, 0, st>>>(b, vel);
+  if (fused) k_velocity_smoothing_apply<true><<<blocks_for(b), kBlock, 0, st>>>(b);
+  else k_velocity_smoothing_apply<false><<<blocks_for(b), kBlock, 0, st>>>(b);
+}
+
+void launch_pressure_smoothing(const DevBatch& b, bool refresh_f32, cudaStream_t st) {
+  if (b.dim == 3) k_pressure_smoothing<3><<<blocks_for(b), kBlock, 0, st>>>(b);
+  else k_pressure_smoothing<2><<<blocks_for(b), kBlock, 0, st>>>(b);
+  k_pressure_smoothing_apply<<<blocks_for(b), kBlock, 0, st>>>(b, refresh_f32 ? 1 : 0);
+}
 void launch_dt_reduce(const DevBatch& b, cudaStream_t st) { k_dt_reduce<<<blocks_for(b), kBlock, 0, st>>>(b); }
 void launch_finalize(const DevBatch& b, int mode, cudaStream_t st) {
   k_finalize<<<(b.nsims + 127) / 128, 128, 0, st>>>(b, mode);

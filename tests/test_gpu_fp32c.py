@@ -83,3 +83,21 @@ def test_fields_follow_fp64_oracle(make, nsteps, oracle_lib):
     assert rel_l2(g.rho, s["rho"]) <= FIELD_TOL
     assert rel_l2(g.v, s["v"]) <= FIELD_TOL
     assert rel_l2(g.x, s["x"]) <= FIELD_TOL
+
+
+def test_smoothed_fields_follow_fp64_oracle(oracle_lib):
+    """Partial smoothing (TetaP = TetaV = 0.2, FP64 in both forms) under the
+    FP32-compensated pair passes."""
+    case = cases.dam_break_2d()
+    case.params.teta_v = 0.2
+    case.params.teta_p = 0.2
+    o = oracle_lib.Oracle(case)
+    o.prepare()
+    o.step(300)
+    s = o.get()
+    sim = Simulation(_fp32c(case))
+    sim.upload(case.state)
+    sim.step(300)
+    g = sim.download()
+    assert rel_l2(g.rho, s["rho"]) <= FIELD_TOL
+    assert rel_l2(g.v, s["v"]) <= FIELD_TOL

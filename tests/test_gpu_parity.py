@@ -184,3 +184,49 @@ def test_sloshing_forcing_follows_oracle(oracle_lib):
     acc = sim2.rhs_momentum()
     o2.rhs_momentum()
     assert rel_l2(acc, o2.get()["acc"]) <= RATE_TOL
+
+
+@pytest.mark.parametrize("name,nsteps", [("dam_break_2d", 100), ("dam_break_3d_dx02", 40)])
+def test_partial_smoothing_follows_oracle(name, nsteps, oracle_lib):
+    """TetaP = TetaV = 0.2 (the tutorial decks' values): velocity smoothing
+    after Leapfrog_momentum and pressure smoothing after the EoS, with the
+    particle's own term at its place in the reference's neighbour order."""
+    case = CASES[name]()
+    case.params.teta_v = 0.2
+    case.params.teta_p = 0.2
+    sim, o = make_pair(case, oracle_lib)
+    info = sim.step(nsteps)
+    o.step(nsteps)
+    s = o.get()
+    g = sim.download()
+    assert info.time == pytest.approx(o.time, rel=1e-12)
+    assert rel_l2(g.x, s["x"]) <= 1e-12
+    assert rel_l2(g.v, s["v"]) <= 1e-9
+    assert rel_l2(g.p, s["p"]) <= 1e-9
+
+
+def test_partial_smoothing_fine_grained_equals_fused(oracle_lib):
+    """The per-call ABI smooths in sph_leapfrog_momentum and sph_eos, as the
+    fused step graph does."""
+    case = cases.dam_break_2d(dx=0.04)
+    case.params.teta_v = 0.2
+    case.params.teta_p = 0.2
+    a = Simulation(case)
+    a.upload(case.state)
+    b = Simulation(case)
+    b.upload(case.state)
+    for _ in range(5):
+        a.step(1)
+        b.time_step_duration()
+        b.rhs_momentum(want=False)
+        b.leapfrog_momentum()
+        b.leapfrog_trajectories()
+        b.ord_grid()
+        b.boundary_data_tab()
+        b.continuity(want=False)
+        b.leapfrog_continuity()
+        b.eos()
+    sa, sb = a.download(), b.download()
+    assert np.array_equal(sa.x, sb.x)
+    assert np.array_equal(sa.v, sb.v)
+    assert np.array_equal(sa.p, sb.p)
