@@ -1710,12 +1710,13 @@ __global__ void __launch_bounds__(kBlock, 3) k_momentum_f32(DevBatch b) {
     Kahan tp0, tp1, tp2, td0, td1, td2, tv0, tv1, tv2;
     tp0.zero(); tp1.zero(); tp2.zero(); td0.zero(); td1.zero(); td2.zero(); tv0.zero(); tv1.zero(); tv2.zero();
     float cp0 = 0.f, cp1 = 0.f, cp2 = 0.f, cd0 = 0.f, cd1 = 0.f, cd2 = 0.f, cv0 = 0.f, cv1 = 0.f, cv2 = 0.f;
-    ListPrefetcher lr;
-    lr.init(b.nlist, p, b.list_cap4, cnt);
-    const int nmax = __reduce_max_sync(0xffffffffu, (unsigned)cnt);
-    for (int k = 0; k < nmax; ++k) {
-      const int e = lr.get(k);
-      if (k >= cnt) continue;
+    // one list chunk (4 entries) per iteration: entries, compensation and
+    // the next chunk's load handled once per chunk
+    const int nch = (cnt + 3) >> 2;
+    const int nchmax = __reduce_max_sync(0xffffffffu, (unsigned)nch);
+    const int4* lbase = reinterpret_cast<const int4*>(b.nlist) + list_base4(p, b.list_cap4);
+    int4 nxt = nch > 0 ? __ldg(lbase) : make_int4(0, 0, 0, 0);
+    auto pair = [&](int e) {
       const int q = e & kSlotMask;
       const float4 xj = P.XF[q], vj = P.VF[q], rfj = P.RF[q];
       float d0, d1, d2;
@@ -1744,12 +1745,20 @@ __global__ void __launch_bounds__(kBlock, 3) k_momentum_f32(DevBatch b) {
         if (DIM == 3) cv1 = fmaf(vf, dv1, cv1);
         cv2 = fmaf(vf, dv2, cv2);
       }
-      if ((k & 3) == 3 || k == cnt - 1) {
-        tp0.add(cp0); tp1.add(cp1); tp2.add(cp2);
-        td0.add(cd0); td1.add(cd1); td2.add(cd2);
-        tv0.add(cv0); tv1.add(cv1); tv2.add(cv2);
-        cp0 = cp1 = cp2 = cd0 = cd1 = cd2 = cv0 = cv1 = cv2 = 0.f;
-      }
+    };
+    for (int c = 0; c < nchmax; ++c) {
+      const int4 ch = nxt;
+      if (c + 1 < nch) nxt = __ldg(lbase + (size_t)(c + 1) * 32);
+      if (c >= nch) continue;
+      const int rem = cnt - 4 * c;   // >= 1
+      pair(ch.x);
+      if (rem > 1) pair(ch.y);
+      if (rem > 2) pair(ch.z);
+      if (rem > 3) pair(ch.w);
+      tp0.add(cp0); tp1.add(cp1); tp2.add(cp2);
+      td0.add(cd0); td1.add(cd1); td2.add(cd2);
+      tv0.add(cv0); tv1.add(cv1); tv2.add(cv2);
+      cp0 = cp1 = cp2 = cd0 = cd1 = cd2 = cv0 = cv1 = cv2 = 0.f;
     }
     if (active) {
       double* o = P.MSUM + p;
