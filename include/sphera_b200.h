@@ -248,7 +248,7 @@ int  sph_rhs_momentum(SphHandle* h, double* acc_out);
 int  sph_leapfrog_momentum(SphHandle* h);
 /* Leapfrog_trajectories.f90:52-66 (time_step_loop.f90:262). */
 int  sph_leapfrog_trajectories(SphHandle* h);
-/* OrdGrid1.f90:50-105 followed by the list-free replacement of
+/* OrdGrid1.f90:50-105 followed by the neighbour-list replacement of
  * CalcVarLength.f90:133-269 (time_step_loop.f90:286,292).                 */
 int  sph_ord_grid(SphHandle* h);
 /* ComputeBoundaryDataTab_3D.f90:67-105 / _2D.f90:70-157

@@ -714,7 +714,7 @@ int create_batch(int nsims, const SphParams* params, const SphGeometry* geoms, c
     // particle (Gest_Trans.f90:90), far more than a flow uses
     bdt_cap += hs.prm.bdt_capacity > 0 ? (size_t)hs.prm.bdt_capacity : (size_t)hs.cap * (h->dim == 3 ? 3 : 2);
   }
-  if (poff >= (1 << 28)) { delete h; return SPH_ERR_INVALID_ARGUMENT; }   // FIFO entries carry 28-bit slots
+  if (poff >= (1 << 28)) { delete h; return SPH_ERR_INVALID_ARGUMENT; }   // list entries carry 28-bit slots
   h->total_slots = poff;
   h->total_cells = coff;
   h->total_faces = foff;

@@ -1031,7 +1031,7 @@ __device__ __forceinline__ void elastic_reaction(const SimDev& s, const DevBatch
 }
 
 // ==========================================================================
-// Neighbour lists (the list-free-kernel-values replacement of
+// Neighbour lists (the replacement of
 // CalcVarLength.f90:133-269).  One pass after the sort stores, per particle,
 // the slots of its accepted neighbours (the particle itself excluded, its
 // acceptance still counted for the NMAXPARTJ cap) in the reference's
