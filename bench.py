@@ -334,6 +334,8 @@ def main():
                     help="lattice spacing of the 3D dam break (0.005: the 864000-particle workload)")
     ap.add_argument("--forms", default="both", choices=["both", "fp32c", "fp64"])
     ap.add_argument("--autotune", type=int, default=1, help="size the persistent grids on the live state first")
+    ap.add_argument("--teta", type=float, default=0.0,
+                    help="partial smoothing coefficient TetaP = TetaV of the dam-break workload (0: off)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     if args.t_end is None:
@@ -366,7 +368,10 @@ def main():
     def make_case(precision, n=None):
         if args.workload == "random_box":
             return cases.random_box(n=n or args.n, precision=precision)
-        return cases.dam_break_3d(dx=args.dx, precision=precision)
+        c = cases.dam_break_3d(dx=args.dx, precision=precision)
+        c.params.teta_p = args.teta
+        c.params.teta_v = args.teta
+        return c
 
     def run_form(precision):
         case = make_case(precision)
@@ -432,7 +437,8 @@ def main():
     else:
         workload = "dam_break_3d" if args.dx == 0.005 else f"dam_break_3d_dx{args.dx:g}"
         desc = (f"dam_break_3d: tank 1.6x0.6x0.6 m, block 0.6x0.3x0.6 m, dx {args.dx:g} m, "
-                f"{n} particles per GPU, SA-SPH walls")
+                f"{n} particles per GPU, SA-SPH walls"
+                + (f", partial smoothing TetaP = TetaV = {args.teta:g}" if args.teta > 0 else ""))
     traffic = _traffic(workload)
 
     # end to end through the C ABI with pinned host buffers
@@ -509,7 +515,8 @@ def main():
         "phases_ms_per_step": r32["phases"],
         "pairs_per_particle": cnt["pairs"] / nprof / n,
         "candidates_per_particle": cnt["candidates"] / nprof / n,
-        "gpu_launches": KERNELS_PER_STEP * args.steps,
+        # + 2 launches each for the velocity and the pressure smoothing passes
+        "gpu_launches": (KERNELS_PER_STEP + (4 if args.teta > 0 else 0)) * args.steps,
         "clocks": clocks,
         "cpu_baseline": cpu,
     }
