@@ -619,7 +619,7 @@ void refresh_copies(SphHandle* h, cudaStream_t st) {
 // beside the boundary pass too and adds the wall term after the join.
 void step_sequence(SphHandle* h, cudaStream_t st) {
   momentum_pass(h, true, st);
-  if (h->any_teta_v) launch_velocity_smoothing(h->db, true, st);
+  if (h->any_teta_v) launch_velocity_smoothing(h->db, true, h->precision == SPH_PREC_FP32C, st);
   sort_sequence(h, st);
   cudaEventRecord(h->ev_fork, st);
   cudaStreamWaitEvent(h->stream2, h->ev_fork, 0);
@@ -1072,7 +1072,7 @@ int sph_rhs_momentum(SphHandle* h, double* acc_out) {
 int sph_leapfrog_momentum(SphHandle* h) {
   if (!h || !h->uploaded) return SPH_ERR_INVALID_ARGUMENT;
   launch_leapfrog_momentum(h->db, h->stream);
-  if (h->any_teta_v) launch_velocity_smoothing(h->db, false, h->stream);
+  if (h->any_teta_v) launch_velocity_smoothing(h->db, false, h->precision == SPH_PREC_FP32C, h->stream);
   refresh_copies(h, h->stream);
   SPH_CUDA(cudaGetLastError());
   return sync_dyn(h);
@@ -1120,7 +1120,7 @@ int sph_leapfrog_continuity(SphHandle* h) {
 int sph_eos(SphHandle* h) {
   if (!h || !h->uploaded) return SPH_ERR_INVALID_ARGUMENT;
   launch_eos(h->db, h->stream);
-  if (h->any_teta_p) launch_pressure_smoothing(h->db, false, h->stream);
+  if (h->any_teta_p) launch_pressure_smoothing(h->db, h->precision == SPH_PREC_FP32C, h->stream);
   refresh_copies(h, h->stream);
   launch_dt_reduce(h->db, h->stream);
   launch_finalize(h->db, 1, h->stream);
@@ -1277,7 +1277,7 @@ int sph_profile_phases(SphHandle* h, int32_t nsteps, double* ms) {
   for (int s = 0; s < nsteps && e == cudaSuccess; ++s) {
     cudaEventRecord(ev[0], q);
     momentum_pass(h, true, q);
-    if (h->any_teta_v) launch_velocity_smoothing(h->db, true, q);
+    if (h->any_teta_v) launch_velocity_smoothing(h->db, true, h->precision == SPH_PREC_FP32C, q);
     cudaEventRecord(ev[1], q);
     sort_sequence(h, q);
     cudaEventRecord(ev[2], q);

@@ -1991,6 +1991,85 @@ __device__ __forceinline__ double kernel_w(const SimDev& s, double rr) {
   return wu * s.coefke;
 }
 
+// velocity_smoothing_SA_SPH_3D.f90:61-125 / _2D.f90:66-117 (fixe/tapi
+// walls, slip mode 1): adds the wall terms of particle p to var.
+template <int DIM>
+__device__ __forceinline__ void smoothing_wall_velocity(const SimDev& s, const DevBatch& b, int p, const double4& vi,
+                                                        double* var) {
+  const Particles& P = b.P;
+  const int nb = P.bdt_count[p];
+  const int bstart = nb > 0 ? P.bdt_start[p] : 0;
+  for (int u = 0; u < nb; ++u) {
+    const BdtEntry& e = P.bdt[bstart + u];
+    if (DIM == 3) {
+      const FaceDev& f = b.faces[s.face_off + e.clobonum - 1];
+      const double vv[3] = {vi.x, vi.y, vi.z};
+      double DVGlo[3], DVLoc[3], BCLoc[3];
+      for (int i = 0; i < 3; ++i) DVGlo[i] = 2.0 * (f.velocity[i] - vv[i]);
+      for (int i = 0; i < 3; ++i) {
+        double a = 0.0;
+        for (int j = 0; j < 3; ++j) a = a + f.T[j][i] * DVGlo[j];
+        DVLoc[i] = a;
+      }
+      double IntWdV = e.bi[1];
+      BCLoc[0] = DVLoc[0] * IntWdV * f.slip;
+      BCLoc[1] = DVLoc[1] * IntWdV * f.slip;
+      BCLoc[2] = DVLoc[2] * IntWdV;
+      for (int i = 0; i < 3; ++i) {
+        double g = 0.0;
+        for (int j = 0; j < 3; ++j) g = g + f.T[i][j] * BCLoc[j];
+        var[i] = var[i] + g;
+      }
+    } else {
+      const SideDev& S = b.sides[s.side_off + e.clobonum - 1];
+      double DVGlo0 = 2.0 * (S.velocity[0] - vi.x), DVGlo1 = 2.0 * (S.velocity[2] - vi.z);
+      double DVLoc0 = S.sss[0] * DVGlo0 + S.sss[1] * DVGlo1;
+      double DVLoc1 = S.nnn[0] * DVGlo0 + S.nnn[1] * DVGlo1;
+      double IntWdV = e.bi[2];
+      double BCLoc0 = DVLoc0 * IntWdV * S.slip;
+      double BCLoc1 = DVLoc1 * IntWdV;
+      var[0] = var[0] + (S.sss[0] * BCLoc0 + S.nnn[0] * BCLoc1);
+      var[2] = var[2] + (S.sss[1] * BCLoc0 + S.nnn[1] * BCLoc1);
+    }
+  }
+}
+
+// The wall terms and the update of PressureSmoothing_3D.f90:111-134 /
+// _2D.f90:140-212 for particle p with pair sums sompW and AppUnity: the
+// smoothed pressure.
+template <int DIM>
+__device__ __forceinline__ double smoothing_pressure(const SimDev& s, const DevBatch& b, const SimDyn* dyn, int p,
+                                                     double pi, double sompW, double AppUnity) {
+  const Particles& P = b.P;
+  const double TetaP1 = s.teta_p * s.celerita * dyn->dt / s.h;
+  const double p0i = s.p_ref;
+  const int nb = P.bdt_count[p];
+  const int bstart = nb > 0 ? P.bdt_start[p] : 0;
+  double vpres;
+  if (DIM == 3) {
+    for (int u = 0; u < nb; ++u) {
+      const BdtEntry& e = P.bdt[bstart + u];
+      if (e.loc[2] > 0.0) AppUnity = AppUnity + e.bi[1];
+    }
+    double DiffP = (AppUnity < 0.95) ? sompW + (p0i - pi) * (1.0 - AppUnity) : sompW / AppUnity;
+    vpres = pi + TetaP1 * DiffP;
+  } else {
+    const double* g = dyn->geff;
+    double VIntWdV_FT = 0.0;
+    for (int u = 0; u < nb; ++u) {
+      const BdtEntry& e = P.bdt[bstart + u];
+      const SideDev& S = b.sides[s.side_off + e.clobonum - 1];
+      double mf0 = S.sss[0] * g[0] + S.sss[1] * g[2];
+      double mf1 = S.nnn[0] * g[0] + S.nnn[1] * g[2];
+      VIntWdV_FT = VIntWdV_FT + e.bi[1];
+      sompW = sompW + s.den0 * (mf0 * e.bi[3] + mf1 * e.bi[4]);
+    }
+    AppUnity = AppUnity + VIntWdV_FT + 0.0 + 0.0 + 0.0;
+    vpres = pi + TetaP1 * (sompW + (pi - pi) * 0.0 + (pi - pi) * 0.0 + (p0i - pi) * (1.0 - AppUnity));
+  }
+  return vpres;
+}
+
 // velocity_smoothing.f90:85-132 with velocity_smoothing_SA_SPH_3D.f90:61-125
 // / _2D.f90:66-117 (fixe/tapi walls, slip mode 1): ACC = var, the smoothing
 // increment, from the velocities `vel` (the step's leapfrog velocities).
@@ -2045,42 +2124,130 @@ __global__ void __launch_bounds__(kBlock) k_velocity_smoothing(DevBatch b, const
       var[1] = var[1] + (vi.y - vi.y) * self_w;
       var[2] = var[2] + (vi.z - vi.z) * self_w;
     }
-    const int nb = P.bdt_count[p];
-    const int bstart = nb > 0 ? P.bdt_start[p] : 0;
-    for (int u = 0; u < nb; ++u) {
-      const BdtEntry& e = P.bdt[bstart + u];
-      if (DIM == 3) {
-        const FaceDev& f = b.faces[s.face_off + e.clobonum - 1];
-        const double vv[3] = {vi.x, vi.y, vi.z};
-        double DVGlo[3], DVLoc[3], BCLoc[3];
-        for (int i = 0; i < 3; ++i) DVGlo[i] = 2.0 * (f.velocity[i] - vv[i]);
-        for (int i = 0; i < 3; ++i) {
-          double a = 0.0;
-          for (int j = 0; j < 3; ++j) a = a + f.T[j][i] * DVGlo[j];
-          DVLoc[i] = a;
-        }
-        double IntWdV = e.bi[1];
-        BCLoc[0] = DVLoc[0] * IntWdV * f.slip;
-        BCLoc[1] = DVLoc[1] * IntWdV * f.slip;
-        BCLoc[2] = DVLoc[2] * IntWdV;
-        for (int i = 0; i < 3; ++i) {
-          double g = 0.0;
-          for (int j = 0; j < 3; ++j) g = g + f.T[i][j] * BCLoc[j];
-          var[i] = var[i] + g;
-        }
-      } else {
-        const SideDev& S = b.sides[s.side_off + e.clobonum - 1];
-        double DVGlo0 = 2.0 * (S.velocity[0] - vi.x), DVGlo1 = 2.0 * (S.velocity[2] - vi.z);
-        double DVLoc0 = S.sss[0] * DVGlo0 + S.sss[1] * DVGlo1;
-        double DVLoc1 = S.nnn[0] * DVGlo0 + S.nnn[1] * DVGlo1;
-        double IntWdV = e.bi[2];
-        double BCLoc0 = DVLoc0 * IntWdV * S.slip;
-        double BCLoc1 = DVLoc1 * IntWdV;
-        var[0] = var[0] + (S.sss[0] * BCLoc0 + S.nnn[0] * BCLoc1);
-        var[2] = var[2] + (S.sss[1] * BCLoc0 + S.nnn[1] * BCLoc1);
+    smoothing_wall_velocity<DIM>(s, b, p, vi, var);
+    P.ACC[p] = make_double4(var[0], var[1], var[2], 0.0);
+  }
+}
+
+// The FP32c form's smoothing sums: the same terms in FP32 from the FP32
+// records (XF, RF) with compensated 4-entry chunk sums, the velocity and
+// pressure differences formed in FP64 first; the particle's own term (zero
+// for velocities) and the wall terms in FP64.
+__device__ __forceinline__ float kernel_w_f32(float rr, float hinv, float coefke) {
+  float r = rr * rsqrtf(rr);
+  float q = r * hinv;
+  if (!(q < 2.0f)) return 0.f;
+  float wu = (q < 1.0f) ? fmaf(q * q, fmaf(q, 0.5f, -1.0f), 0.666666667f)
+                        : (2.0f - q) * (2.0f - q) * (2.0f - q) * (1.0f / 6.0f);
+  return wu * coefke;
+}
+
+template <int DIM>
+__global__ void __launch_bounds__(kBlock, 4) k_velocity_smoothing_f32(DevBatch b, const double4* __restrict__ vel) {
+  __shared__ SimDev s;
+  int cur = -1;
+  const Particles& P = b.P;
+  for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
+    Tile tl = b.tiles[t];
+    load_sim(s, b.sims, tl.sim, cur);
+    SimDyn* dyn = b.dyn + tl.sim;
+    int p = tl.start + threadIdx.x;
+    const bool active = threadIdx.x < tl.count && p < s.p_off + dyn->nag && !dyn->frozen && s.teta_v > 1.0e-9;
+    const float hinv = (float)(1.0 / s.h), coefke = (float)s.coefke;
+    int ci = 0, cj = 0, ck = 0, cnt = 0;
+    float4 xfi = make_float4(0.f, 0.f, 0.f, 0.f);
+    double4 vi = make_double4(0.0, 0.0, 0.0, 0.0);
+    if (active) {
+      const double4 xi = P.X[p];
+      particle_cell(s, xi.x, xi.y, xi.z, ci, cj, ck);
+      xfi = P.XF[p];
+      vi = vel[p];
+      cnt = b.ncount[p];
+    }
+    Kahan k0, k1, k2;
+    k0.zero(); k1.zero(); k2.zero();
+    float c0 = 0.f, c1 = 0.f, c2 = 0.f;
+    ListPrefetcher lr;
+    lr.init(b.nlist, p, b.list_cap4, cnt);
+    const int nmax = __reduce_max_sync(0xffffffffu, (unsigned)cnt);
+    for (int k = 0; k < nmax; ++k) {
+      int e = lr.get(k);
+      if (k >= cnt) continue;
+      int q = e & kSlotMask;
+      const float4 xj = P.XF[q], rfj = P.RF[q];
+      const double4 vj = vel[q];
+      float d0, d1, d2;
+      separation_cols<DIM>(s, (int)((unsigned)e >> kSlotBits), xj, xfi, ci, cj, ck, d0, d1, d2);
+      float rr = fmaf(d2, d2, fmaf(d1, d1, d0 * d0));
+      float pes = __fdividef(rfj.z * kernel_w_f32(rr, hinv, coefke), rfj.x);
+      c0 = fmaf((float)(vj.x - vi.x), pes, c0);
+      if (DIM == 3) c1 = fmaf((float)(vj.y - vi.y), pes, c1);
+      c2 = fmaf((float)(vj.z - vi.z), pes, c2);
+      if ((k & 3) == 3 || k == cnt - 1) {
+        k0.add(c0); k1.add(c1); k2.add(c2);
+        c0 = c1 = c2 = 0.f;
       }
     }
+    if (!active) continue;
+    double var[3] = {k0.val(), k1.val(), k2.val()};
+    smoothing_wall_velocity<DIM>(s, b, p, vi, var);
     P.ACC[p] = make_double4(var[0], var[1], var[2], 0.0);
+  }
+}
+
+template <int DIM>
+__global__ void __launch_bounds__(kBlock, 4) k_pressure_smoothing_f32(DevBatch b) {
+  __shared__ SimDev s;
+  int cur = -1;
+  const Particles& P = b.P;
+  for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
+    Tile tl = b.tiles[t];
+    load_sim(s, b.sims, tl.sim, cur);
+    SimDyn* dyn = b.dyn + tl.sim;
+    int p = tl.start + threadIdx.x;
+    const bool active = threadIdx.x < tl.count && p < s.p_off + dyn->nag && !dyn->frozen && s.teta_p > 0.0;
+    const float hinv = (float)(1.0 / s.h), coefke = (float)s.coefke;
+    int ci = 0, cj = 0, ck = 0, cnt = 0;
+    float4 xfi = make_float4(0.f, 0.f, 0.f, 0.f);
+    double pi = 0.0;
+    float self = 0.f;
+    if (active) {
+      const double4 xi = P.X[p];
+      particle_cell(s, xi.x, xi.y, xi.z, ci, cj, ck);
+      xfi = P.XF[p];
+      const float4 rfi = P.RF[p];
+      pi = P.RP[p].y;
+      self = __fdividef(rfi.z * (0.666666667f * coefke), rfi.x);
+      cnt = b.ncount[p];
+    }
+    Kahan ka, ks;
+    ka.zero();
+    ks.zero();
+    float ca = self, cs = 0.f;
+    ListPrefetcher lr;
+    lr.init(b.nlist, p, b.list_cap4, cnt);
+    const int nmax = __reduce_max_sync(0xffffffffu, (unsigned)cnt);
+    for (int k = 0; k < nmax; ++k) {
+      int e = lr.get(k);
+      if (k >= cnt) continue;
+      int q = e & kSlotMask;
+      const float4 xj = P.XF[q], rfj = P.RF[q];
+      const float dp = (float)(P.RP[q].y - pi);
+      float d0, d1, d2;
+      separation_cols<DIM>(s, (int)((unsigned)e >> kSlotBits), xj, xfi, ci, cj, ck, d0, d1, d2);
+      float rr = fmaf(d2, d2, fmaf(d1, d1, d0 * d0));
+      float pes = __fdividef(rfj.z * kernel_w_f32(rr, hinv, coefke), rfj.x);
+      ca += pes;
+      cs = fmaf(dp, pes, cs);
+      if ((k & 3) == 3 || k == cnt - 1) {
+        ka.add(ca);
+        ks.add(cs);
+        ca = cs = 0.f;
+      }
+    }
+    if (!active) continue;
+    if (cnt == 0) ka.add(ca);   // the particle's own term alone
+    P.DDEN[p] = smoothing_pressure<DIM>(s, b, dyn, p, pi, ks.val(), ka.val());
   }
 }
 
@@ -2177,33 +2344,7 @@ __global__ void __launch_bounds__(kBlock) k_pressure_smoothing(DevBatch b) {
       AppUnity = AppUnity + self_w;
       sompW = sompW + (pi - pi) * self_w;
     }
-    const double TetaP1 = s.teta_p * s.celerita * dyn->dt / s.h;
-    const double p0i = s.p_ref;
-    const int nb = P.bdt_count[p];
-    const int bstart = nb > 0 ? P.bdt_start[p] : 0;
-    double vpres;
-    if (DIM == 3) {
-      for (int u = 0; u < nb; ++u) {
-        const BdtEntry& e = P.bdt[bstart + u];
-        if (e.loc[2] > 0.0) AppUnity = AppUnity + e.bi[1];
-      }
-      double DiffP = (AppUnity < 0.95) ? sompW + (p0i - pi) * (1.0 - AppUnity) : sompW / AppUnity;
-      vpres = pi + TetaP1 * DiffP;
-    } else {
-      const double* g = dyn->geff;
-      double VIntWdV_FT = 0.0;
-      for (int u = 0; u < nb; ++u) {
-        const BdtEntry& e = P.bdt[bstart + u];
-        const SideDev& S = b.sides[s.side_off + e.clobonum - 1];
-        double mf0 = S.sss[0] * g[0] + S.sss[1] * g[2];
-        double mf1 = S.nnn[0] * g[0] + S.nnn[1] * g[2];
-        VIntWdV_FT = VIntWdV_FT + e.bi[1];
-        sompW = sompW + s.den0 * (mf0 * e.bi[3] + mf1 * e.bi[4]);
-      }
-      AppUnity = AppUnity + VIntWdV_FT + 0.0 + 0.0 + 0.0;
-      vpres = pi + TetaP1 * (sompW + (pi - pi) * 0.0 + (pi - pi) * 0.0 + (p0i - pi) * (1.0 - AppUnity));
-    }
-    P.DDEN[p] = vpres;
+    P.DDEN[p] = smoothing_pressure<DIM>(s, b, dyn, p, pi, sompW, AppUnity);
   }
 }
 
@@ -2730,17 +2871,28 @@ void launch_leapfrog_continuity(const DevBatch& b, cudaStream_t st) {
 }
 void launch_eos(const DevBatch& b, cudaStream_t st) { k_eos<<<blocks_for(b), kBlock, 0, st>>>(b); }
 
-void launch_velocity_smoothing(const DevBatch& b, bool fused, cudaStream_t st) {
+void launch_velocity_smoothing(const DevBatch& b, bool fused, bool fp32c, cudaStream_t st) {
   const double4* vel = fused ? b.P.V2 : b.P.V;
-  if (b.dim == 3) k_velocity_smoothing<3><<<blocks_for(b), kBlock, 0, st>>>(b, vel);
-  else k_velocity_smoothing<2><<<blocks_for(b), kBlock, 0, st>>>(b, vel);
+  if (fp32c) {
+    if (b.dim == 3) k_velocity_smoothing_f32<3><<<blocks_for(b), kBlock, 0, st>>>(b, vel);
+    else k_velocity_smoothing_f32<2><<<blocks_for(b), kBlock, 0, st>>>(b, vel);
+  } else {
+    if (b.dim == 3) k_velocity_smoothing<3><<<blocks_for(b), kBlock, 0, st>>>(b, vel);
+    else k_velocity_smoothing<2><<<blocks_for(b), kBlock, 0, st>>>(b, vel);
+  }
   if (fused) k_velocity_smoothing_apply<true><<<blocks_for(b), kBlock, 0, st>>>(b);
   else k_velocity_smoothing_apply<false><<<blocks_for(b), kBlock, 0, st>>>(b);
 }
 
-void launch_pressure_smoothing(const DevBatch& b, bool refresh_f32, cudaStream_t st) {
-  if (b.dim == 3) k_pressure_smoothing<3><<<blocks_for(b), kBlock, 0, st>>>(b);
-  else k_pressure_smoothing<2><<<blocks_for(b), kBlock, 0, st>>>(b);
+void launch_pressure_smoothing(const DevBatch& b, bool fp32c, cudaStream_t st) {
+  const bool refresh_f32 = fp32c;
+  if (fp32c) {
+    if (b.dim == 3) k_pressure_smoothing_f32<3><<<blocks_for(b), kBlock, 0, st>>>(b);
+    else k_pressure_smoothing_f32<2><<<blocks_for(b), kBlock, 0, st>>>(b);
+  } else {
+    if (b.dim == 3) k_pressure_smoothing<3><<<blocks_for(b), kBlock, 0, st>>>(b);
+    else k_pressure_smoothing<2><<<blocks_for(b), kBlock, 0, st>>>(b);
+  }
   k_pressure_smoothing_apply<<<blocks_for(b), kBlock, 0, st>>>(b, refresh_f32 ? 1 : 0);
 }
 void launch_dt_reduce(const DevBatch& b, cudaStream_t st) { k_dt_reduce<<<blocks_for(b), kBlock, 0, st>>>(b); }

@@ -66,8 +66,8 @@ void launch_leapfrog_continuity(const DevBatch& b, cudaStream_t st);
 void launch_eos(const DevBatch& b, cudaStream_t st);
 // partial smoothing (TetaV > 1e-9, TetaP > 0): fused = on the step record
 // V2/X2 (step graph), else in place (per-call ABI)
-void launch_velocity_smoothing(const DevBatch& b, bool fused, cudaStream_t st);
-void launch_pressure_smoothing(const DevBatch& b, bool refresh_f32, cudaStream_t st);
+void launch_velocity_smoothing(const DevBatch& b, bool fused, bool fp32c, cudaStream_t st);
+void launch_pressure_smoothing(const DevBatch& b, bool fp32c, cudaStream_t st);
 void launch_dt_reduce(const DevBatch& b, cudaStream_t st);
 void launch_finalize(const DevBatch& b, int mode, cudaStream_t st);
 // host <-> device in caller order
