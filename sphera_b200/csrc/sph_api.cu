@@ -747,6 +747,7 @@ int create_batch(int nsims, const SphParams* params, const SphGeometry* geoms, c
   A(P.tmp_src, N); A(P.tmp_id, N); A(P.tmp_key, N);
   A(P.ACC, N); A(P.DDEN, N);
   if (h->precision == SPH_PREC_FP32C) A(P.MSUM, 9 * N);
+  if (h->precision == SPH_PREC_FP32C && h->any_teta_v) A(P.VF2, N);
   A(P.out_flag, N); A(P.id_remap, N); A(P.cur_of, N);
   A(h->d_cx, 3 * N); A(h->d_cv, 3 * N); A(h->d_crho, N); A(h->d_cp, N); A(h->d_cm, N);
   A(h->d_cacc, 3 * N); A(h->d_cdden, N);

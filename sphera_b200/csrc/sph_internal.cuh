@@ -159,6 +159,7 @@ struct Particles {
   double4* ACC;     // dv/dt
   double* DDEN;     // drho/dt
   double* MSUM;     // FP32c momentum pair sums of a slot: 9 values (pressure, Monaghan, Morris x 3)
+  float4* VF2;      // FP32c with velocity smoothing: the step's leapfrog velocities in FP32
   // removal replay
   uint8_t* out_flag;   // by caller index
   int* id_remap;       // by caller index

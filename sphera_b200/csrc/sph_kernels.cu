@@ -1844,6 +1844,7 @@ __global__ void __launch_bounds__(kBlock) k_momentum_f32_finish(DevBatch b) {
         for (int d = 0; d < 3; ++d) vn[d] = vi[d] + dtvel * acc[d];
         P.X2[p] = make_double4(xi.x + dt * vn[0], xi.y + dt * vn[1], xi.z + dt * vn[2], xi.w);
         P.V2[p] = make_double4(vn[0], vn[1], vn[2], rhoi);
+        if (P.VF2) P.VF2[p] = make_float4((float)vn[0], (float)vn[1], (float)vn[2], 0.f);
         P.P2[p] = pi;
         P.I2[p] = P.I[p];
         P.L2[p] = (uint8_t)lam_new;
@@ -2130,9 +2131,10 @@ __global__ void __launch_bounds__(kBlock) k_velocity_smoothing(DevBatch b, const
 }
 
 // The FP32c form's smoothing sums: the same terms in FP32 from the FP32
-// records (XF, RF) with compensated 4-entry chunk sums, the velocity and
-// pressure differences formed in FP64 first; the particle's own term (zero
-// for velocities) and the wall terms in FP64.
+// records (XF, RF, and VF2, the leapfrog velocities the momentum pass
+// writes in FP32) with compensated 4-entry chunk sums, the pressure
+// differences formed in FP64 first; the particle's own term (zero for
+// velocities) and the wall terms in FP64.
 __device__ __forceinline__ float kernel_w_f32(float rr, float hinv, float coefke) {
   float r = rr * rsqrtf(rr);
   float q = r * hinv;
@@ -2164,6 +2166,7 @@ __global__ void __launch_bounds__(kBlock, 4) k_velocity_smoothing_f32(DevBatch b
       vi = vel[p];
       cnt = b.ncount[p];
     }
+    const float4 vif = make_float4((float)vi.x, (float)vi.y, (float)vi.z, 0.f);
     Kahan k0, k1, k2;
     k0.zero(); k1.zero(); k2.zero();
     float c0 = 0.f, c1 = 0.f, c2 = 0.f;
@@ -2174,15 +2177,14 @@ __global__ void __launch_bounds__(kBlock, 4) k_velocity_smoothing_f32(DevBatch b
       int e = lr.get(k);
       if (k >= cnt) continue;
       int q = e & kSlotMask;
-      const float4 xj = P.XF[q], rfj = P.RF[q];
-      const double4 vj = vel[q];
+      const float4 xj = P.XF[q], rfj = P.RF[q], vj = P.VF2[q];
       float d0, d1, d2;
       separation_cols<DIM>(s, (int)((unsigned)e >> kSlotBits), xj, xfi, ci, cj, ck, d0, d1, d2);
       float rr = fmaf(d2, d2, fmaf(d1, d1, d0 * d0));
       float pes = __fdividef(rfj.z * kernel_w_f32(rr, hinv, coefke), rfj.x);
-      c0 = fmaf((float)(vj.x - vi.x), pes, c0);
-      if (DIM == 3) c1 = fmaf((float)(vj.y - vi.y), pes, c1);
-      c2 = fmaf((float)(vj.z - vi.z), pes, c2);
+      c0 = fmaf(vj.x - vif.x, pes, c0);
+      if (DIM == 3) c1 = fmaf(vj.y - vif.y, pes, c1);
+      c2 = fmaf(vj.z - vif.z, pes, c2);
       if ((k & 3) == 3 || k == cnt - 1) {
         k0.add(c0); k1.add(c1); k2.add(c2);
         c0 = c1 = c2 = 0.f;
@@ -2386,6 +2388,7 @@ __global__ void k_leapfrog_momentum(DevBatch b) {
     v.y = v.y + dtvel * a.y;
     v.z = v.z + dtvel * a.z;
     b.P.V[p] = v;
+    if (b.P.VF2) b.P.VF2[p] = make_float4((float)v.x, (float)v.y, (float)v.z, 0.f);
   }
 }
 
