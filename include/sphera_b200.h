@@ -98,6 +98,15 @@ typedef struct SphParams {
      * disables it.                                                        */
     double  forcing_amplitude;      /* A [m]                                          */
     double  forcing_period;         /* T [s]                                          */
+    /* 1st-order consistency (input_any_t%C1_BE, %C1_divu, %invB_det_thresh):
+     * the pressure-gradient terms of the momentum equation are renormalised
+     * with B_ren_gradp and, with c1_divu as well, the velocity gradients of
+     * the continuity equation with B_ren_divu.  3D, FP64 form (otherwise
+     * SPH_ERR_UNSUPPORTED); a matrix whose |det| is below invb_det_thresh
+     * is replaced by -I (B_ren_gradp_inversion.f90:62-73).  0 disables.   */
+    int32_t c1_be;
+    int32_t c1_divu;
+    double  invb_det_thresh;        /* >= 0                                           */
 } SphParams;
 
 /* One boundary zone (Tratto). */
@@ -284,6 +293,12 @@ int  sph_dump_neighbours(SphHandle* h, int32_t nmaxj, int32_t* counts, int32_t* 
  * IntGiWrRdV(3,3) column-major ([n][max_per][20]).                        */
 int  sph_dump_boundary(SphHandle* h, int32_t max_per, int32_t* ncb,
                        int32_t* clobonum, double* values);
+/* With c1_be: pg%B_ren_gradp and (with c1_divu) pg%B_ren_divu in caller
+ * order, 9 doubles per particle, B(i,j) at [9 k + 3 (i-1) + (j-1)].  After
+ * a search they hold the fluid sums of CalcVarLength.f90:285-324; after a
+ * continuity pass the inverses of the completed matrices.  Either pointer
+ * may be NULL.                                                            */
+int  sph_dump_renormalisation(SphHandle* h, double* b_gradp, double* b_divu);
 
 /* ---------------------------------------------------------------------- */
 /* Allocation-free entry point                                             */

@@ -47,6 +47,7 @@ def lib():
         L.ora_time.argtypes = [vp]
         L.ora_time.restype = C.c_double
         L.ora_get.argtypes = [vp, dp, dp, dp, dp, dp, dp, dp]
+        L.ora_get_c1.argtypes = [vp, dp, dp]
         L.ora_grid.argtypes = [vp, ip, ip, ip]
         L.ora_grid_info.argtypes = [vp, ip, dp, dp]
         L.ora_neighbours.argtypes = [vp, C.c_int, ip, ip]
@@ -77,6 +78,8 @@ class Oracle:
     """One simulation held by the oracle, in the reference's particle order."""
 
     def __init__(self, case, nthreads=0):
+        if case.params.dim == 2 and case.params.c1_be:
+            raise NotImplementedError("the 1st-order consistency renormalisation is restated for 3D only")
         L = lib()
         self.case = case
         st = case.state
@@ -156,6 +159,13 @@ class Oracle:
         out.update({k: np.zeros(n) for k in ("rho", "p", "m", "dden")})
         lib().ora_get(self._h, *(abi.dptr(out[k]) for k in ("x", "v", "rho", "p", "m", "acc", "dden")))
         return out
+
+    def get_c1(self):
+        """B_ren_gradp and B_ren_divu, (n, 3, 3) each."""
+        bg = np.zeros((self.n, 3, 3))
+        bd = np.zeros((self.n, 3, 3))
+        lib().ora_get_c1(self._h, abi.dptr(bg), abi.dptr(bd))
+        return bg, bd
 
     def grid(self):
         n = self.n

@@ -89,6 +89,7 @@ struct Particle {
   double coord[3], vel[3], var[3], acc[3], velass[3];
   double dens, pres, mass, dden, kin_visc;
   int cella, kodvel, koddens, laminar_flag;
+  double Bg[3][3], Bd[3][3];   // B_ren_gradp, B_ren_divu: Bg[i][j] = B(i+1,j+1)
 };
 
 struct Face {           // TyBoundaryFace
@@ -277,6 +278,84 @@ void OrdGrid1(Oracle& o) {
 }
 
 // CalcVarLength.f90:133-269, SA-SPH branch (C1_BE, KTGF, bodies off)
+// grad_W_sub.f90:52-91 (3D): gradient of the beta-spline (kernel_ID 1) or
+// anti-cluster (kernel_ID 2) kernel at r_vec; PIGRECO as
+// Static_allocation_module.f90:50.
+static void grad_W_sub(const Oracle& o, int kernel_ID, const double* r_vec, double* grad_W) {
+  const double PIGRECO = 3.14159265358979;
+  grad_W[0] = grad_W[1] = grad_W[2] = 0.0;
+  double abs_r = std::sqrt(r_vec[0] * r_vec[0] + r_vec[1] * r_vec[1] + r_vec[2] * r_vec[2]);
+  if (abs_r < o.h * 1.0e-6) return;
+  double q = abs_r / o.h;
+  double h3 = o.h * o.h * o.h;
+  double dW = 0.0;
+  if (kernel_ID == 1) {
+    if (q <= 1.0) dW = 1.0 / (PIGRECO * h3) * (9.0 / 4.0 * (q * q) - 3.0 * q);
+    else if (q >= 2.0) dW = 0.0;
+    else dW = -(3.0 / (4.0 * PIGRECO * h3) * ((2.0 - q) * (2.0 - q)));
+  } else {
+    if (q <= 2.0) dW = -(3.0 * ((2.0 - q) * (2.0 - q)) * (15.0 / (64.0 * PIGRECO * h3)));
+  }
+  for (int k = 0; k < 3; ++k) grad_W[k] = dW / o.h * r_vec[k] / abs_r;
+}
+
+// Matrix_Inversion_3x3.f90:50-74 inside B_ren_gradp_inversion.f90 /
+// B_ren_divu_inversion.f90:58-75: the inverse when |det| >= thresh, else -I.
+static void B_ren_inversion(double B[3][3], double thresh) {
+  double det = B[0][0] * B[1][1] * B[2][2] + B[1][0] * B[2][1] * B[0][2] + B[2][0] * B[0][1] * B[1][2] -
+               B[0][0] * B[2][1] * B[1][2] - B[2][0] * B[1][1] * B[0][2] - B[1][0] * B[0][1] * B[2][2];
+  if (std::fabs(det) >= thresh) {
+    double inv[3][3];
+    inv[0][0] = B[1][1] * B[2][2] - B[1][2] * B[2][1];
+    inv[0][1] = B[0][2] * B[2][1] - B[0][1] * B[2][2];
+    inv[0][2] = B[0][1] * B[1][2] - B[0][2] * B[1][1];
+    inv[1][0] = B[1][2] * B[2][0] - B[1][0] * B[2][2];
+    inv[1][1] = B[0][0] * B[2][2] - B[0][2] * B[2][0];
+    inv[1][2] = B[0][2] * B[1][0] - B[0][0] * B[1][2];
+    inv[2][0] = B[1][0] * B[2][1] - B[1][1] * B[2][0];
+    inv[2][1] = B[0][1] * B[2][0] - B[0][0] * B[2][1];
+    inv[2][2] = B[0][0] * B[1][1] - B[0][1] * B[1][0];
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) B[i][j] = inv[i][j] / det;
+  } else {
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) B[i][j] = 0.0;
+    B[0][0] = B[1][1] = B[2][2] = -1.0;
+  }
+}
+
+// v = -(B v) (MatrixProduct.f90:55-63, then the sign of the callers).
+static void B_renormalise(const double B[3][3], double* v) {
+  double a[3];
+  for (int i = 0; i < 3; ++i) {
+    double sum = 0.0;
+    for (int k = 0; k < 3; ++k) sum = sum + B[i][k] * v[k];
+    a[i] = sum;
+  }
+  for (int i = 0; i < 3; ++i) v[i] = -a[i];
+}
+
+// T (IntGiWrRdV T^T): the SA-SPH frontier's contribution to the
+// renormalisation matrices (AddBoundaryContributions_to_ME3D.f90:172-187,
+// AddBoundaryContribution_to_CE3D.f90:93-112).
+static void frontier_B(const Face& f, const BDT& e, double out[3][3]) {
+  double Tt[3][3], m2[3][3];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) Tt[i][j] = f.T[j][i];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      double sum = 0.0;
+      for (int k = 0; k < 3; ++k) sum = sum + e.IntGiWrRdV[i][k] * Tt[k][j];
+      m2[i][j] = sum;
+    }
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      double sum = 0.0;
+      for (int k = 0; k < 3; ++k) sum = sum + f.T[i][k] * m2[k][j];
+      out[i][j] = sum;
+    }
+}
+
 void CalcVarLength(Oracle& o) {
   const double ke_coef = o.coefke / o.h;
   const double kacl_coef = o.coefkacl / o.h;
@@ -285,9 +364,11 @@ void CalcVarLength(Oracle& o) {
   int trunc_count = 0;
 #pragma omp parallel for schedule(static) num_threads(o.nthreads) reduction(+:trunc_count)
   for (int npi = 1; npi <= o.nag; ++npi) {
-    const Particle& pi = o.pg[npi];
+    Particle& pi = o.pg[npi];
     int nceli = pi.cella;
     if (nceli == 0) continue;
+    for (int a = 0; a < 3; ++a)
+      for (int c = 0; c < 3; ++c) pi.Bg[a][c] = pi.Bd[a][c] = 0.0;   // CalcVarLength.f90:181-182
     int igridi, jgridi, kgridi;
     CellIndices(o, nceli, igridi, jgridi, kgridi);
     int jgrid1 = jgridi - (o.ncord - 2);
@@ -335,6 +416,21 @@ void CalcVarLength(Oracle& o) {
             pk[1] = pk[0] / (rijtemp2 + o.eta2);
             pk[2] = gradmodwacl * denom;
             pk[3] = wu * o.coefke;
+            if (o.prm.c1_be) {
+              // CalcVarLength.f90:285-324: the renormalisation matrices
+              double r_vec[3] = {-rt[0], -rt[1], -rt[2]}, gW[3], gWo[3];
+              const double dxj[3] = {pj.coord[0] - pi.coord[0], pj.coord[1] - pi.coord[1], pj.coord[2] - pi.coord[2]};
+              grad_W_sub(o, 2, r_vec, gW);
+              for (int k = 0; k < 3; ++k) gWo[k] = gW[k] * pj.mass / pj.dens;
+              for (int c = 0; c < 3; ++c)
+                for (int k = 0; k < 3; ++k) pi.Bg[k][c] = pi.Bg[k][c] + dxj[c] * gWo[k];
+              if (o.prm.c1_divu) {
+                grad_W_sub(o, 1, r_vec, gW);
+                for (int k = 0; k < 3; ++k) gWo[k] = gW[k] * pj.mass / pj.dens;
+                for (int c = 0; c < 3; ++c)
+                  for (int k = 0; k < 3; ++k) pi.Bd[k][c] = pi.Bd[k][c] + dxj[c] * gWo[k];
+              }
+            }
           }
         }
     if (warned) trunc_count += 1;
@@ -1117,13 +1213,22 @@ int ComputeBoundaryDataTab_2D(Oracle& o) {
 // ------------------------------------------------------------------------
 
 // AddBoundaryContribution_to_CE3D.f90:82-169 (C1_BE and ALE3 off)
-void AddBoundaryContribution_to_CE3D(const Oracle& o, int npi, int Ncbf, double* gu, double* gv, double* gw) {
-  const Particle& p = o.pg[npi];
+void AddBoundaryContribution_to_CE3D(Oracle& o, int npi, int Ncbf, double* gu, double* gv, double* gw) {
+  Particle& p = o.pg[npi];
   int ibdt = o.BDP[3 * (npi - 1) + 2];
   for (int icbf = 1; icbf <= Ncbf; ++icbf) {
     const BDT& e = o.BDTab[ibdt + icbf - 2];
     const Face& f = o.faces[e.CloBoNum - 1];
     if (e.LocXYZ[2] > 0.0) {
+      if (o.prm.c1_be) {   // AddBoundaryContribution_to_CE3D.f90:93-112
+        double m[3][3];
+        frontier_B(f, e, m);
+        for (int a = 0; a < 3; ++a)
+          for (int c = 0; c < 3; ++c) {
+            if (o.prm.c1_divu) p.Bd[a][c] = p.Bd[a][c] + m[a][c];
+            p.Bg[a][c] = p.Bg[a][c] + m[a][c];
+          }
+      }
       double aux2[3], n[3], dvel[3], av[3];
       for (int d = 0; d < 3; ++d) aux2[d] = 2.0 * (f.velocity[d] - p.var[d]);
       for (int d = 0; d < 3; ++d) n[d] = f.T[d][2];
@@ -1184,6 +1289,15 @@ void SASPH_continuity(Oracle& o, int npi, int& Ncbf_Max_local) {
     active = Ncbs > 0 && IntNcbs > 0;
     if (active) AddBoundaryContribution_to_CE2D(o, npi, IntNcbs, gu, gw);
   }
+  if (o.prm.c1_be) {   // SASPH_continuity.f90:112-119
+    if (o.prm.c1_divu) B_ren_inversion(p.Bd, o.prm.invb_det_thresh);
+    B_ren_inversion(p.Bg, o.prm.invb_det_thresh);
+  }
+  if (active && o.prm.c1_be && o.prm.c1_divu) {   // SASPH_continuity.f90:126-140
+    B_renormalise(p.Bd, gu);
+    if (o.dim == 3) B_renormalise(p.Bd, gv);
+    B_renormalise(p.Bd, gw);
+  }
   if (active && p.koddens == 0)
     p.dden = p.dden - p.dens * (gu[0] + gv[1] + gw[2]);
 }
@@ -1192,6 +1306,29 @@ void SASPH_continuity(Oracle& o, int npi, int& Ncbf_Max_local) {
 void Continuity_Equation(Oracle& o, int npi) {
   Particle& p = o.pg[npi];
   if (p.cella <= 0) return;
+  if (o.prm.c1_be && o.prm.c1_divu) {
+    // Continuity_Equation.f90:119-126,201-217: the whole velocity-gradient
+    // vectors, renormalised with B_ren_divu
+    double v1[3] = {0, 0, 0}, v2[3] = {0, 0, 0}, v3[3] = {0, 0, 0};
+    for (int contj = 1; contj <= o.nPartIntorno[npi]; ++contj) {
+      long npartint = (long)(npi - 1) * o.NMAXPARTJ + contj;
+      const Particle& q = o.pg[o.PartIntorno[npartint]];
+      double rhoi = p.dens, rhoj = q.dens, amassj = q.mass;
+      double dvar[3] = {q.var[0] - p.var[0], q.var[1] - p.var[1], q.var[2] - p.var[2]};
+      const double* rg = &o.rag[npartint * 3];
+      double c = rhoi * (amassj / rhoj) * o.PartKernel[npartint * 4];
+      for (int k = 0; k < 3; ++k) {
+        v1[k] = v1[k] + c * dvar[0] * rg[k];
+        if (o.dim == 3) v2[k] = v2[k] + c * dvar[1] * rg[k];
+        v3[k] = v3[k] + c * dvar[2] * rg[k];
+      }
+    }
+    B_renormalise(p.Bd, v1);
+    if (o.dim == 3) B_renormalise(p.Bd, v2);
+    B_renormalise(p.Bd, v3);
+    p.dden = p.dden - (v1[0] + v2[1] + v3[2]);
+    return;
+  }
   double a1 = 0.0, a2 = 0.0, a3 = 0.0;
   const int NM = o.NMAXPARTJ;
   for (int contj = 1; contj <= o.nPartIntorno[npi]; ++contj) {
@@ -1216,8 +1353,9 @@ void Continuity_Equation(Oracle& o, int npi) {
 // ------------------------------------------------------------------------
 
 // AddBoundaryContributions_to_ME3D.f90:105-336 (fixe/tapi, mode 1, C1/ALE3 off)
-void AddBoundaryContributions_to_ME3D(const Oracle& o, int npi, int Ncbf, double* tpres, double* tdiss, double* tvisc) {
-  const Particle& p = o.pg[npi];
+void AddBoundaryContributions_to_ME3D(Oracle& o, int npi, int Ncbf, double* tpres, double* tdiss, double* tvisc) {
+  Particle& p = o.pg[npi];
+  const bool c1_first = o.prm.c1_be && o.on_going_time_step == 1;
   double vi[3] = {p.var[0], p.var[1], p.var[2]};
   double ALEt[3] = {0, 0, 0}, gradpt[3] = {0, 0, 0}, VMon[3] = {0, 0, 0}, VShear[3] = {0, 0, 0};
   for (int icbf = 1; icbf <= Ncbf; ++icbf) {
@@ -1256,6 +1394,12 @@ void AddBoundaryContributions_to_ME3D(const Oracle& o, int npi, int Ncbf, double
       aglob[i] = s;
     }
     for (int d = 0; d < 3; ++d) ALEt[d] = ALEt[d] + aglob[d];
+    if (c1_first) {
+      double m[3][3];
+      frontier_B(f, e, m);
+      for (int a = 0; a < 3; ++a)
+        for (int c = 0; c < 3; ++c) p.Bg[a][c] = p.Bg[a][c] + m[a][c];
+    }
     double IntGWZrm1dV = e.BoundaryIntegral[6];
     double IntdWrm1dV = e.BoundaryIntegral[2];
     double alfaMon = o.prm.alfa_mon;
@@ -1276,7 +1420,10 @@ void AddBoundaryContributions_to_ME3D(const Oracle& o, int npi, int Ncbf, double
       }
     }
   }
+  // AddBoundaryContributions_to_ME3D.f90:314-325
+  if (c1_first) B_ren_inversion(p.Bg, o.prm.invb_det_thresh);
   if (Ncbf == 0) return;
+  if (o.prm.c1_be) B_renormalise(p.Bg, gradpt);
   for (int d = 0; d < 3; ++d) {
     tpres[d] = tpres[d] + ALEt[d] + gradpt[d];
     tdiss[d] = tdiss[d] - VMon[d];
@@ -1397,6 +1544,7 @@ void inter_EqMoto(Oracle& o, int npi, double* tpres, double* tdiss, double* tvis
       }
     }
   }
+  if (o.prm.c1_be) B_renormalise(p.Bg, t_pres_aux);   // inter_EqMoto.f90:255-260
   for (int d = 0; d < 3; ++d) tpres[d] = tpres[d] + t_pres_aux[d] + ALE1[d];
   p.laminar_flag = 0;
   if (p.kin_visc > 0.0) {
@@ -1467,7 +1615,7 @@ void RHS_momentum_equation(Oracle& o) {
     int ncb = o.BDP[3 * (npi - 1)];
     int intn = o.BDP[3 * (npi - 1) + 1];
     bool active = (o.dim == 3) ? (ncb > 0) : (ncb > 0 && intn > 0);
-    if (active) {
+    if (active || o.prm.c1_be) {   // RHS_momentum_equation.f90:133-150
       if (o.dim == 3) AddBoundaryContributions_to_ME3D(o, npi, ncb, tpres, tdiss, tvisc);
       else AddBoundaryContributions_to_ME2D(o, npi, intn, tpres, tdiss, tvisc);
     }
@@ -1865,7 +2013,17 @@ int ora_search(void* h) {
   return check(o, boundary_tab(o));
 }
 
-int ora_rhs_momentum(void* h) { RHS_momentum_equation(*static_cast<Oracle*>(h)); return 0; }
+// RHS_momentum_equation as time_step_loop.f90 calls it, after advancing
+// on_going_time_step: a call between steps evaluates the momentum of the
+// next step (which matters only for the step-1 completion of B_ren_gradp).
+int ora_rhs_momentum(void* h) {
+  Oracle& o = *static_cast<Oracle*>(h);
+  const int saved = o.on_going_time_step;
+  o.on_going_time_step = saved < 0 ? 1 : saved + 1;
+  RHS_momentum_equation(o);
+  o.on_going_time_step = saved;
+  return 0;
+}
 int ora_continuity(void* h) { Oracle& o = *static_cast<Oracle*>(h); return check(o, continuity_block(o)); }
 int ora_time_step_duration(void* h) { time_step_duration(*static_cast<Oracle*>(h)); return 0; }
 
@@ -1910,6 +2068,21 @@ int ora_get(void* h, double* x, double* v, double* rho, double* p, double* m, do
     if (p) p[i] = q.pres;
     if (m) m[i] = q.mass;
     if (dden) dden[i] = q.dden;
+  }
+  return o.nag;
+}
+
+// The renormalisation matrices B_ren_gradp and B_ren_divu in pg order, 9
+// doubles per particle, B(i,j) at [9 k + 3 i + j].  Either pointer may be NULL.
+int ora_get_c1(void* h, double* bg, double* bd) {
+  Oracle& o = *static_cast<Oracle*>(h);
+  for (int i = 0; i < o.nag; ++i) {
+    const Particle& q = o.pg[i + 1];
+    for (int a = 0; a < 3; ++a)
+      for (int c = 0; c < 3; ++c) {
+        if (bg) bg[9 * i + 3 * a + c] = q.Bg[a][c];
+        if (bd) bd[9 * i + 3 * a + c] = q.Bd[a][c];
+      }
   }
   return o.nag;
 }

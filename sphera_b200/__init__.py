@@ -71,6 +71,7 @@ def lib():
         "sph_dump_grid": ([vp, ip, ip, ip], C.c_int),
         "sph_dump_neighbours": ([vp, C.c_int32, ip, ip], C.c_int),
         "sph_dump_boundary": ([vp, C.c_int32, ip, ip, dp], C.c_int),
+        "sph_dump_renormalisation": ([vp, dp, dp], C.c_int),
         "sph_profile_phases": ([vp, C.c_int32, dp], C.c_int),
         "sph_get_counters": ([vp, C.POINTER(C.c_uint64), C.c_int32], C.c_int),
         "sph_measure_fp64_peak": ([dp], C.c_int),
@@ -247,6 +248,14 @@ class Simulation:
         _chk(lib().sph_dump_boundary(self._h, max_per, abi.iptr(ncb), abi.iptr(clob), abi.dptr(vals)),
              "sph_dump_boundary")
         return ncb, clob, vals
+
+    def dump_renormalisation(self, divu=True):
+        """B_ren_gradp and (divu) B_ren_divu in caller order, (n, 3, 3)."""
+        bg = np.zeros((self.n, 3, 3))
+        bd = np.zeros((self.n, 3, 3)) if divu else None
+        _chk(lib().sph_dump_renormalisation(self._h, abi.dptr(bg), abi.dptr(bd)),
+             "sph_dump_renormalisation")
+        return bg, bd
 
 
 def memory_required(cases):

@@ -73,6 +73,9 @@ class SphParams(C.Structure):
         ("teta_v", C.c_double),
         ("forcing_amplitude", C.c_double),
         ("forcing_period", C.c_double),
+        ("c1_be", C.c_int32),
+        ("c1_divu", C.c_int32),
+        ("invb_det_thresh", C.c_double),
     ]
 
 

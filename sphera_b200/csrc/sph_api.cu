@@ -175,6 +175,15 @@ int prepare_sim(const SphParams& prm, const SphGeometry& g, int cap, HostSim& hs
   s.forcing_aw2 = prm.forcing_amplitude * s.forcing_w * s.forcing_w;
   s.teta_p = prm.teta_p;
   s.teta_v = prm.teta_v;
+  // 1st-order consistency: 3D, FP64 form; C1_divu acts only with C1_BE
+  // (CalcVarLength.f90:285, Continuity_Equation.f90:201)
+  if (prm.c1_be) {
+    if (s.dim != 3 || prm.precision != SPH_PREC_FP64) return SPH_ERR_UNSUPPORTED;
+    if (!(prm.invb_det_thresh >= 0.0)) return SPH_ERR_INVALID_ARGUMENT;
+  }
+  s.c1_be = prm.c1_be ? 1 : 0;
+  s.c1_divu = (prm.c1_be && prm.c1_divu) ? 1 : 0;
+  s.invb_det_thresh = prm.invb_det_thresh;
   s.dt_alfa_mon = prm.dt_alfa_mon;
   s.density_thresholds = prm.density_thresholds;
   s.zpmin = 0.05 * s.h;
@@ -540,6 +549,8 @@ struct SphHandle {
   std::vector<SimDyn> h_dyn;
   bool any_teta_v = false;          // some simulation smooths velocities / pressures
   bool any_teta_p = false;
+  bool any_c1 = false;              // some simulation renormalises (C1_BE)
+  bool any_c1_divu = false;
   size_t device_bytes = 0;          // bytes of the arrays below `owned`
   bool dry = false;                 // size the arrays only (sph_memory_required)
 };
@@ -596,6 +607,13 @@ void sort_sequence(SphHandle* h, cudaStream_t st) {
   launch_rank_permute(h->db, st);
 }
 
+// CalcVarLength: the neighbour lists and, with C1_BE, the fluid part of
+// the renormalisation matrices summed over them.
+void lists_pass(SphHandle* h, cudaStream_t st) {
+  launch_neighbour_lists(h->db, st);
+  if (h->any_c1) launch_renormalisation(h->db, st);
+}
+
 void momentum_pass(SphHandle* h, bool fused, cudaStream_t st) {
   if (h->precision == SPH_PREC_FP32C) launch_momentum_f32(h->db, fused, st);
   else launch_momentum(h->db, fused, st);
@@ -625,7 +643,7 @@ void step_sequence(SphHandle* h, cudaStream_t st) {
   cudaStreamWaitEvent(h->stream2, h->ev_fork, 0);
   launch_boundary(h->db, h->stream2);
   cudaEventRecord(h->ev_join, h->stream2);
-  launch_neighbour_lists(h->db, st);
+  lists_pass(h, st);
   if (h->precision == SPH_PREC_FP32C) {
     launch_continuity_f32_pairs(h->db, st);
     cudaStreamWaitEvent(st, h->ev_join, 0);
@@ -682,6 +700,8 @@ int create_batch(int nsims, const SphParams* params, const SphGeometry* geoms, c
     if (st != SPH_OK) { delete h; return st; }
     if (params[s].teta_v > 1.0e-9) h->any_teta_v = true;
     if (params[s].teta_p > 0.0) h->any_teta_p = true;
+    if (h->sims[s].dev.c1_be) h->any_c1 = true;
+    if (h->sims[s].dev.c1_divu) h->any_c1_divu = true;
   }
   // layout of the concatenated arrays; simulations start on tile boundaries
   std::vector<Tile> tiles;
@@ -748,6 +768,8 @@ int create_batch(int nsims, const SphParams* params, const SphGeometry* geoms, c
   A(P.ACC, N); A(P.DDEN, N);
   if (h->precision == SPH_PREC_FP32C) A(P.MSUM, 9 * N);
   if (h->precision == SPH_PREC_FP32C && h->any_teta_v) A(P.VF2, N);
+  if (h->any_c1) A(P.BG, 9 * N);
+  if (h->any_c1_divu) A(P.BD, 9 * N);
   A(P.out_flag, N); A(P.id_remap, N); A(P.cur_of, N);
   A(h->d_cx, 3 * N); A(h->d_cv, 3 * N); A(h->d_crho, N); A(h->d_cp, N); A(h->d_cm, N);
   A(h->d_cacc, 3 * N); A(h->d_cdden, N);
@@ -844,6 +866,7 @@ int create_batch(int nsims, const SphParams* params, const SphGeometry* geoms, c
   b.grid_blocks = prop.multiProcessorCount * 8;
   b.sms = prop.multiProcessorCount;
   for (int c = 0; c < kGridClasses; ++c) b.grid[c] = 0;
+  b.c1 = h->any_c1 ? 1 : 0;
   *out = h;
   return SPH_OK;
 }
@@ -877,7 +900,7 @@ int initialise(SphHandle* h) {
   launch_init_from_caller(h->db, h->d_cx, h->d_cv, h->d_crho, h->d_cp, h->d_cm, q);
   sort_sequence(h, q);
   launch_boundary(h->db, q);
-  launch_neighbour_lists(h->db, q);
+  lists_pass(h, q);
   launch_dt_reduce(h->db, q);
   launch_finalize(h->db, 0, q);
   SPH_CUDA(cudaGetLastError());
@@ -1090,7 +1113,7 @@ int sph_ord_grid(SphHandle* h) {
   if (!h || !h->uploaded) return SPH_ERR_INVALID_ARGUMENT;
   launch_stage(h->db, h->stream);
   sort_sequence(h, h->stream);
-  launch_neighbour_lists(h->db, h->stream);
+  lists_pass(h, h->stream);
   SPH_CUDA(cudaGetLastError());
   return sync_dyn(h);
 }
@@ -1196,6 +1219,25 @@ int sph_dump_boundary(SphHandle* h, int32_t max_per, int32_t* ncb, int32_t* clob
   return cuda_status(e);
 }
 
+int sph_dump_renormalisation(SphHandle* h, double* b_gradp, double* b_divu) {
+  if (!h || !h->uploaded || h->nsims != 1 || !h->any_c1) return SPH_ERR_INVALID_ARGUMENT;
+  if (b_divu && !h->any_c1_divu) return SPH_ERR_INVALID_ARGUMENT;
+  SPH_TRY(sync_dyn(h));
+  int n = h->h_dyn[0].nag;
+  double *dg = nullptr, *dd = nullptr;
+  if (b_gradp) SPH_TRY(dalloc(&dg, (size_t)n * 9));
+  if (b_divu && dalloc(&dd, (size_t)n * 9) != SPH_OK) { cudaFree(dg); return SPH_ERR_ALLOC; }
+  cudaStream_t q = h->stream;
+  launch_dump_renormalisation(h->db, dg, dd, q);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess && dg) e = cudaMemcpyAsync(b_gradp, dg, sizeof(double) * 9 * (size_t)n, cudaMemcpyDeviceToHost, q);
+  if (e == cudaSuccess && dd) e = cudaMemcpyAsync(b_divu, dd, sizeof(double) * 9 * (size_t)n, cudaMemcpyDeviceToHost, q);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(q);
+  cudaFree(dg);
+  cudaFree(dd);
+  return cuda_status(e);
+}
+
 // ---------------------------------------------------------------- autotuner
 // Sizes the persistent grid of each kernel class on the live state: every
 // candidate (1 to 32 blocks per SM) is timed over `reps` launches of a
@@ -1213,7 +1255,19 @@ int sph_autotune(SphHandle* h, int32_t reps, int32_t* grid_out) {
   if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) { cudaGetLastError(); return SPH_ERR_CUDA; }
   // the rate-only momentum pass rewrites the laminar flags: keep them
   SPH_CUDA(cudaMemcpyAsync(b.P.L2, b.P.L, (size_t)h->total_slots, cudaMemcpyDeviceToDevice, q));
+  // with C1 the momentum (first step) and continuity passes complete and
+  // invert the renormalisation matrices in place: keep them too
+  const size_t nb_bytes = sizeof(double) * 9 * (size_t)h->total_slots;
+  double *keep_g = nullptr, *keep_d = nullptr;
   cudaError_t e = cudaSuccess;
+  if (h->any_c1) {
+    e = cudaMallocAsync(&keep_g, nb_bytes, q);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(keep_g, b.P.BG, nb_bytes, cudaMemcpyDeviceToDevice, q);
+  }
+  if (e == cudaSuccess && h->any_c1_divu) {
+    e = cudaMallocAsync(&keep_d, nb_bytes, q);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(keep_d, b.P.BD, nb_bytes, cudaMemcpyDeviceToDevice, q);
+  }
   for (int cls = 0; cls < kGridClasses && e == cudaSuccess; ++cls) {
     if (cls == kGridIntegrals && h->dim != 3) continue;
     float best = 1e30f;
@@ -1246,6 +1300,10 @@ int sph_autotune(SphHandle* h, int32_t reps, int32_t* grid_out) {
     if (grid_out) grid_out[cls] = best_g;
   }
   if (e == cudaSuccess) e = cudaMemcpyAsync(b.P.L, b.P.L2, (size_t)h->total_slots, cudaMemcpyDeviceToDevice, q);
+  if (e == cudaSuccess && keep_g) e = cudaMemcpyAsync(b.P.BG, keep_g, nb_bytes, cudaMemcpyDeviceToDevice, q);
+  if (e == cudaSuccess && keep_d) e = cudaMemcpyAsync(b.P.BD, keep_d, nb_bytes, cudaMemcpyDeviceToDevice, q);
+  if (keep_g) cudaFreeAsync(keep_g, q);
+  if (keep_d) cudaFreeAsync(keep_d, q);
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   if (e != cudaSuccess) return cuda_status(e);
@@ -1284,7 +1342,7 @@ int sph_profile_phases(SphHandle* h, int32_t nsteps, double* ms) {
     cudaEventRecord(ev[2], q);
     launch_boundary(h->db, q);
     cudaEventRecord(ev[3], q);
-    launch_neighbour_lists(h->db, q);
+    lists_pass(h, q);
     cudaEventRecord(ev[4], q);
     continuity_pass(h, true, q);
     if (h->any_teta_p) launch_pressure_smoothing(h->db, h->precision == SPH_PREC_FP32C, q);

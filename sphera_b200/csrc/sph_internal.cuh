@@ -54,6 +54,8 @@ struct SimDev {
   double forcing_aw2;     // A (2 pi / T)^2 of the lateral tank forcing (0: none)
   double forcing_w;       // 2 pi / T
   double teta_p, teta_v;  // input_any_t%TetaP, TetaV (partial smoothing)
+  int c1_be, c1_divu;     // input_any_t%C1_BE, %C1_divu (renormalisation, 3D)
+  double invb_det_thresh; // input_any_t%invB_det_thresh
   double zpmin;           // 0.05 h, ComputeBoundaryVolumeIntegrals_P0.f90
   double ktdelta;         // kernel-table step
   float dcdf[3];          // (float)dcd: cell origins differ by multiples of it
@@ -160,6 +162,8 @@ struct Particles {
   double* DDEN;     // drho/dt
   double* MSUM;     // FP32c momentum pair sums of a slot: 9 values (pressure, Monaghan, Morris x 3)
   float4* VF2;      // FP32c with velocity smoothing: the step's leapfrog velocities in FP32
+  double* BG;      // with C1: B_ren_gradp, B(i,j) at [(3 i + j) total_slots + slot]
+  double* BD;      // with C1_divu: B_ren_divu, same layout
   // removal replay
   uint8_t* out_flag;   // by caller index
   int* id_remap;       // by caller index

@@ -880,9 +880,102 @@ __global__ void __launch_bounds__(kBlock) k_boundary2d(DevBatch b) {
 // Leapfrog_trajectories and the CFL part of time_step_duration.
 // ==========================================================================
 
+// ---------------------------------------------------------------------------
+// 1st-order consistency (input_any_t%C1_BE, %C1_divu; 3D).  The matrices are
+// held as 9 doubles B(i,j) at 3 i + j, component-major over the slots.
+// ---------------------------------------------------------------------------
+// grad_W_sub.f90:52-91 (3D): gradient of the beta-spline (kernel_id 1) or of
+// the anti-cluster kernel (kernel_id 2) at r.  PIGRECO is the reference's
+// 14-digit constant.
+__device__ __forceinline__ void grad_w_sub(const SimDev& s, int kernel_id, const double* r, double* g) {
+  const double PIGRECO = 3.14159265358979;
+  g[0] = g[1] = g[2] = 0.0;
+  double abs_r = sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+  if (abs_r < s.h * 1.0e-6) return;
+  double q = abs_r / s.h;
+  double h3 = s.h * s.h * s.h;
+  double dW = 0.0;
+  if (kernel_id == 1) {
+    if (q <= 1.0) dW = 1.0 / (PIGRECO * h3) * (9.0 / 4.0 * (q * q) - 3.0 * q);
+    else if (q >= 2.0) dW = 0.0;
+    else dW = -(3.0 / (4.0 * PIGRECO * h3) * ((2.0 - q) * (2.0 - q)));
+  } else {
+    if (q <= 2.0) dW = -(3.0 * ((2.0 - q) * (2.0 - q)) * (15.0 / (64.0 * PIGRECO * h3)));
+  }
+  for (int k = 0; k < 3; ++k) g[k] = dW / s.h * r[k] / abs_r;
+}
+
+__device__ __forceinline__ void load_b(const double* __restrict__ src, int total, int p, double* B) {
+  for (int k = 0; k < 9; ++k) B[k] = src[(size_t)k * total + p];
+}
+
+__device__ __forceinline__ void store_b(double* dst, int total, int p, const double* B) {
+  for (int k = 0; k < 9; ++k) dst[(size_t)k * total + p] = B[k];
+}
+
+// Matrix_Inversion_3x3.f90:50-74 as B_ren_gradp_inversion.f90:58-74 and
+// B_ren_divu_inversion.f90 use it: the inverse where |det| >= the
+// threshold, else -I.
+__device__ __forceinline__ void b_inversion(double* B, double thresh) {
+  const double det = B[0] * B[4] * B[8] + B[3] * B[7] * B[2] + B[6] * B[1] * B[5] - B[0] * B[7] * B[5] -
+                     B[6] * B[4] * B[2] - B[3] * B[1] * B[8];
+  if (fabs(det) >= thresh) {
+    double inv[9];
+    inv[0] = B[4] * B[8] - B[5] * B[7];
+    inv[1] = B[2] * B[7] - B[1] * B[8];
+    inv[2] = B[1] * B[5] - B[2] * B[4];
+    inv[3] = B[5] * B[6] - B[3] * B[8];
+    inv[4] = B[0] * B[8] - B[2] * B[6];
+    inv[5] = B[2] * B[3] - B[0] * B[5];
+    inv[6] = B[3] * B[7] - B[4] * B[6];
+    inv[7] = B[1] * B[6] - B[0] * B[7];
+    inv[8] = B[0] * B[4] - B[1] * B[3];
+    for (int k = 0; k < 9; ++k) B[k] = inv[k] / det;
+  } else {
+    for (int k = 0; k < 9; ++k) B[k] = 0.0;
+    B[0] = B[4] = B[8] = -1.0;
+  }
+}
+
+// v <- -(B v): MatrixProduct.f90 followed by the sign change of
+// inter_EqMoto.f90:255-260, AddBoundaryContributions_to_ME3D.f90:320-325,
+// SASPH_continuity.f90:126-140 and Continuity_Equation.f90:201-217.
+__device__ __forceinline__ void b_renormalise(const double* B, double* v) {
+  double a[3];
+  for (int i = 0; i < 3; ++i) {
+    double sum = 0.0;
+    for (int k = 0; k < 3; ++k) sum = sum + B[3 * i + k] * v[k];
+    a[i] = sum;
+  }
+  for (int i = 0; i < 3; ++i) v[i] = -a[i];
+}
+
+// The SA-SPH frontier's contribution T (IntGiWrRdV T^T) to the matrices,
+// AddBoundaryContributions_to_ME3D.f90:172-187 and
+// AddBoundaryContribution_to_CE3D.f90:93-112, added into B.
+__device__ __forceinline__ void add_frontier_b(const FaceDev& f, const BdtEntry& e, double* B) {
+  double m2[9];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      double sum = 0.0;
+      for (int k = 0; k < 3; ++k) sum = sum + e.ig[3 * i + k] * f.T[j][k];
+      m2[3 * i + j] = sum;
+    }
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      double sum = 0.0;
+      for (int k = 0; k < 3; ++k) sum = sum + f.T[i][k] * m2[3 * k + j];
+      B[3 * i + j] = B[3 * i + j] + sum;
+    }
+}
+
 // AddBoundaryContributions_to_ME3D.f90:105-336 (fixe/tapi, slip mode 1).
+// C1: B is B_ren_gradp; on the first step (first) the frontiers add to it
+// and it is inverted here, after the face loop; gradpt is renormalised.
+template <bool C1 = false>
 __device__ __forceinline__ void me_boundary3d(const SimDev& s, const DevBatch& b, int nb, int start, const double* vi, double rhoi,
-                              double pres, int lam, const double* grav, double* tpres, double* tdiss, double* tvisc) {
+                              double pres, int lam, const double* grav, double* tpres, double* tdiss, double* tvisc,
+                              double* B = nullptr, bool first = false) {
   double ALEt[3] = {0, 0, 0}, gradpt[3] = {0, 0, 0}, VMon[3] = {0, 0, 0}, VShear[3] = {0, 0, 0};
   for (int u = 0; u < nb; ++u) {
     const BdtEntry& e = b.P.bdt[start + u];
@@ -917,6 +1010,7 @@ __device__ __forceinline__ void me_boundary3d(const SimDev& s, const DevBatch& b
       for (int k = 0; k < 3; ++k) a = a + f.T[i][k] * aloc[k];
       ALEt[i] = ALEt[i] + a;
     }
+    if (C1 && first) add_frontier_b(f, e, B);
     double IntGWZrm1dV = e.bi[6];
     double IntdWrm1dV = e.bi[2];
     if (s.alfa_mon > 0.0) {
@@ -929,6 +1023,10 @@ __device__ __forceinline__ void me_boundary3d(const SimDev& s, const DevBatch& b
       double cinviscmult = cinvisci * IntdWrm1dV * f.slip;
       for (int d = 0; d < 3; ++d) VShear[d] = VShear[d] + cinviscmult * (2.0 * (vi[d] - f.velocity[d]));
     }
+  }
+  if (C1) {
+    if (first) b_inversion(B, s.invb_det_thresh);
+    b_renormalise(B, gradpt);
   }
   for (int d = 0; d < 3; ++d) {
     tpres[d] = tpres[d] + ALEt[d] + gradpt[d];
@@ -1311,7 +1409,67 @@ __global__ void __launch_bounds__(kBlock, 4) k_neighbour_lists(DevBatch b) {
 // velocity_smoothing_2 (TetaV = 0), Leapfrog_trajectories and the CFL part of
 // time_step_duration.  The list is drained in warp lockstep.
 // ==========================================================================
-template <int DIM, bool FUSED>
+// CalcVarLength.f90:285-324 (3D, C1_BE): the fluid part of the
+// renormalisation matrices, summed over the particle's list in its order.
+// A pair adds (x_j - x_i)_c grad_W_k m_j / rho_j to B(k,c), grad_W that of
+// the anti-cluster kernel for B_ren_gradp and of the beta-spline for
+// B_ren_divu; a pair with r >= 2h adds nothing (CalcVarLength.f90:254),
+// nor does the particle itself (r = 0).  The frontier terms are added by
+// the momentum (first step) and continuity passes, which also invert.
+__global__ void __launch_bounds__(kBlock) k_renormalisation(DevBatch b) {
+  __shared__ SimDev s;
+  int cur = -1;
+  const Particles& P = b.P;
+  const int total = P.total_slots;
+  for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
+    Tile tl = b.tiles[t];
+    load_sim(s, b.sims, tl.sim, cur);
+    if (!s.c1_be) continue;
+    const bool divu = s.c1_divu != 0;
+    int p = tl.start + threadIdx.x;
+    bool active = threadIdx.x < tl.count && p < s.p_off + b.dyn[tl.sim].nag;
+    double4 xi = make_double4(0.0, 0.0, 0.0, 0.0);
+    int cnt = 0;
+    if (active) {
+      xi = P.X[p];
+      cnt = b.ncount[p];
+    }
+    double Bg[9], Bd[9];
+    for (int k = 0; k < 9; ++k) Bg[k] = Bd[k] = 0.0;
+    ListPrefetcher lr;
+    lr.init(b.nlist, p, b.list_cap4, cnt);
+    const int nmax = __reduce_max_sync(0xffffffffu, (unsigned)cnt);
+    for (int k = 0; k < nmax; ++k) {
+      int e = lr.get(k);
+      if (k >= cnt) continue;
+      int q = e & kSlotMask;
+      double4 xj = P.X[q];
+      double r[3] = {xj.x - xi.x, xj.y - xi.y, xj.z - xi.z};
+      double rr = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
+      if ((int)(sqrt(rr) / s.h) >= 2) continue;
+      double mj = xj.w, rhoj = P.RP[q].x;
+      double g[3], go[3];
+      grad_w_sub(s, 2, r, g);
+      for (int c = 0; c < 3; ++c) go[c] = g[c] * mj / rhoj;
+      for (int c = 0; c < 3; ++c)
+        for (int kk = 0; kk < 3; ++kk) Bg[3 * kk + c] = Bg[3 * kk + c] + r[c] * go[kk];
+      if (divu) {
+        grad_w_sub(s, 1, r, g);
+        for (int c = 0; c < 3; ++c) go[c] = g[c] * mj / rhoj;
+        for (int c = 0; c < 3; ++c)
+          for (int kk = 0; kk < 3; ++kk) Bd[3 * kk + c] = Bd[3 * kk + c] + r[c] * go[kk];
+      }
+    }
+    if (active) {
+      store_b(P.BG, total, p, Bg);
+      if (divu) store_b(P.BD, total, p, Bd);
+    }
+  }
+}
+
+// C1: with input_any_t%C1_BE the pressure terms are renormalised with
+// B_ren_gradp (3D only).
+template <int DIM, bool FUSED, bool C1 = false>
 __global__ void __launch_bounds__(kBlock, 2) k_momentum(DevBatch b) {
   __shared__ SimDev s;
   __shared__ double stpres[3][kBlock];   // the wall pressure term, kept out of the pair loop's registers
@@ -1353,7 +1511,19 @@ __global__ void __launch_bounds__(kBlock, 2) k_momentum(DevBatch b) {
       cnt = b.ncount[p];
       const int nb = P.bdt_count[p];
       double tpres[3] = {0, 0, 0};
-      if (nb > 0) {
+      // C1: on the first step the frontiers complete B_ren_gradp and it is
+      // inverted, for every particle (RHS_momentum_equation.f90:130-150)
+      const bool c1 = C1 && s.c1_be;
+      const bool first = c1 && dyn->step == 0;
+      if (c1) {
+        double B[9];
+        load_b(P.BG, P.total_slots, p, B);
+        if (nb > 0)
+          me_boundary3d<true>(s, b, nb, P.bdt_start[p], vi, rhoi, pi, P.L[p], geff, tpres, tdiss, tvisc, B, first);
+        else if (first)
+          b_inversion(B, s.invb_det_thresh);
+        if (first) store_b(P.BG, P.total_slots, p, B);
+      } else if (nb > 0) {
         const int lam = P.L[p];
         const int bstart = P.bdt_start[p];
         if (DIM == 3) me_boundary3d(s, b, nb, bstart, vi, rhoi, pi, lam, geff, tpres, tdiss, tvisc);
@@ -1420,6 +1590,15 @@ __global__ void __launch_bounds__(kBlock, 2) k_momentum(DevBatch b) {
     }
     double dtc = 1.0e300;
     if (active) {
+      if (C1 && s.c1_be) {
+        // inter_EqMoto.f90:255-260
+        double B[9], tp[3] = {tp0, tp1, tp2};
+        load_b(P.BG, P.total_slots, p, B);
+        b_renormalise(B, tp);
+        tp0 = tp[0];
+        tp1 = tp[1];
+        tp2 = tp[2];
+      }
       double tpres[3];
       tpres[0] = stpres[0][threadIdx.x] + tp0 + al0;
       tpres[1] = stpres[1][threadIdx.x] + tp1 + al1;
@@ -1530,9 +1709,61 @@ __device__ __forceinline__ double continuity_boundary(const SimDev& s, const Dev
   return 0.0 - rhoi * (gu0 + gv1 + gw2);
 }
 
+// SASPH_continuity.f90:89-169 with C1_BE (3D): the frontiers complete the
+// renormalisation matrices (AddBoundaryContribution_to_CE3D.f90:93-112),
+// both are inverted for every particle, and with C1_divu the wall velocity
+// gradients are renormalised before they enter drho/dt.
+__device__ __forceinline__ double continuity_boundary_c1(const SimDev& s, const DevBatch& b, SimDyn* dyn, int nb,
+                                                         int bstart, const double4& vi, double rhoi, int p) {
+  const Particles& P = b.P;
+  const int total = P.total_slots;
+  const bool divu = s.c1_divu != 0;
+  double Bg[9], Bd[9];
+  load_b(P.BG, total, p, Bg);
+  if (divu) load_b(P.BD, total, p, Bd);
+  double gu[3] = {0, 0, 0}, gv[3] = {0, 0, 0}, gw[3] = {0, 0, 0};
+  const double var[3] = {vi.x, vi.y, vi.z};
+  for (int u = 0; u < nb; ++u) {
+    const BdtEntry& e = P.bdt[bstart + u];
+    const FaceDev& f = b.faces[s.face_off + e.clobonum - 1];
+    if (!(e.loc[2] > 0.0)) continue;
+    if (divu) add_frontier_b(f, e, Bd);
+    add_frontier_b(f, e, Bg);
+    double dp = 0.0;
+    for (int d = 0; d < 3; ++d) dp = dp + (2.0 * (f.velocity[d] - var[d])) * f.T[d][2];
+    double dvel[3] = {dp * f.T[0][2], dp * f.T[1][2], dp * f.T[2][2]};
+    double av[3];
+    for (int i = 0; i < 3; ++i) {
+      double a = 0.0;
+      for (int k = 0; k < 3; ++k) a = a + f.T[i][k] * e.bi[3 + k];
+      av[i] = a;
+    }
+    for (int d = 0; d < 3; ++d) {
+      gu[d] = gu[d] - dvel[0] * av[d];
+      gv[d] = gv[d] - dvel[1] * av[d];
+      gw[d] = gw[d] - dvel[2] * av[d];
+    }
+  }
+  if (divu) b_inversion(Bd, s.invb_det_thresh);
+  b_inversion(Bg, s.invb_det_thresh);
+  store_b(P.BG, total, p, Bg);
+  if (divu) store_b(P.BD, total, p, Bd);
+  if (nb == 0) return 0.0;
+  atomicMax(&dyn->ncbf_max, nb);
+  if (divu) {
+    b_renormalise(Bd, gu);
+    b_renormalise(Bd, gv);
+    b_renormalise(Bd, gw);
+  }
+  return 0.0 - rhoi * (gu[0] + gv[1] + gw[2]);
+}
+
 // Continuity, FP64 form: SASPH_continuity + Continuity_Equation, optionally
-// fused with Leapfrog_continuity and the EoS.
-template <int DIM, bool FUSED>
+// fused with Leapfrog_continuity and the EoS.  C1 (3D): the renormalised
+// form, Continuity_Equation.f90:119-126,201-217 -- the whole velocity
+// gradient vectors are summed, and renormalised with B_ren_divu when
+// C1_divu is set; their trace equals the plain form's sum bit for bit.
+template <int DIM, bool FUSED, bool C1 = false>
 __global__ void __launch_bounds__(kBlock, 2) k_continuity(DevBatch b) {
   __shared__ SimDev s;
   int cur = -1;
@@ -1553,9 +1784,11 @@ __global__ void __launch_bounds__(kBlock, 2) k_continuity(DevBatch b) {
       rhoi = P.RP[p].x;
       cnt = b.ncount[p];
       int nb = P.bdt_count[p];
-      if (nb > 0) dden = continuity_boundary<DIM>(s, b, dyn, nb, P.bdt_start[p], vi, rhoi);
+      if (C1 && s.c1_be) dden = continuity_boundary_c1(s, b, dyn, nb, nb > 0 ? P.bdt_start[p] : 0, vi, rhoi, p);
+      else if (nb > 0) dden = continuity_boundary<DIM>(s, b, dyn, nb, P.bdt_start[p], vi, rhoi);
     }
     double a1 = 0.0, a2 = 0.0, a3 = 0.0;
+    double g1[3] = {0, 0, 0}, g2[3] = {0, 0, 0}, g3[3] = {0, 0, 0};
     ListPrefetcher lr;
     lr.init(b.nlist, p, b.list_cap4, cnt);
     const int nmax = __reduce_max_sync(0xffffffffu, (unsigned)cnt);
@@ -1570,13 +1803,38 @@ __global__ void __launch_bounds__(kBlock, 2) k_continuity(DevBatch b) {
       kernel_values(s, rr, PK1, PK2, PK3);
       double4 vj = P.V[q];
       double c = rhoi * vj.w * PK1;     // rhoi * (amassj / rhoj) * PK1
-      a1 = a1 + c * (vj.x - vi.x) * r0;
-      if (DIM == 3) a2 = a2 + c * (vj.y - vi.y) * r1;
-      a3 = a3 + c * (vj.z - vi.z) * r2;
+      if (C1) {
+        const double c0 = c * (vj.x - vi.x), c1 = c * (vj.y - vi.y), c2 = c * (vj.z - vi.z);
+        g1[0] = g1[0] + c0 * r0;
+        g1[1] = g1[1] + c0 * r1;
+        g1[2] = g1[2] + c0 * r2;
+        g2[0] = g2[0] + c1 * r0;
+        g2[1] = g2[1] + c1 * r1;
+        g2[2] = g2[2] + c1 * r2;
+        g3[0] = g3[0] + c2 * r0;
+        g3[1] = g3[1] + c2 * r1;
+        g3[2] = g3[2] + c2 * r2;
+      } else {
+        a1 = a1 + c * (vj.x - vi.x) * r0;
+        if (DIM == 3) a2 = a2 + c * (vj.y - vi.y) * r1;
+        a3 = a3 + c * (vj.z - vi.z) * r2;
+      }
     }
     if (active) {
-      if (DIM == 3) dden = dden - (a1 + a2 + a3);
-      else dden = dden - (a1 + a3);
+      if (C1) {
+        if (s.c1_be && s.c1_divu) {
+          double B[9];
+          load_b(P.BD, P.total_slots, p, B);
+          b_renormalise(B, g1);
+          b_renormalise(B, g2);
+          b_renormalise(B, g3);
+        }
+        dden = dden - (g1[0] + g2[1] + g3[2]);
+      } else if (DIM == 3) {
+        dden = dden - (a1 + a2 + a3);
+      } else {
+        dden = dden - (a1 + a3);
+      }
       if (FUSED) {
         // Leapfrog_continuity.f90:54-68, EoS_barotropic_linear.f90:49-55
         double rho = rhoi + dyn->dt * dden;
@@ -2685,6 +2943,24 @@ __global__ void k_dump_boundary(DevBatch b, int max_per, int* ncb, int* clob, do
   }
 }
 
+// B_ren_gradp / B_ren_divu by caller index, B(i,j) at [9 row + 3 i + j].
+__global__ void k_dump_renormalisation(DevBatch b, double* bg, double* bd) {
+  __shared__ SimDev s;
+  int cur = -1;
+  const Particles& P = b.P;
+  for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
+    Tile tl = b.tiles[t];
+    load_sim(s, b.sims, tl.sim, cur);
+    int p = tl.start + threadIdx.x;
+    if (threadIdx.x >= tl.count || p >= s.p_off + b.dyn[tl.sim].nag) continue;
+    size_t row = (size_t)s.p_off + P.I[p] - 1;
+    for (int k = 0; k < 9; ++k) {
+      if (bg && P.BG) bg[9 * row + k] = P.BG[(size_t)k * P.total_slots + p];
+      if (bd && P.BD) bd[9 * row + k] = P.BD[(size_t)k * P.total_slots + p];
+    }
+  }
+}
+
 __global__ void k_dump_cella(DevBatch b, int* cella) {
   __shared__ SimDev s;
   int cur = -1;
@@ -2799,7 +3075,10 @@ void launch_boundary(const DevBatch& b, cudaStream_t st) {
 
 void launch_momentum(const DevBatch& b, bool fused, cudaStream_t st) {
   int g = blocks_for(b, kGridMomentum);
-  if (b.dim == 3) {
+  if (b.dim == 3 && b.c1) {
+    if (fused) k_momentum<3, true, true><<<g, kBlock, 0, st>>>(b);
+    else k_momentum<3, false, true><<<g, kBlock, 0, st>>>(b);
+  } else if (b.dim == 3) {
     if (fused) k_momentum<3, true><<<g, kBlock, 0, st>>>(b);
     else k_momentum<3, false><<<g, kBlock, 0, st>>>(b);
   } else {
@@ -2812,6 +3091,10 @@ void launch_neighbour_lists(const DevBatch& b, cudaStream_t st) {
   int g = blocks_for(b, kGridLists);
   if (b.dim == 3) k_neighbour_lists<3><<<g, kBlock, 0, st>>>(b);
   else k_neighbour_lists<2><<<g, kBlock, 0, st>>>(b);
+}
+
+void launch_renormalisation(const DevBatch& b, cudaStream_t st) {
+  if (b.dim == 3 && b.c1) k_renormalisation<<<blocks_for(b, kGridLists), kBlock, 0, st>>>(b);
 }
 
 void launch_momentum_f32(const DevBatch& b, bool fused, cudaStream_t st) {
@@ -2854,7 +3137,10 @@ void launch_refresh_f32(const DevBatch& b, cudaStream_t st) { k_refresh_f32<<<bl
 
 void launch_continuity(const DevBatch& b, bool fused, cudaStream_t st) {
   int g = blocks_for(b, kGridContinuity);
-  if (b.dim == 3) {
+  if (b.dim == 3 && b.c1) {
+    if (fused) k_continuity<3, true, true><<<g, kBlock, 0, st>>>(b);
+    else k_continuity<3, false, true><<<g, kBlock, 0, st>>>(b);
+  } else if (b.dim == 3) {
     if (fused) k_continuity<3, true><<<g, kBlock, 0, st>>>(b);
     else k_continuity<3, false><<<g, kBlock, 0, st>>>(b);
   } else {
@@ -2917,6 +3203,9 @@ void launch_dump_neighbours(const DevBatch& b, int nmaxj, int* counts, int* list
 }
 void launch_dump_boundary(const DevBatch& b, int max_per, int* ncb, int* clob, double* vals, cudaStream_t st) {
   k_dump_boundary<<<blocks_for(b), kBlock, 0, st>>>(b, max_per, ncb, clob, vals);
+}
+void launch_dump_renormalisation(const DevBatch& b, double* bg, double* bd, cudaStream_t st) {
+  k_dump_renormalisation<<<blocks_for(b), kBlock, 0, st>>>(b, bg, bd);
 }
 void launch_dump_cella(const DevBatch& b, int* cella, cudaStream_t st) {
   k_dump_cella<<<blocks_for(b), kBlock, 0, st>>>(b, cella);

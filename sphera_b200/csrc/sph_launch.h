@@ -34,6 +34,7 @@ struct DevBatch {
   int grid_blocks;         // blocks of the persistent particle kernels (default)
   int sms;                 // streaming multiprocessors of the device
   int grid[kGridClasses];  // autotuned blocks per kernel class (0 = grid_blocks)
+  int c1;                  // some simulation renormalises (C1_BE, 3D FP64): P.BG (and P.BD) allocated
 };
 
 enum class KeyKind { Sort = 0, Reference = 1 };
@@ -50,6 +51,7 @@ void launch_rank_permute(const DevBatch& b, cudaStream_t st);
 void launch_rank_reference(const DevBatch& b, const int* cell_start_ref, int* npartord, cudaStream_t st);
 // neighbour lists (CalcVarLength replacement)
 void launch_neighbour_lists(const DevBatch& b, cudaStream_t st);
+void launch_renormalisation(const DevBatch& b, cudaStream_t st);   // C1: fluid part of the matrices
 // physics (FP64)
 void launch_boundary(const DevBatch& b, cudaStream_t st);
 void launch_momentum(const DevBatch& b, bool fused, cudaStream_t st);
@@ -78,6 +80,7 @@ void launch_to_caller(const DevBatch& b, double* x, double* v, double* rho, doub
 // verification
 void launch_dump_neighbours(const DevBatch& b, int nmaxj, int* counts, int* lists, cudaStream_t st);
 void launch_dump_boundary(const DevBatch& b, int max_per, int* ncb, int* clob, double* vals, cudaStream_t st);
+void launch_dump_renormalisation(const DevBatch& b, double* bg, double* bd, cudaStream_t st);
 void launch_dump_cella(const DevBatch& b, int* cella, cudaStream_t st);
 // FP64 FMA throughput probe: returns flops per launch
 double launch_fp64_probe(double* sink, int blocks, cudaStream_t st);
