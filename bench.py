@@ -38,8 +38,9 @@ METRIC = "particle-steps/s FP32c vs FP64 at ≤1e-3 rel L2; ensemble p50/p99 tim
 UNIT = "particle-steps/s"
 # launches of one FP32c step graph (3D, sph_api.cu step_sequence): momentum
 # pair sums and finish, 8 sort, 3 boundary, lists, continuity pair sums and
-# finish, finalize
+# finish, finalize; the FP64 graph has one momentum and one continuity kernel
 KERNELS_PER_STEP = 17
+KERNELS_PER_STEP_FP64 = 15
 # algorithmic bytes of the fused FP32c momentum pass (k_momentum_f32 pair
 # sums + k_momentum_f32_finish): per particle, each record read once -- X 32,
 # V 32, RP 16, XF 16, VF 16, RF 16 (the neighbours' XF/VF/RF are these same
@@ -336,7 +337,12 @@ def main():
     ap.add_argument("--autotune", type=int, default=1, help="size the persistent grids on the live state first")
     ap.add_argument("--teta", type=float, default=0.0,
                     help="partial smoothing coefficient TetaP = TetaV of the dam-break workload (0: off)")
+    ap.add_argument("--c1", action="store_true",
+                    help="dam break with the 1st-order consistency renormalisation (C1_BE and C1_divu, "
+                         "invB_det_thresh 1e-3); FP64 form only")
     args = ap.parse_args()
+    if args.c1 and args.forms != "fp64":
+        ap.error("--c1 runs in the FP64 form only: add --forms fp64")
     args.warmup = max(3, args.warmup)
     if args.t_end is None:
         args.t_end = 0.3 if args.workload == "serving" else 0.5
@@ -371,6 +377,10 @@ def main():
         c = cases.dam_break_3d(dx=args.dx, precision=precision)
         c.params.teta_p = args.teta
         c.params.teta_v = args.teta
+        if args.c1:
+            c.params.c1_be = 1
+            c.params.c1_divu = 1
+            c.params.invb_det_thresh = 1.0e-3
         return c
 
     def run_form(precision):
@@ -438,7 +448,8 @@ def main():
         workload = "dam_break_3d" if args.dx == 0.005 else f"dam_break_3d_dx{args.dx:g}"
         desc = (f"dam_break_3d: tank 1.6x0.6x0.6 m, block 0.6x0.3x0.6 m, dx {args.dx:g} m, "
                 f"{n} particles per GPU, SA-SPH walls"
-                + (f", partial smoothing TetaP = TetaV = {args.teta:g}" if args.teta > 0 else ""))
+                + (f", partial smoothing TetaP = TetaV = {args.teta:g}" if args.teta > 0 else "")
+                + (", C1 renormalisation (C1_BE, C1_divu)" if args.c1 else ""))
     traffic = _traffic(workload)
 
     # end to end through the C ABI with pinned host buffers
@@ -494,7 +505,8 @@ def main():
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None,
-        "dtype": "fp32c (f32 pair sums, compensated; f64 positions/integration/boundary terms)",
+        "dtype": ("fp32c (f32 pair sums, compensated; f64 positions/integration/boundary terms)"
+                  if args.forms != "fp64" else "f64"),
         "data": f"synthetic (seeded {args.workload} generated in-repo)",
         "config": {"workload": desc,
                    "particles_per_gpu": n, "form": "fp32c" if args.forms != "fp64" else "fp64",
@@ -505,18 +517,22 @@ def main():
         "speedup_fp32c_vs_fp64": value / r64["value"] if r64 else None,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": state_bytes,
                 "d2h_bytes_per_step": state_bytes, "steps": args.e2e_steps,
-                "path": "sph_upload + sph_step_async(1) + sph_download per step, pinned host buffers, fp32c form"},
+                "path": "sph_upload + sph_step_async(1) + sph_download per step, pinned host buffers, "
+                        + ("fp32c" if args.forms != "fp64" else "fp64") + " form"},
         "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": hbm_peak, "unit": "GB/s",
                      "frac": achieved_gbs / hbm_peak, "traffic": traffic,
-                     "kernel": "k_momentum_f32<3> + k_momentum_f32_finish<3,true> (momentum pair sums; wall terms, leapfrog)",
+                     "kernel": ("k_momentum_f32<3> + k_momentum_f32_finish<3,true> (momentum pair sums; wall terms, leapfrog)"
+                                if args.forms != "fp64" else "k_momentum<3,true> (FP64 momentum, wall terms, leapfrog)"),
                      "peak_kind": f"{peak_kind} HBM copy bandwidth",
                      "fp": {"achieved_tflops": mom_tflops, "peak_tflops": fp32_peak,
                             "frac": mom_tflops / fp32_peak, "peak_kind": "measured FP32 FMA rate (in-run)"}},
         "phases_ms_per_step": r32["phases"],
         "pairs_per_particle": cnt["pairs"] / nprof / n,
         "candidates_per_particle": cnt["candidates"] / nprof / n,
-        # + 2 launches each for the velocity and the pressure smoothing passes
-        "gpu_launches": (KERNELS_PER_STEP + (4 if args.teta > 0 else 0)) * args.steps,
+        # + 2 launches each for the velocity and the pressure smoothing
+        # passes, + 1 for the renormalisation matrices
+        "gpu_launches": ((KERNELS_PER_STEP if args.forms != "fp64" else KERNELS_PER_STEP_FP64)
+                         + (4 if args.teta > 0 else 0) + (1 if args.c1 else 0)) * args.steps,
         "clocks": clocks,
         "cpu_baseline": cpu,
     }
