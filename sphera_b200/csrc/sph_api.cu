@@ -184,6 +184,15 @@ int prepare_sim(const SphParams& prm, const SphGeometry& g, int cap, HostSim& hs
   s.c1_be = prm.c1_be ? 1 : 0;
   s.c1_divu = (prm.c1_be && prm.c1_divu) ? 1 : 0;
   s.invb_det_thresh = prm.invb_det_thresh;
+  {
+    // grad_W_sub.f90:75-88 (3D) with the reference's 14-digit PIGRECO: the
+    // per-pair expressions' constant factors, formed as they are there
+    const double PIGRECO = 3.14159265358979;
+    const double h3 = s.h * s.h * s.h;
+    s.c1_w1a = 1.0 / (PIGRECO * h3);
+    s.c1_w1b = 3.0 / (4.0 * PIGRECO * h3);
+    s.c1_w2 = 15.0 / (64.0 * PIGRECO * h3);
+  }
   s.dt_alfa_mon = prm.dt_alfa_mon;
   s.density_thresholds = prm.density_thresholds;
   s.zpmin = 0.05 * s.h;

@@ -56,6 +56,7 @@ struct SimDev {
   double teta_p, teta_v;  // input_any_t%TetaP, TetaV (partial smoothing)
   int c1_be, c1_divu;     // input_any_t%C1_BE, %C1_divu (renormalisation, 3D)
   double invb_det_thresh; // input_any_t%invB_det_thresh
+  double c1_w1a, c1_w1b, c1_w2;  // grad_W_sub.f90 factors 1/(pi h^3), 3/(4 pi h^3), 15/(64 pi h^3)
   double zpmin;           // 0.05 h, ComputeBoundaryVolumeIntegrals_P0.f90
   double ktdelta;         // kernel-table step
   float dcdf[3];          // (float)dcd: cell origins differ by multiples of it

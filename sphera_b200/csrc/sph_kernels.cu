@@ -884,27 +884,6 @@ __global__ void __launch_bounds__(kBlock) k_boundary2d(DevBatch b) {
 // 1st-order consistency (input_any_t%C1_BE, %C1_divu; 3D).  The matrices are
 // held as 9 doubles B(i,j) at 3 i + j, component-major over the slots.
 // ---------------------------------------------------------------------------
-// grad_W_sub.f90:52-91 (3D): gradient of the beta-spline (kernel_id 1) or of
-// the anti-cluster kernel (kernel_id 2) at r.  PIGRECO is the reference's
-// 14-digit constant.
-__device__ __forceinline__ void grad_w_sub(const SimDev& s, int kernel_id, const double* r, double* g) {
-  const double PIGRECO = 3.14159265358979;
-  g[0] = g[1] = g[2] = 0.0;
-  double abs_r = sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
-  if (abs_r < s.h * 1.0e-6) return;
-  double q = abs_r / s.h;
-  double h3 = s.h * s.h * s.h;
-  double dW = 0.0;
-  if (kernel_id == 1) {
-    if (q <= 1.0) dW = 1.0 / (PIGRECO * h3) * (9.0 / 4.0 * (q * q) - 3.0 * q);
-    else if (q >= 2.0) dW = 0.0;
-    else dW = -(3.0 / (4.0 * PIGRECO * h3) * ((2.0 - q) * (2.0 - q)));
-  } else {
-    if (q <= 2.0) dW = -(3.0 * ((2.0 - q) * (2.0 - q)) * (15.0 / (64.0 * PIGRECO * h3)));
-  }
-  for (int k = 0; k < 3; ++k) g[k] = dW / s.h * r[k] / abs_r;
-}
-
 __device__ __forceinline__ void load_b(const double* __restrict__ src, int total, int p, double* B) {
   for (int k = 0; k < 9; ++k) B[k] = src[(size_t)k * total + p];
 }
@@ -1413,10 +1392,14 @@ __global__ void __launch_bounds__(kBlock, 4) k_neighbour_lists(DevBatch b) {
 // renormalisation matrices, summed over the particle's list in its order.
 // A pair adds (x_j - x_i)_c grad_W_k m_j / rho_j to B(k,c), grad_W that of
 // the anti-cluster kernel for B_ren_gradp and of the beta-spline for
-// B_ren_divu; a pair with r >= 2h adds nothing (CalcVarLength.f90:254),
-// nor does the particle itself (r = 0).  The frontier terms are added by
-// the momentum (first step) and continuity passes, which also invert.
-__global__ void __launch_bounds__(kBlock) k_renormalisation(DevBatch b) {
+// B_ren_divu (grad_W_sub.f90:52-91, 3D); a pair with r >= 2h adds nothing
+// (CalcVarLength.f90:254), nor does a zero gradient (r < 1e-6 h, the
+// particle itself): the sums start at +0, so skipping a +-0 addend leaves
+// them as they are.  The frontier terms are added by the momentum (first
+// step) and continuity passes, which also invert.  One sqrt and the
+// division r / h are shared by the range test and both gradients; the
+// constant factors come from the host (SimDev::c1_w*).
+__global__ void __launch_bounds__(kBlock, 2) k_renormalisation(DevBatch b) {
   __shared__ SimDev s;
   int cur = -1;
   const Particles& P = b.P;
@@ -1445,17 +1428,21 @@ __global__ void __launch_bounds__(kBlock) k_renormalisation(DevBatch b) {
       int q = e & kSlotMask;
       double4 xj = P.X[q];
       double r[3] = {xj.x - xi.x, xj.y - xi.y, xj.z - xi.z};
-      double rr = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
-      if ((int)(sqrt(rr) / s.h) >= 2) continue;
-      double mj = xj.w, rhoj = P.RP[q].x;
-      double g[3], go[3];
-      grad_w_sub(s, 2, r, g);
-      for (int c = 0; c < 3; ++c) go[c] = g[c] * mj / rhoj;
+      double abs_r = sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+      double qh = abs_r / s.h;
+      if ((int)qh >= 2 || abs_r < s.h * 1.0e-6) continue;
+      const double mj = xj.w, rhoj = P.RP[q].x;
+      const double w = 2.0 - qh;
+      double go[3];
+      // anti-cluster kernel (q <= 2 here)
+      double t = -(3.0 * (w * w) * s.c1_w2) / s.h;
+      for (int c = 0; c < 3; ++c) go[c] = t * r[c] / abs_r * mj / rhoj;
       for (int c = 0; c < 3; ++c)
         for (int kk = 0; kk < 3; ++kk) Bg[3 * kk + c] = Bg[3 * kk + c] + r[c] * go[kk];
       if (divu) {
-        grad_w_sub(s, 1, r, g);
-        for (int c = 0; c < 3; ++c) go[c] = g[c] * mj / rhoj;
+        // beta-spline (q < 2 here)
+        t = (qh <= 1.0 ? s.c1_w1a * (9.0 / 4.0 * (qh * qh) - 3.0 * qh) : -(s.c1_w1b * (w * w))) / s.h;
+        for (int c = 0; c < 3; ++c) go[c] = t * r[c] / abs_r * mj / rhoj;
         for (int c = 0; c < 3; ++c)
           for (int kk = 0; kk < 3; ++kk) Bd[3 * kk + c] = Bd[3 * kk + c] + r[c] * go[kk];
       }
