@@ -1212,6 +1212,53 @@ __device__ __forceinline__ void screen_tile(const float4* wbuf, int nt, float ax
   lom = lm;
 }
 
+// screen_tile<DIM, true> on Blackwell's paired FP32 instructions: the tile
+// is staged a second time as negated x, y, z arrays, and candidates u, u+1
+// share each add, multiply and fused multiply-add (__fadd2_rn, __fmul2_rn,
+// __ffma2_rn round each half as the scalar instruction does, and x + (-y)
+// rounds as x - y, so every r^2 and both masks are bit-identical to
+// screen_tile's).
+template <int DIM>
+__device__ __forceinline__ void screen_tile_x2(const float* nx, const float* ny, const float* nz, int nt, float ax,
+                                               float ay, float zi, float rr_lo, float rr_hi, unsigned& hitm,
+                                               unsigned& lom) {
+  const float2 ax2 = make_float2(ax, ax), ay2 = make_float2(ay, ay), zi2 = make_float2(zi, zi);
+  unsigned hm = 0u, lm = 0u;
+  for (int u0 = 0; u0 < nt; u0 += 8) {
+    unsigned h8 = 0u, l8 = 0u;
+#pragma unroll
+    for (int c = 0; c < 8; c += 4) {
+      const float4 X = *reinterpret_cast<const float4*>(nx + u0 + c);
+      const float4 Z = *reinterpret_cast<const float4*>(nz + u0 + c);
+      float2 ra = __fadd2_rn(ax2, make_float2(X.x, X.y));
+      float2 rb = __fadd2_rn(ax2, make_float2(X.z, X.w));
+      const float2 za = __fadd2_rn(zi2, make_float2(Z.x, Z.y));
+      const float2 zb = __fadd2_rn(zi2, make_float2(Z.z, Z.w));
+      ra = __fmul2_rn(ra, ra);
+      rb = __fmul2_rn(rb, rb);
+      if (DIM == 3) {
+        const float4 Y = *reinterpret_cast<const float4*>(ny + u0 + c);
+        const float2 ya = __fadd2_rn(ay2, make_float2(Y.x, Y.y));
+        const float2 yb = __fadd2_rn(ay2, make_float2(Y.z, Y.w));
+        ra = __ffma2_rn(ya, ya, ra);
+        rb = __ffma2_rn(yb, yb, rb);
+      }
+      ra = __ffma2_rn(za, za, ra);
+      rb = __ffma2_rn(zb, zb, rb);
+      const float rf[4] = {ra.x, ra.y, rb.x, rb.y};
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        if (!(rf[j] > rr_hi)) h8 |= 1u << (c + j);
+        if (rf[j] < rr_lo) l8 |= 1u << (c + j);
+      }
+    }
+    hm |= h8 << u0;
+    lm |= l8 << u0;
+  }
+  hitm = hm;
+  lom = lm;
+}
+
 // Whether any staged candidate u0 <= u < nt lies in the lane's 3-cell z
 // window (the truncation test once NMAXPARTJ is reached; rare).
 __device__ __forceinline__ bool window_candidate(const float4* wbuf, int u0, int nt, int ck) {
@@ -1224,10 +1271,14 @@ template <int DIM>
 __global__ void __launch_bounds__(kBlock, 4) k_neighbour_lists(DevBatch b) {
   __shared__ SimDev s;
   __shared__ float4 cbuf[kBlock];
+  __shared__ __align__(16) float cneg[3][kBlock];   // the tile again: -x, -y, -z (paired screening)
   int cur = -1;
   const Particles& P = b.P;
   const int lane = threadIdx.x & 31;
   float4* wbuf = cbuf + (threadIdx.x & ~31);
+  float* wnx = &cneg[0][threadIdx.x & ~31];
+  float* wny = &cneg[1][threadIdx.x & ~31];
+  float* wnz = &cneg[2][threadIdx.x & ~31];
   constexpr int NR = (DIM == 3) ? 9 : 3;
   const unsigned FULL = 0xffffffffu;
   for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
@@ -1291,12 +1342,17 @@ __global__ void __launch_bounds__(kBlock, 4) k_neighbour_lists(DevBatch b) {
           if (rebase && cidx < ue) st.z = (float)(__float_as_int(st.w) - kmin) * dz + st.z;
           __syncwarp();
           wbuf[lane] = st;
+          if (rebase) {
+            wnx[lane] = -st.x;
+            wny[lane] = -st.y;
+            wnz[lane] = -st.z;
+          }
           __syncwarp();
           if (!mine) continue;
           int nt = ue - c0 < 32 ? ue - c0 : 32;
           // phase 1: screening masks of the tile
           unsigned hitm, lom;
-          if (rebase) screen_tile<DIM, true>(wbuf, nt, ax, ay, zi, xf.z, ck, dz, rr_lo, rr_hi, hitm, lom);
+          if (rebase) screen_tile_x2<DIM>(wnx, wny, wnz, nt, ax, ay, zi, rr_lo, rr_hi, hitm, lom);
           else screen_tile<DIM, false>(wbuf, nt, ax, ay, zi, xf.z, ck, dz, rr_lo, rr_hi, hitm, lom);
           if (full) {
             // NMAXPARTJ reached: every later candidate of the window is refused
