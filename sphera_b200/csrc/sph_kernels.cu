@@ -1215,19 +1215,20 @@ __device__ __forceinline__ void screen_tile(const float4* wbuf, int nt, float ax
 // screen_tile<DIM, true> on Blackwell's paired FP32 instructions: the tile
 // is staged a second time as negated x, y, z arrays, and candidates u, u+1
 // share each add, multiply and fused multiply-add (__fadd2_rn, __fmul2_rn,
-// __ffma2_rn round each half as the scalar instruction does, and x + (-y)
-// rounds as x - y, so every r^2 and both masks are bit-identical to
-// screen_tile's).
+// __ffma2_rn round each half as the scalar instruction does, x + (-y)
+// rounds as x - y and fma(r, -1, y) as y - r, so every r^2 and both masks
+// are bit-identical to screen_tile's).
 template <int DIM>
 __device__ __forceinline__ void screen_tile_x2(const float* nx, const float* ny, const float* nz, int nt, float ax,
                                                float ay, float zi, float rr_lo, float rr_hi, unsigned& hitm,
                                                unsigned& lom) {
   const float2 ax2 = make_float2(ax, ax), ay2 = make_float2(ay, ay), zi2 = make_float2(zi, zi);
+  const float2 hi2 = make_float2(rr_hi, rr_hi), nlo2 = make_float2(-rr_lo, -rr_lo), m1 = make_float2(-1.f, -1.f);
   unsigned hm = 0u, lm = 0u;
   for (int u0 = 0; u0 < nt; u0 += 8) {
     unsigned h8 = 0u, l8 = 0u;
 #pragma unroll
-    for (int c = 0; c < 8; c += 4) {
+    for (int c = 4; c >= 0; c -= 4) {
       const float4 X = *reinterpret_cast<const float4*>(nx + u0 + c);
       const float4 Z = *reinterpret_cast<const float4*>(nz + u0 + c);
       float2 ra = __fadd2_rn(ax2, make_float2(X.x, X.y));
@@ -1245,15 +1246,23 @@ __device__ __forceinline__ void screen_tile_x2(const float* nx, const float* ny,
       }
       ra = __ffma2_rn(za, za, ra);
       rb = __ffma2_rn(zb, zb, rb);
-      const float rf[4] = {ra.x, ra.y, rb.x, rb.y};
-#pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        if (!(rf[j] > rr_hi)) h8 |= 1u << (c + j);
-        if (rf[j] < rr_lo) l8 |= 1u << (c + j);
-      }
+      // sign bits: rr_hi - r^2 < 0 exactly when r^2 > rr_hi, r^2 - rr_lo < 0
+      // exactly when r^2 < rr_lo (finite inputs; a difference of two floats
+      // is zero only when they are equal); one funnel shift per candidate
+      // and mask moves the sign in, candidate u ending in bit u
+      const float2 ha = __ffma2_rn(ra, m1, hi2), hb = __ffma2_rn(rb, m1, hi2);
+      const float2 la = __fadd2_rn(ra, nlo2), lb = __fadd2_rn(rb, nlo2);
+      h8 = __funnelshift_l(__float_as_uint(hb.y), h8, 1);
+      h8 = __funnelshift_l(__float_as_uint(hb.x), h8, 1);
+      h8 = __funnelshift_l(__float_as_uint(ha.y), h8, 1);
+      h8 = __funnelshift_l(__float_as_uint(ha.x), h8, 1);
+      l8 = __funnelshift_l(__float_as_uint(lb.y), l8, 1);
+      l8 = __funnelshift_l(__float_as_uint(lb.x), l8, 1);
+      l8 = __funnelshift_l(__float_as_uint(la.y), l8, 1);
+      l8 = __funnelshift_l(__float_as_uint(la.x), l8, 1);
     }
-    hm |= h8 << u0;
-    lm |= l8 << u0;
+    hm |= (~h8 & 0xffu) << u0;   // h8: rejected; l8: below rr_lo
+    lm |= (l8 & 0xffu) << u0;
   }
   hitm = hm;
   lom = lm;
