@@ -1225,7 +1225,9 @@ __device__ __forceinline__ void screen_tile_x2(const float* nx, const float* ny,
   const float2 ax2 = make_float2(ax, ax), ay2 = make_float2(ay, ay), zi2 = make_float2(zi, zi);
   const float2 hi2 = make_float2(rr_hi, rr_hi), nlo2 = make_float2(-rr_lo, -rr_lo), m1 = make_float2(-1.f, -1.f);
   unsigned hm = 0u, lm = 0u;
-  for (int u0 = 0; u0 < nt; u0 += 8) {
+#pragma unroll
+  for (int u0 = 0; u0 < 32; u0 += 8) {
+    if (u0 >= nt) break;
     unsigned h8 = 0u, l8 = 0u;
 #pragma unroll
     for (int c = 4; c >= 0; c -= 4) {
