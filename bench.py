@@ -473,10 +473,8 @@ def main():
     for _ in range(args.e2e_steps):
         if lib.sph_upload(sim._h, C.byref(hs)) != 0:
             raise RuntimeError("sph_upload failed")
-        if lib.sph_step_async(sim._h, 1) != 0:
-            raise RuntimeError("sph_step failed")
-        if lib.sph_download(sim._h, C.byref(hs)) != 0:
-            raise RuntimeError("sph_download failed")
+        if lib.sph_step_download(sim._h, 1, C.byref(hs)) != 0:
+            raise RuntimeError("sph_step_download failed")
     e1.record(stream)
     e1.synchronize()
     wall_e2e = time.perf_counter() - t0
@@ -517,7 +515,7 @@ def main():
         "speedup_fp32c_vs_fp64": value / r64["value"] if r64 else None,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": state_bytes,
                 "d2h_bytes_per_step": state_bytes, "steps": args.e2e_steps,
-                "path": "sph_upload + sph_step_async(1) + sph_download per step, pinned host buffers, "
+                "path": "sph_upload + sph_step_download(1) per step, pinned host buffers, "
                         + ("fp32c" if args.forms != "fp64" else "fp64") + " form"},
         "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": hbm_peak, "unit": "GB/s",
                      "frac": achieved_gbs / hbm_peak, "traffic": traffic,

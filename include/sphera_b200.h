@@ -199,6 +199,15 @@ int  sph_get_diagnostics(SphHandle* h, SphDiagnostics* diag);
  * from a CUDA graph built on the first call.                              */
 int  sph_step_async(SphHandle* h, int32_t nsteps);
 int  sph_sync(SphHandle* h);
+/* sph_step(h, nsteps) followed by sph_download(h, state), for a host that
+ * keeps the state in its own memory between steps (time_step_loop.f90 with
+ * pg(:) on the CPU).  The positions, velocities and masses of the last
+ * step are copied to the host while that step's neighbour search, boundary
+ * data and continuity pass still run.  The buffers must hold the particle
+ * count before the call; state->n returns the count after it (lower after
+ * out-of-grid removals; rows from there on are unspecified).  Single
+ * simulations only.                                                        */
+int  sph_step_download(SphHandle* h, int32_t nsteps, SphState* state);
 /* The handle's cudaStream_t, for callers that order their own work after
  * the library's.                                                          */
 void* sph_stream(SphHandle* h);

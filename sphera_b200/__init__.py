@@ -56,6 +56,7 @@ def lib():
         "sph_batch_info": ([vp, C.c_int32, C.POINTER(abi.SphStepInfo), ip], C.c_int),
         "sph_step": ([vp, C.c_int32, C.POINTER(abi.SphStepInfo)], C.c_int),
         "sph_step_async": ([vp, C.c_int32], C.c_int),
+        "sph_step_download": ([vp, C.c_int32, C.POINTER(abi.SphState)], C.c_int),
         "sph_sync": ([vp], C.c_int),
         "sph_stream": ([vp], vp),
         "sph_get_diagnostics": ([vp, C.POINTER(abi.SphDiagnostics)], C.c_int),
@@ -152,6 +153,18 @@ class Simulation:
 
     def step_async(self, nsteps=1):
         _chk(lib().sph_step_async(self._h, int(nsteps)), "sph_step_async")
+
+    def step_download(self, nsteps=1):
+        """step(nsteps) then download(), the last step's x, v, m copied to
+        the host while that step finishes (sph_step_download)."""
+        n = self.n
+        st = abi.State.empty(n)
+        _chk(lib().sph_step_download(self._h, int(nsteps), C.byref(st.struct)), "sph_step_download")
+        n2 = st.struct.n
+        if n2 != n:
+            st = abi.State(st.x[:n2], st.v[:n2], st.rho[:n2], st.p[:n2], st.m[:n2])
+            self.n = n2
+        return st
 
     def sync(self):
         _chk(lib().sph_sync(self._h), "sph_sync")

@@ -522,6 +522,8 @@ struct SphHandle {
   cudaStream_t stream = nullptr;
   cudaStream_t stream2 = nullptr;   // the boundary pass beside the lists (step graph)
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  cudaStream_t stream3 = nullptr;   // sph_step_download: x, v, m to the host beside the step's end
+  cudaEvent_t ev_sorted = nullptr;
   int nsims = 0;
   int dim = 3;
   int precision = SPH_PREC_FP64;
@@ -637,6 +639,32 @@ void refresh_copies(SphHandle* h, cudaStream_t st) {
   if (h->precision == SPH_PREC_FP32C) launch_refresh_f32(h->db, st);
 }
 
+// The early half of sph_step_download: positions, velocities and masses
+// are final once a step's sort has run (the passes after it write only
+// rho, p and their FP32 copies), so their scatter to caller order and their
+// copy to the host run on a third stream beside the lists, boundary and
+// continuity passes.  n rows are copied: the count before the step, which
+// removals can only lower.
+struct EarlyCopy {
+  SphState* state;
+  int n;
+  cudaError_t err;
+};
+
+void enqueue_early_copy(SphHandle* h, cudaStream_t st, EarlyCopy& ec) {
+  cudaEventRecord(h->ev_sorted, st);
+  cudaStreamWaitEvent(h->stream3, h->ev_sorted, 0);
+  cudaStream_t q = h->stream3;
+  launch_to_caller(h->db, h->d_cx, h->d_cv, nullptr, nullptr, h->d_cm, nullptr, nullptr, q);
+  cudaError_t e = cudaGetLastError();
+  const size_t o = h->sims[0].dev.p_off, n = (size_t)ec.n;
+  SphState* sta = ec.state;
+  if (e == cudaSuccess && sta->x) e = cudaMemcpyAsync(sta->x, h->d_cx + 3 * o, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, q);
+  if (e == cudaSuccess && sta->v) e = cudaMemcpyAsync(sta->v, h->d_cv + 3 * o, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, q);
+  if (e == cudaSuccess && sta->m) e = cudaMemcpyAsync(sta->m, h->d_cm + o, sizeof(double) * n, cudaMemcpyDeviceToHost, q);
+  ec.err = e;
+}
+
 // One whole step.  The boundary data (SA-SPH, FP64, latency-bound) and the
 // neighbour lists (FP32 screening, issue-bound) both read the freshly sorted
 // state and nothing the other writes, so the boundary pass runs on a second
@@ -644,10 +672,11 @@ void refresh_copies(SphHandle* h, cudaStream_t st) {
 // a join.  The FP64 continuity pass starts its sum from the wall term (the
 // reference's order) and waits for both; the FP32c pass sums the pairs
 // beside the boundary pass too and adds the wall term after the join.
-void step_sequence(SphHandle* h, cudaStream_t st) {
+void step_sequence(SphHandle* h, cudaStream_t st, EarlyCopy* early = nullptr) {
   momentum_pass(h, true, st);
   if (h->any_teta_v) launch_velocity_smoothing(h->db, true, h->precision == SPH_PREC_FP32C, st);
   sort_sequence(h, st);
+  if (early) enqueue_early_copy(h, st, *early);
   cudaEventRecord(h->ev_fork, st);
   cudaStreamWaitEvent(h->stream2, h->ev_fork, 0);
   launch_boundary(h->db, h->stream2);
@@ -944,6 +973,11 @@ void sph_destroy(SphHandle* h) {
     cudaStreamDestroy(h->stream);
   }
   if (h->stream2) cudaStreamDestroy(h->stream2);
+  if (h->stream3) {
+    cudaStreamSynchronize(h->stream3);
+    cudaStreamDestroy(h->stream3);
+  }
+  if (h->ev_sorted) cudaEventDestroy(h->ev_sorted);
   if (h->ev_fork) cudaEventDestroy(h->ev_fork);
   if (h->ev_join) cudaEventDestroy(h->ev_join);
   cudaGetLastError();
@@ -1032,6 +1066,38 @@ int sph_step(SphHandle* h, int32_t nsteps, SphStepInfo* info) {
   for (int s = 0; s < nsteps; ++s) SPH_CUDA(cudaGraphLaunch(h->graph, h->stream));
   SPH_TRY(sync_dyn(h));
   if (info) fill_info(h, 0, info);
+  return SPH_OK;
+}
+
+// nsteps steps, then the state in caller order, as sph_step followed by
+// sph_download, with the last step's positions, velocities and masses
+// copied to the host while that step's lists, boundary data and continuity
+// pass still run (see enqueue_early_copy).  The last step is launched
+// without the graph so that the copy can start inside it.
+int sph_step_download(SphHandle* h, int32_t nsteps, SphState* state) {
+  if (!h || !h->uploaded || h->nsims != 1 || nsteps < 0 || !state) return SPH_ERR_INVALID_ARGUMENT;
+  if (nsteps == 0) return download_impl(h, 0, state, nullptr, nullptr);
+  SPH_TRY(build_graph(h));
+  if (!h->stream3) {
+    SPH_CUDA(cudaStreamCreateWithFlags(&h->stream3, cudaStreamNonBlocking));
+    SPH_CUDA(cudaEventCreateWithFlags(&h->ev_sorted, cudaEventDisableTiming));
+  }
+  for (int s = 0; s + 1 < nsteps; ++s) SPH_CUDA(cudaGraphLaunch(h->graph, h->stream));
+  SPH_TRY(sync_dyn(h));
+  EarlyCopy ec{state, h->h_dyn[0].nag, cudaSuccess};
+  cudaStream_t q = h->stream;
+  step_sequence(h, q, &ec);
+  launch_to_caller(h->db, nullptr, nullptr, h->d_crho, h->d_cp, nullptr, nullptr, nullptr, q);
+  cudaError_t e = cudaGetLastError();
+  const size_t o = h->sims[0].dev.p_off, n = (size_t)ec.n;
+  if (e == cudaSuccess && state->rho) e = cudaMemcpyAsync(state->rho, h->d_crho + o, sizeof(double) * n, cudaMemcpyDeviceToHost, q);
+  if (e == cudaSuccess && state->p) e = cudaMemcpyAsync(state->p, h->d_cp + o, sizeof(double) * n, cudaMemcpyDeviceToHost, q);
+  cudaError_t e3 = cudaStreamSynchronize(h->stream3);
+  if (e == cudaSuccess) e = ec.err;
+  if (e == cudaSuccess) e = e3;
+  SPH_TRY(sync_dyn(h));
+  if (e != cudaSuccess) return cuda_status(e);
+  state->n = h->h_dyn[0].nag;
   return SPH_OK;
 }
 
