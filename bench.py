@@ -8,21 +8,30 @@ step of time_step_loop.f90 (momentum + leapfrog, cell sort, SA-SPH boundary
 data, continuity + EoS, time step), replayed from a CUDA graph.
 
   value       particle-steps/s over all ranks, state resident on the device
-              (device time, CUDA events on the library's stream, max over ranks)
+              (device time, CUDA events on the library's stream, max over
+              ranks): the median of repeated windows of --steps graph
+              replays, repeated until at least --min-seconds are timed
   e2e         the same metric through the C ABI with the state in pinned host
               memory: every step uploads pg(:), advances and downloads it
-  roofline    dominant kernel (momentum pass) against the measured HBM copy
-              bandwidth; fp64 gives the same kernel against the measured FP64
-              FMA rate, the bound that actually applies to the pair passes
+              (both forms; the top-level e2e is the headline form's)
+  roofline    dominant kernel (momentum pass) against the larger of its two
+              roofs: the measured HBM copy bandwidth and the FMA rate of its
+              arithmetic (FP32 for the FP32c form, FP64 for the FP64 form),
+              measured in the run with its clocks recorded
   cpu_baseline  the oracle (FP64 OpenMP restatement) on the host cores
 
 `--impl reference` times the oracle alone (the reference is Fortran and
-cannot be built here) on the same workload.  Multi-GPU (torchrun) runs one
-independent replica per rank (no data-path collective: weak scaling).
+cannot be built here) on the same workload.  `--gpus N` runs N ranks, one
+per GPU: under torchrun it reads the ranks from the environment, otherwise
+it starts them itself through torch.distributed.run.  Each rank advances
+an independent replica (no data-path collective: weak scaling).
+`--dry-run` exercises the rank plumbing without a GPU.
 """
 import argparse
 import json
+import math
 import os
+import socket
 import statistics
 import subprocess
 import sys
@@ -47,8 +56,11 @@ KERNELS_PER_STEP_FP64 = 15
 # records), L 1, I 4, ncount 4, bdt_count 4 -- and written once -- X2 32,
 # V2 32, P2 8, I2 4, L2 1 -- plus the nine pair sums passed between the two
 # launches (72 B written, 72 B read); 4 B per neighbour-list entry and 168 B
-# per boundary entry
+# per boundary entry.  The FP64 pass (one launch) reads X, V, RP, L, I,
+# ncount, bdt_count and the neighbours' X, V, RP and writes the same record:
+# 218 B per particle.
 MOM_BYTES_PER_PARTICLE = 362
+MOM_BYTES_PER_PARTICLE_FP64 = 218
 LIST_ENTRY_BYTES = 4
 BDT_ENTRY_BYTES = 168
 # Operations per accepted non-self pair: 107 in the momentum pass, 34 in the
@@ -57,13 +69,33 @@ BDT_ENTRY_BYTES = 168
 FLOP_CAND, FLOP_MOM_PAIR, FLOP_CONT_PAIR = 9, 107, 34
 
 
+def _free_port():
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    return port
+
+
+def _spawn_ranks(nranks):
+    """`bench.py --gpus N` started without torchrun: run the same command
+    line as N ranks of torch.distributed.run (one per GPU) and return its
+    exit status."""
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={nranks}",
+           "--master-addr=127.0.0.1", f"--master-port={_free_port()}", os.path.abspath(__file__), *sys.argv[1:]]
+    return subprocess.call(cmd)
+
+
 def _dist():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if ws > 1:
+        import datetime
         import torch.distributed as dist
-        dist.init_process_group("gloo", init_method="env://")
+        # gloo carries only scalars here (timings, work counts); a rank that
+        # never arrives ends the others' next collective with an error
+        dist.init_process_group("gloo", init_method="env://", timeout=datetime.timedelta(seconds=600))
     return ws, rank, local
 
 
@@ -91,6 +123,12 @@ def _sum_over_ranks(ws, v):
     t = torch.tensor([v], dtype=torch.float64)
     dist.all_reduce(t, op=dist.ReduceOp.SUM)
     return float(t.item())
+
+
+def _finish_dist(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
 
 
 class ClockSampler:
@@ -195,7 +233,7 @@ def run_reference(args, ws, rank):
     el = time.perf_counter() - t0
     v = case.n * steps / el
     line = {
-        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": ws,
         "steps": steps, "warmup": min(args.warmup, 3), "ms_per_step": el / steps * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded 3D dam break generated in-repo)",
@@ -304,16 +342,43 @@ def run_serving(args, ws, rank):
     return 0
 
 
-def _fp64_summary(r64, n, steps, fp64_peak):
-    if r64 is None:
+def _fp_summary(r, n, fp_peak, flop_pair):
+    if r is None:
         return None
-    c64, nprof = r64["cnt"], r64["nprof"]
-    mom64_ms = r64["phases"]["momentum"]
-    mom64_flops = (c64["pairs"] - n * nprof) * FLOP_MOM_PAIR / nprof
-    return {"value": r64["value"], "ms_per_step": r64["ms"] / steps,
-            "phases_ms_per_step": r64["phases"], "clocks": r64["clocks"],
-            "momentum_fp64_tflops": mom64_flops / (mom64_ms * 1e-3) / 1e12,
-            "fp64_peak_tflops": fp64_peak}
+    c, nprof = r["cnt"], r["nprof"]
+    mom_ms = r["phases"]["momentum"]
+    flops = (c["pairs"] - n * nprof) * flop_pair / nprof
+    return {"value": r["value"], "ms_per_step": r["ms_step"], "ms_per_step_spread": r["spread"],
+            "windows": r["windows"], "phases_ms_per_step": r["phases"], "clocks": r["clocks"],
+            "momentum_tflops": flops / (mom_ms * 1e-3) / 1e12, "fma_peak_tflops": fp_peak,
+            "e2e": r["e2e"], "autotuned_grids": r["grids"]}
+
+
+def _measure_peak(fp32, gpu_id):
+    """Dense FMA rate of the device (FP32 or FP64), the best of repeated
+    probes over about half a second, with the clocks seen meanwhile."""
+    from sphera_b200 import measure_fp32_peak, measure_fp64_peak
+    f = measure_fp32_peak if fp32 else measure_fp64_peak
+    f()
+    sampler = ClockSampler(gpu_id)
+    best, t0 = 0.0, time.perf_counter()
+    while time.perf_counter() - t0 < 0.6:
+        best = max(best, f())
+    return best, sampler.stop()
+
+
+def run_dry(args, ws, rank):
+    """The rank plumbing of a multi-GPU run without a GPU: each rank reports
+    one unit of work and its rank; rank 0 prints the line the real run
+    would print, with n_gpus taken from the ranks that reported."""
+    ranks = _sum_over_ranks(ws, 1.0)
+    ids = _sum_over_ranks(ws, float(rank))
+    wall = _max_over_ranks(ws, 1.0 + rank)
+    if rank == 0:
+        print(json.dumps({"metric": METRIC, "dry_run": True, "n_gpus": ws, "ranks_reporting": int(ranks),
+                          "rank_id_sum": int(ids), "max_over_ranks": wall, "unit": UNIT,
+                          "scaling": "weak"}), flush=True)
+    return 0
 
 
 def main():
@@ -321,10 +386,13 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--min-seconds", type=float, default=2.0,
+                    help="repeat the timed window of --steps replays until this much device time is timed")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--cpu-steps", type=int, default=3)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--dry-run", action="store_true", help="rank plumbing only, no GPU work")
     ap.add_argument("--workload", default="dam_break_3d", choices=["dam_break_3d", "random_box", "ensemble", "serving"])
     ap.add_argument("--n", type=int, default=16_000_000, help="particles of the random-box workload")
     ap.add_argument("--n-sims", type=int, default=256)
@@ -346,30 +414,40 @@ def main():
     args.warmup = max(3, args.warmup)
     if args.t_end is None:
         args.t_end = 0.3 if args.workload == "serving" else 0.5
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        return _spawn_ranks(args.gpus)
     ws, rank, local = _dist()
-    if args.workload in ("ensemble", "serving") and args.impl == "ours":
-        rc = (run_ensemble if args.workload == "ensemble" else run_serving)(args, ws, rank)
-        if ws > 1:
-            import torch.distributed as dist
-            dist.destroy_process_group()
-        return rc
-    if args.impl == "reference":
+    if ws != args.gpus:
+        sys.stderr.write(f"bench.py: --gpus {args.gpus} but {ws} ranks were started\n")
+        _finish_dist(ws)
+        return 2
+    if args.dry_run:
+        rc = run_dry(args, ws, rank)
+    elif args.impl == "reference":
         rc = run_reference(args, ws, rank)
-        if ws > 1:
-            import torch.distributed as dist
-            dist.destroy_process_group()
-        return rc
+    elif args.workload == "ensemble":
+        rc = run_ensemble(args, ws, rank)
+    elif args.workload == "serving":
+        rc = run_serving(args, ws, rank)
+    else:
+        rc = run_step_bench(args, ws, rank, local)
+    _finish_dist(ws)
+    return rc
+
+
+def run_step_bench(args, ws, rank, local):
+    import ctypes as C
 
     import torch
     torch.cuda.set_device(local)
-    from sphera_b200 import Simulation, abi, cases, measure_fp32_peak, measure_fp64_peak
+    from sphera_b200 import Simulation, abi, cases
 
-    fp64_peak = measure_fp64_peak()
-    fp32_peak = measure_fp32_peak()
     try:
         gpu_id = "GPU-" + str(torch.cuda.get_device_properties(local).uuid)
     except Exception:
         gpu_id = str(local)
+    fp64_peak, fp64_peak_clocks = _measure_peak(False, gpu_id)
+    fp32_peak, fp32_peak_clocks = _measure_peak(True, gpu_id)
 
     def make_case(precision, n=None):
         if args.workload == "random_box":
@@ -383,20 +461,10 @@ def main():
             c.params.invb_det_thresh = 1.0e-3
         return c
 
-    def run_form(precision):
-        case = make_case(precision)
-        n = case.n
-        sim = Simulation(case)
-        sim.upload(case.state)
-        grids = sim.autotune(reps=3) if args.autotune else None
-        sim.step(args.warmup)
-        stream = torch.cuda.ExternalStream(sim.stream)
-        sampler = ClockSampler(gpu_id)
+    def timed_window(sim, stream, e0, e1):
         _barrier(ws)
         torch.cuda.synchronize()
         sim.sync()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         sim.step_async(args.steps)
         e1.record(stream)
@@ -404,42 +472,97 @@ def main():
         sim.sync()
         torch.cuda.synchronize()
         _barrier(ws)
-        ms = e0.elapsed_time(e1)
+        return _max_over_ranks(ws, e0.elapsed_time(e1))
+
+    def e2e_leg(sim, case, stream, e0, e1):
+        """Every step through the C ABI from pinned host memory: sph_upload
+        (the IC part included) and sph_step_download(1)."""
+        n = case.n
+        pin = {k: torch.empty(sh, dtype=torch.float64, pin_memory=True)
+               for k, sh in (("x", (n, 3)), ("v", (n, 3)), ("rho", (n,)), ("p", (n,)), ("m", (n,)))}
+        st0 = sim.download()
+        for k in pin:
+            pin[k].numpy()[...] = getattr(st0, k)
+        hs = abi.SphState()
+        hs.n = n
+        for k in pin:
+            setattr(hs, k, C.cast(pin[k].data_ptr(), C.POINTER(C.c_double)))
+        lib = __import__("sphera_b200").lib()
+        _barrier(ws)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        e0.record(stream)
+        for _ in range(args.e2e_steps):
+            hs.n = n
+            if lib.sph_upload(sim._h, C.byref(hs)) != 0:
+                raise RuntimeError("sph_upload failed")
+            if lib.sph_step_download(sim._h, 1, C.byref(hs)) != 0:
+                raise RuntimeError("sph_step_download failed")
+        e1.record(stream)
+        e1.synchronize()
+        wall = time.perf_counter() - t0
+        ms = _max_over_ranks(ws, max(e0.elapsed_time(e1), wall * 1e3))
+        state_bytes = n * (3 + 3 + 1 + 1 + 1) * 8
+        return {"value": ws * n * args.e2e_steps / (ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": state_bytes,
+                "d2h_bytes_per_step": state_bytes, "steps": args.e2e_steps,
+                "path": "sph_upload + sph_step_download(1) per step, pinned host buffers"}
+
+    def run_form(precision, keep):
+        case = make_case(precision)
+        n = case.n
+        sim = Simulation(case)
+        sim.upload(case.state)
+        grids = sim.autotune(reps=3) if args.autotune else None
+        sim.step(args.warmup)
+        stream = torch.cuda.ExternalStream(sim.stream)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        sampler = ClockSampler(gpu_id)
+        wins = [timed_window(sim, stream, e0, e1)]
+        # the same window count on every rank: it follows from the first
+        # window's time, which is already the max over ranks
+        nwin = max(1, math.ceil(args.min_seconds * 1e3 / wins[0]))
+        for _ in range(nwin - 1):
+            wins.append(timed_window(sim, stream, e0, e1))
         clocks = sampler.stop()
-        ms_max = _max_over_ranks(ws, ms)
-        value = ws * n * args.steps / (ms_max * 1e-3)
+        ms = statistics.median(wins)
+        value = ws * n * args.steps / (ms * 1e-3)
         # phase times and counters of the same workload (un-graphed steps)
         sim.counters(reset=True)
         nprof = 10
         phases = sim.profile_phases(nprof)
         cnt = sim.counters(reset=True)
         diag = sim.diagnostics()
-        return dict(case=case, n=n, sim=sim, stream=stream, value=value, ms=ms_max, clocks=clocks, grids=grids,
-                    phases={k: v / nprof for k, v in phases.items()}, nprof=nprof, cnt=cnt, diag=diag,
-                    e0=e0, e1=e1)
+        e2e = e2e_leg(sim, case, stream, e0, e1)
+        r = dict(case=case, n=n, value=value, ms=ms, ms_step=ms / args.steps,
+                 spread=[min(wins) / args.steps, max(wins) / args.steps], windows=len(wins),
+                 clocks=clocks, grids=grids, phases={k: v / nprof for k, v in phases.items()},
+                 nprof=nprof, cnt=cnt, diag=diag, e2e=e2e)
+        if keep:
+            r["sim"] = sim
+        else:
+            sim.close()
+        return r
 
     r64 = r32 = None
     if args.forms in ("both", "fp64"):
-        r64 = run_form(abi.SPH_PREC_FP64)
-        r64["sim"].close()
+        r64 = run_form(abi.SPH_PREC_FP64, keep=args.forms == "fp64")
     if args.forms in ("both", "fp32c"):
-        r32 = run_form(abi.SPH_PREC_FP32C)
-    else:
-        r32 = r64
-        r32["sim"] = Simulation(r64["case"])
-        r32["sim"].upload(r64["case"].state)
-        r32["stream"] = torch.cuda.ExternalStream(r32["sim"].stream)
-    case, n, sim, stream = r32["case"], r32["n"], r32["sim"], r32["stream"]
-    e0, e1 = r32["e0"], r32["e1"]
-    value, ms_max, clocks, cnt, diag = r32["value"], r32["ms"], r32["clocks"], r32["cnt"], r32["diag"]
-    nprof = r32["nprof"]
-    mom_ms = r32["phases"]["momentum"]
+        r32 = run_form(abi.SPH_PREC_FP32C, keep=True)
+    fp32c = r32 is not None
+    head = r32 if fp32c else r64
+    case, n, sim = head["case"], head["n"], head["sim"]
+    cnt, diag, nprof = head["cnt"], head["diag"], head["nprof"]
+    mom_ms = head["phases"]["momentum"]
     list_entries = cnt["pairs"] / nprof - n          # accepted pairs less the particle itself
-    alg_bytes = n * MOM_BYTES_PER_PARTICLE + list_entries * LIST_ENTRY_BYTES + diag.bdt_entries * BDT_ENTRY_BYTES
+    per_particle = MOM_BYTES_PER_PARTICLE if fp32c else MOM_BYTES_PER_PARTICLE_FP64
+    alg_bytes = n * per_particle + list_entries * LIST_ENTRY_BYTES + diag.bdt_entries * BDT_ENTRY_BYTES
     hbm_peak, peak_kind = _peaks()
     achieved_gbs = alg_bytes / (mom_ms * 1e-3) / 1e9
     mom_flops = (cnt["pairs"] - n * nprof) * FLOP_MOM_PAIR / nprof
     mom_tflops = mom_flops / (mom_ms * 1e-3) / 1e12
+    fp_peak = fp32_peak if fp32c else fp64_peak
+    fp_clocks = fp32_peak_clocks if fp32c else fp64_peak_clocks
     if args.workload == "random_box":
         workload = f"random_box_{n}"
         desc = (f"random_box: {n} particles uniform in a cube at mean spacing 0.01 m, rho = 1000 (1 + N(0, 1e-3)), "
@@ -450,38 +573,20 @@ def main():
                 f"{n} particles per GPU, SA-SPH walls"
                 + (f", partial smoothing TetaP = TetaV = {args.teta:g}" if args.teta > 0 else "")
                 + (", C1 renormalisation (C1_BE, C1_divu)" if args.c1 else ""))
-    traffic = _traffic(workload)
-
-    # end to end through the C ABI with pinned host buffers
-    pin = {k: torch.empty(sh, dtype=torch.float64, pin_memory=True)
-           for k, sh in (("x", (n, 3)), ("v", (n, 3)), ("rho", (n,)), ("p", (n,)), ("m", (n,)))}
-    st0 = sim.download()
-    for k in pin:
-        pin[k].numpy()[...] = getattr(st0, k)
-    from sphera_b200 import abi
-    import ctypes as C
-    hs = abi.SphState()
-    hs.n = n
-    for k in pin:
-        setattr(hs, k, C.cast(pin[k].data_ptr(), C.POINTER(C.c_double)))
-
-    lib = __import__("sphera_b200").lib()
-    _barrier(ws)
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    e0.record(stream)
-    for _ in range(args.e2e_steps):
-        if lib.sph_upload(sim._h, C.byref(hs)) != 0:
-            raise RuntimeError("sph_upload failed")
-        if lib.sph_step_download(sim._h, 1, C.byref(hs)) != 0:
-            raise RuntimeError("sph_step_download failed")
-    e1.record(stream)
-    e1.synchronize()
-    wall_e2e = time.perf_counter() - t0
-    e2e_ms = max(e0.elapsed_time(e1), wall_e2e * 1e3)
-    e2e_ms = _max_over_ranks(ws, e2e_ms)
-    e2e_value = ws * n * args.e2e_steps / (e2e_ms * 1e-3)
-    state_bytes = n * (3 + 3 + 1 + 1 + 1) * 8
+    traffic = _traffic(workload) if fp32c else None
+    roof_hbm = {"achieved": achieved_gbs, "peak": hbm_peak, "unit": "GB/s", "frac": achieved_gbs / hbm_peak,
+                "peak_kind": f"{peak_kind} HBM copy bandwidth", "algorithmic_bytes": alg_bytes}
+    roof_fp = {"achieved": mom_tflops, "peak": fp_peak, "unit": "TFLOP/s", "frac": mom_tflops / fp_peak,
+               "peak_kind": ("measured FP32" if fp32c else "measured FP64") + " FMA rate (in-run probe)",
+               "peak_clocks": fp_clocks, "flops_per_pair": FLOP_MOM_PAIR}
+    fp_bound = roof_fp["frac"] > roof_hbm["frac"]
+    main_roof = roof_fp if fp_bound else roof_hbm
+    roofline = {"bound": ("fp32" if fp32c else "fp64") if fp_bound else "hbm",
+                "achieved": main_roof["achieved"], "peak": main_roof["peak"], "unit": main_roof["unit"],
+                "frac": main_roof["frac"], "traffic": traffic,
+                "kernel": ("k_momentum_f32<3> + k_momentum_f32_finish<3,true> (momentum pair sums; wall terms, "
+                           "leapfrog)" if fp32c else "k_momentum<3,true> (FP64 momentum, wall terms, leapfrog)"),
+                "hbm": roof_hbm, "fp": roof_fp}
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
@@ -499,47 +604,42 @@ def main():
                       f"its IC ({el:.1f} s), FP64 oracle, OpenMP on all host threads")
         cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample}
 
+    e2e = dict(head["e2e"])
+    e2e["path"] += ", " + ("fp32c" if fp32c else "fp64") + " form"
     line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+        "metric": METRIC, "value": head["value"], "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": head["ms_step"], "ms_per_step_spread": head["spread"],
+        "timed_windows": head["windows"], "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None,
         "dtype": ("fp32c (f32 pair sums, compensated; f64 positions/integration/boundary terms)"
-                  if args.forms != "fp64" else "f64"),
+                  if fp32c else "f64"),
         "data": f"synthetic (seeded {args.workload} generated in-repo)",
         "config": {"workload": desc,
-                   "particles_per_gpu": n, "form": "fp32c" if args.forms != "fp64" else "fp64",
-                   "autotuned_grids": r32.get("grids"),
+                   "particles_per_gpu": n, "form": "fp32c" if fp32c else "fp64",
+                   "autotuned_grids": head["grids"],
                    "l2": "state and scratch (~250 MB per step) exceed the 126 MB L2; no flush",
+                   "timing": f"median of {head['windows']} windows of {args.steps} graph replays "
+                             f"(at least {args.min_seconds:g} s of device time), each bracketed by a barrier "
+                             f"and synchronisation, max over ranks",
                    "parallelism": f"replicas x{ws} (independent simulations, no collective)"},
-        "fp64": _fp64_summary(r64, n, args.steps, fp64_peak),
-        "speedup_fp32c_vs_fp64": value / r64["value"] if r64 else None,
-        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": state_bytes,
-                "d2h_bytes_per_step": state_bytes, "steps": args.e2e_steps,
-                "path": "sph_upload + sph_step_download(1) per step, pinned host buffers, "
-                        + ("fp32c" if args.forms != "fp64" else "fp64") + " form"},
-        "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": hbm_peak, "unit": "GB/s",
-                     "frac": achieved_gbs / hbm_peak, "traffic": traffic,
-                     "kernel": ("k_momentum_f32<3> + k_momentum_f32_finish<3,true> (momentum pair sums; wall terms, leapfrog)"
-                                if args.forms != "fp64" else "k_momentum<3,true> (FP64 momentum, wall terms, leapfrog)"),
-                     "peak_kind": f"{peak_kind} HBM copy bandwidth",
-                     "fp": {"achieved_tflops": mom_tflops, "peak_tflops": fp32_peak,
-                            "frac": mom_tflops / fp32_peak, "peak_kind": "measured FP32 FMA rate (in-run)"}},
-        "phases_ms_per_step": r32["phases"],
+        "fp64": _fp_summary(r64, n, fp64_peak, FLOP_MOM_PAIR),
+        "fp32c": _fp_summary(r32, n, fp32_peak, FLOP_MOM_PAIR),
+        "speedup_fp32c_vs_fp64": r32["value"] / r64["value"] if (r32 and r64) else None,
+        "e2e": e2e,
+        "roofline": roofline,
+        "phases_ms_per_step": head["phases"],
         "pairs_per_particle": cnt["pairs"] / nprof / n,
         "candidates_per_particle": cnt["candidates"] / nprof / n,
         # + 2 launches each for the velocity and the pressure smoothing
         # passes, + 1 for the renormalisation matrices
-        "gpu_launches": ((KERNELS_PER_STEP if args.forms != "fp64" else KERNELS_PER_STEP_FP64)
+        "gpu_launches": ((KERNELS_PER_STEP if fp32c else KERNELS_PER_STEP_FP64)
                          + (4 if args.teta > 0 else 0) + (1 if args.c1 else 0)) * args.steps,
-        "clocks": clocks,
+        "clocks": head["clocks"],
         "cpu_baseline": cpu,
     }
     if rank == 0:
         print(json.dumps(line), flush=True)
     sim.close()
-    if ws > 1:
-        import torch.distributed as dist
-        dist.destroy_process_group()
     return 0
 
 

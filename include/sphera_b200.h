@@ -204,9 +204,12 @@ int  sph_sync(SphHandle* h);
  * pg(:) on the CPU).  The positions, velocities and masses of the last
  * step are copied to the host while that step's neighbour search, boundary
  * data and continuity pass still run.  The buffers must hold the particle
- * count before the call; state->n returns the count after it (lower after
- * out-of-grid removals; rows from there on are unspecified).  Single
- * simulations only.                                                        */
+ * count before the call, as the host last saw it (sph_upload, or the last
+ * call that returned a count); state->n returns the count after it (lower
+ * after out-of-grid removals; rows from there on are unspecified).  The
+ * overlap needs page-locked buffers (cudaHostAlloc / cudaHostRegister):
+ * pageable ones give the same results without it.  Single simulations
+ * only.                                                                    */
 int  sph_step_download(SphHandle* h, int32_t nsteps, SphState* state);
 /* The handle's cudaStream_t, for callers that order their own work after
  * the library's.                                                          */
@@ -284,6 +287,21 @@ int  sph_leapfrog_continuity(SphHandle* h);
 int  sph_eos(SphHandle* h);
 
 /* ---------------------------------------------------------------------- */
+/* Post-processing                                                         */
+/* ---------------------------------------------------------------------- */
+
+/* fluid_global_quantities.f90:59-72 (called by time_step_post_processing.f90:81
+ * every Domain%icpoi_fr steps): FP64 sums over pg(1:nag) of the mass, the
+ * linear momentum m v, the angular momentum m (coord x vel) about the origin
+ * (Vector_Product.f90) and the volume m / rho, computed on the device.
+ * out[0] mass, out[1..3] linear momentum, out[4..6] angular momentum,
+ * out[7] volume.  sim selects one simulation of a batch (0 for sph_create);
+ * sim = -1 fills out[nsims][8] for all of them.  The sums are compensated
+ * and reduced in a fixed order, so they are the exact sums to within a few
+ * ulps whatever the particle order.                                       */
+int  sph_global_quantities(SphHandle* h, int32_t sim, double* out);
+
+/* ---------------------------------------------------------------------- */
 /* Verification                                                            */
 /* ---------------------------------------------------------------------- */
 
@@ -302,6 +320,9 @@ int  sph_dump_neighbours(SphHandle* h, int32_t nmaxj, int32_t* counts, int32_t* 
  * IntGiWrRdV(3,3) column-major ([n][max_per][20]).                        */
 int  sph_dump_boundary(SphHandle* h, int32_t max_per, int32_t* ncb,
                        int32_t* clobonum, double* values);
+/* pg%laminar_flag ([n], caller order) as the last momentum pass set it
+ * (inter_EqMoto.f90:269-283).                                             */
+int  sph_dump_laminar(SphHandle* h, int32_t* flags);
 /* With c1_be: pg%B_ren_gradp and (with c1_divu) pg%B_ren_divu in caller
  * order, 9 doubles per particle, B(i,j) at [9 k + 3 (i-1) + (j-1)].  After
  * a search they hold the fluid sums of CalcVarLength.f90:285-324; after a
@@ -331,8 +352,13 @@ int  sph_dump_renormalisation(SphHandle* h, double* b_gradp, double* b_divu);
  * Limits: n <= 1048576 and Grid%nmax <= 1048576, else
  * SPH_ERR_INVALID_ARGUMENT.  The first call on a device looks up the address
  * of the device array (with that device current) and must come before any
- * stream capture on that device.  Every call shares the one array: calls
- * whose work overlaps on the GPU race and must be serialised.             */
+ * stream capture on that device; the address is kept per device context,
+ * so after a cudaDeviceReset the next call looks it up again (and must
+ * again come before any capture).  Every call shares the one array: calls
+ * whose work overlaps on the GPU race and must be serialised.  Particles
+ * outside the grid get cella 0 and are left out of NPartOrd (its last
+ * n - Icont(nmax+1) + 1 rows are then unspecified); unlike sph_ord_grid,
+ * nothing is removed or reordered.                                        */
 int  sph_ord_grid_static(const SphParams* params, int32_t n, const double* d_x, int32_t* d_cella,
                          int32_t* d_icont, int32_t* d_npartord, void* stream);
 

@@ -48,6 +48,8 @@ def lib():
         L.ora_time.restype = C.c_double
         L.ora_get.argtypes = [vp, dp, dp, dp, dp, dp, dp, dp]
         L.ora_get_c1.argtypes = [vp, dp, dp]
+        L.ora_global_quantities.argtypes = [vp, dp]
+        L.ora_laminar.argtypes = [vp, ip]
         L.ora_grid.argtypes = [vp, ip, ip, ip]
         L.ora_grid_info.argtypes = [vp, ip, dp, dp]
         L.ora_neighbours.argtypes = [vp, C.c_int, ip, ip]
@@ -159,6 +161,19 @@ class Oracle:
         out.update({k: np.zeros(n) for k in ("rho", "p", "m", "dden")})
         lib().ora_get(self._h, *(abi.dptr(out[k]) for k in ("x", "v", "rho", "p", "m", "acc", "dden")))
         return out
+
+    def global_quantities(self):
+        """fluid_global_quantities: [mass, linear momentum (3), angular
+        momentum (3), volume], FP64 sums in pg order."""
+        out = np.zeros(8)
+        lib().ora_global_quantities(self._h, abi.dptr(out))
+        return out
+
+    def laminar(self):
+        """pg%laminar_flag as the last momentum evaluation set it."""
+        f = np.zeros(self.n, np.int32)
+        lib().ora_laminar(self._h, abi.iptr(f))
+        return f
 
     def get_c1(self):
         """B_ren_gradp and B_ren_divu, (n, 3, 3) each."""

@@ -2072,6 +2072,26 @@ int ora_get(void* h, double* x, double* v, double* rho, double* p, double* m, do
   return o.nag;
 }
 
+// fluid_global_quantities.f90:59-72: mass, linear momentum, angular momentum
+// about the origin (Vector_Product of coord and vel) and volume sum(m / rho)
+// over pg(1:nag), summed sequentially in pg order.  out[0] mass, out[1..3]
+// linear momentum, out[4..6] angular momentum, out[7] volume.
+void ora_global_quantities(void* h, double* out) {
+  Oracle& o = *static_cast<Oracle*>(h);
+  double glob_mass = 0.0, glob_vol = 0.0, lin[3] = {0, 0, 0}, ang[3] = {0, 0, 0}, aux[3];
+  for (int ip = 1; ip <= o.nag; ++ip) {
+    const Particle& q = o.pg[ip];
+    glob_mass = glob_mass + q.mass;
+    for (int d = 0; d < 3; ++d) lin[d] = lin[d] + q.mass * q.vel[d];
+    Vector_Product(q.coord, q.vel, aux);
+    for (int d = 0; d < 3; ++d) ang[d] = ang[d] + q.mass * aux[d];
+    glob_vol = glob_vol + q.mass / q.dens;
+  }
+  out[0] = glob_mass;
+  for (int d = 0; d < 3; ++d) { out[1 + d] = lin[d]; out[4 + d] = ang[d]; }
+  out[7] = glob_vol;
+}
+
 // The renormalisation matrices B_ren_gradp and B_ren_divu in pg order, 9
 // doubles per particle, B(i,j) at [9 k + 3 i + j].  Either pointer may be NULL.
 int ora_get_c1(void* h, double* bg, double* bd) {
@@ -2084,6 +2104,12 @@ int ora_get_c1(void* h, double* bg, double* bd) {
         if (bd) bd[9 * i + 3 * a + c] = q.Bd[a][c];
       }
   }
+  return o.nag;
+}
+
+int ora_laminar(void* h, int* flags) {
+  Oracle& o = *static_cast<Oracle*>(h);
+  for (int i = 0; i < o.nag; ++i) flags[i] = o.pg[i + 1].laminar_flag;
   return o.nag;
 }
 

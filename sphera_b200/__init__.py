@@ -82,6 +82,8 @@ def lib():
         "sph_memory_required": ([C.c_int32, C.POINTER(abi.SphParams), C.POINTER(abi.SphGeometry), ip,
                                  C.POINTER(C.c_uint64)], C.c_int),
         "sph_idle": ([vp, ip], C.c_int),
+        "sph_global_quantities": ([vp, C.c_int32, dp], C.c_int),
+        "sph_dump_laminar": ([vp, ip], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -218,6 +220,13 @@ class Simulation:
     def eos(self):
         _chk(lib().sph_eos(self._h), "sph_eos")
 
+    def global_quantities(self):
+        """fluid_global_quantities: [mass, linear momentum (3), angular
+        momentum about the origin (3), volume], FP64 sums on the device."""
+        out = np.zeros(8)
+        _chk(lib().sph_global_quantities(self._h, 0, abi.dptr(out)), "sph_global_quantities")
+        return out
+
     # ------------------------------------------------------------ autotuner
     def autotune(self, reps=3):
         """Sizes the persistent grids of the pair, list and boundary kernels."""
@@ -261,6 +270,12 @@ class Simulation:
         _chk(lib().sph_dump_boundary(self._h, max_per, abi.iptr(ncb), abi.iptr(clob), abi.dptr(vals)),
              "sph_dump_boundary")
         return ncb, clob, vals
+
+    def dump_laminar(self):
+        """pg%laminar_flag of the last momentum pass, caller order."""
+        f = np.zeros(self.n, np.int32)
+        _chk(lib().sph_dump_laminar(self._h, abi.iptr(f)), "sph_dump_laminar")
+        return f
 
     def dump_renormalisation(self, divu=True):
         """B_ren_gradp and (divu) B_ren_divu in caller order, (n, 3, 3)."""
@@ -365,6 +380,12 @@ class Batch:
         st = np.zeros(n, np.int32)
         _chk(lib().sph_batch_status(self._h, abi.iptr(fr), abi.dptr(t), abi.iptr(st)), "sph_batch_status")
         return fr.astype(bool), t, st
+
+    def global_quantities(self):
+        """fluid_global_quantities of every simulation, (nsims, 8)."""
+        out = np.zeros((len(self.cases), 8))
+        _chk(lib().sph_global_quantities(self._h, -1, abi.dptr(out)), "sph_global_quantities")
+        return out
 
     def download(self, sim):
         n = self.cases[sim].n

@@ -1,10 +1,11 @@
 """Builds the CUDA library sphera_b200/libsphera_b200.so for sm_100a.
 
-Each translation unit is compiled on its own so it can carry its own
-floating-point flags: the FP64 path is built with --fmad=false (the
-reference's arithmetic has no fused multiply-add), the FP32-compensated
-pair kernels with contraction allowed.  Host code is built with
--ffp-contract=off for the same reason.
+Every translation unit is built with --fmad=false: the FP64 path must not
+contract a multiply and an add (the reference's arithmetic has no fused
+multiply-add), and the compensated sums of the FP32-compensated form need
+their additions rounded one by one.  Where the FP32c pair arithmetic wants a
+fused multiply-add it writes fmaf / __ffma2_rn explicitly.  Host code is
+built with -ffp-contract=off for the same reason.
 """
 import os
 import subprocess

@@ -546,6 +546,8 @@ struct SphHandle {
   int* d_ncount = nullptr;
   int list_cap = 0;
   unsigned long long* d_counters = nullptr;
+  double2* d_gq_part = nullptr;     // fluid_global_quantities: per-tile partial sums
+  double* d_gq_out = nullptr;       // [nsims][8]
   Particles P{};
   std::vector<void*> owned;
   // caller-order staging
@@ -815,6 +817,8 @@ int create_batch(int nsims, const SphParams* params, const SphGeometry* geoms, c
   int nb = (int)((C + 4095) / 4096) + 1;
   A(h->d_scan, nb);
   A(h->d_counters, 4);
+  A(h->d_gq_part, tiles.size() * 8);
+  A(h->d_gq_out, (size_t)nsims * 8);
   for (int s = 0; s < nsims; ++s) h->list_cap = std::max(h->list_cap, h->sims[s].dev.nmaxpartj);
   h->list_cap = (h->list_cap + 3) / 4 * 4;
   A(h->d_nlist, N * (size_t)h->list_cap);
@@ -1083,7 +1087,9 @@ int sph_step_download(SphHandle* h, int32_t nsteps, SphState* state) {
     SPH_CUDA(cudaEventCreateWithFlags(&h->ev_sorted, cudaEventDisableTiming));
   }
   for (int s = 0; s + 1 < nsteps; ++s) SPH_CUDA(cudaGraphLaunch(h->graph, h->stream));
-  SPH_TRY(sync_dyn(h));
+  // rows to copy early: the count the host last read back, which the steps
+  // enqueued since can only have lowered (removals), so no wait is needed
+  // between the graph launches and the last step's launches
   EarlyCopy ec{state, h->h_dyn[0].nag, cudaSuccess};
   cudaStream_t q = h->stream;
   step_sequence(h, q, &ec);
@@ -1227,6 +1233,19 @@ int sph_eos(SphHandle* h) {
   return sync_dyn(h);
 }
 
+// ------------------------------------------------------- global quantities
+// fluid_global_quantities.f90:59-72 for simulation `sim` (out[8]) or, with
+// sim = -1, for every simulation of the handle (out[nsims][8]).
+int sph_global_quantities(SphHandle* h, int32_t sim, double* out) {
+  if (!h || !h->uploaded || !out || sim < -1 || sim >= h->nsims) return SPH_ERR_INVALID_ARGUMENT;
+  cudaStream_t q = h->stream;
+  launch_global_quantities(h->db, h->d_gq_part, h->d_gq_out, q);
+  SPH_CUDA(cudaGetLastError());
+  const size_t first = sim < 0 ? 0 : (size_t)sim, count = sim < 0 ? (size_t)h->nsims : 1;
+  SPH_CUDA(cudaMemcpyAsync(out, h->d_gq_out + 8 * first, sizeof(double) * 8 * count, cudaMemcpyDeviceToHost, q));
+  return sync_dyn(h);
+}
+
 // ---------------------------------------------------------------- verification
 int sph_dump_grid(SphHandle* h, int32_t* cella, int32_t* icont, int32_t* npartord) {
   if (!h || !h->uploaded || h->nsims != 1) return SPH_ERR_INVALID_ARGUMENT;
@@ -1292,6 +1311,17 @@ int sph_dump_boundary(SphHandle* h, int32_t max_per, int32_t* ncb, int32_t* clob
   cudaFree(dc);
   cudaFree(dv);
   return cuda_status(e);
+}
+
+int sph_dump_laminar(SphHandle* h, int32_t* flags) {
+  if (!h || !h->uploaded || h->nsims != 1 || !flags) return SPH_ERR_INVALID_ARGUMENT;
+  SPH_TRY(sync_dyn(h));
+  int n = h->h_dyn[0].nag;
+  cudaStream_t q = h->stream;
+  launch_dump_laminar(h->db, h->d_ci1, q);
+  SPH_CUDA(cudaGetLastError());
+  SPH_CUDA(cudaMemcpyAsync(flags, h->d_ci1, sizeof(int) * n, cudaMemcpyDeviceToHost, q));
+  return cuda_status(cudaStreamSynchronize(q));
 }
 
 int sph_dump_renormalisation(SphHandle* h, double* b_gradp, double* b_divu) {

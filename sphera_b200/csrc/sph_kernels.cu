@@ -2887,6 +2887,101 @@ __global__ void k_bdt_reset(DevBatch b) {
 }
 
 // ==========================================================================
+// Global quantities (fluid_global_quantities.f90:59-72): FP64 sums over the
+// fluid of mass, linear momentum, angular momentum about the origin
+// (Vector_Product.f90 of coord and vel) and volume m / rho.  The reference
+// sums sequentially in pg order; here each tile's particles are summed by a
+// fixed shuffle tree and the tiles of a simulation in tile order, every
+// addition compensated (a sum and its rounding error), so the result is the
+// exact sum up to a few ulps and does not depend on the launch shape.
+// ==========================================================================
+struct CSum {
+  double s, c;   // sum, accumulated rounding error
+};
+
+// TwoSum (Knuth) of the leading parts, the trailing parts added, then
+// renormalised so |c| stays below an ulp of s.
+__device__ __forceinline__ CSum csum_add(CSum a, CSum b) {
+  const double s = a.s + b.s;
+  const double bb = s - a.s;
+  const double e = (a.s - (s - bb)) + (b.s - bb);
+  const double c = (a.c + b.c) + e;
+  const double t = s + c;
+  return CSum{t, c - (t - s)};
+}
+
+__device__ __forceinline__ CSum csum_warp(CSum a) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    CSum b{__shfl_down_sync(0xffffffffu, a.s, o), __shfl_down_sync(0xffffffffu, a.c, o)};
+    a = csum_add(a, b);
+  }
+  return a;
+}
+
+constexpr int kGlobalQ = 8;
+
+// Per-tile compensated partial sums: part[t][q] = (s, c).
+__global__ void __launch_bounds__(kBlock) k_global_partials(DevBatch b, double2* part) {
+  __shared__ SimDev s;
+  __shared__ CSum ws[kBlock / 32][kGlobalQ];
+  int cur = -1;
+  const Particles& P = b.P;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
+    Tile tl = b.tiles[t];
+    load_sim(s, b.sims, tl.sim, cur);
+    const int p = tl.start + threadIdx.x;
+    double q[kGlobalQ];
+#pragma unroll
+    for (int k = 0; k < kGlobalQ; ++k) q[k] = 0.0;
+    if (threadIdx.x < tl.count && p < s.p_off + b.dyn[tl.sim].nag) {
+      const double4 x = P.X[p];
+      const double4 u = P.V[p];
+      const double m = x.w;
+      q[0] = m;
+      q[1] = m * u.x;
+      q[2] = m * u.y;
+      q[3] = m * u.z;
+      q[4] = m * (x.y * u.z - x.z * u.y);
+      q[5] = m * (x.z * u.x - x.x * u.z);
+      q[6] = m * (x.x * u.y - x.y * u.x);
+      q[7] = m / P.RP[p].x;
+    }
+#pragma unroll
+    for (int k = 0; k < kGlobalQ; ++k) {
+      CSum a = csum_warp(CSum{q[k], 0.0});
+      if (lane == 0) ws[warp][k] = a;
+    }
+    __syncthreads();
+    if (threadIdx.x < kGlobalQ) {
+      CSum a = ws[0][threadIdx.x];
+      for (int w = 1; w < kBlock / 32; ++w) a = csum_add(a, ws[w][threadIdx.x]);
+      part[(size_t)t * kGlobalQ + threadIdx.x] = make_double2(a.s, a.c);
+    }
+    __syncthreads();
+  }
+}
+
+// One warp per simulation: its tiles' partials in tile order (lane l takes
+// tiles l, l + 32, ...), then the fixed shuffle tree.
+__global__ void k_global_final(DevBatch b, const double2* __restrict__ part, double* out) {
+  const int sim = blockIdx.x;
+  const int lane = threadIdx.x;
+  const int t0 = b.sims[sim].p_off / kBlock;
+  const int t1 = t0 + (b.sims[sim].cap + kBlock - 1) / kBlock;
+  for (int k = 0; k < kGlobalQ; ++k) {
+    CSum a{0.0, 0.0};
+    for (int t = t0 + lane; t < t1; t += 32) {
+      const double2 v = part[(size_t)t * kGlobalQ + k];
+      a = csum_add(a, CSum{v.x, v.y});
+    }
+    a = csum_warp(a);
+    if (lane == 0) out[(size_t)sim * kGlobalQ + k] = a.s + a.c;
+  }
+}
+
+// ==========================================================================
 // Caller-order transfer and verification dumps
 // ==========================================================================
 __global__ void k_init_from_caller(DevBatch b, const double* x, const double* v, const double* rho, const double* p,
@@ -3029,6 +3124,21 @@ __global__ void k_dump_cella(DevBatch b, int* cella) {
     int c = 0;
     if (particle_cell(s, xi.x, xi.y, xi.z, i, j, k)) c = ((k - 1) * s.ncd[1] + (j - 1)) * s.ncd[0] + i;
     cella[(size_t)s.p_off + P.I[p] - 1] = c;
+  }
+}
+
+// pg%laminar_flag (inter_EqMoto.f90:269-283) of the last momentum pass, in
+// caller order.
+__global__ void k_dump_laminar(DevBatch b, int* flags) {
+  __shared__ SimDev s;
+  int cur = -1;
+  const Particles& P = b.P;
+  for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
+    Tile tl = b.tiles[t];
+    load_sim(s, b.sims, tl.sim, cur);
+    int p = tl.start + threadIdx.x;
+    if (threadIdx.x >= tl.count || p >= s.p_off + b.dyn[tl.sim].nag) continue;
+    flags[(size_t)s.p_off + P.I[p] - 1] = P.L[p];
   }
 }
 
@@ -3261,8 +3371,17 @@ void launch_dump_boundary(const DevBatch& b, int max_per, int* ncb, int* clob, d
 void launch_dump_renormalisation(const DevBatch& b, double* bg, double* bd, cudaStream_t st) {
   k_dump_renormalisation<<<blocks_for(b), kBlock, 0, st>>>(b, bg, bd);
 }
+void launch_global_quantities(const DevBatch& b, double2* part, double* out, cudaStream_t st) {
+  k_global_partials<<<blocks_for(b), kBlock, 0, st>>>(b, part);
+  k_global_final<<<b.nsims, 32, 0, st>>>(b, part, out);
+}
+
 void launch_dump_cella(const DevBatch& b, int* cella, cudaStream_t st) {
   k_dump_cella<<<blocks_for(b), kBlock, 0, st>>>(b, cella);
+}
+
+void launch_dump_laminar(const DevBatch& b, int* flags, cudaStream_t st) {
+  k_dump_laminar<<<blocks_for(b), kBlock, 0, st>>>(b, flags);
 }
 
 }  // namespace sph

@@ -82,6 +82,9 @@ void launch_dump_neighbours(const DevBatch& b, int nmaxj, int* counts, int* list
 void launch_dump_boundary(const DevBatch& b, int max_per, int* ncb, int* clob, double* vals, cudaStream_t st);
 void launch_dump_renormalisation(const DevBatch& b, double* bg, double* bd, cudaStream_t st);
 void launch_dump_cella(const DevBatch& b, int* cella, cudaStream_t st);
+void launch_dump_laminar(const DevBatch& b, int* flags, cudaStream_t st);
+// fluid_global_quantities: part [ntiles][8] scratch, out [nsims][8]
+void launch_global_quantities(const DevBatch& b, double2* part, double* out, cudaStream_t st);
 // FP64 FMA throughput probe: returns flops per launch
 double launch_fp64_probe(double* sink, int blocks, cudaStream_t st);
 double launch_fp32_probe(float* sink, int blocks, cudaStream_t st);

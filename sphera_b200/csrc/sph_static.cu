@@ -17,9 +17,18 @@
 // race on it and must be serialised by the caller.  The array keeps the
 // contents of the previous call; the counters are cleared at the start of
 // each call.
+//
+// Set-up: the first call in a device's context looks up the array's device
+// address (cudaGetSymbolAddress, which may load the module) and must come
+// before any stream capture on that device; later calls reuse the address
+// until the context changes (a cudaDeviceReset), when it is looked up again.
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <mutex>
+
+#include <cuda.h>
+#include <cuda_runtime.h>
 
 #include "../../include/sphera_b200.h"
 
@@ -168,10 +177,75 @@ __global__ void k_static_tail(int* icont, int ncells, const int* bsum, int nb, c
   }
 }
 
-// Scratch address of each device, taken once per device (cudaGetSymbolAddress
-// must run with that device current).
+// Scratch address of each device, taken once per device context
+// (cudaGetSymbolAddress must run with that device current).  The entry is
+// keyed on the context's process-unique id (cuCtxGetId, reached through
+// cudaGetDriverEntryPoint so the library needs no libcuda link): after a
+// cudaDeviceReset the runtime creates a new primary context, the module and
+// its array are loaded again, possibly at another address, and the next
+// call looks the address up afresh instead of using the old one.  A mutex
+// makes the check-then-store safe when several host threads call at once.
 constexpr int kMaxDevices = 64;
-int* g_scratch_ptr[kMaxDevices] = {nullptr};
+struct ScratchEntry {
+  unsigned long long ctx_id;
+  int* ptr;
+};
+ScratchEntry g_scratch[kMaxDevices] = {};
+std::mutex g_scratch_mutex;
+
+typedef CUresult (*PfnCtxGetCurrent)(CUcontext*);
+typedef CUresult (*PfnCtxGetId)(CUcontext, unsigned long long*);
+
+// Id of the context current on this thread; false if none can be had.
+bool current_context_id(unsigned long long* id) {
+  static PfnCtxGetCurrent get_current = nullptr;
+  static PfnCtxGetId get_id = nullptr;
+  if (!get_current || !get_id) {
+    void* f1 = nullptr;
+    void* f2 = nullptr;
+    cudaDriverEntryPointQueryResult q1 = cudaDriverEntryPointSymbolNotFound, q2 = q1;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f1, cudaEnableDefault, &q1) != cudaSuccess ||
+        cudaGetDriverEntryPoint("cuCtxGetId", &f2, cudaEnableDefault, &q2) != cudaSuccess ||
+        q1 != cudaDriverEntryPointSuccess || q2 != cudaDriverEntryPointSuccess || !f1 || !f2) {
+      cudaGetLastError();
+      return false;
+    }
+    get_current = (PfnCtxGetCurrent)f1;
+    get_id = (PfnCtxGetId)f2;
+  }
+  CUcontext ctx = nullptr;
+  if (get_current(&ctx) != CUDA_SUCCESS || !ctx) return false;
+  return get_id(ctx, id) == CUDA_SUCCESS;
+}
+
+// The device address of g_ordgrid_scratch in the current context of
+// device dev (looked up on the first call in that context).
+int scratch_address(int dev, int** out) {
+  unsigned long long id = 0;
+  if (!current_context_id(&id)) {
+    // no context current on this thread yet: cudaSetDevice initialises the
+    // device's primary context and makes it current, the context the
+    // kernels of this call will run in
+    if (cudaSetDevice(dev) != cudaSuccess) {
+      cudaGetLastError();
+      return SPH_ERR_NO_DEVICE;
+    }
+    if (!current_context_id(&id)) return SPH_ERR_CUDA;
+  }
+  std::lock_guard<std::mutex> lock(g_scratch_mutex);
+  ScratchEntry& e = g_scratch[dev];
+  if (!e.ptr || e.ctx_id != id) {
+    int* p = nullptr;
+    if (cudaGetSymbolAddress((void**)&p, g_ordgrid_scratch) != cudaSuccess || !p) {
+      cudaGetLastError();
+      return SPH_ERR_CUDA;
+    }
+    e.ptr = p;
+    e.ctx_id = id;
+  }
+  *out = e.ptr;
+  return SPH_OK;
+}
 
 }  // namespace
 
@@ -206,17 +280,13 @@ extern "C" int sph_ord_grid_static(const SphParams* params, int32_t n, const dou
     cudaGetLastError();
     return SPH_ERR_NO_DEVICE;
   }
-  // one-time set-up on this device (the first call on a device must not be
-  // inside a stream capture)
-  if (!g_scratch_ptr[dev]) {
-    int* p = nullptr;
-    if (cudaGetSymbolAddress((void**)&p, g_ordgrid_scratch) != cudaSuccess || !p) {
-      cudaGetLastError();
-      return SPH_ERR_CUDA;
-    }
-    g_scratch_ptr[dev] = p;
+  // set-up on the first call in this device's context (that call must not
+  // be inside a stream capture)
+  int* base = nullptr;
+  {
+    int st = scratch_address(dev, &base);
+    if (st != SPH_OK) return st;
   }
-  int* base = g_scratch_ptr[dev];
   int* counts = base;
   int* starts = counts + (kStaticMaxCells + 1);
   int* slot = starts + (kStaticMaxCells + 1);

@@ -5,6 +5,7 @@ alone while the other rank returns at once without work."""
 import json
 import os
 import socket
+import subprocess
 import sys
 
 import pytest
@@ -41,6 +42,30 @@ def _worker(rank, ws, port, out_dir):
     dist.destroy_process_group()
     with open(os.path.join(out_dir, f"r{rank}.json"), "w") as f:
         json.dump(res, f)
+
+
+@pytest.mark.timeout(180)
+def test_gpus_flag_starts_the_ranks():
+    """`python bench.py --gpus 2` without torchrun starts two ranks itself
+    (torch.distributed.run); the line rank 0 prints counts both."""
+    env = {k: v for k, v in os.environ.items() if k not in ("WORLD_SIZE", "RANK", "LOCAL_RANK")}
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--gpus", "2", "--dry-run"],
+                       capture_output=True, text=True, timeout=170, env=env)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [json.loads(x) for x in r.stdout.splitlines() if x.startswith("{")]
+    assert len(lines) == 1
+    assert lines[0]["n_gpus"] == 2
+    assert lines[0]["ranks_reporting"] == 2
+    assert lines[0]["rank_id_sum"] == 1
+
+
+def test_gpus_flag_must_match_the_ranks():
+    """Under a launcher that started fewer ranks than --gpus asks for, the
+    run refuses instead of reporting the wrong GPU count."""
+    env = dict(os.environ, WORLD_SIZE="1", RANK="0", LOCAL_RANK="0")
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--gpus", "2", "--dry-run"],
+                       capture_output=True, text=True, timeout=120, env=env)
+    assert r.returncode == 2
 
 
 @pytest.mark.timeout(120)

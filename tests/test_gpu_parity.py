@@ -155,14 +155,6 @@ def test_download_roundtrip_is_caller_order():
     assert np.array_equal(st.m, case.state.m)
 
 
-def test_full_size_dam_break_3d_rates(oracle_lib):
-    """864,000 particles (the 3D dam break at dx = 0.005): one IC pass of
-    neighbour counts and rates on the identical state."""
-    case = cases.dam_break_3d()
-    acc, dden, s = _rates_identical_state(case, oracle_lib, 0)
-    assert rel_l2(acc, s["acc"]) <= RATE_TOL
-
-
 def test_sloshing_forcing_follows_oracle(oracle_lib):
     """The lateral tank forcing (same sine sequence on host and device):
     the FP64 form follows the oracle as in the unforced cases."""

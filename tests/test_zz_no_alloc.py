@@ -51,6 +51,42 @@ def test_static_ord_grid_matches_regular_path(make):
         assert np.array_equal(npo.cpu().numpy(), ref_npo)
 
 
+def test_static_ord_grid_with_particles_outside_the_grid():
+    """Particles outside the grid get cella 0 and stay out of NPartOrd; the
+    rest is OrdGrid1 of the particles inside, with their own indices (the
+    static call removes nothing, unlike the regular path)."""
+    import torch
+    base = cases.dam_break_2d(dx=0.04)
+    x = base.state.x.copy()
+    out = np.array([3, 50, 51, 400])
+    x[out, 0] = base.params.domain_hi[0] + 5.0
+    keep = np.setdiff1d(np.arange(base.n), out)
+    st = base.state
+    inside = abi.State(x[keep], st.v[keep], st.rho[keep], st.p[keep], st.m[keep])
+    sim = Simulation(cases.Case(base.name, base.params, base.geometry, inside))
+    sim.upload(inside)
+    sub_cella, sub_icont, sub_npo = sim.dump_grid()
+    n = base.n
+    want_cella = np.zeros(n, np.int32)
+    want_cella[keep] = sub_cella
+    want_npo = (keep[sub_npo - 1] + 1).astype(np.int32)
+    xd = torch.tensor(x, dtype=torch.float64, device="cuda")
+    cella = torch.empty(n, dtype=torch.int32, device="cuda")
+    icont = torch.empty(len(sub_icont), dtype=torch.int32, device="cuda")
+    npo = torch.empty(n, dtype=torch.int32, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    for _ in range(2):
+        cella.fill_(-7)
+        icont.fill_(-7)
+        npo.fill_(-7)
+        rc = _static(base.params, xd, n, cella, icont, npo, stream)
+        torch.cuda.synchronize()
+        assert rc == abi.SPH_OK
+        assert np.array_equal(cella.cpu().numpy(), want_cella)
+        assert np.array_equal(icont.cpu().numpy(), sub_icont)
+        assert np.array_equal(npo.cpu().numpy()[:len(keep)], want_npo)
+
+
 def test_static_ord_grid_rejects_oversize():
     import torch
     case = cases.dam_break_2d()
