@@ -50,6 +50,8 @@ def lib():
         L.ora_get_c1.argtypes = [vp, dp, dp]
         L.ora_global_quantities.argtypes = [vp, dp]
         L.ora_laminar.argtypes = [vp, ip]
+        L.ora_convex_edges.argtypes = [vp, ip]
+        L.ora_convex_edges.restype = C.c_int
         L.ora_grid.argtypes = [vp, ip, ip, ip]
         L.ora_grid_info.argtypes = [vp, ip, dp, dp]
         L.ora_neighbours.argtypes = [vp, C.c_int, ip, ip]
@@ -168,6 +170,13 @@ class Oracle:
         out = np.zeros(8)
         lib().ora_global_quantities(self._h, abi.dptr(out))
         return out
+
+    def convex_edges(self):
+        """(n_edges, 2) face ids of the convex edges, in the order found."""
+        n = lib().ora_convex_edges(self._h, None)
+        f = np.zeros((max(n, 1), 2), np.int32)
+        lib().ora_convex_edges(self._h, abi.iptr(f))
+        return f[:n]
 
     def laminar(self):
         """pg%laminar_flag as the last momentum evaluation set it."""

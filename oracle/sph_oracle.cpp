@@ -114,6 +114,13 @@ struct Side {           // TyBoundarySide
   int previous_side;    // 1-based, 0 = none
 };
 
+struct ConvexEdge {     // TyBoundaryConvexEdge
+  int face[2];          // 1-based face ids
+  double GX1[3];        // node(1)%GX
+  double component[3];
+  double length;
+};
+
 struct BDT {            // TyBoundaryData
   int CloBoNum;
   double LocXYZ[3];
@@ -147,6 +154,7 @@ struct Oracle {
   // 3D faces
   std::vector<Face> faces;         // index nf-1
   std::vector<int> BFaceList;      // 1-based face ids
+  std::vector<ConvexEdge> BoundaryConvexEdge;
   std::vector<int> GCBFptr_n, GCBFptr_s;  // per cell (1-based)
   std::vector<int> GCBFVector;     // 1-based positions
   double kerneltab[ktrows + 1][5];
@@ -1557,12 +1565,75 @@ void inter_EqMoto(Oracle& o, int npi, double* tpres, double* tdiss, double* tvis
 }
 
 // AddElasticBoundaryReaction_3D.f90:67-154 (no convex edges)
+// FindBoundaryConvexEdges3D.f90:64-150.  The reference runs the kf loop in
+// parallel with the additions in a critical section, so its edge order
+// depends on the threads; this is the order of a serial run.  After its
+// first find for face nf the reference leaves the kf1 loop too (the second
+// `if (EdgeFound) exit`), so every face contributes at most one edge.
+void FindBoundaryConvexEdges3D(Oracle& o) {
+  const int iseg[2][4] = {{2, 3, 1, 0}, {2, 3, 4, 1}};
+  const int NumFacce = (int)o.BFaceList.size();
+  o.BoundaryConvexEdge.clear();
+  for (int kf = 1; kf <= NumFacce - 1; ++kf) {
+    const int nf = o.BFaceList[kf - 1];
+    const Face& F = o.faces[nf - 1];
+    const int nodes = F.nodes, fk = nodes - 2;
+    for (int kf1 = kf + 1; kf1 <= NumFacce; ++kf1) {
+      const int nf1 = o.BFaceList[kf1 - 1];
+      const Face& F1 = o.faces[nf1 - 1];
+      const int nodes1 = F1.nodes, fk1 = nodes1 - 2;
+      bool EdgeFound = false;
+      for (int i = 1; i <= nodes; ++i) {
+        const int j = iseg[fk - 1][i - 1];
+        const int nodi = F.name[i - 1], nodj = F.name[j - 1];
+        for (int ii = 1; ii <= nodes1; ++ii) {
+          const int jj = iseg[fk1 - 1][ii - 1];
+          const int nodii = F1.name[ii - 1], nodjj = F1.name[jj - 1];
+          if ((nodi == nodii && nodj == nodjj) || (nodi == nodjj && nodj == nodii)) {
+            const int kk = iseg[fk1 - 1][jj - 1];
+            const int nodkk = F1.name[kk - 1];
+            double zitakk = 0.0;
+            for (int sd = 0; sd < 3; ++sd)
+              zitakk = zitakk + F.T[sd][2] * (o.vert[3 * (nodkk - 1) + sd] - F.GX[nodes - 1][sd]);
+            if (zitakk < 0.0) {
+              ConvexEdge E;
+              E.face[0] = nf;
+              E.face[1] = nf1;
+              double length2 = 0.0;
+              for (int sd = 0; sd < 3; ++sd) {
+                E.GX1[sd] = o.vert[3 * (nodi - 1) + sd];
+                const double delta = o.vert[3 * (nodj - 1) + sd] - o.vert[3 * (nodi - 1) + sd];
+                E.component[sd] = delta;
+                length2 = length2 + delta * delta;
+              }
+              E.length = std::sqrt(length2);
+              o.BoundaryConvexEdge.push_back(E);
+              EdgeFound = true;
+              break;
+            }
+          }
+        }
+        if (EdgeFound) break;
+      }
+      if (EdgeFound) break;
+    }
+  }
+}
+
 void AddElasticBoundaryReaction_3D(const Oracle& o, int npi, int Ncbf, double* R) {
   const Particle& p = o.pg[npi];
   R[0] = R[1] = R[2] = 0.0;
   double zimin = 0.25 * o.prm.dx;
   double celer02 = o.prm.eps / o.prm.den0;
   int ibdt = o.BDP[3 * (npi - 1) + 2];
+  char rea_local[256];
+  std::vector<char> rea_heap;
+  char* ReaFace = rea_local;
+  if (Ncbf > 256) {
+    rea_heap.assign(Ncbf, 0);
+    ReaFace = rea_heap.data();
+  }
+  for (int icbf = 1; icbf <= Ncbf; ++icbf) ReaFace[icbf - 1] = 0;
   for (int icbf = 1; icbf <= Ncbf; ++icbf) {
     const BDT& e = o.BDTab[ibdt + icbf - 2];
     const Face& f = o.faces[e.CloBoNum - 1];
@@ -1576,6 +1647,37 @@ void AddElasticBoundaryReaction_3D(const Oracle& o, int npi, int Ncbf, double* R
         if (vin < 0.0) {
           double normreact = -(1.0 * celer02 * std::log((o.h + zi - zimin) / o.h) / o.h);
           for (int d = 0; d < 3; ++d) R[d] = R[d] + normreact * f.T[d][2];
+        }
+        ReaFace[icbf - 1] = true;
+      }
+    }
+  }
+  // AddElasticBoundaryReaction_3D.f90:106-153: reaction from close convex edges
+  for (const ConvexEdge& E : o.BoundaryConvexEdge) {
+    int NCloseEdgeF = 0;
+    for (int icbf = 1; icbf <= Ncbf; ++icbf) {
+      const int iface = o.BDTab[ibdt + icbf - 2].CloBoNum;
+      if (iface == E.face[0] && !ReaFace[icbf - 1]) NCloseEdgeF = NCloseEdgeF + 1;
+      else if (iface == E.face[1] && !ReaFace[icbf - 1]) NCloseEdgeF = NCloseEdgeF + 1;
+    }
+    if (NCloseEdgeF != 2) return;
+    double scaprod = 0.0;
+    for (int sd = 0; sd < 3; ++sd) scaprod = scaprod + (p.coord[sd] - E.GX1[sd]) * E.component[sd];
+    double edgelen2 = E.length * E.length;
+    double tau = scaprod / edgelen2;
+    if (tau >= 0.0 && tau <= 1.0) {
+      double edgedist2 = 0.0, XQ[3], QP[3];
+      for (int sd = 0; sd < 3; ++sd) XQ[sd] = E.GX1[sd] + E.component[sd] * tau;
+      for (int sd = 0; sd < 3; ++sd) QP[sd] = p.coord[sd] - XQ[sd];
+      for (int sd = 0; sd < 3; ++sd) edgedist2 = edgedist2 + QP[sd] * QP[sd];
+      double zi = std::sqrt(edgedist2);
+      if (zi < zimin) {
+        double vin = 0.0, QPcosdir[3];
+        for (int sd = 0; sd < 3; ++sd) QPcosdir[sd] = QP[sd] / zi;
+        for (int sd = 0; sd < 3; ++sd) vin = vin + p.var[sd] * QPcosdir[sd];
+        if (vin < 0.0) {
+          double normreact = -(1.0 * celer02 * std::log(zi / zimin) / zimin);
+          for (int sd = 0; sd < 3; ++sd) R[sd] = R[sd] + normreact * QPcosdir[sd];
         }
       }
     }
@@ -1941,6 +2043,7 @@ void* ora_create(const SphParams* prm, const SphGeometry* g, int n, const double
     for (int nt = 1; nt <= g->n_zones; ++nt)
       for (int f = 0; f < g->n_faces; ++f)
         if (o->faces[f].stretch == nt) o->BFaceList.push_back(f + 1);
+    FindBoundaryConvexEdges3D(*o);
     GridCellBoundaryFacesIntersections3D(*o);
     ComputeBoundaryIntegralTab(*o);
     ComputeKernelTable(*o);
@@ -2105,6 +2208,19 @@ int ora_get_c1(void* h, double* bg, double* bd) {
       }
   }
   return o.nag;
+}
+
+// The convex edges FindBoundaryConvexEdges3D found: their count, and the
+// two face ids of each in faces[2 * ne], [2 * ne + 1] (faces may be NULL).
+int ora_convex_edges(void* h, int* faces) {
+  Oracle& o = *static_cast<Oracle*>(h);
+  const int ne = (int)o.BoundaryConvexEdge.size();
+  if (faces)
+    for (int e = 0; e < ne; ++e) {
+      faces[2 * e] = o.BoundaryConvexEdge[e].face[0];
+      faces[2 * e + 1] = o.BoundaryConvexEdge[e].face[1];
+    }
+  return ne;
 }
 
 int ora_laminar(void* h, int* flags) {

@@ -92,6 +92,32 @@ def tank_3d(lx, ly, lz, zone=None):
     return abi.Geometry(V, [z], faces=F, face_zone=np.ones(len(F), dtype=np.int32))
 
 
+def tank_with_block_3d(lx, ly, lz, block, zone=None):
+    """The box tank plus a block standing on its floor, block = (x0, x1,
+    y0, y1, z1): five more quads (top and four sides; the base lies on the
+    floor) with normals pointing away from the block, into the fluid.  The
+    block's top and side edges are convex edges of the boundary
+    (FindBoundaryConvexEdges3D.f90)."""
+    V, F = _box_faces(lx, ly, lz)
+    x0, x1, y0, y1, z1 = block
+    B = np.array([[x0, y0, 0], [x1, y0, 0], [x1, y1, 0], [x0, y1, 0],
+                  [x0, y0, z1], [x1, y0, z1], [x1, y1, z1], [x0, y1, z1]], dtype=np.float64)
+    quads = [(5, 6, 7, 8), (1, 5, 6, 2), (4, 3, 7, 8), (1, 4, 8, 5), (2, 6, 7, 3)]
+    centre = B.mean(axis=0)
+    bf = []
+    for q in quads:
+        a, b, c, d = (B[i - 1] for i in q)
+        nrm = np.cross(a - d, c - d)
+        fc = (a + b + c + d) / 4.0
+        if np.dot(nrm, fc - centre) < 0:
+            q = q[::-1]
+        bf.append(tuple(i + len(V) for i in q))
+    V = np.vstack([V, B])
+    F = np.vstack([F, np.array(bf, dtype=np.int32)])
+    z = zone or abi.make_zone()
+    return abi.Geometry(V, [z], faces=F, face_zone=np.ones(len(F), dtype=np.int32))
+
+
 def tank_2d(lx, lz, zone=None):
     # counter-clockwise in the x-z plane: the side normal (-sz, sx) points inside
     V = np.array([[0, 0, 0], [lx, 0, 0], [lx, 0, lz], [0, 0, lz]], dtype=np.float64)
@@ -136,6 +162,29 @@ def dam_break_3d(dx=0.005, tank=(1.6, 0.6, 0.6), block=(0.6, 0.3, 0.6), jitter=0
     st = abi.State(x, np.zeros_like(x), rho, p, m)
     return Case("dam_break_3d", prm, tank_3d(*tank), st,
                 dict(dx=dx, tank=tank, block=block, seed=seed, t_end=0.5))
+
+
+def block_tank_3d(dx=0.02, tank=(0.4, 0.2, 0.3), block=(0.15, 0.25, 0.05, 0.15, 0.1), level=0.2, jitter=0.01,
+                  seed=0xC6, precision=abi.SPH_PREC_FP64):
+    """Still water to `level` in a box tank around a block standing on its
+    floor (tank_with_block_3d): a geometry with convex edges.  Lattice points
+    closer than dx / 2 to the block are left out."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    nx, ny, nz = (int(round(v / dx)) for v in (tank[0], tank[1], level))
+    i, j, k = np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing="ij")
+    x = np.stack([(i.ravel() + 0.5) * dx, (j.ravel() + 0.5) * dx, (k.ravel() + 0.5) * dx], axis=1)
+    x0, x1, y0, y1, z1 = block
+    h = dx / 2
+    inside = ((x[:, 0] > x0 - h) & (x[:, 0] < x1 + h) & (x[:, 1] > y0 - h) & (x[:, 1] < y1 + h)
+              & (x[:, 2] < z1 + h))
+    x = x[~inside]
+    x += _jitter(rng, x.shape, dx, jitter)
+    prm = _params(3, dx, (0.0, 0.0, 0.0), tank, precision=precision)
+    p, rho = _hydrostatic(x[:, 2], dx, prm.den0, prm.eps, prm.p_ref)
+    m = np.full(len(p), dx ** 3 * prm.den0)
+    st = abi.State(x, np.zeros_like(x), rho, p, m)
+    return Case("block_tank_3d", prm, tank_with_block_3d(*tank, block), st,
+                dict(dx=dx, tank=tank, block=block, level=level, seed=seed))
 
 
 def random_box(n=16_000_000, spacing=0.01, seed=0xC2, precision=abi.SPH_PREC_FP64):

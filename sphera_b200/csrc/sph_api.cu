@@ -56,6 +56,7 @@ struct HostSim {
   SimDev dev{};
   std::vector<FaceDev> faces;
   std::vector<SideDev> sides;
+  std::vector<EdgeDev> edges;          // convex edges (3D)
   std::vector<double> bit;             // 256 x 7
   std::vector<int> cf_count, cf_start, cf_list;
   std::vector<uint8_t> near;
@@ -363,6 +364,58 @@ int prepare_sim(const SphParams& prm, const SphGeometry& g, int cap, HostSim& hs
     for (int nt = 1; nt <= g.n_zones; ++nt)
       for (int f = 0; f < g.n_faces; ++f)
         if (geo[f].zone == nt) bface.push_back(f + 1);
+    // FindBoundaryConvexEdges3D.f90:64-150: for each face of BFaceList, the
+    // first later face that shares a side with it, when the shared side is
+    // convex (the other face's next node lies behind the first face's
+    // plane).  Each face contributes at most one edge, as the reference's
+    // loop exits after its first find.  The reference runs the face loop in
+    // parallel, so its edge order depends on the threads; this is the order
+    // of a serial run.
+    hs.edges.clear();
+    {
+      const int iseg[2][4] = {{2, 3, 1, 0}, {2, 3, 4, 1}};
+      auto name = [&](int nf, int i) { return g.face_nodes[4 * (nf - 1) + (i - 1)]; };
+      const int nbf = (int)bface.size();
+      for (int kf = 0; kf + 1 < nbf; ++kf) {
+        const int nf = bface[kf];
+        const FaceGeo& F = geo[nf - 1];
+        const int nodes = F.nodes, fk = nodes - 2;
+        bool found = false;
+        for (int kf1 = kf + 1; kf1 < nbf && !found; ++kf1) {
+          const int nf1 = bface[kf1];
+          const int nodes1 = geo[nf1 - 1].nodes, fk1 = nodes1 - 2;
+          for (int i = 1; i <= nodes && !found; ++i) {
+            const int nodi = name(nf, i), nodj = name(nf, iseg[fk - 1][i - 1]);
+            for (int ii = 1; ii <= nodes1; ++ii) {
+              const int jj = iseg[fk1 - 1][ii - 1];
+              const int nodii = name(nf1, ii), nodjj = name(nf1, jj);
+              if (!((nodi == nodii && nodj == nodjj) || (nodi == nodjj && nodj == nodii))) continue;
+              const int nodkk = name(nf1, iseg[fk1 - 1][jj - 1]);
+              double zitakk = 0.0;
+              for (int sd = 0; sd < 3; ++sd) zitakk = zitakk + F.T[sd][2] * (vtx(nodkk, sd) - F.GX[nodes - 1][sd]);
+              if (zitakk < 0.0) {
+                EdgeDev E;
+                std::memset(&E, 0, sizeof(E));
+                E.face[0] = nf;
+                E.face[1] = nf1;
+                double length2 = 0.0;
+                for (int sd = 0; sd < 3; ++sd) {
+                  E.gx[sd] = vtx(nodi, sd);
+                  const double delta = vtx(nodj, sd) - vtx(nodi, sd);
+                  E.comp[sd] = delta;
+                  length2 = length2 + delta * delta;
+                }
+                E.length = std::sqrt(length2);
+                hs.edges.push_back(E);
+                found = true;
+                break;
+              }
+            }
+          }
+        }
+      }
+    }
+    s.nedges = (int)hs.edges.size();
     // GridCellBoundaryFacesIntersections3D.f90:89-210, stored by sort key
     hs.cf_count.assign(s.ncells + 1, 0);
     hs.cf_start.assign(s.ncells + 1, 0);
@@ -538,6 +591,7 @@ struct SphHandle {
   Tile* d_tiles = nullptr;
   FaceDev* d_faces = nullptr;
   SideDev* d_sides = nullptr;
+  EdgeDev* d_edges = nullptr;
   double* d_bit = nullptr;
   int *d_cf_start = nullptr, *d_cf_count = nullptr, *d_cf_list = nullptr;
   uint8_t* d_near = nullptr;
@@ -745,7 +799,7 @@ int create_batch(int nsims, const SphParams* params, const SphGeometry* geoms, c
   }
   // layout of the concatenated arrays; simulations start on tile boundaries
   std::vector<Tile> tiles;
-  int poff = 0, coff = 0, foff = 0, soff = 0;
+  int poff = 0, coff = 0, foff = 0, soff = 0, eoff = 0;
   size_t bdt_cap = 0;
   for (int s = 0; s < nsims; ++s) {
     HostSim& hs = h->sims[s];
@@ -754,6 +808,7 @@ int create_batch(int nsims, const SphParams* params, const SphGeometry* geoms, c
     hs.dev.cell_off = coff;
     hs.dev.face_off = foff;
     hs.dev.side_off = soff;
+    hs.dev.edge_off = eoff;
     // tiles cover the padded segment: every slot, padding included, takes
     // part in the sort, so each simulation's segment stays in place
     for (int t = 0; t < hs.cap; t += kBlock) {
@@ -769,6 +824,7 @@ int create_batch(int nsims, const SphParams* params, const SphGeometry* geoms, c
     coff += hs.dev.ncells + 1;
     foff += (int)hs.faces.size();
     soff += (int)hs.sides.size();
+    eoff += (int)hs.edges.size();
     // default: room for three close faces (two close sides) per particle,
     // a box corner's worth; the reference reserves MAXCLOSEBOUNDFACES per
     // particle (Gest_Trans.f90:90), far more than a flow uses
@@ -796,6 +852,7 @@ int create_batch(int nsims, const SphParams* params, const SphGeometry* geoms, c
   A(h->d_tiles, tiles.size());
   A(h->d_faces, foff);
   A(h->d_sides, soff);
+  A(h->d_edges, eoff);
   A(h->d_bit, (size_t)nsims * kBitRows * 7);
   A(h->d_cf_start, C);
   A(h->d_cf_count, C);
@@ -832,6 +889,7 @@ int create_batch(int nsims, const SphParams* params, const SphGeometry* geoms, c
   std::vector<SimDev> hsd(nsims);
   std::vector<FaceDev> hf;
   std::vector<SideDev> hsi;
+  std::vector<EdgeDev> hed;
   std::vector<double> hbit;
   std::vector<int> cfs(C, 0), cfc(C, 0), cfl;
   std::vector<uint8_t> nr(C, 0);
@@ -840,6 +898,7 @@ int create_batch(int nsims, const SphParams* params, const SphGeometry* geoms, c
     hsd[s] = hs.dev;
     hf.insert(hf.end(), hs.faces.begin(), hs.faces.end());
     hsi.insert(hsi.end(), hs.sides.begin(), hs.sides.end());
+    hed.insert(hed.end(), hs.edges.begin(), hs.edges.end());
     hbit.insert(hbit.end(), hs.bit.begin(), hs.bit.end());
     int base = (int)cfl.size();
     for (int k = 0; k < hs.dev.ncells; ++k) {
@@ -869,6 +928,7 @@ int create_batch(int nsims, const SphParams* params, const SphGeometry* geoms, c
   if (e == cudaSuccess) e = cudaMemcpyAsync(h->d_tiles, tiles.data(), sizeof(Tile) * tiles.size(), cudaMemcpyHostToDevice, q);
   if (e == cudaSuccess && !hf.empty()) e = cudaMemcpyAsync(h->d_faces, hf.data(), sizeof(FaceDev) * hf.size(), cudaMemcpyHostToDevice, q);
   if (e == cudaSuccess && !hsi.empty()) e = cudaMemcpyAsync(h->d_sides, hsi.data(), sizeof(SideDev) * hsi.size(), cudaMemcpyHostToDevice, q);
+  if (e == cudaSuccess && !hed.empty()) e = cudaMemcpyAsync(h->d_edges, hed.data(), sizeof(EdgeDev) * hed.size(), cudaMemcpyHostToDevice, q);
   if (e == cudaSuccess) e = cudaMemcpyAsync(h->d_bit, hbit.data(), sizeof(double) * hbit.size(), cudaMemcpyHostToDevice, q);
   if (e == cudaSuccess) e = cudaMemcpyAsync(h->d_cf_start, cfs.data(), sizeof(int) * C, cudaMemcpyHostToDevice, q);
   if (e == cudaSuccess) e = cudaMemcpyAsync(h->d_cf_count, cfc.data(), sizeof(int) * C, cudaMemcpyHostToDevice, q);
@@ -894,6 +954,7 @@ int create_batch(int nsims, const SphParams* params, const SphGeometry* geoms, c
   b.P = P;
   b.faces = h->d_faces;
   b.sides = h->d_sides;
+  b.edges = h->d_edges;
   b.bit = h->d_bit;
   b.cf_start = h->d_cf_start;
   b.cf_count = h->d_cf_count;

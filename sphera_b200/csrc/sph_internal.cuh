@@ -45,6 +45,7 @@ struct SimDev {
   int maxcb;              // MAXCLOSEBOUNDFACES (3D) / MAXCLOSEBOUNDSIDES (2D)
   int face_off, nfaces;   // faces (3D)
   int side_off, nsides;   // sides (2D)
+  int edge_off, nedges;   // convex edges (3D)
   int dt_alfa_mon, density_thresholds;
   double h, doubleh, squareh, square_doubleh, eta, eta2;
   double coefke, coefkacl, ke_coef, kacl_coef;
@@ -95,6 +96,15 @@ struct FaceDev {
   int laminar_no_slip_check;
   int zone_type;
   int pad;
+};
+
+// Convex edge shared by two solid faces (TyBoundaryConvexEdge), found on the
+// host as FindBoundaryConvexEdges3D.f90 does.
+struct EdgeDev {
+  int face[2];            // the two faces, 1-based within the simulation
+  double gx[3];           // node(1)%GX
+  double comp[3];         // node(2)%GX - node(1)%GX
+  double length;
 };
 
 // Boundary side (TyBoundarySide, 2D) prepared on the host.

@@ -55,14 +55,16 @@ __device__ __forceinline__ bool particle_cell(const SimDev& s, double x, double 
   return true;
 }
 
-// FP32 offset of a particle from the origin of its cell (w: the cell's k).
+// FP32 offset of a particle from the origin of its cell; w holds the cell's
+// k index as a float (exact: k < 2^24), so cell differences are FP32
+// subtractions, exact, with no integer-to-float conversion in the pair loops.
 __device__ __forceinline__ float4 screening_copy(const SimDev& s, const double4& x) {
   int i, j, k;
-  if (!particle_cell(s, x.x, x.y, x.z, i, j, k)) return make_float4(0.f, 0.f, 0.f, __int_as_float(-8));
+  if (!particle_cell(s, x.x, x.y, x.z, i, j, k)) return make_float4(0.f, 0.f, 0.f, -8.0f);
   double ox = s.extr_lo[0] + s.dcd[0] * (i - 1);
   double oy = (s.dim == 3) ? s.extr_lo[1] + s.dcd[1] * (j - 1) : 0.0;
   double oz = s.extr_lo[2] + s.dcd[2] * (k - 1);
-  return make_float4((float)(x.x - ox), (float)(x.y - oy), (float)(x.z - oz), __int_as_float(k));
+  return make_float4((float)(x.x - ox), (float)(x.y - oy), (float)(x.z - oz), (float)k);
 }
 
 // Contiguous slot range of neighbour column r (reference order: y, then x).
@@ -1070,9 +1072,11 @@ __device__ __forceinline__ void me_boundary2d(const SimDev& s, const DevBatch& b
   }
 }
 
-// AddElasticBoundaryReaction_3D.f90:67-154 (no convex edges) / _2D.f90:63-97.
+// AddElasticBoundaryReaction_3D.f90:67-154 / _2D.f90:63-97; xi is
+// pg%coord, vi pg%var (= pg%vel).
 template <int DIM>
-__device__ __forceinline__ void elastic_reaction(const SimDev& s, const DevBatch& b, int nb, int start, const double* vi, double* R) {
+__device__ __forceinline__ void elastic_reaction(const SimDev& s, const DevBatch& b, int nb, int start, const double* xi,
+                                                 const double* vi, double* R) {
   R[0] = R[1] = R[2] = 0.0;
   double zimin = 0.25 * s.dx;
   double celer02 = s.eps / s.den0;
@@ -1101,6 +1105,46 @@ __device__ __forceinline__ void elastic_reaction(const SimDev& s, const DevBatch
           double normreact = -(1.0 * celer02 * log((s.h + ypi - zimin) / s.h) / s.h);
           R[0] = R[0] + normreact * S.nnn[0];
           R[2] = R[2] + normreact * S.nnn[1];
+        }
+      }
+    }
+  }
+  if (DIM == 3 && s.nedges > 0) {
+    // Reaction from close convex edges (AddElasticBoundaryReaction_3D.f90:106-153).
+    // ReaFace(icbf) -- the face term above applied its test to the entry --
+    // is recomputed from the entry here.  An edge counts only when both of
+    // its faces are close faces of the particle without a face reaction;
+    // the reference leaves the routine at the first edge that fails this,
+    // and so does this loop.
+    auto rea_face = [&](const BdtEntry& e) {
+      const FaceDev& f = b.faces[s.face_off + e.clobonum - 1];
+      return e.loc[2] < zimin && point_internal(f, e.loc[0], e.loc[1]);
+    };
+    for (int ne = 0; ne < s.nedges; ++ne) {
+      const EdgeDev& E = b.edges[s.edge_off + ne];
+      int nclose = 0;
+      for (int u = 0; u < nb; ++u) {
+        const BdtEntry& e = b.P.bdt[start + u];
+        if ((e.clobonum == E.face[0] || e.clobonum == E.face[1]) && !rea_face(e)) nclose++;
+      }
+      if (nclose != 2) break;
+      double scaprod = 0.0;
+      for (int sd = 0; sd < 3; ++sd) scaprod = scaprod + (xi[sd] - E.gx[sd]) * E.comp[sd];
+      const double edgelen2 = E.length * E.length;
+      const double tau = scaprod / edgelen2;
+      if (tau >= 0.0 && tau <= 1.0) {
+        double QP[3], edgedist2 = 0.0;
+        for (int sd = 0; sd < 3; ++sd) QP[sd] = xi[sd] - (E.gx[sd] + E.comp[sd] * tau);
+        for (int sd = 0; sd < 3; ++sd) edgedist2 = edgedist2 + QP[sd] * QP[sd];
+        const double zi = sqrt(edgedist2);
+        if (zi < zimin) {
+          double cosdir[3], vin = 0.0;
+          for (int sd = 0; sd < 3; ++sd) cosdir[sd] = QP[sd] / zi;
+          for (int sd = 0; sd < 3; ++sd) vin = vin + vi[sd] * cosdir[sd];
+          if (vin < 0.0) {
+            const double normreact = -(1.0 * celer02 * log(zi / zimin) / zimin);
+            for (int sd = 0; sd < 3; ++sd) R[sd] = R[sd] + normreact * cosdir[sd];
+          }
         }
       }
     }
@@ -1182,7 +1226,7 @@ template <int DIM, bool REBASE>
 __device__ __forceinline__ float screen_rf(const float4& xj, float ax, float ay, float zi, float fz, int ck, float dz) {
   float d0 = ax - xj.x;
   float d1 = (DIM == 3) ? ay - xj.y : 0.f;
-  float d2 = REBASE ? zi - xj.z : ((float)(ck - __float_as_int(xj.w)) * dz + fz) - xj.z;
+  float d2 = REBASE ? zi - xj.z : (((float)ck - xj.w) * dz + fz) - xj.z;
   return __fmaf_rn(d2, d2, __fmaf_rn(d1, d1, __fmul_rn(d0, d0)));
 }
 
@@ -1272,9 +1316,11 @@ __device__ __forceinline__ void screen_tile_x2(const float* nx, const float* ny,
 
 // Whether any staged candidate u0 <= u < nt lies in the lane's 3-cell z
 // window (the truncation test once NMAXPARTJ is reached; rare).
+__device__ __forceinline__ bool in_window(float kj, int ck) { return fabsf(kj - (float)ck) <= 1.0f; }
+
 __device__ __forceinline__ bool window_candidate(const float4* wbuf, int u0, int nt, int ck) {
   for (int u = u0; u < nt; ++u)
-    if ((unsigned)(__float_as_int(wbuf[u].w) - (ck - 1)) <= 2u) return true;
+    if (in_window(wbuf[u].w, ck)) return true;
   return false;
 }
 
@@ -1349,8 +1395,8 @@ __global__ void __launch_bounds__(kBlock, 4) k_neighbour_lists(DevBatch b) {
         const int tag = r << kSlotBits;
         for (int c0 = ub; c0 < ue; c0 += 32) {
           int cidx = c0 + lane;
-          float4 st = (cidx < ue) ? P.XF[cidx] : make_float4(3.0e18f, 3.0e18f, 3.0e18f, __int_as_float(-0x3fffffff));
-          if (rebase && cidx < ue) st.z = (float)(__float_as_int(st.w) - kmin) * dz + st.z;
+          float4 st = (cidx < ue) ? P.XF[cidx] : make_float4(3.0e18f, 3.0e18f, 3.0e18f, -1.0e9f);
+          if (rebase && cidx < ue) st.z = (st.w - (float)kmin) * dz + st.z;
           __syncwarp();
           wbuf[lane] = st;
           if (rebase) {
@@ -1377,7 +1423,7 @@ __global__ void __launch_bounds__(kBlock, 4) k_neighbour_lists(DevBatch b) {
           while (band) {
             int u = __ffs(band) - 1;
             band &= band - 1;
-            bool keep = (unsigned)(__float_as_int(wbuf[u].w) - (ck - 1)) <= 2u;
+            bool keep = in_window(wbuf[u].w, ck);
             if (keep) {
               double4 xq = P.X[c0 + u], xi = P.X[p];
               double r0 = xi.x - xq.x, r1 = xi.y - xq.y, r2 = xi.z - xq.z;
@@ -1674,7 +1720,8 @@ __global__ void __launch_bounds__(kBlock, 2) k_momentum(DevBatch b) {
       acc[2] = tpres[2] + td2 + tv2 + geff[2];
       if (nb > 0) {
         double R[3];
-        elastic_reaction<DIM>(s, b, nb, bstart, vi, R);
+        const double xa[3] = {xi.x, xi.y, xi.z};
+        elastic_reaction<DIM>(s, b, nb, bstart, xa, vi, R);
         for (int d = 0; d < 3; ++d) acc[d] = acc[d] + R[d];
       }
       if (FUSED) {
@@ -1943,40 +1990,85 @@ struct F32Const {
   }
 };
 
-// FAST: r from the reciprocal square root (rr > 0: list pairs are distinct
-// particles), else the correctly rounded sqrtf.
-template <bool FAST>
+// The PTX approximate reciprocal and reciprocal square root (one special
+// function unit instruction each, relative error about 2^-23, subnormals
+// flushed): the FP32c pair terms' divisions and square roots.
+__device__ __forceinline__ float rcp_approx(float x) {
+  float y;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
+__device__ __forceinline__ float rsqrt_approx(float x) {
+  float y;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
+// Distance of a list pair from its squared distance: rr is positive for any
+// two particles of distinct positions; the floor keeps r finite (0) should
+// two FP32 offsets coincide.
+__device__ __forceinline__ float pair_distance(float rr) {
+  const float rq = fmaxf(rr, 1.0e-30f);
+  return rq * rsqrt_approx(rq);
+}
+
+// Beta-spline gradient factors of a list pair (CalcVarLength.f90:230-262):
+// PK1 = g ke / (r + eta), PK2 = PK1 / (rr + eta2), PK3 = gw kacl / (r + eta).
+// The two divisions share one reciprocal: 1/a = b/(ab), 1/b = a/(ab).  A
+// list pair has r <= 2h in FP64; its FP32 q may round a hair past 2, where
+// both polynomials vanish to within rounding, so no support test is needed.
 __device__ __forceinline__ void kernel_values_f32(const F32Const& c, float rr, float& PK1, float& PK2, float& PK3) {
-  float r = FAST ? rr * rsqrtf(rr) : sqrtf(rr);
-  float q = r * c.hinv;
-  float q2 = rr * c.h2inv;
-  if (q >= 2.0f) {
-    PK1 = 0.f;
-    PK2 = 0.f;
-    PK3 = 0.f;
-    return;
-  }
-  float denom = __fdividef(1.0f, r + c.eta);
-  float g = (q < 1.0f) ? fmaf(1.5f, q2, -2.0f * q) : fmaf(-0.5f, q2, fmaf(2.0f, q, -2.0f));
-  float gw = fmaf(12.0f, q, fmaf(-3.0f, q2, -12.0f));
+  const float r = pair_distance(rr);
+  const float q = r * c.hinv;
+  const float q2 = rr * c.h2inv;
+  const float a = r + c.eta, bq = rr + c.eta2;
+  const float inv = rcp_approx(a * bq);
+  const float denom = bq * inv;
+  const float g = (q < 1.0f) ? fmaf(1.5f, q2, -2.0f * q) : fmaf(-0.5f, q2, fmaf(2.0f, q, -2.0f));
+  const float gw = fmaf(12.0f, q, fmaf(-3.0f, q2, -12.0f));
   PK1 = g * c.ke * denom;
-  PK2 = __fdividef(PK1, rr + c.eta2);
+  PK2 = PK1 * (a * inv);
   PK3 = gw * c.kacl * denom;
 }
 
-// FP32 separation from a neighbour's XF record xj reached through run r,
-// the run's cell-origin offset formed from the particle's column.
+// PK1 alone (the continuity pass).
+__device__ __forceinline__ float kernel_pk1_f32(const F32Const& c, float rr) {
+  const float r = pair_distance(rr);
+  const float q = r * c.hinv;
+  const float q2 = rr * c.h2inv;
+  const float g = (q < 1.0f) ? fmaf(1.5f, q2, -2.0f * q) : fmaf(-0.5f, q2, fmaf(2.0f, q, -2.0f));
+  return g * c.ke * rcp_approx(r + c.eta);
+}
+
+// Cell-origin offset of the neighbour column (run) a list entry names.  A
+// lane's entries are stored run by run, so the offsets are formed again only
+// when the run changes: (ci - ir) dcd = (1 - rx) dcd for the run's x column
+// rx = r % 3 (r in 2D) and likewise in y.
 template <int DIM>
-__device__ __forceinline__ void separation_cols(const SimDev& s, int r, const float4& xj, const float4& xfi, int ci,
-                                               int cj, int ck, float& d0, float& d1, float& d2) {
-  int jr = (DIM == 3) ? cj - 1 + r / 3 : cj;
-  int ir = ci - 1 + ((DIM == 3) ? r % 3 : r);
-  float Dx = (float)(ci - ir) * s.dcdf[0];
-  float Dy = (DIM == 3) ? (float)(cj - jr) * s.dcdf[1] : 0.f;
-  float Dz = (float)(ck - __float_as_int(xj.w)) * s.dcdf[2];
-  d0 = Dx + (xfi.x - xj.x);
-  d1 = (DIM == 3) ? Dy + (xfi.y - xj.y) : 0.f;
-  d2 = Dz + (xfi.z - xj.z);
+struct RunCursor {
+  int r = -1;
+  float Dx = 0.f, Dy = 0.f;
+  __device__ __forceinline__ void update(const SimDev& s, int run) {
+    if (run == r) return;
+    r = run;
+    const int rx = (DIM == 3) ? run % 3 : run;
+    Dx = (float)(1 - rx) * s.dcdf[0];
+    Dy = (DIM == 3) ? (float)(1 - run / 3) * s.dcdf[1] : 0.f;
+  }
+};
+
+// FP32 separation x_i - x_j of list entry e with neighbour record xj: the
+// cell-origin difference (run offsets in x and y, (k_i - k_j) dcd in z, all
+// exact small multiples) plus the offsets' difference.
+template <int DIM>
+__device__ __forceinline__ void separation_f32(const SimDev& s, RunCursor<DIM>& rc, int e, const float4& xj,
+                                               const float4& xfi, float ckf, float dz, float& d0, float& d1,
+                                               float& d2) {
+  rc.update(s, (int)((unsigned)e >> kSlotBits));
+  d0 = rc.Dx + (xfi.x - xj.x);
+  d1 = (DIM == 3) ? rc.Dy + (xfi.y - xj.y) : 0.f;
+  d2 = (ckf - xj.w) * dz + (xfi.z - xj.z);
 }
 
 // Momentum, FP32c form, in two launches.  k_momentum_f32 holds only what
@@ -2001,14 +2093,12 @@ __global__ void __launch_bounds__(kBlock, 3) k_momentum_f32(DevBatch b) {
     SimDyn* dyn = b.dyn + tl.sim;
     int p = tl.start + threadIdx.x;
     const bool active = threadIdx.x < tl.count && p < s.p_off + dyn->nag && !dyn->frozen;
-    int ci = 0, cj = 0, ck = 0, cnt = 0;
+    int cnt = 0;
     float4 xfi = make_float4(0.f, 0.f, 0.f, 0.f);
     float vix = 0.f, viy = 0.f, viz = 0.f, rhof = 1.f, Pi = 0.f;
     if (active) {
-      double4 xi = P.X[p];
       double4 v4 = P.V[p];
       double2 rp = P.RP[p];
-      particle_cell(s, xi.x, xi.y, xi.z, ci, cj, ck);
       xfi = P.XF[p];
       vix = (float)v4.x;
       viy = (float)v4.y;
@@ -2017,6 +2107,8 @@ __global__ void __launch_bounds__(kBlock, 3) k_momentum_f32(DevBatch b) {
       Pi = (float)(rp.y / (rp.x * rp.x));
       cnt = b.ncount[p];
     }
+    const float ckf = xfi.w, dz = s.dcdf[2];
+    RunCursor<DIM> rc;
     const bool morris = s.kin_visc > 1.0e-12;
     // compensated sums of 4-entry partial sums (one list chunk each)
     Kahan tp0, tp1, tp2, td0, td1, td2, tv0, tv1, tv2;
@@ -2030,12 +2122,12 @@ __global__ void __launch_bounds__(kBlock, 3) k_momentum_f32(DevBatch b) {
     int4 nxt = nch > 0 ? __ldg(lbase) : make_int4(0, 0, 0, 0);
     auto pair = [&](int e) {
       const int q = e & kSlotMask;
-      const float4 xj = P.XF[q], vj = P.VF[q], rfj = P.RF[q];
+      const float4 xj = __ldg(P.XF + q), vj = __ldg(P.VF + q), rfj = __ldg(P.RF + q);
       float d0, d1, d2;
-      separation_cols<DIM>(s, (int)((unsigned)e >> kSlotBits), xj, xfi, ci, cj, ck, d0, d1, d2);
+      separation_f32<DIM>(s, rc, e, xj, xfi, ckf, dz, d0, d1, d2);
       float rr = fmaf(d2, d2, fmaf(d1, d1, d0 * d0));
       float PK1, PK2, PK3;
-      kernel_values_f32<true>(fc, rr, PK1, PK2, PK3);
+      kernel_values_f32(fc, rr, PK1, PK2, PK3);
       float mj = rfj.z;
       // pressure (both accumulators of inter_EqMoto together)
       float pf = -(mj * (Pi + rfj.y) * PK3);
@@ -2043,16 +2135,18 @@ __global__ void __launch_bounds__(kBlock, 3) k_momentum_f32(DevBatch b) {
       if (DIM == 3) cp1 = fmaf(pf, d1, cp1);
       cp2 = fmaf(pf, d2, cp2);
       float dv0 = vj.x - vix, dv1 = vj.y - viy, dv2 = vj.z - viz;
-      float rsum = rhof + rfj.x;
-      // viscomon
+      // viscomon amon / rsum and viscomorris nu4 / (nu rsum + 1e-3) from one
+      // reciprocal of their denominators' product
+      const float rsum = rhof + rfj.x;
+      const float bm = fmaf(fc.nu, rsum, 1.0e-3f);
+      const float iv = rcp_approx(rsum * bm);
       float vr = -fmaf(dv2, d2, fmaf(dv1, d1, dv0 * d0));
-      float df = mj * __fdividef(fc.amon, rsum) * vr * PK2;
+      float df = mj * (fc.amon * (bm * iv)) * vr * PK2;
       cd0 = fmaf(df, d0, cd0);
       if (DIM == 3) cd1 = fmaf(df, d1, cd1);
       cd2 = fmaf(df, d2, cd2);
-      // viscomorris
       if (morris) {
-        float vf = -(__fdividef(mj * fc.nu4, fmaf(fc.nu, rsum, 1.0e-3f)) * PK2 * rr);
+        float vf = -((mj * fc.nu4) * (rsum * iv) * PK2 * rr);
         cv0 = fmaf(vf, dv0, cv0);
         if (DIM == 3) cv1 = fmaf(vf, dv1, cv1);
         cv2 = fmaf(vf, dv2, cv2);
@@ -2144,13 +2238,14 @@ __global__ void __launch_bounds__(kBlock) k_momentum_f32_finish(DevBatch b) {
       acc[0] = tpres[0] + (tdiss[0] + ms[3]) + (tvisc[0] + rs0) + geff[0];
       acc[1] = tpres[1] + (tdiss[1] + ms[4]) + (tvisc[1] + rs1) + geff[1];
       acc[2] = tpres[2] + (tdiss[2] + ms[5]) + (tvisc[2] + rs2) + geff[2];
+      const double4 xi = P.X[p];
       if (nb > 0) {
         double R[3];
-        elastic_reaction<DIM>(s, b, nb, bstart, vi, R);
+        const double xa[3] = {xi.x, xi.y, xi.z};
+        elastic_reaction<DIM>(s, b, nb, bstart, xa, vi, R);
         for (int d = 0; d < 3; ++d) acc[d] = acc[d] + R[d];
       }
       if (FUSED) {
-        double4 xi = P.X[p];
         double dtvel = dyn->dtvel, dt = dyn->dt;
         double vn[3];
         for (int d = 0; d < 3; ++d) vn[d] = vi[d] + dtvel * acc[d];
@@ -2195,13 +2290,11 @@ __global__ void __launch_bounds__(kBlock, 5) k_continuity_f32(DevBatch b) {
     SimDyn* dyn = b.dyn + tl.sim;
     int p = tl.start + threadIdx.x;
     bool active = threadIdx.x < tl.count && p < s.p_off + dyn->nag && !dyn->frozen;
-    int ci = 0, cj = 0, ck = 0, cnt = 0;
+    int cnt = 0;
     float4 xfi = make_float4(0.f, 0.f, 0.f, 0.f);
     float vix = 0.f, viy = 0.f, viz = 0.f, rhof = 1.f;
     if (active) {
-      double4 xi = P.X[p];
       double4 vi = P.V[p];
-      particle_cell(s, xi.x, xi.y, xi.z, ci, cj, ck);
       xfi = P.XF[p];
       vix = (float)vi.x;
       viy = (float)vi.y;
@@ -2209,6 +2302,8 @@ __global__ void __launch_bounds__(kBlock, 5) k_continuity_f32(DevBatch b) {
       rhof = (float)P.RP[p].x;
       cnt = b.ncount[p];
     }
+    const float ckf = xfi.w, dz = s.dcdf[2];
+    RunCursor<DIM> rc;
     Kahan sum;
     sum.zero();
     float part = 0.f;   // 4-entry partial sum, compensated into sum per chunk
@@ -2218,12 +2313,11 @@ __global__ void __launch_bounds__(kBlock, 5) k_continuity_f32(DevBatch b) {
     for (int k = 0; k < nmax; ++k) {
       const int e = lr.get(k);
       if (k >= cnt) continue;
-      const float4 xj = P.XF[e & kSlotMask], vj = P.VF[e & kSlotMask];
+      const float4 xj = __ldg(P.XF + (e & kSlotMask)), vj = __ldg(P.VF + (e & kSlotMask));
       float d0, d1, d2;
-      separation_cols<DIM>(s, (int)((unsigned)e >> kSlotBits), xj, xfi, ci, cj, ck, d0, d1, d2);
+      separation_f32<DIM>(s, rc, e, xj, xfi, ckf, dz, d0, d1, d2);
       float rr = fmaf(d2, d2, fmaf(d1, d1, d0 * d0));
-      float PK1, PK2, PK3;
-      kernel_values_f32<true>(fc, rr, PK1, PK2, PK3);
+      const float PK1 = kernel_pk1_f32(fc, rr);
       float c = rhof * vj.w * PK1;    // rho_i (m_j / rho_j) PK1
       part = fmaf(c, fmaf(vj.z - viz, d2, fmaf(vj.y - viy, d1, (vj.x - vix) * d0)), part);
       if ((k & 3) == 3 || k == cnt - 1) {
@@ -2468,16 +2562,16 @@ __global__ void __launch_bounds__(kBlock, 4) k_velocity_smoothing_f32(DevBatch b
     int p = tl.start + threadIdx.x;
     const bool active = threadIdx.x < tl.count && p < s.p_off + dyn->nag && !dyn->frozen && s.teta_v > 1.0e-9;
     const float hinv = (float)(1.0 / s.h), coefke = (float)s.coefke;
-    int ci = 0, cj = 0, ck = 0, cnt = 0;
+    int cnt = 0;
     float4 xfi = make_float4(0.f, 0.f, 0.f, 0.f);
     double4 vi = make_double4(0.0, 0.0, 0.0, 0.0);
     if (active) {
-      const double4 xi = P.X[p];
-      particle_cell(s, xi.x, xi.y, xi.z, ci, cj, ck);
       xfi = P.XF[p];
       vi = vel[p];
       cnt = b.ncount[p];
     }
+    const float ckf = xfi.w, dz = s.dcdf[2];
+    RunCursor<DIM> rc;
     const float4 vif = make_float4((float)vi.x, (float)vi.y, (float)vi.z, 0.f);
     Kahan k0, k1, k2;
     k0.zero(); k1.zero(); k2.zero();
@@ -2491,7 +2585,7 @@ __global__ void __launch_bounds__(kBlock, 4) k_velocity_smoothing_f32(DevBatch b
       int q = e & kSlotMask;
       const float4 xj = P.XF[q], rfj = P.RF[q], vj = P.VF2[q];
       float d0, d1, d2;
-      separation_cols<DIM>(s, (int)((unsigned)e >> kSlotBits), xj, xfi, ci, cj, ck, d0, d1, d2);
+      separation_f32<DIM>(s, rc, e, xj, xfi, ckf, dz, d0, d1, d2);
       float rr = fmaf(d2, d2, fmaf(d1, d1, d0 * d0));
       float pes = __fdividef(rfj.z * kernel_w_f32(rr, hinv, coefke), rfj.x);
       c0 = fmaf(vj.x - vif.x, pes, c0);
@@ -2521,19 +2615,19 @@ __global__ void __launch_bounds__(kBlock, 4) k_pressure_smoothing_f32(DevBatch b
     int p = tl.start + threadIdx.x;
     const bool active = threadIdx.x < tl.count && p < s.p_off + dyn->nag && !dyn->frozen && s.teta_p > 0.0;
     const float hinv = (float)(1.0 / s.h), coefke = (float)s.coefke;
-    int ci = 0, cj = 0, ck = 0, cnt = 0;
+    int cnt = 0;
     float4 xfi = make_float4(0.f, 0.f, 0.f, 0.f);
     double pi = 0.0;
     float self = 0.f;
     if (active) {
-      const double4 xi = P.X[p];
-      particle_cell(s, xi.x, xi.y, xi.z, ci, cj, ck);
       xfi = P.XF[p];
       const float4 rfi = P.RF[p];
       pi = P.RP[p].y;
       self = __fdividef(rfi.z * (0.666666667f * coefke), rfi.x);
       cnt = b.ncount[p];
     }
+    const float ckf = xfi.w, dz = s.dcdf[2];
+    RunCursor<DIM> rc;
     Kahan ka, ks;
     ka.zero();
     ks.zero();
@@ -2548,7 +2642,7 @@ __global__ void __launch_bounds__(kBlock, 4) k_pressure_smoothing_f32(DevBatch b
       const float4 xj = P.XF[q], rfj = P.RF[q];
       const float dp = (float)(P.RP[q].y - pi);
       float d0, d1, d2;
-      separation_cols<DIM>(s, (int)((unsigned)e >> kSlotBits), xj, xfi, ci, cj, ck, d0, d1, d2);
+      separation_f32<DIM>(s, rc, e, xj, xfi, ckf, dz, d0, d1, d2);
       float rr = fmaf(d2, d2, fmaf(d1, d1, d0 * d0));
       float pes = __fdividef(rfj.z * kernel_w_f32(rr, hinv, coefke), rfj.x);
       ca += pes;

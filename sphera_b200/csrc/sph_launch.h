@@ -19,6 +19,7 @@ struct DevBatch {
   Particles P;
   const FaceDev* faces;
   const SideDev* sides;
+  const EdgeDev* edges;    // convex edges of all simulations (3D)
   const double* bit;       // per-sim BoundIntegralTab, 256 x 7 each
   const int* cf_start;     // per global cell: first entry in cf_list
   const int* cf_count;     // per global cell: faces cutting the cell

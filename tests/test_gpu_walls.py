@@ -92,3 +92,29 @@ def test_laminar_flag_matches_oracle(oracle_lib):
     sim.step(1)
     o.step(1)
     assert np.array_equal(sim.dump_laminar(), o.laminar())
+
+
+@pytest.mark.parametrize("precision", [abi.SPH_PREC_FP64, abi.SPH_PREC_FP32C])
+def test_convex_edge_reaction_follows_oracle(precision, oracle_lib):
+    """A block standing in the tank gives the boundary convex edges
+    (FindBoundaryConvexEdges3D.f90); a particle just outside the first one,
+    off both faces' projections and approaching it, gets the edge reaction
+    of AddElasticBoundaryReaction_3D.f90:106-153."""
+    from .test_convex_edges import edge_case
+    case, i = edge_case(precision=precision)
+    sim = Simulation(case)
+    sim.upload(case.state)
+    o = oracle_lib.Oracle(case)
+    o.prepare()
+    acc = sim.rhs_momentum()
+    o.rhs_momentum()
+    ref = o.get()["acc"]
+    assert ref[i, 2] > 1.0e4
+    tol = RATE_TOL if precision == abi.SPH_PREC_FP64 else 1e-5
+    assert rel_l2(acc, ref) <= tol
+    assert rel_l2(acc[i], ref[i]) <= tol
+    if precision == abi.SPH_PREC_FP64:
+        # whole steps on the non-box geometry follow the oracle too
+        sim.step(30)
+        o.step(30)
+        assert rel_l2(sim.download().x, o.get()["x"]) <= 1e-12
