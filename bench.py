@@ -272,14 +272,14 @@ def run_ensemble(args, ws, rank):
     t0 = time.perf_counter()
     while True:
         b.step_async(chunk)
-        fr, tt, st = b.status()
+        fr, tt, st, _ = b.status()
         now = time.perf_counter() - t0
         newly = fr & np.isnan(done_at)
         done_at[newly] = now
         if fr.all():
             break
     elapsed = time.perf_counter() - t0
-    fr, tt, st = b.status()
+    fr, tt, st, _ = b.status()
     psteps = float(sum(c.n * int(k) for c, k in zip(cs, st)))
     elapsed = _max_over_ranks(ws, elapsed)
     line = {

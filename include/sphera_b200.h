@@ -43,6 +43,7 @@ extern "C" {
 #define SPH_ERR_CUDA                 3   /* a CUDA runtime call failed              */
 #define SPH_ERR_NO_DEVICE            5   /* no sm_100 device visible                */
 #define SPH_ERR_TIMEOUT              6   /* a bounded device wait gave up           */
+#define SPH_CANCELLED                7   /* the host cancelled the simulation       */
 #define SPH_ERR_ALLOC              400   /* diagnostic(4): allocation failure       */
 #define SPH_ERR_BDT_OVERFLOW       802   /* diagnostic(8,2): BoundaryDataTab full   */
 #define SPH_ERR_CLOSE_FACES        807   /* diagnostic(8,7): > MAXCLOSEBOUNDFACES   */
@@ -228,9 +229,19 @@ int  sph_batch_download(SphHandle* h, int32_t sim, SphState* state);
  * stays on the device for download while the others continue.             */
 int  sph_batch_set_end_time(SphHandle* h, int32_t sim, double t_end);
 int  sph_batch_info(SphHandle* h, int32_t sim, SphStepInfo* info, int32_t* frozen);
-/* Every simulation's frozen flag, time and completed steps ([nsims] each,
- * any may be NULL) from one read-back of the device state.                */
-int  sph_batch_status(SphHandle* h, int32_t* frozen, double* time, int32_t* steps);
+/* Every simulation's frozen flag, time, completed steps and status
+ * ([nsims] each, any may be NULL) from one read-back of the device state.
+ * A simulation that meets a fatal condition (status != SPH_OK, e.g.
+ * SPH_ERR_BDT_OVERFLOW from its own share of the boundary-data pool)
+ * freezes at the end of that step while the others advance unchanged;
+ * this call reports it in status[] and itself fails only on CUDA errors
+ * (sph_step / sph_sync return the first member's fatal status).           */
+int  sph_batch_status(SphHandle* h, int32_t* frozen, double* time, int32_t* steps, int32_t* status);
+/* Cancels simulation `sim` of a batch: from the next launch enqueued on the
+ * handle's stream it is frozen with status SPH_CANCELLED, its state kept
+ * (no wait; the counterpart of the reference's kill file,
+ * time_step_loop.f90:485-487, for one member).                            */
+int  sph_batch_cancel(SphHandle* h, int32_t sim);
 
 /* Device memory, in bytes, that sph_batch_create would allocate for these
  * arguments (sph_create: nsims = 1), computed on the host without touching

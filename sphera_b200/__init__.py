@@ -78,7 +78,8 @@ def lib():
         "sph_measure_fp64_peak": ([dp], C.c_int),
         "sph_measure_fma_peak": ([C.c_int32, dp], C.c_int),
         "sph_autotune": ([vp, C.c_int32, ip], C.c_int),
-        "sph_batch_status": ([vp, ip, dp, ip], C.c_int),
+        "sph_batch_status": ([vp, ip, dp, ip, ip], C.c_int),
+        "sph_batch_cancel": ([vp, C.c_int32], C.c_int),
         "sph_memory_required": ([C.c_int32, C.POINTER(abi.SphParams), C.POINTER(abi.SphGeometry), ip,
                                  C.POINTER(C.c_uint64)], C.c_int),
         "sph_idle": ([vp, ip], C.c_int),
@@ -373,13 +374,20 @@ class Batch:
         return info, bool(fr.value)
 
     def status(self):
-        """(frozen, time, steps) arrays of all simulations, one read-back."""
+        """(frozen, time, steps, status) arrays of all simulations, one
+        read-back; status holds each member's fatal code (0: none)."""
         n = len(self.cases)
         fr = np.zeros(n, np.int32)
         t = np.zeros(n)
         st = np.zeros(n, np.int32)
-        _chk(lib().sph_batch_status(self._h, abi.iptr(fr), abi.dptr(t), abi.iptr(st)), "sph_batch_status")
-        return fr.astype(bool), t, st
+        code = np.zeros(n, np.int32)
+        _chk(lib().sph_batch_status(self._h, abi.iptr(fr), abi.dptr(t), abi.iptr(st), abi.iptr(code)),
+             "sph_batch_status")
+        return fr.astype(bool), t, st, code
+
+    def cancel(self, sim):
+        """Freezes member `sim` from the next launch on (SPH_CANCELLED)."""
+        _chk(lib().sph_batch_cancel(self._h, int(sim)), "sph_batch_cancel")
 
     def global_quantities(self):
         """fluid_global_quantities of every simulation, (nsims, 8)."""

@@ -14,6 +14,7 @@ SPH_ERR_UNSUPPORTED = 2
 SPH_ERR_CUDA = 3
 SPH_ERR_NO_DEVICE = 5
 SPH_ERR_TIMEOUT = 6
+SPH_CANCELLED = 7
 SPH_ERR_ALLOC = 400
 SPH_ERR_BDT_OVERFLOW = 802
 SPH_ERR_CLOSE_FACES = 807
@@ -36,6 +37,7 @@ STATUS_NAMES = {
     SPH_ERR_CUDA: "CUDA runtime error",
     SPH_ERR_NO_DEVICE: "no sm_100 device",
     SPH_ERR_TIMEOUT: "bounded device wait timed out",
+    SPH_CANCELLED: "cancelled by the host",
     SPH_ERR_ALLOC: "allocation failure (diagnostic 4)",
     SPH_ERR_BDT_OVERFLOW: "BoundaryDataTab overflow (diagnostic 8/2)",
     SPH_ERR_CLOSE_FACES: "too many close boundary faces (diagnostic 8/7)",

@@ -656,10 +656,16 @@ int halloc(SphHandle* h, T** p, size_t n) {
   return SPH_OK;
 }
 
-int sync_dyn(SphHandle* h) {
+// Reads every simulation's device scalars back (CUDA errors only).
+int read_dyn(SphHandle* h) {
   SPH_CUDA(cudaMemcpyAsync(h->h_dyn.data(), h->d_dyn, sizeof(SimDyn) * (h->nsims + 1), cudaMemcpyDeviceToHost,
                            h->stream));
-  SPH_CUDA(cudaStreamSynchronize(h->stream));
+  return cuda_status(cudaStreamSynchronize(h->stream));
+}
+
+// read_dyn, then the first simulation's fatal status (SPH_OK if none).
+int sync_dyn(SphHandle* h) {
+  SPH_TRY(read_dyn(h));
   for (int s = 0; s < h->nsims; ++s)
     if (h->h_dyn[s].status != 0) return h->h_dyn[s].status;
   return SPH_OK;
@@ -828,7 +834,10 @@ int create_batch(int nsims, const SphParams* params, const SphGeometry* geoms, c
     // default: room for three close faces (two close sides) per particle,
     // a box corner's worth; the reference reserves MAXCLOSEBOUNDFACES per
     // particle (Gest_Trans.f90:90), far more than a flow uses
-    bdt_cap += hs.prm.bdt_capacity > 0 ? (size_t)hs.prm.bdt_capacity : (size_t)hs.cap * (h->dim == 3 ? 3 : 2);
+    const size_t quota = hs.prm.bdt_capacity > 0 ? (size_t)hs.prm.bdt_capacity : (size_t)hs.cap * (h->dim == 3 ? 3 : 2);
+    if (quota > 0x7fffffff) { delete h; return SPH_ERR_INVALID_ARGUMENT; }
+    hs.dev.bdt_quota = (int)quota;
+    bdt_cap += quota;
   }
   if (poff >= (1 << 28)) { delete h; return SPH_ERR_INVALID_ARGUMENT; }   // list entries carry 28-bit slots
   h->total_slots = poff;
@@ -1191,16 +1200,27 @@ int sph_batch_info(SphHandle* h, int32_t sim, SphStepInfo* info, int32_t* frozen
 
 void* sph_stream(SphHandle* h) { return h ? (void*)h->stream : nullptr; }
 
-// All simulations' progress in one read-back: frozen flag, time and steps.
-int sph_batch_status(SphHandle* h, int32_t* frozen, double* time, int32_t* steps) {
+// All simulations' progress in one read-back: frozen flag, time, steps and
+// fatal status.  A member's failure is reported in status[], not as the
+// call's result, so a server can retire it and keep the others running.
+int sph_batch_status(SphHandle* h, int32_t* frozen, double* time, int32_t* steps, int32_t* status) {
   if (!h) return SPH_ERR_INVALID_ARGUMENT;
-  SPH_TRY(sync_dyn(h));
+  SPH_TRY(read_dyn(h));
   for (int s = 0; s < h->nsims; ++s) {
     if (frozen) frozen[s] = h->h_dyn[s].frozen;
     if (time) time[s] = h->h_dyn[s].time;
     if (steps) steps[s] = h->h_dyn[s].step;
+    if (status) status[s] = h->h_dyn[s].status;
   }
   return SPH_OK;
+}
+
+// Stops simulation `sim` from the next enqueued launch on (stream-ordered,
+// no wait): it freezes with status SPH_CANCELLED and keeps its state.
+int sph_batch_cancel(SphHandle* h, int32_t sim) {
+  if (!h || !h->uploaded || sim < 0 || sim >= h->nsims) return SPH_ERR_INVALID_ARGUMENT;
+  launch_cancel(h->db, sim, h->stream);
+  return cuda_status(cudaGetLastError());
 }
 
 int sph_get_diagnostics(SphHandle* h, SphDiagnostics* diag) {

@@ -43,6 +43,8 @@ struct SimDev {
   int cap;                // particle slots reserved
   int nmaxpartj;          // NMAXPARTJ
   int maxcb;              // MAXCLOSEBOUNDFACES (3D) / MAXCLOSEBOUNDSIDES (2D)
+  int bdt_quota;          // BoundaryDataTab entries this simulation may take from the pool
+  int pad_quota;
   int face_off, nfaces;   // faces (3D)
   int side_off, nsides;   // sides (2D)
   int edge_off, nedges;   // convex edges (3D)
@@ -79,7 +81,9 @@ struct SimDyn {
   int ncbf_max;
   int max_neigh;
   int bdt_used;
-  int frozen;                      // reached t_end: state kept, no longer advanced
+  int bdt_sim_used;                // entries this simulation took in the current pass
+  int pad_used;
+  int frozen;                      // reached t_end, failed or cancelled: state kept, no longer advanced
   double t_end;                    // 0 = run without end
   double geff[3];                  // body force of the next step: grav (+ tank forcing)
 };
@@ -142,7 +146,7 @@ struct Tile {
 // Device view of the particle storage.
 struct Particles {
   double4* X;       // x, y, z, mass          (sorted)
-  float4* XF;       // offset from the cell origin in FP32, w = the cell's k index (int bits)
+  float4* XF;       // offset from the cell origin in FP32, w = the cell's k index (as a float)
   float4* VF;       // FP32 form: vx, vy, vz, m/rho
   float4* RF;       // FP32 form: rho, p/rho^2, m, 0
   double4* V;       // vx, vy, vz, rho (density entering the continuity pass)

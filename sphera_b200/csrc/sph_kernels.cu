@@ -604,6 +604,12 @@ __global__ void __launch_bounds__(kBlock) k_boundary3d(DevBatch b) {
       continue;
     }
     if (ncbf == 0) continue;
+    // each simulation draws on its own quota of the shared pool first, so
+    // one that overflows fails alone and the others' entries are unaffected
+    if (atomicAdd(&dyn->bdt_sim_used, ncbf) + ncbf > s.bdt_quota) {
+      set_status(dyn, SPH_ERR_BDT_OVERFLOW);
+      continue;
+    }
     int gbase = atomicAdd(&b.dyn[b.nsims].bdt_used, ncbf);  // global allocation counter
     if (gbase + ncbf > P.bdt_cap) {
       set_status(dyn, SPH_ERR_BDT_OVERFLOW);
@@ -745,6 +751,10 @@ __global__ void __launch_bounds__(kBlock) k_boundary2d(DevBatch b) {
         nint++;
       }
     if (nint == 0) continue;
+    if (atomicAdd(&dyn->bdt_sim_used, nint) + nint > s.bdt_quota) {
+      set_status(dyn, SPH_ERR_BDT_OVERFLOW);
+      continue;
+    }
     int gbase = atomicAdd(&b.dyn[b.nsims].bdt_used, nint);
     if (gbase + nint > P.bdt_cap) {
       set_status(dyn, SPH_ERR_BDT_OVERFLOW);
@@ -2956,6 +2966,9 @@ __global__ void k_finalize(DevBatch b, int mode) {
     tsd_close(s, d, dtmin_cfl, d.step + 1);
     d.dt_prev = dt_cur;
     if (d.t_end > 0.0 && d.time >= d.t_end) d.frozen = 1;
+    // a simulation with a fatal status stops advancing; the others of its
+    // batch go on (its segment, cells and boundary quota are its own)
+    if (d.status != 0) d.frozen = 1;
   }
   d.dtvel = 0.5 * (d.dt + d.dt_prev);
   // body force of the next step, taken at that step's end time d.time + d.dt
@@ -2969,6 +2982,16 @@ __global__ void k_finalize(DevBatch b, int mode) {
   d.geff[2] = s.grav[2];
 }
 
+// sph_batch_cancel: a simulation still advancing stops from the next launch
+// on, with status SPH_CANCELLED; one already frozen (finished or failed)
+// keeps its status.
+__global__ void k_cancel(DevBatch b, int sim) {
+  if (threadIdx.x == 0 && sim < b.nsims && !b.dyn[sim].frozen) {
+    atomicCAS(&b.dyn[sim].status, 0, SPH_CANCELLED);
+    b.dyn[sim].frozen = 1;
+  }
+}
+
 __global__ void k_sort_reset(DevBatch b) {
   int sim = blockIdx.x * blockDim.x + threadIdx.x;
   if (sim < b.nsims) b.dyn[sim].n_out = 0;
@@ -2976,7 +2999,10 @@ __global__ void k_sort_reset(DevBatch b) {
 
 __global__ void k_bdt_reset(DevBatch b) {
   int sim = blockIdx.x * blockDim.x + threadIdx.x;
-  if (sim < b.nsims) b.dyn[sim].ncbf_max = 0;
+  if (sim < b.nsims) {
+    b.dyn[sim].ncbf_max = 0;
+    b.dyn[sim].bdt_sim_used = 0;
+  }
   if (sim == 0) b.dyn[b.nsims].bdt_used = 0;
 }
 
@@ -3299,6 +3325,8 @@ void launch_scan(const DevBatch& b, int* cell_start, cudaStream_t st) {
   k_scan2<<<1, kScanThreads, 0, st>>>(b.scan_block_sums, nb, cell_start, n);
   k_scan3<<<nb, kScanThreads, 0, st>>>(b.P.cell_count, n, b.scan_block_sums, cell_start);
 }
+
+void launch_cancel(const DevBatch& b, int sim, cudaStream_t st) { k_cancel<<<1, 32, 0, st>>>(b, sim); }
 
 void launch_sort_reset(const DevBatch& b, cudaStream_t st) {
   k_sort_reset<<<(b.nsims + 127) / 128, 128, 0, st>>>(b);

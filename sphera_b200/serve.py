@@ -20,6 +20,20 @@ another make progress:
 * a group whose members have all finished is destroyed and its bytes return
   to the budget, which may admit the next group.
 
+Failures stay with their request.  The reference's only failure path is
+fatal (``diagnostic`` ends with ``stop``, src/Memory_I_O/diagnostic.f90) and
+its only clean stop is the kill file (time_step_loop.f90:485-487); here:
+
+* a member whose device status turns fatal (for example its share of the
+  boundary-data pool overflowing, diagnostic 8/2) freezes on the device at
+  the end of that step; the server reports it failed with the code, and the
+  other members of its group run on, unchanged;
+* ``cancel(rid)`` withdraws a queued request or freezes a running one
+  (``sph_batch_cancel``); it is reported cancelled;
+* a group whose creation or upload fails on the device (for example an
+  allocation the budget did not foresee) reports its requests failed with
+  that code and returns their bytes.
+
 Every kernel treats each member of a group independently, so a request's
 result does not depend on what else is admitted: it equals the same
 request run alone, bit for bit.
@@ -34,6 +48,8 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
+CANCELLED = 7          # SPH_CANCELLED
+
 
 @dataclass
 class Result:
@@ -46,11 +62,18 @@ class Result:
     sim_time: float = 0.0
     state: object = None
     rejected: bool = False
+    failed: bool = False
+    cancelled: bool = False
+    status: int = 0
     group: int = -1
 
     @property
     def time_to_result(self):
         return self.finished - self.arrival
+
+    @property
+    def completed(self):
+        return not (self.rejected or self.failed or self.cancelled)
 
 
 @dataclass
@@ -96,6 +119,12 @@ class Server:
         self.peak_used = 0
         self.groups_formed = 0
         self.max_concurrent = 0
+        self._cancel = set()
+
+    def cancel(self, rid):
+        """Withdraws request `rid`: taken out of the queue if it waits, frozen
+        on the device (and its result reported cancelled) if it runs."""
+        self._cancel.add(rid)
 
     def _admit(self, waiting, now, results):
         """Forms one group from the head of the queue (FIFO, no overtaking)."""
@@ -116,31 +145,80 @@ class Server:
             waiting.popleft()
         if not group:
             return None
-        batch = self.factory([r.case for r in group])
-        batch.upload([r.case.state for r in group])
-        for i, r in enumerate(group):
-            batch.set_end_time(i, r.t_end)
+        gid = self.groups_formed
+        self.groups_formed += 1
+        try:
+            batch = self.factory([r.case for r in group])
+        except RuntimeError as e:
+            self._fail_group(group, gid, getattr(e, "code", -1), now, results)
+            return None
+        try:
+            try:
+                batch.upload([r.case.state for r in group])
+            except RuntimeError:
+                # the upload returns the first member's fatal status; when
+                # members hold one, they alone failed (their IC pass): the
+                # status poll reports them and the others run
+                if not any(batch.status()[3]):
+                    raise
+            for i, r in enumerate(group):
+                batch.set_end_time(i, r.t_end)
+        except RuntimeError as e:
+            batch.close()
+            self._fail_group(group, gid, getattr(e, "code", -1), now, results)
+            return None
+        for r in group:
             results[r.rid].admitted = now
-            results[r.rid].group = self.groups_formed
+            results[r.rid].group = gid
         self.used += need
         self.peak_used = max(self.peak_used, self.used)
-        g = _Group(self.groups_formed, batch, group, need, [False] * len(group))
-        self.groups_formed += 1
+        g = _Group(gid, batch, group, need, [False] * len(group))
         batch.step_async(self.chunk)
         return g
 
-    def run(self, requests, poll=2e-4):
+    @staticmethod
+    def _fail_group(group, gid, code, now, results):
+        for r in group:
+            res = results[r.rid]
+            res.admitted = res.finished = now
+            res.group = gid
+            res.failed = True
+            res.status = int(code)
+
+    def _apply_cancels(self, waiting, active, now, results):
+        for rid in list(self._cancel):
+            for r in list(waiting):
+                if r.rid == rid:
+                    waiting.remove(r)
+                    res = results[rid]
+                    res.cancelled = True
+                    res.status = CANCELLED
+                    res.finished = now
+                    self._cancel.discard(rid)
+            for g in active:
+                for i, r in enumerate(g.requests):
+                    if r.rid == rid and not g.done[i]:
+                        g.batch.cancel(i)   # takes effect from the next launch on
+                        self._cancel.discard(rid)
+
+    def run(self, requests, poll=2e-4, cancel_at=None):
         """Serves `requests` (arrival times in seconds from the start) in real
-        time and returns {rid: Result}."""
+        time and returns {rid: Result}.  cancel_at: {rid: time} of cancels
+        to issue during the run (as cancel() would from another thread)."""
         pending = deque(sorted(requests, key=lambda r: (r.arrival, r.rid)))
         results = {r.rid: Result(r.rid, r.arrival) for r in requests}
+        cancels = sorted((t, rid) for rid, t in (cancel_at or {}).items())
         waiting = deque()
         active = []
         t0 = self.clock()
         while pending or waiting or active:
             now = self.clock() - t0
+            while cancels and cancels[0][0] <= now:
+                self.cancel(cancels.pop(0)[1])
             while pending and pending[0].arrival <= now:
                 waiting.append(pending.popleft())
+            if self._cancel:
+                self._apply_cancels(waiting, active, now, results)
             while waiting:
                 g = self._admit(waiting, now, results)
                 if g is None:
@@ -152,20 +230,25 @@ class Server:
                 if not g.batch.idle():
                     continue
                 progressed = True
-                frozen, t, steps = g.batch.status()
-                now = self.clock() - t0
+                frozen, t, steps, status = g.batch.status()
                 for i, r in enumerate(g.requests):
-                    if frozen[i] and not g.done[i]:
-                        g.done[i] = True
-                        res = results[r.rid]
-                        if self.keep_state:
-                            res.state = g.batch.download(i)
-                            res.n = res.state.n
-                        else:
-                            res.n = r.case.n
-                        res.finished = self.clock() - t0
-                        res.steps = int(steps[i])
-                        res.sim_time = float(t[i])
+                    if g.done[i] or not (frozen[i] or status[i]):
+                        continue
+                    g.done[i] = True
+                    res = results[r.rid]
+                    res.steps = int(steps[i])
+                    res.sim_time = float(t[i])
+                    res.status = int(status[i])
+                    if status[i] == CANCELLED:
+                        res.cancelled = True
+                    elif status[i]:
+                        res.failed = True
+                    elif self.keep_state:
+                        res.state = g.batch.download(i)
+                        res.n = res.state.n
+                    else:
+                        res.n = r.case.n
+                    res.finished = self.clock() - t0
                 if all(g.done):
                     g.batch.close()
                     self.used -= g.bytes
@@ -174,18 +257,22 @@ class Server:
                     g.batch.step_async(self.chunk)
             if not progressed:
                 nxt = pending[0].arrival - (self.clock() - t0) if pending and not waiting else poll
+                if cancels:
+                    nxt = min(nxt, cancels[0][0] - (self.clock() - t0))
                 time.sleep(max(0.0, min(poll, nxt)))
         self.wall = self.clock() - t0
         return results
 
 
 def summarize(results, wall):
-    """p50/p99 time-to-result and aggregate particle-steps/s of a run."""
-    done = [r for r in results.values() if not r.rejected]
+    """p50/p99 time-to-result and aggregate particle-steps/s of a run (over
+    the completed requests; failed, cancelled and rejected ones counted)."""
+    done = [r for r in results.values() if r.completed]
     ttr = np.array([r.time_to_result for r in done])
     work = float(sum(r.n * r.steps for r in done))
     return dict(
         requests=len(results), completed=len(done), rejected=sum(r.rejected for r in results.values()),
+        failed=sum(r.failed for r in results.values()), cancelled=sum(r.cancelled for r in results.values()),
         p50_s=float(np.percentile(ttr, 50)) if len(ttr) else None,
         p99_s=float(np.percentile(ttr, 99)) if len(ttr) else None,
         mean_queue_s=float(np.mean([r.admitted - r.arrival for r in done])) if done else None,

@@ -9,12 +9,26 @@ import pytest
 from sphera_b200.serve import Server, summarize
 
 
+CANCELLED = 7            # SPH_CANCELLED
+BDT_OVERFLOW = 802       # SPH_ERR_BDT_OVERFLOW
+ALLOC = 400              # SPH_ERR_ALLOC
+
+
 @dataclass
 class FakeCase:
     n: int
     dt: float
     nbytes: int
     state: object = None
+    fail_after: object = None     # steps after which the member reports fail_code
+    fail_code: int = BDT_OVERFLOW
+    oom: bool = False             # creating a batch that holds it fails (allocation)
+
+
+class FakeSphError(RuntimeError):
+    def __init__(self, code):
+        self.code = code
+        super().__init__(f"status {code}")
 
 
 @dataclass
@@ -43,6 +57,7 @@ class FakeBatch:
         self.t = [0.0] * len(cases)
         self.steps = [0] * len(cases)
         self.t_end = [0.0] * len(cases)
+        self.code = [0] * len(cases)
         self.closed = False
         FakeBatch.live.append(self)
 
@@ -55,7 +70,7 @@ class FakeBatch:
     def step_async(self, k):
         for i, c in enumerate(self.cases):
             for _ in range(k):
-                if self.t[i] >= self.t_end[i]:
+                if self.t[i] >= self.t_end[i] or self.code[i]:
                     break
                 self.t[i] += c.dt
                 self.steps[i] += 1
@@ -64,8 +79,17 @@ class FakeBatch:
         return True
 
     def status(self):
-        fr = [self.t[i] >= self.t_end[i] for i in range(len(self.cases))]
-        return fr, list(self.t), list(self.steps)
+        for i, c in enumerate(self.cases):
+            # host-side injection of a device failure: the member reports a
+            # fatal code once it has run `fail_after` steps, and freezes
+            if c.fail_after is not None and self.steps[i] >= c.fail_after and not self.code[i]:
+                self.code[i] = c.fail_code
+        fr = [self.t[i] >= self.t_end[i] or self.code[i] != 0 for i in range(len(self.cases))]
+        return fr, list(self.t), list(self.steps), list(self.code)
+
+    def cancel(self, i):
+        if not (self.t[i] >= self.t_end[i] or self.code[i]):
+            self.code[i] = CANCELLED
 
     def download(self, i):
         return None
@@ -79,6 +103,8 @@ def _server(budget, peak_log):
         return sum(c.nbytes for c in cases)
 
     def factory(cases):
+        if any(c.oom for c in cases):
+            raise FakeSphError(ALLOC)
         b = FakeBatch(cases)
         return b
 
@@ -142,3 +168,67 @@ def test_budget_bounds_resident_bytes(budget):
     srv = _server(budget, None)
     srv.run(_requests(), poll=0.0)
     assert srv.peak_used <= budget
+
+
+def _steps_alone(q):
+    return math.ceil(q.t_end / q.case.dt)
+
+
+def test_a_failed_member_is_reported_and_the_others_finish():
+    """Host-side injection of a device failure: request 1 reports
+    diagnostic 8/2 after 3 steps; it is reported failed with that code, its
+    group mates finish with the step counts they have alone, and every
+    group's bytes are returned."""
+    FakeBatch.live = []
+    srv = _server(1000, None)
+    reqs = _requests()
+    for q in reqs:
+        q.arrival = 0.0
+    reqs[1].case.fail_after = 3
+    res = srv.run(reqs, poll=0.0)
+    assert res[1].failed and res[1].status == BDT_OVERFLOW and not res[1].completed
+    assert res[1].steps < _steps_alone(reqs[1])
+    for q in reqs:
+        if q.rid != 1:
+            assert res[q.rid].completed and res[q.rid].steps == _steps_alone(q)
+    assert res[0].group == res[1].group == res[2].group
+    assert srv.used == 0 and all(b.closed for b in FakeBatch.live)
+    s = summarize(res, srv.wall)
+    assert s["failed"] == 1 and s["completed"] == len(reqs) - 1
+
+
+def test_admission_oom_fails_the_group_and_frees_its_bytes():
+    """A batch whose allocation fails on the device although the budget
+    admitted it (injected: the factory raises diagnostic 4): its requests
+    are reported failed, its bytes are never held, later requests run."""
+    FakeBatch.live = []
+    srv = _server(1000, None)
+    reqs = _requests()
+    for q in reqs:
+        q.arrival = 0.0
+    reqs[0].case.oom = True            # the first group: requests 0, 1, 2
+    res = srv.run(reqs, poll=0.0)
+    for rid in (0, 1, 2):
+        assert res[rid].failed and res[rid].status == ALLOC
+    for rid in (3, 4, 5):
+        assert res[rid].completed
+    assert srv.used == 0
+
+
+def test_cancel_while_queued_and_while_running():
+    """cancel() withdraws a queued request at once and freezes a running
+    one from its next chunk on; both are reported cancelled and the others
+    finish as alone."""
+    FakeBatch.live = []
+    srv = _server(1000, None)
+    reqs = _requests()
+    for q in reqs:
+        q.arrival = 0.0
+    # request 0 runs in the first group; request 5 waits for memory
+    res = srv.run(reqs, poll=0.0, cancel_at={0: 0.0025, 5: 0.0025})
+    assert res[0].cancelled and res[0].status == CANCELLED
+    assert 0 < res[0].steps < _steps_alone(reqs[0])
+    assert res[5].cancelled and res[5].steps == 0 and res[5].group == -1
+    for rid in (1, 2, 3, 4):
+        assert res[rid].completed and res[rid].steps == _steps_alone(reqs[rid])
+    assert srv.used == 0
