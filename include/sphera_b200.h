@@ -102,9 +102,12 @@ typedef struct SphParams {
     /* 1st-order consistency (input_any_t%C1_BE, %C1_divu, %invB_det_thresh):
      * the pressure-gradient terms of the momentum equation are renormalised
      * with B_ren_gradp and, with c1_divu as well, the velocity gradients of
-     * the continuity equation with B_ren_divu.  3D, FP64 form (otherwise
-     * SPH_ERR_UNSUPPORTED); a matrix whose |det| is below invb_det_thresh
-     * is replaced by -I (B_ren_gradp_inversion.f90:62-73).  0 disables.   */
+     * the continuity equation with B_ren_divu.  3D, both precision forms
+     * (the matrices, their inversion and the renormalisation in FP64; in
+     * the FP32c form the renormalised pair sums are compensated FP32 sums);
+     * 2D returns SPH_ERR_UNSUPPORTED.  A matrix whose |det| is below
+     * invb_det_thresh is replaced by -I (B_ren_gradp_inversion.f90:62-73).
+     * 0 disables.                                                          */
     int32_t c1_be;
     int32_t c1_divu;
     double  invb_det_thresh;        /* >= 0                                           */

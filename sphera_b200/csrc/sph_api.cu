@@ -179,7 +179,7 @@ int prepare_sim(const SphParams& prm, const SphGeometry& g, int cap, HostSim& hs
   // 1st-order consistency: 3D, FP64 form; C1_divu acts only with C1_BE
   // (CalcVarLength.f90:285, Continuity_Equation.f90:201)
   if (prm.c1_be) {
-    if (s.dim != 3 || prm.precision != SPH_PREC_FP64) return SPH_ERR_UNSUPPORTED;
+    if (s.dim != 3) return SPH_ERR_UNSUPPORTED;
     if (!(prm.invb_det_thresh >= 0.0)) return SPH_ERR_INVALID_ARGUMENT;
   }
   s.c1_be = prm.c1_be ? 1 : 0;
@@ -872,7 +872,7 @@ int create_batch(int nsims, const SphParams* params, const SphGeometry* geoms, c
   A(P.key, N); A(P.slot, N); A(P.cell_count, C + 1); A(P.cell_start, C + 1);
   A(P.tmp_src, N); A(P.tmp_id, N); A(P.tmp_key, N);
   A(P.ACC, N); A(P.DDEN, N);
-  if (h->precision == SPH_PREC_FP32C) A(P.MSUM, 9 * N);
+  if (h->precision == SPH_PREC_FP32C) A(P.MSUM, (h->any_c1 ? 12 : 9) * N);   // C1: + the pressure-gradient sums
   if (h->precision == SPH_PREC_FP32C && h->any_teta_v) A(P.VF2, N);
   if (h->any_c1) A(P.BG, 9 * N);
   if (h->any_c1_divu) A(P.BD, 9 * N);
@@ -979,6 +979,7 @@ int create_batch(int nsims, const SphParams* params, const SphGeometry* geoms, c
   b.sms = prop.multiProcessorCount;
   for (int c = 0; c < kGridClasses; ++c) b.grid[c] = 0;
   b.c1 = h->any_c1 ? 1 : 0;
+  b.c1_divu = h->any_c1_divu ? 1 : 0;
   *out = h;
   return SPH_OK;
 }

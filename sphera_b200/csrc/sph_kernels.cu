@@ -2090,8 +2090,13 @@ __device__ __forceinline__ void separation_f32(const SimDev& s, RunCursor<DIM>& 
 // k_momentum_f32_finish adds the FP64 wall terms (an independent sum), the
 // laminar flag, gravity and the elastic reaction and, in the fused step,
 // the leapfrog update and the CFL minimum.
-template <int DIM>
-__global__ void __launch_bounds__(kBlock, 3) k_momentum_f32(DevBatch b) {
+// C1 (C1_BE): the pressure-gradient accumulator of inter_EqMoto.f90:195-204,
+// -m_j (p_j - p_i) / (rho_i rho_j) PK3 r, is summed apart as well (the
+// pressure difference formed in FP64), so the finishing launch can
+// renormalise it with B_ren_gradp (inter_EqMoto.f90:255-260) and keep the
+// ALE1 accumulator, the symmetric sum less it, as it is.
+template <int DIM, bool C1 = false>
+__global__ void __launch_bounds__(kBlock, C1 ? 2 : 3) k_momentum_f32(DevBatch b) {
   __shared__ SimDev s;
   int cur = -1;
   const Particles& P = b.P;
@@ -2106,6 +2111,7 @@ __global__ void __launch_bounds__(kBlock, 3) k_momentum_f32(DevBatch b) {
     int cnt = 0;
     float4 xfi = make_float4(0.f, 0.f, 0.f, 0.f);
     float vix = 0.f, viy = 0.f, viz = 0.f, rhof = 1.f, Pi = 0.f;
+    double piD = 0.0;
     if (active) {
       double4 v4 = P.V[p];
       double2 rp = P.RP[p];
@@ -2115,6 +2121,7 @@ __global__ void __launch_bounds__(kBlock, 3) k_momentum_f32(DevBatch b) {
       viz = (float)v4.z;
       rhof = (float)rp.x;
       Pi = (float)(rp.y / (rp.x * rp.x));
+      piD = rp.y;
       cnt = b.ncount[p];
     }
     const float ckf = xfi.w, dz = s.dcdf[2];
@@ -2124,6 +2131,9 @@ __global__ void __launch_bounds__(kBlock, 3) k_momentum_f32(DevBatch b) {
     Kahan tp0, tp1, tp2, td0, td1, td2, tv0, tv1, tv2;
     tp0.zero(); tp1.zero(); tp2.zero(); td0.zero(); td1.zero(); td2.zero(); tv0.zero(); tv1.zero(); tv2.zero();
     float cp0 = 0.f, cp1 = 0.f, cp2 = 0.f, cd0 = 0.f, cd1 = 0.f, cd2 = 0.f, cv0 = 0.f, cv1 = 0.f, cv2 = 0.f;
+    Kahan tg0, tg1, tg2;
+    tg0.zero(); tg1.zero(); tg2.zero();
+    float cg0 = 0.f, cg1 = 0.f, cg2 = 0.f;
     // one list chunk (4 entries) per iteration: entries, compensation and
     // the next chunk's load handled once per chunk
     const int nch = (cnt + 3) >> 2;
@@ -2144,6 +2154,13 @@ __global__ void __launch_bounds__(kBlock, 3) k_momentum_f32(DevBatch b) {
       cp0 = fmaf(pf, d0, cp0);
       if (DIM == 3) cp1 = fmaf(pf, d1, cp1);
       cp2 = fmaf(pf, d2, cp2);
+      if (C1) {
+        const float dpf = (float)(__ldg(reinterpret_cast<const double*>(P.RP + q) + 1) - piD);
+        const float gf = -(mj * dpf * rcp_approx(rhof * rfj.x) * PK3);
+        cg0 = fmaf(gf, d0, cg0);
+        if (DIM == 3) cg1 = fmaf(gf, d1, cg1);
+        cg2 = fmaf(gf, d2, cg2);
+      }
       float dv0 = vj.x - vix, dv1 = vj.y - viy, dv2 = vj.z - viz;
       // viscomon amon / rsum and viscomorris nu4 / (nu rsum + 1e-3) from one
       // reciprocal of their denominators' product
@@ -2175,6 +2192,10 @@ __global__ void __launch_bounds__(kBlock, 3) k_momentum_f32(DevBatch b) {
       td0.add(cd0); td1.add(cd1); td2.add(cd2);
       tv0.add(cv0); tv1.add(cv1); tv2.add(cv2);
       cp0 = cp1 = cp2 = cd0 = cd1 = cd2 = cv0 = cv1 = cv2 = 0.f;
+      if (C1) {
+        tg0.add(cg0); tg1.add(cg1); tg2.add(cg2);
+        cg0 = cg1 = cg2 = 0.f;
+      }
     }
     if (active) {
       double* o = P.MSUM + p;
@@ -2188,11 +2209,19 @@ __global__ void __launch_bounds__(kBlock, 3) k_momentum_f32(DevBatch b) {
       o[6 * st] = tv0.val();
       o[7 * st] = tv1.val();
       o[8 * st] = tv2.val();
+      if (C1) {
+        o[9 * st] = tg0.val();
+        o[10 * st] = tg1.val();
+        o[11 * st] = tg2.val();
+      }
     }
   }
 }
 
-template <int DIM, bool FUSED>
+// C1: as the FP64 form (k_momentum<3, F, true>): the first step completes
+// and inverts B_ren_gradp in the wall pass; the renormalised pressure-
+// gradient accumulator joins the ALE1 accumulator and the wall terms.
+template <int DIM, bool FUSED, bool C1 = false>
 __global__ void __launch_bounds__(kBlock) k_momentum_f32_finish(DevBatch b) {
   __shared__ SimDev s;
   int cur = -1;
@@ -2227,7 +2256,24 @@ __global__ void __launch_bounds__(kBlock) k_momentum_f32_finish(DevBatch b) {
       const int bstart = nb > 0 ? P.bdt_start[p] : 0;
       double tpres[3] = {0, 0, 0}, tdiss[3] = {0, 0, 0}, tvisc[3] = {0, 0, 0};
       const double* geff = dyn->geff;
-      if (nb > 0) {
+      const bool c1 = C1 && DIM == 3 && s.c1_be;
+      if (c1) {
+        double B[9];
+        const bool first = dyn->step == 0;
+        load_b(P.BG, P.total_slots, p, B);
+        if (nb > 0)
+          me_boundary3d<true>(s, b, nb, bstart, vi, rhoi, pi, P.L[p], geff, tpres, tdiss, tvisc, B, first);
+        else if (first)
+          b_inversion(B, s.invb_det_thresh);
+        if (first) store_b(P.BG, P.total_slots, p, B);
+        // inter_EqMoto.f90:255-260: the pressure-gradient sum renormalised,
+        // the ALE1 sum (the symmetric sum less it) as it is
+        double g[3];
+        for (int d = 0; d < 3; ++d) g[d] = P.MSUM[(size_t)(9 + d) * P.total_slots + p];
+        const double al[3] = {ms[0] - g[0], ms[1] - g[1], ms[2] - g[2]};
+        b_renormalise(B, g);
+        for (int d = 0; d < 3; ++d) ms[d] = g[d] + al[d];
+      } else if (nb > 0) {
         const int lam = P.L[p];
         if (DIM == 3) me_boundary3d(s, b, nb, bstart, vi, rhoi, pi, lam, geff, tpres, tdiss, tvisc);
         else me_boundary2d(s, b, nb, bstart, vi, rhoi, pi, lam, geff, tpres, tdiss, tvisc);
@@ -2287,8 +2333,13 @@ __global__ void __launch_bounds__(kBlock) k_momentum_f32_finish(DevBatch b) {
 // sum of each particle to DDEN, and k_continuity_f32_finish, once the
 // boundary data exist, forms dden = (SA-SPH wall term) - (pair sum) and, in
 // the fused step, Leapfrog_continuity and the EoS.
-template <int DIM>
-__global__ void __launch_bounds__(kBlock, 5) k_continuity_f32(DevBatch b) {
+// DIVU (C1_BE and C1_divu, 3D): a simulation that renormalises sums the
+// whole velocity-gradient tensor, G(a, k) = sum rho_i (m_j / rho_j) PK1
+// (v_j - v_i)_a r_k, nine compensated sums written to MSUM, which the
+// finishing launch renormalises with B_ren_divu (Continuity_Equation.f90:
+// 119-126,201-217); the others of the batch sum as without it.
+template <int DIM, bool DIVU = false>
+__global__ void __launch_bounds__(kBlock, DIVU ? 2 : 5) k_continuity_f32(DevBatch b) {
   __shared__ SimDev s;
   int cur = -1;
   const Particles& P = b.P;
@@ -2314,9 +2365,17 @@ __global__ void __launch_bounds__(kBlock, 5) k_continuity_f32(DevBatch b) {
     }
     const float ckf = xfi.w, dz = s.dcdf[2];
     RunCursor<DIM> rc;
+    const bool tensor = DIVU && DIM == 3 && s.c1_be && s.c1_divu;
     Kahan sum;
     sum.zero();
     float part = 0.f;   // 4-entry partial sum, compensated into sum per chunk
+    Kahan gs[9];
+    float gp[9];
+#pragma unroll
+    for (int a = 0; a < 9; ++a) {
+      gs[a].zero();
+      gp[a] = 0.f;
+    }
     ListPrefetcher lr;
     lr.init(b.nlist, p, b.list_cap4, cnt);
     const int nmax = __reduce_max_sync(0xffffffffu, (unsigned)cnt);
@@ -2329,17 +2388,44 @@ __global__ void __launch_bounds__(kBlock, 5) k_continuity_f32(DevBatch b) {
       float rr = fmaf(d2, d2, fmaf(d1, d1, d0 * d0));
       const float PK1 = kernel_pk1_f32(fc, rr);
       float c = rhof * vj.w * PK1;    // rho_i (m_j / rho_j) PK1
-      part = fmaf(c, fmaf(vj.z - viz, d2, fmaf(vj.y - viy, d1, (vj.x - vix) * d0)), part);
-      if ((k & 3) == 3 || k == cnt - 1) {
-        sum.add(part);
-        part = 0.f;
+      const bool flush = (k & 3) == 3 || k == cnt - 1;
+      if (DIVU && tensor) {
+        const float cv[3] = {c * (vj.x - vix), c * (vj.y - viy), c * (vj.z - viz)};
+        const float dd[3] = {d0, d1, d2};
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+          for (int q = 0; q < 3; ++q) gp[3 * a + q] = fmaf(cv[a], dd[q], gp[3 * a + q]);
+        if (flush) {
+#pragma unroll
+          for (int a = 0; a < 9; ++a) {
+            gs[a].add(gp[a]);
+            gp[a] = 0.f;
+          }
+        }
+      } else {
+        part = fmaf(c, fmaf(vj.z - viz, d2, fmaf(vj.y - viy, d1, (vj.x - vix) * d0)), part);
+        if (flush) {
+          sum.add(part);
+          part = 0.f;
+        }
       }
     }
-    if (active) P.DDEN[p] = sum.val();
+    if (active) {
+      if (DIVU && tensor) {
+#pragma unroll
+        for (int a = 0; a < 9; ++a) P.MSUM[(size_t)a * P.total_slots + p] = gs[a].val();
+      } else {
+        P.DDEN[p] = sum.val();
+      }
+    }
   }
 }
 
-template <int DIM, bool FUSED>
+// C1 (3D): the frontiers complete both matrices, which are inverted for
+// every particle (continuity_boundary_c1, FP64); with C1_divu the pair
+// tensor is renormalised with B_ren_divu and its trace enters drho/dt.
+template <int DIM, bool FUSED, bool C1 = false>
 __global__ void __launch_bounds__(kBlock) k_continuity_f32_finish(DevBatch b) {
   __shared__ SimDev s;
   int cur = -1;
@@ -2354,8 +2440,23 @@ __global__ void __launch_bounds__(kBlock) k_continuity_f32_finish(DevBatch b) {
     const double rhoi = P.RP[p].x;
     double dden = 0.0;
     const int nb = P.bdt_count[p];
-    if (nb > 0) dden = continuity_boundary<DIM>(s, b, dyn, nb, P.bdt_start[p], vi, rhoi);
-    dden = dden - P.DDEN[p];
+    if (C1 && DIM == 3 && s.c1_be) {
+      dden = continuity_boundary_c1(s, b, dyn, nb, nb > 0 ? P.bdt_start[p] : 0, vi, rhoi, p);
+      if (s.c1_divu) {
+        double B[9], g[3][3];
+        load_b(P.BD, P.total_slots, p, B);
+        for (int a = 0; a < 3; ++a) {
+          for (int q = 0; q < 3; ++q) g[a][q] = P.MSUM[(size_t)(3 * a + q) * P.total_slots + p];
+          b_renormalise(B, g[a]);
+        }
+        dden = dden - (g[0][0] + g[1][1] + g[2][2]);
+      } else {
+        dden = dden - P.DDEN[p];
+      }
+    } else {
+      if (nb > 0) dden = continuity_boundary<DIM>(s, b, dyn, nb, P.bdt_start[p], vi, rhoi);
+      dden = dden - P.DDEN[p];
+    }
     if (FUSED) {
       double rho = rhoi + dyn->dt * dden;
       if (s.density_thresholds == 1) {
@@ -3386,7 +3487,11 @@ void launch_renormalisation(const DevBatch& b, cudaStream_t st) {
 void launch_momentum_f32(const DevBatch& b, bool fused, cudaStream_t st) {
   int g = blocks_for(b, kGridMomentum);
   int gf = blocks_for(b);
-  if (b.dim == 3) {
+  if (b.dim == 3 && b.c1) {
+    k_momentum_f32<3, true><<<g, kBlock, 0, st>>>(b);
+    if (fused) k_momentum_f32_finish<3, true, true><<<gf, kBlock, 0, st>>>(b);
+    else k_momentum_f32_finish<3, false, true><<<gf, kBlock, 0, st>>>(b);
+  } else if (b.dim == 3) {
     k_momentum_f32<3><<<g, kBlock, 0, st>>>(b);
     if (fused) k_momentum_f32_finish<3, true><<<gf, kBlock, 0, st>>>(b);
     else k_momentum_f32_finish<3, false><<<gf, kBlock, 0, st>>>(b);
@@ -3399,13 +3504,17 @@ void launch_momentum_f32(const DevBatch& b, bool fused, cudaStream_t st) {
 
 void launch_continuity_f32_pairs(const DevBatch& b, cudaStream_t st) {
   int g = blocks_for(b, kGridContinuity);
-  if (b.dim == 3) k_continuity_f32<3><<<g, kBlock, 0, st>>>(b);
+  if (b.dim == 3 && b.c1_divu) k_continuity_f32<3, true><<<g, kBlock, 0, st>>>(b);
+  else if (b.dim == 3) k_continuity_f32<3><<<g, kBlock, 0, st>>>(b);
   else k_continuity_f32<2><<<g, kBlock, 0, st>>>(b);
 }
 
 void launch_continuity_f32_finish(const DevBatch& b, bool fused, cudaStream_t st) {
   int g = blocks_for(b);
-  if (b.dim == 3) {
+  if (b.dim == 3 && b.c1) {
+    if (fused) k_continuity_f32_finish<3, true, true><<<g, kBlock, 0, st>>>(b);
+    else k_continuity_f32_finish<3, false, true><<<g, kBlock, 0, st>>>(b);
+  } else if (b.dim == 3) {
     if (fused) k_continuity_f32_finish<3, true><<<g, kBlock, 0, st>>>(b);
     else k_continuity_f32_finish<3, false><<<g, kBlock, 0, st>>>(b);
   } else {

@@ -35,7 +35,8 @@ struct DevBatch {
   int grid_blocks;         // blocks of the persistent particle kernels (default)
   int sms;                 // streaming multiprocessors of the device
   int grid[kGridClasses];  // autotuned blocks per kernel class (0 = grid_blocks)
-  int c1;                  // some simulation renormalises (C1_BE, 3D FP64): P.BG (and P.BD) allocated
+  int c1;                  // some simulation renormalises (C1_BE, 3D): P.BG (and P.BD) allocated
+  int c1_divu;             // some simulation renormalises its velocity gradients (C1_divu)
 };
 
 enum class KeyKind { Sort = 0, Reference = 1 };

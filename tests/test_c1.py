@@ -84,16 +84,17 @@ def test_oracle_2d_renormalisation_is_not_restated(oracle_lib):
         oracle_lib.Oracle(case)
 
 
-def test_c1_needs_3d_fp64():
+def test_c1_needs_3d():
     c2 = cases.dam_break_2d(dx=0.04)
     c2.params.c1_be = 1
     with pytest.raises(SphError) as e:
         memory_required([c2])
     assert e.value.code == abi.SPH_ERR_UNSUPPORTED
+    # both precision forms in 3D; the FP32c form with C1 holds three more
+    # pair sums per particle
     c3 = c1_case(precision=abi.SPH_PREC_FP32C)
-    with pytest.raises(SphError) as e:
-        memory_required([c3])
-    assert e.value.code == abi.SPH_ERR_UNSUPPORTED
+    plain = cases.dam_break_3d(dx=0.04, precision=abi.SPH_PREC_FP32C)
+    assert memory_required([c3]) > memory_required([plain])
 
 
 def test_c1_threshold_must_be_non_negative():

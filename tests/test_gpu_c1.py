@@ -132,8 +132,10 @@ def test_autotune_keeps_the_matrices():
     assert np.array_equal(before[1], after[1])
 
 
-def test_fp32c_with_c1_is_unsupported():
-    case = c1_case(precision=abi.SPH_PREC_FP32C)
+def test_c1_in_2d_is_unsupported():
+    case = cases.dam_break_2d(dx=0.04)
+    case.params.c1_be = 1
+    case.params.invb_det_thresh = 1.0e-3
     with pytest.raises(SphError) as e:
         Simulation(case)
     assert e.value.code == abi.SPH_ERR_UNSUPPORTED
