@@ -102,12 +102,14 @@ typedef struct SphParams {
     /* 1st-order consistency (input_any_t%C1_BE, %C1_divu, %invB_det_thresh):
      * the pressure-gradient terms of the momentum equation are renormalised
      * with B_ren_gradp and, with c1_divu as well, the velocity gradients of
-     * the continuity equation with B_ren_divu.  3D, both precision forms
-     * (the matrices, their inversion and the renormalisation in FP64; in
-     * the FP32c form the renormalised pair sums are compensated FP32 sums);
-     * 2D returns SPH_ERR_UNSUPPORTED.  A matrix whose |det| is below
-     * invb_det_thresh is replaced by -I (B_ren_gradp_inversion.f90:62-73).
-     * 0 disables.                                                          */
+     * the continuity equation with B_ren_divu.  Both precision forms (the
+     * matrices, their inversion and the renormalisation in FP64; in the
+     * FP32c form the renormalised pair sums are compensated FP32 sums).  A
+     * matrix whose |det| is below invb_det_thresh is replaced by -I
+     * (B_ren_gradp_inversion.f90:62-73).  In 2D the matrices have a zero y
+     * row and column, so they always take that -I (which renormalises
+     * nothing) and invb_det_thresh must be > 0 (the reference would divide
+     * by the zero determinant).  0 disables.                                */
     int32_t c1_be;
     int32_t c1_divu;
     double  invb_det_thresh;        /* >= 0                                           */

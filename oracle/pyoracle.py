@@ -82,8 +82,6 @@ class Oracle:
     """One simulation held by the oracle, in the reference's particle order."""
 
     def __init__(self, case, nthreads=0):
-        if case.params.dim == 2 and case.params.c1_be:
-            raise NotImplementedError("the 1st-order consistency renormalisation is restated for 3D only")
         L = lib()
         self.case = case
         st = case.state

@@ -305,6 +305,10 @@ static void grad_W_sub(const Oracle& o, int kernel_ID, const double* r_vec, doub
     if (q <= 2.0) dW = -(3.0 * ((2.0 - q) * (2.0 - q)) * (15.0 / (64.0 * PIGRECO * h3)));
   }
   for (int k = 0; k < 3; ++k) grad_W[k] = dW / o.h * r_vec[k] / abs_r;
+  if (o.dim == 2) {   // grad_W_sub.f90:79-88 (SPACE_2D)
+    for (int k = 0; k < 3; ++k)
+      grad_W[k] = (kernel_ID == 1) ? grad_W[k] * o.h * 10.0 / 7.0 : grad_W[k] * o.h * 4.0 / 3.0;
+  }
 }
 
 // Matrix_Inversion_3x3.f90:50-74 inside B_ren_gradp_inversion.f90 /
@@ -1257,15 +1261,24 @@ void AddBoundaryContribution_to_CE3D(Oracle& o, int npi, int Ncbf, double* gu, d
   }
 }
 
-// AddBoundaryContribution_to_CE2D.f90:73-147 (C1_BE and ALE3 off)
-void AddBoundaryContribution_to_CE2D(const Oracle& o, int npi, int IntNcbs, double* gu, double* gw) {
-  const Particle& p = o.pg[npi];
+// AddBoundaryContribution_to_CE2D.f90:73-147 (ALE3 off)
+void AddBoundaryContribution_to_CE2D(Oracle& o, int npi, int IntNcbs, double* gu, double* gw) {
+  Particle& p = o.pg[npi];
   const int acix[2] = {0, 2};
   int ibdt = o.BDP[3 * (npi - 1) + 2];
   for (int icbs = 1; icbs <= IntNcbs; ++icbs) {
     const BDT& e = o.BDTab[ibdt + icbs - 2];
     const Side& s = o.sides[e.CloBoNum - 1];
     const SphZone& z = o.zones[s.stretch - 1];
+    if (o.prm.c1_be) {   // AddBoundaryContribution_to_CE2D.f90:81-94: -RN IntWdV
+      const double IntWdV = e.BoundaryIntegral[2];
+      for (int a = 0; a < 3; ++a)
+        for (int c = 0; c < 3; ++c) {
+          const double aux = -s.RN[a][c] * IntWdV;
+          if (o.prm.c1_divu) p.Bd[a][c] = p.Bd[a][c] + aux;
+          p.Bg[a][c] = p.Bg[a][c] + aux;
+        }
+    }
     double IntWdS = e.BoundaryIntegral[0];
     double dvel[2];
     if (z.type == SPH_ZONE_FIXE) {
@@ -1440,9 +1453,10 @@ void AddBoundaryContributions_to_ME3D(Oracle& o, int npi, int Ncbf, double* tpre
 }
 
 // AddBoundaryContributions_to_ME2D.f90:96-402 (fixe/tapi, mode 1, C1/ALE3 off)
-void AddBoundaryContributions_to_ME2D(const Oracle& o, int npi, int IntNcbs, double* tpres, double* tdiss, double* tvisc) {
+void AddBoundaryContributions_to_ME2D(Oracle& o, int npi, int IntNcbs, double* tpres, double* tdiss, double* tvisc) {
   const double pibmink = 10.0;
-  const Particle& p = o.pg[npi];
+  Particle& p = o.pg[npi];
+  const bool c1_first = o.prm.c1_be && o.on_going_time_step == 1;
   const int acix[2] = {0, 2};
   double ro0 = o.prm.den0, roi = p.dens, pressi = p.pres;
   double distpimin = o.prm.dx;
@@ -1481,6 +1495,10 @@ void AddBoundaryContributions_to_ME2D(const Oracle& o, int npi, int IntNcbs, dou
     }
     RG_sum[0] = RG_sum[0] + RG[0];
     RG_sum[1] = RG_sum[1] + RG[1];
+    if (c1_first) {   // AddBoundaryContributions_to_ME2D.f90:290-300: -RN IntWdV
+      for (int a = 0; a < 3; ++a)
+        for (int c = 0; c < 3; ++c) p.Bg[a][c] = p.Bg[a][c] + -s.RN[a][c] * IntWdV;
+    }
     ALEt[0] = ALEt[0] - nnlocal[0] * QiiIntWdS;
     ALEt[2] = ALEt[2] - nnlocal[1] * QiiIntWdS;
     if (xpi >= 0.0 && xpi <= s.length) {
@@ -1500,7 +1518,18 @@ void AddBoundaryContributions_to_ME2D(const Oracle& o, int npi, int IntNcbs, dou
       }
     }
   }
+  if (c1_first) B_ren_inversion(p.Bg, o.prm.invb_det_thresh);   // :377-383
   if (IntNcbs == 0) return;
+  if (o.prm.c1_be) {   // :384-392: RG_sum renormalised with B_ren_gradp
+    double aux2[3] = {RG_sum[0], 0.0, RG_sum[1]}, aux[3];
+    for (int a = 0; a < 3; ++a) {
+      double sum = 0.0;
+      for (int c = 0; c < 3; ++c) sum = sum + p.Bg[a][c] * aux2[c];
+      aux[a] = sum;
+    }
+    RG_sum[0] = -aux[0];
+    RG_sum[1] = -aux[2];
+  }
   for (int i = 0; i < 2; ++i) {
     tpres[acix[i]] = tpres[acix[i]] - RG_sum[i] - ALEt[acix[i]];
     tdiss[acix[i]] = tdiss[acix[i]] - VMon[i];

@@ -179,8 +179,10 @@ int prepare_sim(const SphParams& prm, const SphGeometry& g, int cap, HostSim& hs
   // 1st-order consistency: 3D, FP64 form; C1_divu acts only with C1_BE
   // (CalcVarLength.f90:285, Continuity_Equation.f90:201)
   if (prm.c1_be) {
-    if (s.dim != 3) return SPH_ERR_UNSUPPORTED;
     if (!(prm.invb_det_thresh >= 0.0)) return SPH_ERR_INVALID_ARGUMENT;
+    // the 2D matrices are singular (zero y row and column): with a zero
+    // threshold the reference's Matrix_Inversion_3x3 divides by det = 0
+    if (s.dim == 2 && !(prm.invb_det_thresh > 0.0)) return SPH_ERR_INVALID_ARGUMENT;
   }
   s.c1_be = prm.c1_be ? 1 : 0;
   s.c1_divu = (prm.c1_be && prm.c1_divu) ? 1 : 0;

@@ -1522,6 +1522,59 @@ __global__ void __launch_bounds__(kBlock, 4) k_neighbour_lists(DevBatch b) {
 // step) and continuity passes, which also invert.  One sqrt and the
 // division r / h are shared by the range test and both gradients; the
 // constant factors come from the host (SimDev::c1_w*).
+// The 2D SA-SPH frontier terms of the renormalisation matrices, -RN IntWdV
+// per close side (AddBoundaryContribution_to_CE2D.f90:81-94 for both
+// matrices in every continuity pass; AddBoundaryContributions_to_ME2D.f90:
+// 290-300 for B_ren_gradp on the first step, GRADP_ONLY), then their
+// inversion (SASPH_continuity.f90:112-119, ME2D.f90:377-383).  In 2D the
+// matrices have a zero y row and column, so their determinant is zero and
+// the inversion always gives the -I of B_ren_gradp_inversion.f90:67-72
+// (a positive invb_det_thresh is required); renormalising with -I leaves
+// every vector as it is, so the rates are the plain form's and only the
+// matrices themselves are formed here.
+template <bool GRADP_ONLY>
+__global__ void k_c1_frontier_2d(DevBatch b) {
+  __shared__ SimDev s;
+  int cur = -1;
+  const Particles& P = b.P;
+  const int total = P.total_slots;
+  for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
+    Tile tl = b.tiles[t];
+    load_sim(s, b.sims, tl.sim, cur);
+    const SimDyn* dyn = b.dyn + tl.sim;
+    if (!s.c1_be || dyn->frozen || (GRADP_ONLY && dyn->step != 0)) continue;
+    const int p = tl.start + threadIdx.x;
+    if (threadIdx.x >= tl.count || p >= s.p_off + dyn->nag) continue;
+    const bool divu = !GRADP_ONLY && s.c1_divu;
+    double Bg[9], Bd[9];
+    load_b(P.BG, total, p, Bg);
+    if (divu) load_b(P.BD, total, p, Bd);
+    const int nb = P.bdt_count[p];
+    const int start = nb > 0 ? P.bdt_start[p] : 0;
+    for (int u = 0; u < nb; ++u) {
+      const BdtEntry& e = P.bdt[start + u];
+      const SideDev& S = b.sides[s.side_off + e.clobonum - 1];
+      const double IntWdV = e.bi[2];
+      const int ax[2] = {0, 2};
+      for (int a = 0; a < 2; ++a)
+        for (int c = 0; c < 2; ++c) {
+          const double aux = -S.RN[a][c] * IntWdV;
+          Bg[3 * ax[a] + ax[c]] = Bg[3 * ax[a] + ax[c]] + aux;
+          if (divu) Bd[3 * ax[a] + ax[c]] = Bd[3 * ax[a] + ax[c]] + aux;
+        }
+    }
+    if (divu) {
+      b_inversion(Bd, s.invb_det_thresh);
+      store_b(P.BD, total, p, Bd);
+    }
+    b_inversion(Bg, s.invb_det_thresh);
+    store_b(P.BG, total, p, Bg);
+  }
+}
+
+// 2D (DIM = 2): grad_W_sub.f90:79-88 scales both gradients by h 10/7
+// (beta-spline) and h 4/3 (anti-cluster); y is zero throughout.
+template <int DIM>
 __global__ void __launch_bounds__(kBlock, 2) k_renormalisation(DevBatch b) {
   __shared__ SimDev s;
   int cur = -1;
@@ -1559,13 +1612,21 @@ __global__ void __launch_bounds__(kBlock, 2) k_renormalisation(DevBatch b) {
       double go[3];
       // anti-cluster kernel (q <= 2 here)
       double t = -(3.0 * (w * w) * s.c1_w2) / s.h;
-      for (int c = 0; c < 3; ++c) go[c] = t * r[c] / abs_r * mj / rhoj;
+      for (int c = 0; c < 3; ++c) {
+        double gw = t * r[c] / abs_r;
+        if (DIM == 2) gw = gw * s.h * 4.0 / 3.0;
+        go[c] = gw * mj / rhoj;
+      }
       for (int c = 0; c < 3; ++c)
         for (int kk = 0; kk < 3; ++kk) Bg[3 * kk + c] = Bg[3 * kk + c] + r[c] * go[kk];
       if (divu) {
         // beta-spline (q < 2 here)
         t = (qh <= 1.0 ? s.c1_w1a * (9.0 / 4.0 * (qh * qh) - 3.0 * qh) : -(s.c1_w1b * (w * w))) / s.h;
-        for (int c = 0; c < 3; ++c) go[c] = t * r[c] / abs_r * mj / rhoj;
+        for (int c = 0; c < 3; ++c) {
+          double gw = t * r[c] / abs_r;
+          if (DIM == 2) gw = gw * s.h * 10.0 / 7.0;
+          go[c] = gw * mj / rhoj;
+        }
         for (int c = 0; c < 3; ++c)
           for (int kk = 0; kk < 3; ++kk) Bd[3 * kk + c] = Bd[3 * kk + c] + r[c] * go[kk];
       }
@@ -3460,8 +3521,17 @@ void launch_boundary(const DevBatch& b, cudaStream_t st) {
   }
 }
 
+// 2D with C1_BE: the frontier terms and inversion of the matrices (their
+// renormalisation is the identity in 2D, see k_c1_frontier_2d)
+static void c1_frontier_2d(const DevBatch& b, bool gradp_only, cudaStream_t st) {
+  if (b.dim != 2 || !b.c1) return;
+  if (gradp_only) k_c1_frontier_2d<true><<<blocks_for(b), kBlock, 0, st>>>(b);
+  else k_c1_frontier_2d<false><<<blocks_for(b), kBlock, 0, st>>>(b);
+}
+
 void launch_momentum(const DevBatch& b, bool fused, cudaStream_t st) {
   int g = blocks_for(b, kGridMomentum);
+  c1_frontier_2d(b, true, st);
   if (b.dim == 3 && b.c1) {
     if (fused) k_momentum<3, true, true><<<g, kBlock, 0, st>>>(b);
     else k_momentum<3, false, true><<<g, kBlock, 0, st>>>(b);
@@ -3481,12 +3551,15 @@ void launch_neighbour_lists(const DevBatch& b, cudaStream_t st) {
 }
 
 void launch_renormalisation(const DevBatch& b, cudaStream_t st) {
-  if (b.dim == 3 && b.c1) k_renormalisation<<<blocks_for(b, kGridLists), kBlock, 0, st>>>(b);
+  if (!b.c1) return;
+  if (b.dim == 3) k_renormalisation<3><<<blocks_for(b, kGridLists), kBlock, 0, st>>>(b);
+  else k_renormalisation<2><<<blocks_for(b, kGridLists), kBlock, 0, st>>>(b);
 }
 
 void launch_momentum_f32(const DevBatch& b, bool fused, cudaStream_t st) {
   int g = blocks_for(b, kGridMomentum);
   int gf = blocks_for(b);
+  c1_frontier_2d(b, true, st);
   if (b.dim == 3 && b.c1) {
     k_momentum_f32<3, true><<<g, kBlock, 0, st>>>(b);
     if (fused) k_momentum_f32_finish<3, true, true><<<gf, kBlock, 0, st>>>(b);
@@ -3511,6 +3584,7 @@ void launch_continuity_f32_pairs(const DevBatch& b, cudaStream_t st) {
 
 void launch_continuity_f32_finish(const DevBatch& b, bool fused, cudaStream_t st) {
   int g = blocks_for(b);
+  c1_frontier_2d(b, false, st);
   if (b.dim == 3 && b.c1) {
     if (fused) k_continuity_f32_finish<3, true, true><<<g, kBlock, 0, st>>>(b);
     else k_continuity_f32_finish<3, false, true><<<g, kBlock, 0, st>>>(b);
@@ -3532,6 +3606,7 @@ void launch_refresh_f32(const DevBatch& b, cudaStream_t st) { k_refresh_f32<<<bl
 
 void launch_continuity(const DevBatch& b, bool fused, cudaStream_t st) {
   int g = blocks_for(b, kGridContinuity);
+  c1_frontier_2d(b, false, st);
   if (b.dim == 3 && b.c1) {
     if (fused) k_continuity<3, true, true><<<g, kBlock, 0, st>>>(b);
     else k_continuity<3, false, true><<<g, kBlock, 0, st>>>(b);

@@ -77,19 +77,64 @@ def test_oracle_minus_identity_fallback_equals_plain_form(oracle_lib):
     assert np.array_equal(sa["rho"], sb["rho"])
 
 
-def test_oracle_2d_renormalisation_is_not_restated(oracle_lib):
-    case = cases.dam_break_2d(dx=0.04)
+def c1_case_2d(dx=0.04, divu=1, thresh=1.0e-3, **kw):
+    case = cases.dam_break_2d(dx=dx, **kw)
     case.params.c1_be = 1
-    with pytest.raises(NotImplementedError):
-        oracle_lib.Oracle(case)
+    case.params.c1_divu = divu
+    case.params.invb_det_thresh = thresh
+    return case
 
 
-def test_c1_needs_3d():
-    c2 = cases.dam_break_2d(dx=0.04)
-    c2.params.c1_be = 1
+def test_oracle_2d_matrices_are_singular_and_fall_back(oracle_lib):
+    """2D: the x-z matrices (grad_W_sub's 2D factors 10/7 and 4/3) have a
+    zero y row and column, so their determinant is zero and the inversion
+    takes the -I fallback; renormalising with -I changes nothing, so the
+    rates equal the plain form's."""
+    case = c1_case_2d()
+    o = oracle_lib.Oracle(case)
+    o.prepare()
+    bg, bd = o.get_c1()
+    m = interior(o.get()["x"], lo=(0.15, -1.0, 0.15), hi=(0.85, 1.0, 1.85))
+    assert m.sum() > 100
+    # the fluid sums: y row and column zero, the x-z block near -I inside
+    assert np.all(bg[:, 1, :] == 0.0) and np.all(bg[:, :, 1] == 0.0)
+    sub = bg[m][:, ::2, ::2]
+    assert np.abs(sub + np.eye(2)).max() < 0.15
+    plain = cases.dam_break_2d(dx=0.04)
+    p = oracle_lib.Oracle(plain)
+    p.prepare()
+    o.rhs_momentum()
+    p.rhs_momentum()
+    bg, _ = o.get_c1()
+    assert np.all(bg == -np.eye(3))
+    # the time loop's order: a search between the momentum and continuity
+    # passes forms the fluid sums again, which the continuity pass completes
+    # and inverts
+    o.search()
+    p.search()
+    o.continuity()
+    p.continuity()
+    a, b = o.get(), p.get()
+    assert np.array_equal(a["acc"], b["acc"])
+    assert np.array_equal(a["dden"], b["dden"])
+    bg, bd = o.get_c1()
+    assert np.all(bg == -np.eye(3)) and np.all(bd == -np.eye(3))
+    # whole steps from the IC (the time loop's order) equal the plain form's
+    o2, p2 = oracle_lib.Oracle(case), oracle_lib.Oracle(plain)
+    o2.prepare()
+    p2.prepare()
+    o2.step(20)
+    p2.step(20)
+    assert np.array_equal(o2.get()["x"], p2.get()["x"])
+    assert np.array_equal(o2.get()["v"], p2.get()["v"])
+
+
+def test_c1_in_2d_needs_a_positive_threshold():
+    c2 = c1_case_2d(thresh=0.0)
     with pytest.raises(SphError) as e:
         memory_required([c2])
-    assert e.value.code == abi.SPH_ERR_UNSUPPORTED
+    assert e.value.code == abi.SPH_ERR_INVALID_ARGUMENT
+    assert memory_required([c1_case_2d()]) > memory_required([cases.dam_break_2d(dx=0.04)])
     # both precision forms in 3D; the FP32c form with C1 holds three more
     # pair sums per particle
     c3 = c1_case(precision=abi.SPH_PREC_FP32C)

@@ -132,10 +132,52 @@ def test_autotune_keeps_the_matrices():
     assert np.array_equal(before[1], after[1])
 
 
-def test_c1_in_2d_is_unsupported():
+@pytest.mark.parametrize("precision", [abi.SPH_PREC_FP64, abi.SPH_PREC_FP32C])
+def test_2d_matrices_bit_exact_and_steps_equal_plain(precision, oracle_lib):
+    """2D (grad_W_sub's 2D factors; frontier terms -RN IntWdV): the matrices
+    after the search, after the first momentum pass and after a continuity
+    pass equal the oracle's bit for bit; being singular they invert to -I,
+    so whole steps equal the plain form's."""
+    case = cases.dam_break_2d(dx=0.04, precision=precision)
+    case.params.c1_be = 1
+    case.params.c1_divu = 1
+    case.params.invb_det_thresh = 1.0e-3
+    ref = cases.dam_break_2d(dx=0.04)
+    ref.params.c1_be = 1
+    ref.params.c1_divu = 1
+    ref.params.invb_det_thresh = 1.0e-3
+    sim = Simulation(case)
+    sim.upload(case.state)
+    o = oracle_lib.Oracle(ref)
+    o.prepare()
+    for stage in ("search", "momentum", "continuity"):
+        if stage == "momentum":
+            sim.rhs_momentum(want=False)
+            o.rhs_momentum()
+        elif stage == "continuity":
+            sim.ord_grid()
+            sim.boundary_data_tab()
+            o.search()
+            sim.continuity(want=False)
+            o.continuity()
+        bg, bd = sim.dump_renormalisation()
+        og, od = o.get_c1()
+        assert np.array_equal(bg, og), stage
+        assert np.array_equal(bd, od), stage
+    a = Simulation(case)
+    a.upload(case.state)
+    plain = cases.dam_break_2d(dx=0.04, precision=precision)
+    b = Simulation(plain)
+    b.upload(plain.state)
+    a.step(30)
+    b.step(30)
+    assert np.array_equal(a.download().x, b.download().x)
+
+
+def test_2d_needs_a_positive_threshold():
     case = cases.dam_break_2d(dx=0.04)
     case.params.c1_be = 1
-    case.params.invb_det_thresh = 1.0e-3
+    case.params.invb_det_thresh = 0.0
     with pytest.raises(SphError) as e:
         Simulation(case)
-    assert e.value.code == abi.SPH_ERR_UNSUPPORTED
+    assert e.value.code == abi.SPH_ERR_INVALID_ARGUMENT
