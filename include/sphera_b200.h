@@ -229,6 +229,9 @@ void* sph_stream(SphHandle* h);
 int  sph_batch_create(int32_t nsims, const SphParams* params, const SphGeometry* geometries,
                       const int32_t* n_capacity, SphHandle** out);
 int  sph_batch_upload(SphHandle* h, int32_t nsims, const SphState* states);
+/* One member's state (as sph_download).  The result is that member's own
+ * status: another member's failure does not affect it, and a failed or
+ * cancelled member's state is still copied while its code is returned.   */
 int  sph_batch_download(SphHandle* h, int32_t sim, SphState* state);
 /* A simulation whose time reaches t_end (> 0) stops advancing; its state
  * stays on the device for download while the others continue.             */
@@ -261,9 +264,19 @@ int  sph_idle(SphHandle* h, int32_t* idle);
 /* Autotuner (no reference counterpart): sizes the persistent grid of the
  * neighbour-list, momentum, continuity and boundary kernels on the live
  * state by timing `reps` launches of each candidate (1 to 32 blocks per
- * SM) of variants that leave the state unchanged, then rebuilds the step
- * graph.  grid_out[0..4] (may be NULL) receives the chosen blocks.        */
+ * SM) of variants that leave the state unchanged, and for the FP32c
+ * momentum and continuity pair loops also picks their shape (0: lean, 3
+ * and 5 blocks per SM; 1: a list chunk's neighbour records loaded
+ * together, 2 and 3 blocks per SM), then rebuilds the step graph.
+ * grid_out (may be NULL; 7 entries) receives in [0..4] the chosen blocks
+ * of lists, momentum, continuity, boundary find and integrals, in [5] and
+ * [6] the momentum and continuity shapes.                                 */
 int  sph_autotune(SphHandle* h, int32_t reps, int32_t* grid_out);
+/* Applies a launch configuration in sph_autotune's 7-entry layout (blocks
+ * per kernel class, 0 = the default, then the two loop shapes), e.g. one
+ * tuned earlier on a similar state; the next step rebuilds its graph.
+ * Launch shapes change no result.                                          */
+int  sph_set_launch_shape(SphHandle* h, const int32_t* shape);
 
 /* ---------------------------------------------------------------------- */
 /* Fine-grained calls, one per replaced Fortran call site                  */

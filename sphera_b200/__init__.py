@@ -85,6 +85,7 @@ def lib():
         "sph_idle": ([vp, ip], C.c_int),
         "sph_global_quantities": ([vp, C.c_int32, dp], C.c_int),
         "sph_dump_laminar": ([vp, ip], C.c_int),
+        "sph_set_launch_shape": ([vp, ip], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -97,6 +98,20 @@ def lib():
 def _chk(code, what):
     if code != abi.SPH_OK:
         raise SphError(code, what)
+
+
+_SHAPE_KEYS = ("lists", "momentum", "continuity", "boundary", "integrals", "momentum_shape", "continuity_shape")
+
+
+def _autotune(h, reps):
+    g = np.zeros(7, np.int32)
+    _chk(lib().sph_autotune(h, int(reps), abi.iptr(g)), "sph_autotune")
+    return dict(zip(_SHAPE_KEYS, g.tolist()))
+
+
+def _set_launch_shape(h, shape):
+    g = np.array([int(shape.get(k, 0)) for k in _SHAPE_KEYS], np.int32)
+    _chk(lib().sph_set_launch_shape(h, abi.iptr(g)), "sph_set_launch_shape")
 
 
 class Simulation:
@@ -230,10 +245,14 @@ class Simulation:
 
     # ------------------------------------------------------------ autotuner
     def autotune(self, reps=3):
-        """Sizes the persistent grids of the pair, list and boundary kernels."""
-        g = np.zeros(5, np.int32)
-        _chk(lib().sph_autotune(self._h, int(reps), abi.iptr(g)), "sph_autotune")
-        return dict(zip(("lists", "momentum", "continuity", "boundary", "integrals"), g.tolist()))
+        """Sizes the persistent grids of the pair, list and boundary kernels
+        and picks the FP32c momentum pair loop's shape (0 lean, 1 batched
+        record loads)."""
+        return _autotune(self._h, reps)
+
+    def set_launch_shape(self, shape):
+        """Applies a launch configuration (autotune's dict; missing keys 0)."""
+        _set_launch_shape(self._h, shape)
 
     # ------------------------------------------------------------ profiling
     PHASES = ("momentum", "ord_grid", "boundary_data_tab", "neighbour_lists", "continuity", "time_step")
@@ -363,9 +382,10 @@ class Batch:
         return bool(v.value)
 
     def autotune(self, reps=3):
-        g = np.zeros(5, np.int32)
-        _chk(lib().sph_autotune(self._h, int(reps), abi.iptr(g)), "sph_autotune")
-        return dict(zip(("lists", "momentum", "continuity", "boundary", "integrals"), g.tolist()))
+        return _autotune(self._h, reps)
+
+    def set_launch_shape(self, shape):
+        _set_launch_shape(self._h, shape)
 
     def info(self, sim):
         info = abi.SphStepInfo()

@@ -982,6 +982,8 @@ int create_batch(int nsims, const SphParams* params, const SphGeometry* geoms, c
   for (int c = 0; c < kGridClasses; ++c) b.grid[c] = 0;
   b.c1 = h->any_c1 ? 1 : 0;
   b.c1_divu = h->any_c1_divu ? 1 : 0;
+  b.mom_batch = 0;
+  b.con_batch = 0;
   *out = h;
   return SPH_OK;
 }
@@ -1097,9 +1099,13 @@ int sph_batch_set_end_time(SphHandle* h, int32_t sim, double t_end) {
   return cuda_status(cudaStreamSynchronize(h->stream));
 }
 
+// Copies one simulation's state back.  Its result is that simulation's own
+// status (another member's failure does not stop the download of a healthy
+// one); a failed or cancelled member's state is still copied, for
+// inspection, and its code returned.
 static int download_impl(SphHandle* h, int sim, SphState* state, double* acc, double* dden) {
   if (!h || !h->uploaded || sim < 0 || sim >= h->nsims) return SPH_ERR_INVALID_ARGUMENT;
-  SPH_TRY(sync_dyn(h));
+  SPH_TRY(read_dyn(h));
   HostSim& hs = h->sims[sim];
   int n = h->h_dyn[sim].nag;
   cudaStream_t q = h->stream;
@@ -1117,7 +1123,8 @@ static int download_impl(SphHandle* h, int sim, SphState* state, double* acc, do
   }
   if (acc) SPH_CUDA(cudaMemcpyAsync(acc, h->d_cacc + 3 * o, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, q));
   if (dden) SPH_CUDA(cudaMemcpyAsync(dden, h->d_cdden + o, sizeof(double) * n, cudaMemcpyDeviceToHost, q));
-  return cuda_status(cudaStreamSynchronize(q));
+  SPH_CUDA(cudaStreamSynchronize(q));
+  return h->h_dyn[sim].status;
 }
 
 int sph_download(SphHandle* h, SphState* state) {
@@ -1434,7 +1441,29 @@ int sph_dump_renormalisation(SphHandle* h, double* b_gradp, double* b_divu) {
 // continuity passes (their laminar-flag write is saved and restored), the
 // neighbour-list and boundary passes (idempotent) -- and the fastest kept.
 // The step graph is rebuilt with the choice.  grid_out[0..4] receives the
-// chosen blocks of lists, momentum, continuity, boundary find, integrals.
+// chosen blocks of lists, momentum, continuity, boundary find, integrals,
+// grid_out[5..6] the FP32c momentum and continuity loop shapes.
+
+// Applies a launch configuration (sph_autotune's output, or a chosen one):
+// blocks per kernel class (0 = the default) and the two pair-loop shapes.
+int sph_set_launch_shape(SphHandle* h, const int32_t* shape) {
+  if (!h || !shape) return SPH_ERR_INVALID_ARGUMENT;
+  for (int c = 0; c < kGridClasses; ++c)
+    if (shape[c] < 0) return SPH_ERR_INVALID_ARGUMENT;
+  if (shape[kGridClasses] < 0 || shape[kGridClasses] > 1 || shape[kGridClasses + 1] < 0 ||
+      shape[kGridClasses + 1] > 1)
+    return SPH_ERR_INVALID_ARGUMENT;
+  SPH_CUDA(cudaStreamSynchronize(h->stream));
+  for (int c = 0; c < kGridClasses; ++c) h->db.grid[c] = shape[c];
+  h->db.mom_batch = shape[kGridClasses];
+  h->db.con_batch = shape[kGridClasses + 1];
+  if (h->graph) {
+    cudaGraphExecDestroy(h->graph);
+    h->graph = nullptr;
+  }
+  return SPH_OK;
+}
+
 int sph_autotune(SphHandle* h, int32_t reps, int32_t* grid_out) {
   if (!h || !h->uploaded || reps <= 0) return SPH_ERR_INVALID_ARGUMENT;
   cudaStream_t q = h->stream;
@@ -1457,11 +1486,19 @@ int sph_autotune(SphHandle* h, int32_t reps, int32_t* grid_out) {
     e = cudaMallocAsync(&keep_d, nb_bytes, q);
     if (e == cudaSuccess) e = cudaMemcpyAsync(keep_d, b.P.BD, nb_bytes, cudaMemcpyDeviceToDevice, q);
   }
+  // the FP32c momentum pair loop comes in two shapes (lean at 3 blocks per
+  // SM, or a list chunk's records loaded together at 2): both are timed
+  const bool two_shapes = h->precision == SPH_PREC_FP32C && !h->any_c1;
+  int best_batch = b.mom_batch, best_cbatch = b.con_batch;
   for (int cls = 0; cls < kGridClasses && e == cudaSuccess; ++cls) {
     if (cls == kGridIntegrals && h->dim != 3) continue;
     float best = 1e30f;
     int best_g = 0;
-    for (int m : mult) {
+    const int nshapes = ((cls == kGridMomentum || cls == kGridContinuity) && two_shapes) ? 2 : 1;
+    for (int cand = 0; cand < nshapes * 6; ++cand) {
+      const int m = mult[cand % 6];
+      if (nshapes == 2 && cls == kGridMomentum) b.mom_batch = cand / 6;
+      if (nshapes == 2 && cls == kGridContinuity) b.con_batch = cand / 6;
       int g = b.sms * m;
       b.grid[cls] = g;
       auto run = [&]() {
@@ -1483,10 +1520,18 @@ int sph_autotune(SphHandle* h, int32_t reps, int32_t* grid_out) {
       if (ms < best) {
         best = ms;
         best_g = g;
+        if (nshapes == 2 && cls == kGridMomentum) best_batch = b.mom_batch;
+        if (nshapes == 2 && cls == kGridContinuity) best_cbatch = b.con_batch;
       }
     }
     b.grid[cls] = best_g;
     if (grid_out) grid_out[cls] = best_g;
+    if (cls == kGridMomentum) b.mom_batch = best_batch;
+    if (cls == kGridContinuity) b.con_batch = best_cbatch;
+  }
+  if (grid_out) {
+    grid_out[kGridClasses] = b.mom_batch;
+    grid_out[kGridClasses + 1] = b.con_batch;
   }
   if (e == cudaSuccess) e = cudaMemcpyAsync(b.P.L, b.P.L2, (size_t)h->total_slots, cudaMemcpyDeviceToDevice, q);
   if (e == cudaSuccess && keep_g) e = cudaMemcpyAsync(b.P.BG, keep_g, nb_bytes, cudaMemcpyDeviceToDevice, q);

@@ -1193,6 +1193,19 @@ __device__ __forceinline__ size_t list_base4(int p, int cap4) {
 }
 
 
+// A warp's list region -- its chunks 0 .. ceil(nmax / 4) - 1, 512 B each
+// and contiguous -- requested into L2 by one bulk prefetch from lane 0, so
+// the chunk loads of the pair loop find it in L2 instead of waiting on HBM
+// (the lists of a full-size step, 4 B per pair, do not stay in L2 between
+// the pass that writes them and the passes that read them).  A hint only:
+// 16-byte aligned address, a size in multiples of 16 bytes, no completion.
+__device__ __forceinline__ void prefetch_list_l2(const int* nlist, int p, int cap4, int nmax) {
+  if ((threadIdx.x & 31) != 0 || nmax <= 0) return;
+  const int4* a = reinterpret_cast<const int4*>(nlist) + (size_t)(p >> 5) * (size_t)cap4 * 32;
+  const unsigned bytes = (unsigned)((nmax + 3) >> 2) * 512u;
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a), "r"(bytes) : "memory");
+}
+
 // Sequential reader that loads chunk c + 1 while chunk c is consumed, so
 // the list's HBM latency overlaps four pairs' work.
 struct ListPrefetcher {
@@ -1598,6 +1611,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_renormalisation(DevBatch b) {
     ListPrefetcher lr;
     lr.init(b.nlist, p, b.list_cap4, cnt);
     const int nmax = __reduce_max_sync(0xffffffffu, (unsigned)cnt);
+    prefetch_list_l2(b.nlist, p, b.list_cap4, nmax);
     for (int k = 0; k < nmax; ++k) {
       int e = lr.get(k);
       if (k >= cnt) continue;
@@ -1712,6 +1726,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_momentum(DevBatch b) {
     ListPrefetcher lr;
     lr.init(b.nlist, p, b.list_cap4, cnt);
     const int nmax = __reduce_max_sync(0xffffffffu, (unsigned)cnt);
+    prefetch_list_l2(b.nlist, p, b.list_cap4, nmax);
     for (int k = 0; k < nmax; ++k) {
       int e = lr.get(k);
       if (k >= cnt) continue;
@@ -1964,6 +1979,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_continuity(DevBatch b) {
     ListPrefetcher lr;
     lr.init(b.nlist, p, b.list_cap4, cnt);
     const int nmax = __reduce_max_sync(0xffffffffu, (unsigned)cnt);
+    prefetch_list_l2(b.nlist, p, b.list_cap4, nmax);
     for (int k = 0; k < nmax; ++k) {
       int e = lr.get(k);
       if (k >= cnt) continue;
@@ -2156,8 +2172,13 @@ __device__ __forceinline__ void separation_f32(const SimDev& s, RunCursor<DIM>& 
 // pressure difference formed in FP64), so the finishing launch can
 // renormalise it with B_ren_gradp (inter_EqMoto.f90:255-260) and keep the
 // ALE1 accumulator, the symmetric sum less it, as it is.
-template <int DIM, bool C1 = false>
-__global__ void __launch_bounds__(kBlock, C1 ? 2 : 3) k_momentum_f32(DevBatch b) {
+// BATCH: the twelve neighbour records of a list chunk are all requested
+// before the first pair's arithmetic, four pairs' loads in flight per lane
+// instead of one, at 2 blocks of 256 per SM (the registers they need); the
+// autotuner chooses it or the lean loop (3 blocks per SM) on the live
+// state.  Both sum the same terms in the same order: identical results.
+template <int DIM, bool C1 = false, bool BATCH = false>
+__global__ void __launch_bounds__(kBlock, (C1 || BATCH) ? 2 : 3) k_momentum_f32(DevBatch b) {
   __shared__ SimDev s;
   int cur = -1;
   const Particles& P = b.P;
@@ -2199,11 +2220,11 @@ __global__ void __launch_bounds__(kBlock, C1 ? 2 : 3) k_momentum_f32(DevBatch b)
     // the next chunk's load handled once per chunk
     const int nch = (cnt + 3) >> 2;
     const int nchmax = __reduce_max_sync(0xffffffffu, (unsigned)nch);
+    prefetch_list_l2(b.nlist, p, b.list_cap4, nchmax * 4);
     const int4* lbase = reinterpret_cast<const int4*>(b.nlist) + list_base4(p, b.list_cap4);
     int4 nxt = nch > 0 ? __ldg(lbase) : make_int4(0, 0, 0, 0);
-    auto pair = [&](int e) {
+    auto pair = [&](int e, const float4& xj, const float4& vj, const float4& rfj) {
       const int q = e & kSlotMask;
-      const float4 xj = __ldg(P.XF + q), vj = __ldg(P.VF + q), rfj = __ldg(P.RF + q);
       float d0, d1, d2;
       separation_f32<DIM>(s, rc, e, xj, xfi, ckf, dz, d0, d1, d2);
       float rr = fmaf(d2, d2, fmaf(d1, d1, d0 * d0));
@@ -2245,10 +2266,27 @@ __global__ void __launch_bounds__(kBlock, C1 ? 2 : 3) k_momentum_f32(DevBatch b)
       if (c + 1 < nch) nxt = __ldg(lbase + (size_t)(c + 1) * 32);
       if (c >= nch) continue;
       const int rem = cnt - 4 * c;   // >= 1
-      pair(ch.x);
-      if (rem > 1) pair(ch.y);
-      if (rem > 2) pair(ch.z);
-      if (rem > 3) pair(ch.w);
+      if (BATCH) {
+        float4 x0, v0, r0, x1, v1, r1, x2, v2, r2, x3, v3, r3;
+        const int q0 = ch.x & kSlotMask, q1 = ch.y & kSlotMask, q2 = ch.z & kSlotMask, q3 = ch.w & kSlotMask;
+        x0 = __ldg(P.XF + q0); v0 = __ldg(P.VF + q0); r0 = __ldg(P.RF + q0);
+        if (rem > 1) { x1 = __ldg(P.XF + q1); v1 = __ldg(P.VF + q1); r1 = __ldg(P.RF + q1); }
+        if (rem > 2) { x2 = __ldg(P.XF + q2); v2 = __ldg(P.VF + q2); r2 = __ldg(P.RF + q2); }
+        if (rem > 3) { x3 = __ldg(P.XF + q3); v3 = __ldg(P.VF + q3); r3 = __ldg(P.RF + q3); }
+        pair(ch.x, x0, v0, r0);
+        if (rem > 1) pair(ch.y, x1, v1, r1);
+        if (rem > 2) pair(ch.z, x2, v2, r2);
+        if (rem > 3) pair(ch.w, x3, v3, r3);
+      } else {
+        auto one = [&](int e) {
+          const int q = e & kSlotMask;
+          pair(e, __ldg(P.XF + q), __ldg(P.VF + q), __ldg(P.RF + q));
+        };
+        one(ch.x);
+        if (rem > 1) one(ch.y);
+        if (rem > 2) one(ch.z);
+        if (rem > 3) one(ch.w);
+      }
       tp0.add(cp0); tp1.add(cp1); tp2.add(cp2);
       td0.add(cd0); td1.add(cd1); td2.add(cd2);
       tv0.add(cv0); tv1.add(cv1); tv2.add(cv2);
@@ -2399,8 +2437,10 @@ __global__ void __launch_bounds__(kBlock) k_momentum_f32_finish(DevBatch b) {
 // (v_j - v_i)_a r_k, nine compensated sums written to MSUM, which the
 // finishing launch renormalises with B_ren_divu (Continuity_Equation.f90:
 // 119-126,201-217); the others of the batch sum as without it.
-template <int DIM, bool DIVU = false>
-__global__ void __launch_bounds__(kBlock, DIVU ? 2 : 5) k_continuity_f32(DevBatch b) {
+// BATCH (not with DIVU): a list chunk's eight neighbour records requested
+// before the chunk's arithmetic, at 3 blocks per SM; the same sums.
+template <int DIM, bool DIVU = false, bool BATCH = false>
+__global__ void __launch_bounds__(kBlock, DIVU ? 2 : (BATCH ? 3 : 5)) k_continuity_f32(DevBatch b) {
   __shared__ SimDev s;
   int cur = -1;
   const Particles& P = b.P;
@@ -2437,10 +2477,42 @@ __global__ void __launch_bounds__(kBlock, DIVU ? 2 : 5) k_continuity_f32(DevBatc
       gs[a].zero();
       gp[a] = 0.f;
     }
-    ListPrefetcher lr;
-    lr.init(b.nlist, p, b.list_cap4, cnt);
     const int nmax = __reduce_max_sync(0xffffffffu, (unsigned)cnt);
-    for (int k = 0; k < nmax; ++k) {
+    prefetch_list_l2(b.nlist, p, b.list_cap4, nmax);
+    if (BATCH && !DIVU) {
+      auto contrib = [&](int e, const float4& xj, const float4& vj) {
+        float d0, d1, d2;
+        separation_f32<DIM>(s, rc, e, xj, xfi, ckf, dz, d0, d1, d2);
+        float rr = fmaf(d2, d2, fmaf(d1, d1, d0 * d0));
+        const float PK1 = kernel_pk1_f32(fc, rr);
+        float c = rhof * vj.w * PK1;
+        part = fmaf(c, fmaf(vj.z - viz, d2, fmaf(vj.y - viy, d1, (vj.x - vix) * d0)), part);
+      };
+      const int nch = (cnt + 3) >> 2, nchmax = (nmax + 3) >> 2;
+      const int4* lbase = reinterpret_cast<const int4*>(b.nlist) + list_base4(p, b.list_cap4);
+      int4 nxt = nch > 0 ? __ldg(lbase) : make_int4(0, 0, 0, 0);
+      for (int c = 0; c < nchmax; ++c) {
+        const int4 ch = nxt;
+        if (c + 1 < nch) nxt = __ldg(lbase + (size_t)(c + 1) * 32);
+        if (c >= nch) continue;
+        const int rem = cnt - 4 * c;
+        const int q0 = ch.x & kSlotMask, q1 = ch.y & kSlotMask, q2 = ch.z & kSlotMask, q3 = ch.w & kSlotMask;
+        float4 x0, v0, x1, v1, x2, v2, x3, v3;
+        x0 = __ldg(P.XF + q0); v0 = __ldg(P.VF + q0);
+        if (rem > 1) { x1 = __ldg(P.XF + q1); v1 = __ldg(P.VF + q1); }
+        if (rem > 2) { x2 = __ldg(P.XF + q2); v2 = __ldg(P.VF + q2); }
+        if (rem > 3) { x3 = __ldg(P.XF + q3); v3 = __ldg(P.VF + q3); }
+        contrib(ch.x, x0, v0);
+        if (rem > 1) contrib(ch.y, x1, v1);
+        if (rem > 2) contrib(ch.z, x2, v2);
+        if (rem > 3) contrib(ch.w, x3, v3);
+        sum.add(part);
+        part = 0.f;
+      }
+    }
+    ListPrefetcher lr;
+    lr.init(b.nlist, p, b.list_cap4, (BATCH && !DIVU) ? 0 : cnt);
+    for (int k = 0; k < ((BATCH && !DIVU) ? 0 : nmax); ++k) {
       const int e = lr.get(k);
       if (k >= cnt) continue;
       const float4 xj = __ldg(P.XF + (e & kSlotMask)), vj = __ldg(P.VF + (e & kSlotMask));
@@ -2677,6 +2749,7 @@ __global__ void __launch_bounds__(kBlock) k_velocity_smoothing(DevBatch b, const
     ListPrefetcher lr;
     lr.init(b.nlist, p, b.list_cap4, cnt);
     const int nmax = __reduce_max_sync(0xffffffffu, (unsigned)cnt);
+    prefetch_list_l2(b.nlist, p, b.list_cap4, nmax);
     for (int k = 0; k < nmax; ++k) {
       int e = lr.get(k);
       if (k >= cnt) continue;
@@ -2751,6 +2824,7 @@ __global__ void __launch_bounds__(kBlock, 4) k_velocity_smoothing_f32(DevBatch b
     ListPrefetcher lr;
     lr.init(b.nlist, p, b.list_cap4, cnt);
     const int nmax = __reduce_max_sync(0xffffffffu, (unsigned)cnt);
+    prefetch_list_l2(b.nlist, p, b.list_cap4, nmax);
     for (int k = 0; k < nmax; ++k) {
       int e = lr.get(k);
       if (k >= cnt) continue;
@@ -2807,6 +2881,7 @@ __global__ void __launch_bounds__(kBlock, 4) k_pressure_smoothing_f32(DevBatch b
     ListPrefetcher lr;
     lr.init(b.nlist, p, b.list_cap4, cnt);
     const int nmax = __reduce_max_sync(0xffffffffu, (unsigned)cnt);
+    prefetch_list_l2(b.nlist, p, b.list_cap4, nmax);
     for (int k = 0; k < nmax; ++k) {
       int e = lr.get(k);
       if (k >= cnt) continue;
@@ -2901,6 +2976,7 @@ __global__ void __launch_bounds__(kBlock) k_pressure_smoothing(DevBatch b) {
     ListPrefetcher lr;
     lr.init(b.nlist, p, b.list_cap4, cnt);
     const int nmax = __reduce_max_sync(0xffffffffu, (unsigned)cnt);
+    prefetch_list_l2(b.nlist, p, b.list_cap4, nmax);
     for (int k = 0; k < nmax; ++k) {
       int e = lr.get(k);
       if (k >= cnt) continue;
@@ -3565,11 +3641,13 @@ void launch_momentum_f32(const DevBatch& b, bool fused, cudaStream_t st) {
     if (fused) k_momentum_f32_finish<3, true, true><<<gf, kBlock, 0, st>>>(b);
     else k_momentum_f32_finish<3, false, true><<<gf, kBlock, 0, st>>>(b);
   } else if (b.dim == 3) {
-    k_momentum_f32<3><<<g, kBlock, 0, st>>>(b);
+    if (b.mom_batch) k_momentum_f32<3, false, true><<<g, kBlock, 0, st>>>(b);
+    else k_momentum_f32<3><<<g, kBlock, 0, st>>>(b);
     if (fused) k_momentum_f32_finish<3, true><<<gf, kBlock, 0, st>>>(b);
     else k_momentum_f32_finish<3, false><<<gf, kBlock, 0, st>>>(b);
   } else {
-    k_momentum_f32<2><<<g, kBlock, 0, st>>>(b);
+    if (b.mom_batch) k_momentum_f32<2, false, true><<<g, kBlock, 0, st>>>(b);
+    else k_momentum_f32<2><<<g, kBlock, 0, st>>>(b);
     if (fused) k_momentum_f32_finish<2, true><<<gf, kBlock, 0, st>>>(b);
     else k_momentum_f32_finish<2, false><<<gf, kBlock, 0, st>>>(b);
   }
@@ -3578,7 +3656,9 @@ void launch_momentum_f32(const DevBatch& b, bool fused, cudaStream_t st) {
 void launch_continuity_f32_pairs(const DevBatch& b, cudaStream_t st) {
   int g = blocks_for(b, kGridContinuity);
   if (b.dim == 3 && b.c1_divu) k_continuity_f32<3, true><<<g, kBlock, 0, st>>>(b);
+  else if (b.dim == 3 && b.con_batch) k_continuity_f32<3, false, true><<<g, kBlock, 0, st>>>(b);
   else if (b.dim == 3) k_continuity_f32<3><<<g, kBlock, 0, st>>>(b);
+  else if (b.con_batch) k_continuity_f32<2, false, true><<<g, kBlock, 0, st>>>(b);
   else k_continuity_f32<2><<<g, kBlock, 0, st>>>(b);
 }
 
