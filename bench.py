@@ -250,7 +250,7 @@ def run_reference(args, ws, rank):
     return 0
 
 
-def run_ensemble(args, ws, rank):
+def run_ensemble(args, ws, rank, emit=True):
     """256 independent 2D dam breaks (column width U[0.5, 2.0] m, height
     U[0.5, 2.5] m, dx 0.01 m) advanced together in the same launches and
     CUDA graph, FP32-compensated form, each to t_end; all requests are
@@ -294,13 +294,15 @@ def run_ensemble(args, ws, rank):
         "steps": {"min": int(st.min()), "max": int(st.max())},
         "elapsed_s": elapsed,
     }
+    b.close()
+    if not emit:
+        return line
     if rank == 0:
         print(json.dumps(line), flush=True)
-    b.close()
     return 0
 
 
-def run_serving(args, ws, rank):
+def run_serving(args, ws, rank, emit=True):
     """A seeded Poisson stream (mean 20 requests/s) of 3D dam-break and
     sloshing-tank requests (dx log-uniform in [0.005, 0.0125] m, 55k-1M
     particles, FP32-compensated form, each run to t = 0.3 s) served in real
@@ -337,9 +339,64 @@ def run_serving(args, ws, rank):
         "max_concurrent_requests": srv.max_concurrent, "result_d2h_bytes": d2h,
         "elapsed_s": wall,
     }
+    if not emit:
+        return line
     if rank == 0:
         print(json.dumps(line), flush=True)
     return 0
+
+
+def _quick_rate(case, steps=5, min_seconds=1.0):
+    """particle-steps/s of graph replays of `case` after the autotuner,
+    timed with CUDA events on the library's stream (median of windows of
+    `steps` replays, repeated to at least min_seconds), and its phase times."""
+    import torch
+    from sphera_b200 import Simulation
+    sim = Simulation(case)
+    sim.upload(case.state)
+    tuned = sim.autotune(reps=2)
+    sim.step(3)
+    stream = torch.cuda.ExternalStream(sim.stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    wins = []
+    while not wins or sum(wins) < min_seconds * 1e3:
+        sim.sync()
+        e0.record(stream)
+        sim.step_async(steps)
+        e1.record(stream)
+        e1.synchronize()
+        sim.sync()
+        wins.append(e0.elapsed_time(e1))
+    ms = statistics.median(wins) / steps
+    sim.counters(reset=True)
+    ph = sim.profile_phases(3)
+    cnt = sim.counters()
+    sim.close()
+    return {"value": case.n / (ms * 1e-3), "ms_per_step": ms, "windows": len(wins), "autotuned": tuned,
+            "phases_ms_per_step": {k: v / 3 for k, v in ph.items()},
+            "pairs_per_particle": cnt["pairs"] / 3 / case.n, "candidates_per_particle": cnt["candidates"] / 3 / case.n}
+
+
+def run_extras(ws, rank):
+    """The other workloads of the metric, one GPU: the neighbour-search and
+    pair-loop microbenchmark (16M-particle random box, one whole step, both
+    forms), the 256-simulation 2D ensemble to 0.5 s and the serving stream
+    (8 Poisson requests to 0.3 s)."""
+    import types
+    from sphera_b200 import abi, cases
+    out = {}
+    rb = {}
+    for name, prec in (("fp32c", abi.SPH_PREC_FP32C), ("fp64", abi.SPH_PREC_FP64)):
+        rb[name] = _quick_rate(cases.random_box(n=16_000_000, precision=prec))
+    rb["workload"] = ("random_box: 16000000 particles uniform in a 2.52 m cube (mean spacing 0.01 m), "
+                      "rho = 1000 (1 + N(0, 1e-3)), v ~ N(0, 0.1) m/s, no walls; whole steps replayed from the graph")
+    rb["speedup_fp32c_vs_fp64"] = rb["fp32c"]["value"] / rb["fp64"]["value"]
+    out["random_box_16m"] = rb
+    ens = types.SimpleNamespace(n_sims=256, t_end=0.5)
+    out["ensemble_256"] = run_ensemble(ens, ws, rank, emit=False)
+    srv = types.SimpleNamespace(requests=8, t_end=0.3, hbm_budget_gib=4.0)
+    out["serving"] = run_serving(srv, ws, rank, emit=False)
+    return out
 
 
 def _fp_summary(r, n, fp_peak, flop_pair):
@@ -392,6 +449,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--cpu-steps", type=int, default=3)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the random-box, ensemble and serving workloads of the default run")
     ap.add_argument("--dry-run", action="store_true", help="rank plumbing only, no GPU work")
     ap.add_argument("--workload", default="dam_break_3d", choices=["dam_break_3d", "random_box", "ensemble", "serving"])
     ap.add_argument("--n", type=int, default=16_000_000, help="particles of the random-box workload")
@@ -637,9 +696,12 @@ def run_step_bench(args, ws, rank, local):
         "clocks": head["clocks"],
         "cpu_baseline": cpu,
     }
+    sim.close()
+    if ws == 1 and not args.no_extras and args.workload == "dam_break_3d" and args.dx == 0.005 \
+            and not args.c1 and args.teta == 0.0:
+        line["workloads"] = run_extras(ws, rank)
     if rank == 0:
         print(json.dumps(line), flush=True)
-    sim.close()
     return 0
 
 
