@@ -462,6 +462,8 @@ def main():
                     help="lattice spacing of the 3D dam break (0.005: the 864000-particle workload)")
     ap.add_argument("--forms", default="both", choices=["both", "fp32c", "fp64"])
     ap.add_argument("--autotune", type=int, default=1, help="size the persistent grids on the live state first")
+    ap.add_argument("--shape", default=None,
+                    help="force the FP32c momentum,continuity pair-loop shapes, e.g. 1,1 (0 lean, 1 batched loads)")
     ap.add_argument("--teta", type=float, default=0.0,
                     help="partial smoothing coefficient TetaP = TetaV of the dam-break workload (0: off)")
     ap.add_argument("--c1", action="store_true",
@@ -572,6 +574,12 @@ def run_step_bench(args, ws, rank, local):
         sim = Simulation(case)
         sim.upload(case.state)
         grids = sim.autotune(reps=3) if args.autotune else None
+        if args.shape is not None:
+            # a fixed launch configuration (profiling the same kernels
+            # without the autotuner's sweeps): pair-loop shapes, default grids
+            m, c = (int(v) for v in args.shape.split(","))
+            sim.set_launch_shape(dict(grids or {}, momentum_shape=m, continuity_shape=c))
+            grids = dict(grids or {}, momentum_shape=m, continuity_shape=c)
         sim.step(args.warmup)
         stream = torch.cuda.ExternalStream(sim.stream)
         e0 = torch.cuda.Event(enable_timing=True)
