@@ -316,6 +316,36 @@ int  sph_leapfrog_continuity(SphHandle* h);
 int  sph_eos(SphHandle* h);
 
 /* ---------------------------------------------------------------------- */
+/* One simulation split into slabs along x (no reference counterpart: the  */
+/* reference runs one shared-memory process).  Each slab is a handle that  */
+/* holds the particles of its x cells plus one layer of ghost cells on     */
+/* each side, copies of the neighbouring slabs' particles; a host          */
+/* orchestrator exchanges them (sphera_b200/slab.py).  With every slab's   */
+/* particles uploaded in increasing order of their index in the whole      */
+/* simulation, each owned particle sees the neighbours, order and          */
+/* arithmetic it has in the undivided run, bit for bit.                    */
+/* ---------------------------------------------------------------------- */
+
+/* A slab: the whole simulation's grid (CreaGrid.f90:51-74 on
+ * params->domain) restricted to x cells cell_lo..cell_hi (1-based,
+ * inclusive), its origin and cell size kept, so a particle lies in the cell
+ * it has in the whole grid.  Partial smoothing, C1 and pesodt != 0 return
+ * SPH_ERR_UNSUPPORTED.                                                     */
+int  sph_create_slab(const SphParams* params, const SphGeometry* geometry, int32_t n_capacity,
+                     int32_t cell_lo, int32_t cell_hi, SphHandle** out);
+/* Replaces the particle set (caller order, as sph_upload) keeping the
+ * simulation's time, step and dt, and runs the search on it: OrdGrid1, the
+ * neighbour lists and ComputeBoundaryDataTab (time_step_loop.f90:286-324).
+ * Every particle must lie inside the slab's grid (nothing is removed in a
+ * slab's particle order).  Single simulations without C1.                  */
+int  sph_replace_particles(SphHandle* h, const SphState* state);
+/* Sets the next step's dt (e.g. the minimum over the slabs of the dt each
+ * closed its step with, which is the whole simulation's dt when pesodt = 0;
+ * before the first step the IC's dt too), with dtvel and the body force
+ * that follow from it.  pesodt != 0 returns SPH_ERR_UNSUPPORTED.            */
+int  sph_set_time_step(SphHandle* h, double dt);
+
+/* ---------------------------------------------------------------------- */
 /* Post-processing                                                         */
 /* ---------------------------------------------------------------------- */
 

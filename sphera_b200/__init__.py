@@ -86,6 +86,10 @@ def lib():
         "sph_global_quantities": ([vp, C.c_int32, dp], C.c_int),
         "sph_dump_laminar": ([vp, ip], C.c_int),
         "sph_set_launch_shape": ([vp, ip], C.c_int),
+        "sph_create_slab": ([C.POINTER(abi.SphParams), C.POINTER(abi.SphGeometry), C.c_int32, C.c_int32,
+                             C.c_int32, hp], C.c_int),
+        "sph_replace_particles": ([vp, C.POINTER(abi.SphState)], C.c_int),
+        "sph_set_time_step": ([vp, C.c_double], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -117,7 +121,9 @@ def _set_launch_shape(h, shape):
 class Simulation:
     """One simulation on the device (a one-entry batch of the C ABI)."""
 
-    def __init__(self, case=None, params=None, geometry=None, capacity=None):
+    def __init__(self, case=None, params=None, geometry=None, capacity=None, cells=None):
+        """cells = (lo, hi): a slab of the simulation, its x cells lo..hi
+        (1-based, inclusive) of the whole grid (sph_create_slab)."""
         if case is not None:
             params, geometry = case.params, case.geometry
             capacity = capacity or case.n
@@ -125,9 +131,21 @@ class Simulation:
         self.geometry = geometry
         self.capacity = int(capacity)
         self._h = C.c_void_p()
-        _chk(lib().sph_create(C.byref(params), C.byref(geometry.struct), self.capacity, C.byref(self._h)),
-             "sph_create")
+        if cells is None:
+            _chk(lib().sph_create(C.byref(params), C.byref(geometry.struct), self.capacity, C.byref(self._h)),
+                 "sph_create")
+        else:
+            _chk(lib().sph_create_slab(C.byref(params), C.byref(geometry.struct), self.capacity, int(cells[0]),
+                                       int(cells[1]), C.byref(self._h)), "sph_create_slab")
         self.n = 0
+
+    def replace_particles(self, state):
+        """A new particle set, the clock kept; the search runs on it."""
+        _chk(lib().sph_replace_particles(self._h, C.byref(state.struct)), "sph_replace_particles")
+        self.n = state.n
+
+    def set_time_step(self, dt):
+        _chk(lib().sph_set_time_step(self._h, float(dt)), "sph_set_time_step")
 
     def close(self):
         if self._h:

@@ -124,7 +124,11 @@ int cell_indices(const SimDev& s, int nc, int& i, int& j, int& k) {   // CellInd
   return ncij;
 }
 
-int prepare_sim(const SphParams& prm, const SphGeometry& g, int cap, HostSim& hs) {
+// cell_lo, cell_hi (1-based, inclusive; 0 = the whole grid): the x cells of
+// a slab of a decomposed simulation, which keeps the whole grid's origin and
+// cell size so every particle lies in the cell it has in the whole grid.
+int prepare_sim(const SphParams& prm, const SphGeometry& g, int cap, HostSim& hs, int cell_lo = 0,
+                int cell_hi = 0) {
   if (prm.dim != 2 && prm.dim != 3) return SPH_ERR_INVALID_ARGUMENT;
   if (!(prm.dx > 0.0) || !(prm.trunc > 0.0) || !(prm.den0 > 0.0) || !(prm.eps > 0.0)) return SPH_ERR_INVALID_ARGUMENT;
   if (!(prm.teta_p >= 0.0) || !(prm.teta_v >= 0.0)) return SPH_ERR_INVALID_ARGUMENT;
@@ -244,6 +248,12 @@ int prepare_sim(const SphParams& prm, const SphGeometry& g, int cap, HostSim& hs
     s.rr_lo = std::nextafter((float)(s.square_doubleh - band), 0.0f);
     s.rr_hi = std::nextafter((float)(s.square_doubleh + band), 3.0e38f);
     s.pad_f = 0.0f;
+  }
+  s.ioff = 0;
+  if (cell_lo > 0) {
+    if (cell_hi < cell_lo || cell_hi > s.ncd[0]) return SPH_ERR_INVALID_ARGUMENT;
+    s.ioff = cell_lo - 1;
+    s.ncd[0] = cell_hi - cell_lo + 1;
   }
   long long ncells = (long long)s.ncd[0] * s.ncd[1] * s.ncd[2];
   if (ncells > (1LL << 30)) return SPH_ERR_INVALID_ARGUMENT;
@@ -429,8 +439,9 @@ int prepare_sim(const SphParams& prm, const SphGeometry& g, int cap, HostSim& hs
       double cxyz[3][2];
       int idx[3] = {i, j, k};
       for (int d = 0; d < 3; ++d) {
-        cxyz[d][0] = s.extr_lo[d] + s.dcd[d] * (idx[d] - 1);
-        cxyz[d][1] = s.extr_lo[d] + s.dcd[d] * idx[d];
+        const int gi = idx[d] + (d == 0 ? s.ioff : 0);   // the whole grid's index
+        cxyz[d][0] = s.extr_lo[d] + s.dcd[d] * (gi - 1);
+        cxyz[d][1] = s.extr_lo[d] + s.dcd[d] * gi;
       }
       double cn[8][3];
       int nv = 0;
@@ -773,7 +784,7 @@ int build_graph(SphHandle* h) {
 // With bytes_out set, nothing touches the device: the arrays are sized,
 // their total goes to *bytes_out and no handle is returned.
 int create_batch(int nsims, const SphParams* params, const SphGeometry* geoms, const int32_t* caps,
-                 SphHandle** out, uint64_t* bytes_out = nullptr) {
+                 SphHandle** out, uint64_t* bytes_out = nullptr, const int32_t* cell_range = nullptr) {
   const bool dry = bytes_out != nullptr;
   if ((!out && !dry) || nsims <= 0 || !params || !geoms || !caps) return SPH_ERR_INVALID_ARGUMENT;
   if (out) *out = nullptr;
@@ -798,7 +809,8 @@ int create_batch(int nsims, const SphParams* params, const SphGeometry* geoms, c
       delete h;
       return SPH_ERR_INVALID_ARGUMENT;
     }
-    int st = prepare_sim(params[s], geoms[s], caps[s], h->sims[s]);
+    int st = cell_range ? prepare_sim(params[s], geoms[s], caps[s], h->sims[s], cell_range[2 * s], cell_range[2 * s + 1])
+                        : prepare_sim(params[s], geoms[s], caps[s], h->sims[s]);
     if (st != SPH_OK) { delete h; return st; }
     if (params[s].teta_v > 1.0e-9) h->any_teta_v = true;
     if (params[s].teta_p > 0.0) h->any_teta_p = true;
@@ -1223,6 +1235,46 @@ int sph_batch_status(SphHandle* h, int32_t* frozen, double* time, int32_t* steps
     if (status) status[s] = h->h_dyn[s].status;
   }
   return SPH_OK;
+}
+
+// ------------------------------------------------------------------- slabs
+int sph_create_slab(const SphParams* params, const SphGeometry* geometry, int32_t n_capacity, int32_t cell_lo,
+                    int32_t cell_hi, SphHandle** out) {
+  if (!params || !geometry || cell_lo < 1) return SPH_ERR_INVALID_ARGUMENT;
+  // the renormalisation matrices and the smoothing passes need exchanges
+  // this decomposition does not make; the time-step override assumes pesodt 0
+  if (params->c1_be || params->teta_v > 1.0e-9 || params->teta_p > 0.0 || params->pesodt != 0.0)
+    return SPH_ERR_UNSUPPORTED;
+  const int32_t range[2] = {cell_lo, cell_hi};
+  return create_batch(1, params, geometry, &n_capacity, out, nullptr, range);
+}
+
+// A new particle set with the simulation's clock kept: OrdGrid1, the
+// neighbour lists and ComputeBoundaryDataTab on it (the search of
+// time_step_loop.f90:286-324), no time-step evaluation.
+int sph_replace_particles(SphHandle* h, const SphState* state) {
+  if (!h || !h->uploaded || h->nsims != 1 || !state) return SPH_ERR_INVALID_ARGUMENT;
+  if (h->any_c1) return SPH_ERR_UNSUPPORTED;
+  SPH_TRY(read_dyn(h));
+  SPH_TRY(upload_sim(h, 0, state));
+  h->h_dyn[0].nag = state->n;
+  cudaStream_t q = h->stream;
+  SPH_CUDA(cudaMemcpyAsync(h->d_dyn, h->h_dyn.data(), sizeof(SimDyn), cudaMemcpyHostToDevice, q));
+  launch_init_from_caller(h->db, h->d_cx, h->d_cv, h->d_crho, h->d_cp, h->d_cm, q);
+  sort_sequence(h, q);
+  launch_boundary(h->db, q);
+  lists_pass(h, q);
+  SPH_CUDA(cudaGetLastError());
+  return sync_dyn(h);
+}
+
+int sph_set_time_step(SphHandle* h, double dt) {
+  if (!h || !h->uploaded || !(dt > 0.0)) return SPH_ERR_INVALID_ARGUMENT;
+  for (int s = 0; s < h->nsims; ++s)
+    if (h->sims[s].prm.pesodt != 0.0) return SPH_ERR_UNSUPPORTED;
+  launch_set_dt(h->db, dt, h->stream);
+  SPH_CUDA(cudaGetLastError());
+  return sync_dyn(h);
 }
 
 // Stops simulation `sim` from the next enqueued launch on (stream-ordered,

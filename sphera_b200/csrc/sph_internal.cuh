@@ -44,7 +44,8 @@ struct SimDev {
   int nmaxpartj;          // NMAXPARTJ
   int maxcb;              // MAXCLOSEBOUNDFACES (3D) / MAXCLOSEBOUNDSIDES (2D)
   int bdt_quota;          // BoundaryDataTab entries this simulation may take from the pool
-  int pad_quota;
+  int ioff;               // slab of a decomposed simulation: local x cell i is global cell i + ioff
+                          // (extr_lo and dcd stay the whole grid's, so cells are assigned as in it)
   int face_off, nfaces;   // faces (3D)
   int side_off, nsides;   // sides (2D)
   int edge_off, nedges;   // convex edges (3D)

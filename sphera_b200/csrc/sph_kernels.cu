@@ -43,7 +43,7 @@ __device__ __forceinline__ void load_sim(SimDev& dst, const SimDev* src, int sim
 // false if outside the grid.
 __device__ __forceinline__ bool particle_cell(const SimDev& s, double x, double y, double z, int& i, int& j,
                                               int& k) {
-  double ci = ceil((x - s.extr_lo[0]) / s.dcd[0]);
+  double ci = ceil((x - s.extr_lo[0]) / s.dcd[0]) - (double)s.ioff;   // exact: whole numbers
   double ck = ceil((z - s.extr_lo[2]) / s.dcd[2]);
   double cj = (s.dim == 3) ? ceil((y - s.extr_lo[1]) / s.dcd[1]) : 1.0;
   if (!(ci >= 1.0 && ci <= (double)s.ncd[0] && cj >= 1.0 && cj <= (double)s.ncd[1] && ck >= 1.0 &&
@@ -61,7 +61,7 @@ __device__ __forceinline__ bool particle_cell(const SimDev& s, double x, double 
 __device__ __forceinline__ float4 screening_copy(const SimDev& s, const double4& x) {
   int i, j, k;
   if (!particle_cell(s, x.x, x.y, x.z, i, j, k)) return make_float4(0.f, 0.f, 0.f, -8.0f);
-  double ox = s.extr_lo[0] + s.dcd[0] * (i - 1);
+  double ox = s.extr_lo[0] + s.dcd[0] * (i + s.ioff - 1);
   double oy = (s.dim == 3) ? s.extr_lo[1] + s.dcd[1] * (j - 1) : 0.0;
   double oz = s.extr_lo[2] + s.dcd[2] * (k - 1);
   return make_float4((float)(x.x - ox), (float)(x.y - oy), (float)(x.z - oz), (float)k);
@@ -3220,6 +3220,24 @@ __global__ void k_finalize(DevBatch b, int mode) {
   d.geff[2] = s.grav[2];
 }
 
+// sph_set_time_step: the next step's dt set from outside (the minimum over
+// the slabs of a decomposed simulation, each of which closed its step with
+// the minimum over its own particles).  With pesodt = 0 the closing's dt is
+// that minimum itself, so the whole simulation's dt is the minimum of the
+// slabs'; before the first step the IC's dt (dt_prev) is the same value.
+// dtvel and the next step's body force follow from it as in k_finalize.
+__global__ void k_set_dt(DevBatch b, double dt) {
+  const int sim = blockIdx.x * blockDim.x + threadIdx.x;
+  if (sim >= b.nsims) return;
+  const SimDev& s = b.sims[sim];
+  SimDyn& d = b.dyn[sim];
+  d.dt = dt;
+  if (d.step == 0) d.dt_prev = dt;
+  d.dtvel = 0.5 * (d.dt + d.dt_prev);
+  d.geff[0] = s.forcing_aw2 != 0.0 ? s.grav[0] + s.forcing_aw2 * forcing_sin(s.forcing_w * (d.time + d.dt))
+                                   : s.grav[0];
+}
+
 // sph_batch_cancel: a simulation still advancing stops from the next launch
 // on, with status SPH_CANCELLED; one already frozen (finished or failed)
 // keeps its status.
@@ -3565,6 +3583,10 @@ void launch_scan(const DevBatch& b, int* cell_start, cudaStream_t st) {
 }
 
 void launch_cancel(const DevBatch& b, int sim, cudaStream_t st) { k_cancel<<<1, 32, 0, st>>>(b, sim); }
+
+void launch_set_dt(const DevBatch& b, double dt, cudaStream_t st) {
+  k_set_dt<<<(b.nsims + 127) / 128, 128, 0, st>>>(b, dt);
+}
 
 void launch_sort_reset(const DevBatch& b, cudaStream_t st) {
   k_sort_reset<<<(b.nsims + 127) / 128, 128, 0, st>>>(b);
