@@ -52,14 +52,14 @@ KERNELS_PER_STEP = 17
 KERNELS_PER_STEP_FP64 = 15
 # algorithmic bytes of the fused FP32c momentum pass (k_momentum_f32 pair
 # sums + k_momentum_f32_finish): per particle, each record read once -- X 32,
-# V 32, RP 16, XF 16, VF 16, RF 16 (the neighbours' XF/VF/RF are these same
+# V 32, RP 16, XF 16, VF 16, RM 8 (the neighbours' XF/VF/RM are these same
 # records), L 1, I 4, ncount 4, bdt_count 4 -- and written once -- X2 32,
 # V2 32, P2 8, I2 4, L2 1 -- plus the nine pair sums passed between the two
 # launches (72 B written, 72 B read); 4 B per neighbour-list entry and 168 B
 # per boundary entry.  The FP64 pass (one launch) reads X, V, RP, L, I,
 # ncount, bdt_count and the neighbours' X, V, RP and writes the same record:
 # 218 B per particle.
-MOM_BYTES_PER_PARTICLE = 362
+MOM_BYTES_PER_PARTICLE = 354
 MOM_BYTES_PER_PARTICLE_FP64 = 218
 LIST_ENTRY_BYTES = 4
 BDT_ENTRY_BYTES = 168

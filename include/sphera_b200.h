@@ -171,6 +171,19 @@ typedef struct SphDiagnostics {
     int32_t n_cells;                /* Grid%nmax                                      */
 } SphDiagnostics;
 
+/* The simulation's clock between steps (a checkpoint of time_step_loop's
+ * own variables): what Memo_Results.f90 writes before pg(1:nag) in a
+ * restart record (it, simulation_time, dt) plus what the next step needs
+ * to continue bit for bit.                                                 */
+typedef struct SphClock {
+    double  time;                   /* simulation_time                                */
+    double  dt;                     /* dt of the next step                            */
+    double  dt_prev;                /* dt of the last completed step (dtvel's other half) */
+    double  dt_average;             /* time_step_duration's running mean (pesodt)     */
+    int32_t step;                   /* on_going_time_step (completed steps)           */
+    int32_t reserved;
+} SphClock;
+
 typedef struct SphHandle SphHandle;
 
 /* ---------------------------------------------------------------------- */
@@ -336,14 +349,32 @@ int  sph_create_slab(const SphParams* params, const SphGeometry* geometry, int32
 /* Replaces the particle set (caller order, as sph_upload) keeping the
  * simulation's time, step and dt, and runs the search on it: OrdGrid1, the
  * neighbour lists and ComputeBoundaryDataTab (time_step_loop.f90:286-324).
- * Every particle must lie inside the slab's grid (nothing is removed in a
- * slab's particle order).  Single simulations without C1.                  */
-int  sph_replace_particles(SphHandle* h, const SphState* state);
+ * laminar ([n], caller order, or NULL for all 0) carries pg%laminar_flag,
+ * which the next momentum pass's wall terms read.  Every particle must lie
+ * inside the slab's grid (nothing is removed in a slab's particle order).
+ * Single simulations without C1.                                           */
+int  sph_replace_particles(SphHandle* h, const SphState* state, const int32_t* laminar);
 /* Sets the next step's dt (e.g. the minimum over the slabs of the dt each
  * closed its step with, which is the whole simulation's dt when pesodt = 0;
  * before the first step the IC's dt too), with dtvel and the body force
  * that follow from it.  pesodt != 0 returns SPH_ERR_UNSUPPORTED.            */
 int  sph_set_time_step(SphHandle* h, double dt);
+
+/* ---------------------------------------------------------------------- */
+/* Checkpoint and resume (the state part of a restart: Memo_Results.f90    */
+/* writes it, pg(1:nag) and the clock; ReadRestartFile.f90 reads it back).  */
+/* ---------------------------------------------------------------------- */
+
+/* The clock of a single simulation.                                       */
+int  sph_get_clock(SphHandle* h, SphClock* clock);
+/* Resume: after sph_upload of a checkpointed state (sph_download), set the
+ * clock it was saved with and pg%laminar_flag ([n], caller order, as
+ * sph_dump_laminar gave it; NULL for all 0, the IC's value).  The next
+ * step then continues as the uninterrupted run would, bit for bit.  dtvel
+ * and the next step's body force follow from the clock.  Single
+ * simulations; C1 returns SPH_ERR_UNSUPPORTED (its inverted matrices are
+ * not part of the state).                                                 */
+int  sph_set_clock(SphHandle* h, const SphClock* clock, const int32_t* laminar);
 
 /* ---------------------------------------------------------------------- */
 /* Post-processing                                                         */

@@ -88,8 +88,10 @@ def lib():
         "sph_set_launch_shape": ([vp, ip], C.c_int),
         "sph_create_slab": ([C.POINTER(abi.SphParams), C.POINTER(abi.SphGeometry), C.c_int32, C.c_int32,
                              C.c_int32, hp], C.c_int),
-        "sph_replace_particles": ([vp, C.POINTER(abi.SphState)], C.c_int),
+        "sph_replace_particles": ([vp, C.POINTER(abi.SphState), ip], C.c_int),
         "sph_set_time_step": ([vp, C.c_double], C.c_int),
+        "sph_get_clock": ([vp, C.POINTER(abi.SphClock)], C.c_int),
+        "sph_set_clock": ([vp, C.POINTER(abi.SphClock), ip], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -139,13 +141,29 @@ class Simulation:
                                        int(cells[1]), C.byref(self._h)), "sph_create_slab")
         self.n = 0
 
-    def replace_particles(self, state):
-        """A new particle set, the clock kept; the search runs on it."""
-        _chk(lib().sph_replace_particles(self._h, C.byref(state.struct)), "sph_replace_particles")
+    def replace_particles(self, state, laminar=None):
+        """A new particle set (and its laminar flags), the clock kept; the
+        search runs on it."""
+        lam = None if laminar is None else np.ascontiguousarray(laminar, dtype=np.int32)
+        _chk(lib().sph_replace_particles(self._h, C.byref(state.struct), abi.iptr(lam)), "sph_replace_particles")
         self.n = state.n
 
     def set_time_step(self, dt):
         _chk(lib().sph_set_time_step(self._h, float(dt)), "sph_set_time_step")
+
+    def clock(self):
+        """time, dt, dt_prev, dt_average and step between steps (sph_get_clock)."""
+        c = abi.SphClock()
+        _chk(lib().sph_get_clock(self._h, C.byref(c)), "sph_get_clock")
+        return {"time": c.time, "dt": c.dt, "dt_prev": c.dt_prev, "dt_average": c.dt_average, "step": c.step}
+
+    def set_clock(self, clock, laminar=None):
+        """Resume after upload(): the saved clock and laminar flags (sph_set_clock)."""
+        c = abi.SphClock()
+        c.time, c.dt, c.dt_prev = float(clock["time"]), float(clock["dt"]), float(clock["dt_prev"])
+        c.dt_average, c.step = float(clock["dt_average"]), int(clock["step"])
+        lam = None if laminar is None else np.ascontiguousarray(laminar, dtype=np.int32)
+        _chk(lib().sph_set_clock(self._h, C.byref(c), abi.iptr(lam)), "sph_set_clock")
 
     def close(self):
         if self._h:

@@ -129,6 +129,17 @@ class SphStepInfo(C.Structure):
     ]
 
 
+class SphClock(C.Structure):
+    _fields_ = [
+        ("time", C.c_double),
+        ("dt", C.c_double),
+        ("dt_prev", C.c_double),
+        ("dt_average", C.c_double),
+        ("step", C.c_int32),
+        ("reserved", C.c_int32),
+    ]
+
+
 class SphDiagnostics(C.Structure):
     _fields_ = [
         ("warnings", C.c_int32),

@@ -880,7 +880,7 @@ int create_batch(int nsims, const SphParams* params, const SphGeometry* geoms, c
   A(h->d_cf_start, C);
   A(h->d_cf_count, C);
   A(h->d_near, C);
-  A(P.X, N); A(P.XF, N); A(P.VF, N); A(P.RF, N); A(P.V, N); A(P.RP, N); A(P.I, N); A(P.L, N);
+  A(P.X, N); A(P.XF, N); A(P.VF, N); A(P.RF, N); A(P.RM, N); A(P.V, N); A(P.RP, N); A(P.I, N); A(P.L, N);
   A(P.X2, N); A(P.V2, N); A(P.P2, N); A(P.I2, N); A(P.L2, N);
   A(P.bdt_count, N); A(P.bdt_start, N); A(P.bdt, bdt_cap);
   A(P.key, N); A(P.slot, N); A(P.cell_count, C + 1); A(P.cell_start, C + 1);
@@ -1252,7 +1252,7 @@ int sph_create_slab(const SphParams* params, const SphGeometry* geometry, int32_
 // A new particle set with the simulation's clock kept: OrdGrid1, the
 // neighbour lists and ComputeBoundaryDataTab on it (the search of
 // time_step_loop.f90:286-324), no time-step evaluation.
-int sph_replace_particles(SphHandle* h, const SphState* state) {
+int sph_replace_particles(SphHandle* h, const SphState* state, const int32_t* laminar) {
   if (!h || !h->uploaded || h->nsims != 1 || !state) return SPH_ERR_INVALID_ARGUMENT;
   if (h->any_c1) return SPH_ERR_UNSUPPORTED;
   SPH_TRY(read_dyn(h));
@@ -1260,8 +1260,11 @@ int sph_replace_particles(SphHandle* h, const SphState* state) {
   h->h_dyn[0].nag = state->n;
   cudaStream_t q = h->stream;
   SPH_CUDA(cudaMemcpyAsync(h->d_dyn, h->h_dyn.data(), sizeof(SimDyn), cudaMemcpyHostToDevice, q));
+  if (laminar && state->n > 0)
+    SPH_CUDA(cudaMemcpyAsync(h->d_ci1, laminar, sizeof(int32_t) * state->n, cudaMemcpyHostToDevice, q));
   launch_init_from_caller(h->db, h->d_cx, h->d_cv, h->d_crho, h->d_cp, h->d_cm, q);
   sort_sequence(h, q);
+  if (laminar && state->n > 0) launch_load_laminar(h->db, h->d_ci1, q);
   launch_boundary(h->db, q);
   lists_pass(h, q);
   SPH_CUDA(cudaGetLastError());
@@ -1273,6 +1276,36 @@ int sph_set_time_step(SphHandle* h, double dt) {
   for (int s = 0; s < h->nsims; ++s)
     if (h->sims[s].prm.pesodt != 0.0) return SPH_ERR_UNSUPPORTED;
   launch_set_dt(h->db, dt, h->stream);
+  SPH_CUDA(cudaGetLastError());
+  return sync_dyn(h);
+}
+
+// ------------------------------------------------------------- checkpoint
+int sph_get_clock(SphHandle* h, SphClock* clock) {
+  if (!h || !h->uploaded || h->nsims != 1 || !clock) return SPH_ERR_INVALID_ARGUMENT;
+  SPH_TRY(sync_dyn(h));
+  const SimDyn& d = h->h_dyn[0];
+  clock->time = d.time;
+  clock->dt = d.dt;
+  clock->dt_prev = d.dt_prev;
+  clock->dt_average = d.dt_average;
+  clock->step = d.step;
+  clock->reserved = 0;
+  return SPH_OK;
+}
+
+int sph_set_clock(SphHandle* h, const SphClock* clock, const int32_t* laminar) {
+  if (!h || !h->uploaded || h->nsims != 1 || !clock) return SPH_ERR_INVALID_ARGUMENT;
+  if (h->any_c1) return SPH_ERR_UNSUPPORTED;
+  if (!(clock->dt > 0.0) || !(clock->dt_prev > 0.0) || clock->step < 0 || !(clock->time >= 0.0))
+    return SPH_ERR_INVALID_ARGUMENT;
+  SPH_TRY(sync_dyn(h));
+  const int n = h->h_dyn[0].nag;
+  cudaStream_t q = h->stream;
+  if (laminar && n > 0)
+    SPH_CUDA(cudaMemcpyAsync(h->d_ci1, laminar, sizeof(int32_t) * n, cudaMemcpyHostToDevice, q));
+  launch_set_clock(h->db, clock->time, clock->step, clock->dt, clock->dt_prev, clock->dt_average,
+                   laminar && n > 0 ? h->d_ci1 : nullptr, q);
   SPH_CUDA(cudaGetLastError());
   return sync_dyn(h);
 }

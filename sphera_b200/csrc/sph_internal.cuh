@@ -150,6 +150,7 @@ struct Particles {
   float4* XF;       // offset from the cell origin in FP32, w = the cell's k index (as a float)
   float4* VF;       // FP32 form: vx, vy, vz, m/rho
   float4* RF;       // FP32 form: rho, p/rho^2, m, 0
+  float2* RM;       // FP32c momentum record: rho, p/rho^2 (m_j = rho_j * VF.w, VF.w kept current)
   double4* V;       // vx, vy, vz, rho (density entering the continuity pass)
   double2* RP;      // current rho, p
   int* I;           // caller index (1-based)

@@ -424,6 +424,7 @@ __global__ void k_rank_permute(DevBatch b) {
     P.RP[fin] = make_double2(v.w, pr);
     P.VF[fin] = make_float4((float)v.x, (float)v.y, (float)v.z, (float)vol);
     P.RF[fin] = make_float4((float)v.w, (float)(pr / (v.w * v.w)), (float)x.w, 0.f);
+    P.RM[fin] = make_float2((float)v.w, (float)(pr / (v.w * v.w)));
     P.I[fin] = myid;
     P.L[fin] = P.L2[src];
   }
@@ -2223,22 +2224,25 @@ __global__ void __launch_bounds__(kBlock, (C1 || BATCH) ? 2 : 3) k_momentum_f32(
     prefetch_list_l2(b.nlist, p, b.list_cap4, nchmax * 4);
     const int4* lbase = reinterpret_cast<const int4*>(b.nlist) + list_base4(p, b.list_cap4);
     int4 nxt = nch > 0 ? __ldg(lbase) : make_int4(0, 0, 0, 0);
-    auto pair = [&](int e, const float4& xj, const float4& vj, const float4& rfj) {
+    // a neighbour's record is 40 B: XF (offset, cell k), VF (velocity,
+    // m/rho) and RM (rho, p/rho^2); its mass is rho (m/rho)
+    auto pair = [&](int e, const float4& xj, const float4& vj, const float2& rmj) {
       const int q = e & kSlotMask;
       float d0, d1, d2;
       separation_f32<DIM>(s, rc, e, xj, xfi, ckf, dz, d0, d1, d2);
       float rr = fmaf(d2, d2, fmaf(d1, d1, d0 * d0));
       float PK1, PK2, PK3;
       kernel_values_f32(fc, rr, PK1, PK2, PK3);
-      float mj = rfj.z;
+      const float rhoj = rmj.x;
+      const float mj = rhoj * vj.w;
       // pressure (both accumulators of inter_EqMoto together)
-      float pf = -(mj * (Pi + rfj.y) * PK3);
+      float pf = -(mj * (Pi + rmj.y) * PK3);
       cp0 = fmaf(pf, d0, cp0);
       if (DIM == 3) cp1 = fmaf(pf, d1, cp1);
       cp2 = fmaf(pf, d2, cp2);
       if (C1) {
         const float dpf = (float)(__ldg(reinterpret_cast<const double*>(P.RP + q) + 1) - piD);
-        const float gf = -(mj * dpf * rcp_approx(rhof * rfj.x) * PK3);
+        const float gf = -(mj * dpf * rcp_approx(rhof * rhoj) * PK3);
         cg0 = fmaf(gf, d0, cg0);
         if (DIM == 3) cg1 = fmaf(gf, d1, cg1);
         cg2 = fmaf(gf, d2, cg2);
@@ -2246,7 +2250,7 @@ __global__ void __launch_bounds__(kBlock, (C1 || BATCH) ? 2 : 3) k_momentum_f32(
       float dv0 = vj.x - vix, dv1 = vj.y - viy, dv2 = vj.z - viz;
       // viscomon amon / rsum and viscomorris nu4 / (nu rsum + 1e-3) from one
       // reciprocal of their denominators' product
-      const float rsum = rhof + rfj.x;
+      const float rsum = rhof + rhoj;
       const float bm = fmaf(fc.nu, rsum, 1.0e-3f);
       const float iv = rcp_approx(rsum * bm);
       float vr = -fmaf(dv2, d2, fmaf(dv1, d1, dv0 * d0));
@@ -2267,12 +2271,13 @@ __global__ void __launch_bounds__(kBlock, (C1 || BATCH) ? 2 : 3) k_momentum_f32(
       if (c >= nch) continue;
       const int rem = cnt - 4 * c;   // >= 1
       if (BATCH) {
-        float4 x0, v0, r0, x1, v1, r1, x2, v2, r2, x3, v3, r3;
+        float4 x0, v0, x1, v1, x2, v2, x3, v3;
+        float2 r0, r1, r2, r3;
         const int q0 = ch.x & kSlotMask, q1 = ch.y & kSlotMask, q2 = ch.z & kSlotMask, q3 = ch.w & kSlotMask;
-        x0 = __ldg(P.XF + q0); v0 = __ldg(P.VF + q0); r0 = __ldg(P.RF + q0);
-        if (rem > 1) { x1 = __ldg(P.XF + q1); v1 = __ldg(P.VF + q1); r1 = __ldg(P.RF + q1); }
-        if (rem > 2) { x2 = __ldg(P.XF + q2); v2 = __ldg(P.VF + q2); r2 = __ldg(P.RF + q2); }
-        if (rem > 3) { x3 = __ldg(P.XF + q3); v3 = __ldg(P.VF + q3); r3 = __ldg(P.RF + q3); }
+        x0 = __ldg(P.XF + q0); v0 = __ldg(P.VF + q0); r0 = __ldg(P.RM + q0);
+        if (rem > 1) { x1 = __ldg(P.XF + q1); v1 = __ldg(P.VF + q1); r1 = __ldg(P.RM + q1); }
+        if (rem > 2) { x2 = __ldg(P.XF + q2); v2 = __ldg(P.VF + q2); r2 = __ldg(P.RM + q2); }
+        if (rem > 3) { x3 = __ldg(P.XF + q3); v3 = __ldg(P.VF + q3); r3 = __ldg(P.RM + q3); }
         pair(ch.x, x0, v0, r0);
         if (rem > 1) pair(ch.y, x1, v1, r1);
         if (rem > 2) pair(ch.z, x2, v2, r2);
@@ -2280,7 +2285,7 @@ __global__ void __launch_bounds__(kBlock, (C1 || BATCH) ? 2 : 3) k_momentum_f32(
       } else {
         auto one = [&](int e) {
           const int q = e & kSlotMask;
-          pair(e, __ldg(P.XF + q), __ldg(P.VF + q), __ldg(P.RF + q));
+          pair(e, __ldg(P.XF + q), __ldg(P.VF + q), __ldg(P.RM + q));
         };
         one(ch.x);
         if (rem > 1) one(ch.y);
@@ -2598,7 +2603,12 @@ __global__ void __launch_bounds__(kBlock) k_continuity_f32_finish(DevBatch b) {
       }
       double pr = s.k_over_rho0 * (rho - s.den0) + s.p_ref;
       P.RP[p] = make_double2(rho, pr);
-      P.RF[p] = make_float4((float)rho, (float)(pr / (rho * rho)), (float)P.X[p].w, 0.f);
+      const double m = P.X[p].w;
+      P.RF[p] = make_float4((float)rho, (float)(pr / (rho * rho)), (float)m, 0.f);
+      // the next momentum pass's records: the new density, and m/rho in
+      // VF.w (the pair sums of this pass, which read the old one, are done)
+      P.RM[p] = make_float2((float)rho, (float)(pr / (rho * rho)));
+      P.VF[p].w = (float)(m / rho);
     } else {
       P.DDEN[p] = dden;
     }
@@ -2618,8 +2628,11 @@ __global__ void k_refresh_f32(DevBatch b) {
     double4 x = b.P.X[p];
     double4 v = b.P.V[p];
     double2 rp = b.P.RP[p];
-    b.P.VF[p] = make_float4((float)v.x, (float)v.y, (float)v.z, (float)v.w);
+    // m/rho of the current density (after a pressure smoothing V.w still
+    // holds the sort's; where they agree this is the same division)
+    b.P.VF[p] = make_float4((float)v.x, (float)v.y, (float)v.z, (float)(x.w / rp.x));
     b.P.RF[p] = make_float4((float)rp.x, (float)(rp.y / (rp.x * rp.x)), (float)x.w, 0.f);
+    b.P.RM[p] = make_float2((float)rp.x, (float)(rp.y / (rp.x * rp.x)));
   }
 }
 
@@ -3020,7 +3033,12 @@ __global__ void __launch_bounds__(kBlock) k_pressure_smoothing_apply(DevBatch b,
     double pr = P.DDEN[p];
     double rho = s.den0 * (1.0 + (pr - s.p_ref) / s.eps);
     P.RP[p] = make_double2(rho, pr);
-    if (refresh_f32) P.RF[p] = make_float4((float)rho, (float)(pr / (rho * rho)), (float)P.X[p].w, 0.f);
+    if (refresh_f32) {
+      const double m = P.X[p].w;
+      P.RF[p] = make_float4((float)rho, (float)(pr / (rho * rho)), (float)m, 0.f);
+      P.RM[p] = make_float2((float)rho, (float)(pr / (rho * rho)));
+      P.VF[p].w = (float)(m / rho);
+    }
   }
 }
 
@@ -3236,6 +3254,36 @@ __global__ void k_set_dt(DevBatch b, double dt) {
   d.dtvel = 0.5 * (d.dt + d.dt_prev);
   d.geff[0] = s.forcing_aw2 != 0.0 ? s.grav[0] + s.forcing_aw2 * forcing_sin(s.forcing_w * (d.time + d.dt))
                                    : s.grav[0];
+}
+
+// sph_set_clock: the clock of a resumed simulation (sim 0), with dtvel and
+// the next step's body force as k_finalize leaves them.
+__global__ void k_set_clock(DevBatch b, double time, int step, double dt, double dt_prev, double dt_average) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  const SimDev& s = b.sims[0];
+  SimDyn& d = b.dyn[0];
+  d.time = time;
+  d.step = step;
+  d.dt = dt;
+  d.dt_prev = dt_prev;
+  d.dt_average = dt_average;
+  d.dtvel = 0.5 * (d.dt + d.dt_prev);
+  d.geff[0] = s.forcing_aw2 != 0.0 ? s.grav[0] + s.forcing_aw2 * forcing_sin(s.forcing_w * (d.time + d.dt))
+                                   : s.grav[0];
+}
+
+// The laminar flags of a resumed simulation, from caller order.
+__global__ void k_load_laminar(DevBatch b, const int* flags) {
+  __shared__ SimDev s;
+  int cur = -1;
+  const Particles& P = b.P;
+  for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
+    Tile tl = b.tiles[t];
+    load_sim(s, b.sims, tl.sim, cur);
+    int p = tl.start + threadIdx.x;
+    if (threadIdx.x >= tl.count || p >= s.p_off + b.dyn[tl.sim].nag) continue;
+    P.L[p] = (uint8_t)(flags[(size_t)s.p_off + P.I[p] - 1] != 0);
+  }
 }
 
 // sph_batch_cancel: a simulation still advancing stops from the next launch
@@ -3584,6 +3632,14 @@ void launch_scan(const DevBatch& b, int* cell_start, cudaStream_t st) {
 
 void launch_cancel(const DevBatch& b, int sim, cudaStream_t st) { k_cancel<<<1, 32, 0, st>>>(b, sim); }
 
+void launch_load_laminar(const DevBatch& b, const int* laminar, cudaStream_t st) {
+  k_load_laminar<<<blocks_for(b), kBlock, 0, st>>>(b, laminar);
+}
+void launch_set_clock(const DevBatch& b, double time, int step, double dt, double dt_prev, double dt_average,
+                      const int* laminar, cudaStream_t st) {
+  k_set_clock<<<1, 32, 0, st>>>(b, time, step, dt, dt_prev, dt_average);
+  if (laminar) launch_load_laminar(b, laminar, st);
+}
 void launch_set_dt(const DevBatch& b, double dt, cudaStream_t st) {
   k_set_dt<<<(b.nsims + 127) / 128, 128, 0, st>>>(b, dt);
 }

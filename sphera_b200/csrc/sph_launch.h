@@ -78,6 +78,9 @@ void launch_dt_reduce(const DevBatch& b, cudaStream_t st);
 void launch_finalize(const DevBatch& b, int mode, cudaStream_t st);
 void launch_cancel(const DevBatch& b, int sim, cudaStream_t st);
 void launch_set_dt(const DevBatch& b, double dt, cudaStream_t st);
+void launch_load_laminar(const DevBatch& b, const int* laminar, cudaStream_t st);
+void launch_set_clock(const DevBatch& b, double time, int step, double dt, double dt_prev, double dt_average,
+                      const int* laminar, cudaStream_t st);
 // host <-> device in caller order
 void launch_init_from_caller(const DevBatch& b, const double* x, const double* v, const double* rho,
                              const double* p, const double* m, cudaStream_t st);

@@ -21,7 +21,8 @@ One step is the per-call sequence of time_step_loop.f90 with two exchanges:
      Leapfrog_trajectories (ghosts get meaningless rates: their
      neighbourhoods are incomplete; they are replaced before use);
   2. exchange: particles that crossed a slab edge migrate, ghosts are taken
-     again from their owners; every slab runs OrdGrid1, CalcVarLength and
+     again from their owners (with the laminar flags the momentum pass just
+     set); every slab runs OrdGrid1, CalcVarLength and
      ComputeBoundaryDataTab on its new set (``sph_replace_particles``);
   3. every slab: the continuity block, Leapfrog_continuity and the EoS;
   4. exchange: ghosts get their owners' new densities and pressures;
@@ -40,8 +41,10 @@ import numpy as np
 
 from . import abi
 
-# record layout of an exchanged particle: global index, x(3), v(3), rho, p, m
-_REC = 10
+# record layout of an exchanged particle: global index, x(3), v(3), rho, p, m,
+# pg%laminar_flag (the one value besides the state that a particle carries
+# from one momentum pass to the next)
+_REC = 11
 
 
 def whole_grid(params):
@@ -91,7 +94,7 @@ def assemble(rec, ci, own, ncd):
     return rows, (c >= a) & (c <= b)
 
 
-def records(gid, st):
+def records(gid, st, laminar=None):
     out = np.empty((st.n, _REC))
     out[:, 0] = gid
     out[:, 1:4] = st.x
@@ -99,6 +102,7 @@ def records(gid, st):
     out[:, 7] = st.rho
     out[:, 8] = st.p
     out[:, 9] = st.m
+    out[:, 10] = 0.0 if laminar is None else laminar
     return out
 
 
@@ -106,6 +110,10 @@ def state_of(rows):
     return abi.State(np.ascontiguousarray(rows[:, 1:4]), np.ascontiguousarray(rows[:, 4:7]),
                      np.ascontiguousarray(rows[:, 7]), np.ascontiguousarray(rows[:, 8]),
                      np.ascontiguousarray(rows[:, 9]))
+
+
+def laminar_of(rows):
+    return np.ascontiguousarray(rows[:, 10], dtype=np.int32)
 
 
 class SlabEngine:
@@ -118,11 +126,14 @@ class SlabEngine:
     def upload(self, st):
         self.sim.upload(st)
 
-    def replace(self, st):
-        self.sim.replace_particles(st)
+    def replace(self, st, laminar):
+        self.sim.replace_particles(st, laminar)
 
     def download(self):
         return self.sim.download()
+
+    def laminar(self):
+        return self.sim.dump_laminar()
 
     def momentum(self):
         self.sim.rhs_momentum(want=False)
@@ -179,13 +190,13 @@ class SlabRun:
 
     def _gather(self):
         for e, (gid, mask) in zip(self.engines, self.owned):
-            r = records(gid, e.download())
+            r = records(gid, e.download(), e.laminar())
             self.rec[gid[mask]] = r[mask]
 
     def _exchange(self):
         self._gather()
         for e, rows in zip(self.engines, self._sets()):
-            e.replace(state_of(rows))
+            e.replace(state_of(rows), laminar_of(rows))
 
     def _global_dt(self):
         dt = min(e.dt() for e in self.engines)
@@ -207,6 +218,11 @@ class SlabRun:
         """The whole simulation's state in its original particle order."""
         self._gather()
         return state_of(self.rec)
+
+    def laminar(self):
+        """pg%laminar_flag of the whole simulation, original particle order."""
+        self._gather()
+        return laminar_of(self.rec)
 
     def counts(self):
         return [int(m.sum()) for _, m in self.owned], [int((~m).sum()) for _, m in self.owned]
@@ -271,7 +287,7 @@ class DistributedSlabRun:
 
     def _exchange(self):
         st = self.engine.download()
-        mine = records(self.rows[:, 0], st)[self.mask]      # my owned particles, updated
+        mine = records(self.rows[:, 0], st, self.engine.laminar())[self.mask]   # my owned particles, updated
         ci = cell_x(mine[:, 1:4], self.lo, self.dcd)
         if np.any((ci < 1) | (ci > self.ncd)):
             raise RuntimeError("a particle left the grid: slab runs do not remove particles")
@@ -289,7 +305,7 @@ class DistributedSlabRun:
         allrec = allrec[first]
         rows, mask = assemble(allrec, cell_x(allrec[:, 1:4], self.lo, self.dcd), self.own, self.ncd)
         self.rows, self.mask = rows, mask
-        self.engine.replace(state_of(rows))
+        self.engine.replace(state_of(rows), laminar_of(rows))
 
     def _global_dt(self):
         import torch
@@ -308,9 +324,10 @@ class DistributedSlabRun:
             self._global_dt()
 
     def owned_records(self):
-        """(global index, x, v, rho, p, m) rows of the particles this rank owns."""
+        """(global index, x, v, rho, p, m, laminar) rows of the particles this
+        rank owns."""
         st = self.engine.download()
-        return records(self.rows[:, 0], st)[self.mask]
+        return records(self.rows[:, 0], st, self.engine.laminar())[self.mask]
 
     def close(self):
         self.engine.close()

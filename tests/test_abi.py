@@ -16,7 +16,8 @@ from sphera_b200 import abi, cases
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 HEADER = os.path.join(ROOT, "include", "sphera_b200.h")
 
-STRUCTS = [abi.SphParams, abi.SphZone, abi.SphGeometry, abi.SphState, abi.SphStepInfo, abi.SphDiagnostics]
+STRUCTS = [abi.SphParams, abi.SphZone, abi.SphGeometry, abi.SphState, abi.SphStepInfo, abi.SphDiagnostics,
+           abi.SphClock]
 
 
 def _declared():

@@ -36,6 +36,14 @@ def moving(case, seed=5, u=3.0):
 def make(name, precision):
     if name == "dam_break_2d":
         return moving(cases.dam_break_2d(dx=0.02, precision=precision))
+    if name == "dam_break_2d_laminar":
+        # no-slip walls that act only where pg%laminar_flag is set, and a
+        # viscosity high enough for the Morris term to set it: the flags a
+        # momentum pass leaves must travel with the particles
+        case = moving(cases.dam_break_2d(dx=0.02, precision=precision))
+        case.params.kin_visc = 1.0e-2
+        case.geometry = cases.tank_2d(*case.meta["tank"], zone=abi.make_zone(slip=0.5, laminar_no_slip_check=1))
+        return case
     return moving(cases.dam_break_3d(dx=0.02, precision=precision), u=6.0)
 
 
@@ -49,7 +57,7 @@ def undivided(case, steps):
 
 @pytest.mark.parametrize("precision", [abi.SPH_PREC_FP64, abi.SPH_PREC_FP32C], ids=["fp64", "fp32c"])
 @pytest.mark.parametrize("name,nslabs,steps", [("dam_break_2d", 2, 60), ("dam_break_2d", 3, 60),
-                                               ("dam_break_3d", 2, 60)])
+                                               ("dam_break_2d_laminar", 2, 60), ("dam_break_3d", 2, 60)])
 def test_slabs_are_the_undivided_run(name, nslabs, steps, precision):
     case = make(name, precision)
     ref, _ = undivided(case, steps)

@@ -51,18 +51,27 @@ class FakeEngine:
 
     def upload(self, st):
         self.st = abi.State(st.x.copy(), st.v.copy(), st.rho.copy(), st.p.copy(), st.m.copy())
+        self.lam = np.zeros(st.n, np.int32)
         self.dt_cur = self._close()
 
-    def replace(self, st):
+    def laminar(self):
+        return self.lam.copy()
+
+    def replace(self, st, laminar):
         self.st = abi.State(st.x.copy(), st.v.copy(), st.rho.copy(), st.p.copy(), st.m.copy())
+        self.lam = laminar.copy()
 
     def download(self):
         s = self.st
         return abi.State(s.x.copy(), s.v.copy(), s.rho.copy(), s.p.copy(), s.m.copy())
 
     def momentum(self):
+        # the flag set by the last pass scales this one's acceleration, as the
+        # laminar flag switches the wall's no-slip term
         s = self.st
         acc = self._sums(lambda i, nb, d, r2: d * ((self.r2 - r2) * s.p[nb] / s.rho[nb])[:, None])
+        acc = acc * (1.0 + 0.5 * self.lam)[:, None]
+        self.lam = (np.abs(acc[:, 0]) > 2e-3).astype(np.int32)
         s.v[:] = s.v + self.dt_cur * 1e-3 * acc
         s.x[:] = s.x + self.dt_cur * s.v
 
@@ -102,7 +111,7 @@ def undivided(case, steps):
     for _ in range(steps):
         e.momentum()
         e.continuity()
-    return slab.records(np.arange(case.n, dtype=np.float64), e.download())
+    return slab.records(np.arange(case.n, dtype=np.float64), e.download(), e.laminar())
 
 
 @pytest.mark.parametrize("name", ["dam_break_2d", "dam_break_3d_dx02", "random_box_5k"])
@@ -163,7 +172,8 @@ def test_slab_run_is_the_undivided_run(nslabs):
     st = run.state()
     assert owned0 != owned1, "no particle crossed a slab edge"
     assert sum(owned1) == case.n and min(ghosts) > 0
-    got = slab.records(np.arange(case.n, dtype=np.float64), st)
+    got = slab.records(np.arange(case.n, dtype=np.float64), st, run.laminar())
+    assert 0 < ref[:, 10].sum() < case.n, "the flags took one value only"
     assert np.array_equal(got, ref)
 
 
