@@ -463,7 +463,8 @@ def main():
     ap.add_argument("--forms", default="both", choices=["both", "fp32c", "fp64"])
     ap.add_argument("--autotune", type=int, default=1, help="size the persistent grids on the live state first")
     ap.add_argument("--shape", default=None,
-                    help="force the FP32c momentum,continuity pair-loop shapes, e.g. 1,1 (0 lean, 1 batched loads)")
+                    help="force the FP32c momentum,continuity pair-loop shapes, e.g. 1,1 (0 lean, 1 batched "
+                         "loads), or all seven values sph_autotune chooses")
     ap.add_argument("--teta", type=float, default=0.0,
                     help="partial smoothing coefficient TetaP = TetaV of the dam-break workload (0: off)")
     ap.add_argument("--c1", action="store_true",
@@ -576,10 +577,18 @@ def run_step_bench(args, ws, rank, local):
         grids = sim.autotune(reps=3) if args.autotune else None
         if args.shape is not None:
             # a fixed launch configuration (profiling the same kernels
-            # without the autotuner's sweeps): pair-loop shapes, default grids
-            m, c = (int(v) for v in args.shape.split(","))
-            sim.set_launch_shape(dict(grids or {}, momentum_shape=m, continuity_shape=c))
-            grids = dict(grids or {}, momentum_shape=m, continuity_shape=c)
+            # without the autotuner's sweeps): "m,c" sets the pair-loop
+            # shapes on the default grids; seven values set everything
+            # sph_autotune chooses (lists, momentum, continuity, boundary,
+            # integrals grids, momentum and continuity shapes)
+            v = [int(t) for t in args.shape.split(",")]
+            if len(v) == 7:
+                grids = dict(zip(__import__("sphera_b200")._SHAPE_KEYS, v))
+            elif len(v) == 2:
+                grids = dict(grids or {}, momentum_shape=v[0], continuity_shape=v[1])
+            else:
+                raise SystemExit("--shape takes m,c or the seven values of sph_autotune")
+            sim.set_launch_shape(grids)
         sim.step(args.warmup)
         stream = torch.cuda.ExternalStream(sim.stream)
         e0 = torch.cuda.Event(enable_timing=True)

@@ -400,9 +400,10 @@ int  sph_global_quantities(SphHandle* h, int32_t sim, double* out);
  * 1-based caller indices), exactly as OrdGrid1.f90:58-105 builds them.
  * Any pointer may be NULL.                                                */
 int  sph_dump_grid(SphHandle* h, int32_t* cella, int32_t* icont, int32_t* npartord);
-/* The neighbour lists CalcVarLength.f90:173-269 would build:
- * counts ([n], nPartIntorno) and lists ([n][nmaxj], PartIntorno, 1-based
- * caller indices in the reference's visiting order).                      */
+/* The neighbour lists the pair passes read, in the form
+ * CalcVarLength.f90:173-269 builds them: counts ([n], nPartIntorno) and
+ * lists ([n][nmaxj], PartIntorno, 1-based caller indices in the
+ * reference's visiting order, the particle itself included).              */
 int  sph_dump_neighbours(SphHandle* h, int32_t nmaxj, int32_t* counts, int32_t* lists);
 /* BoundaryDataTab in caller order: ncb ([n], BoundaryDataPointer(1,:) in
  * 3D, IntNcbs in 2D), and for each particle up to max_per entries of

@@ -1342,6 +1342,16 @@ __device__ __forceinline__ void screen_tile_x2(const float* nx, const float* ny,
 // window (the truncation test once NMAXPARTJ is reached; rare).
 __device__ __forceinline__ bool in_window(float kj, int ck) { return fabsf(kj - (float)ck) <= 1.0f; }
 
+// Bits u of a 32-candidate tile with lo <= u < hi (lo, hi relative to the
+// tile's first slot, any sign).
+__device__ __forceinline__ unsigned window_mask(int lo, int hi) {
+  lo = lo < 0 ? 0 : lo;
+  hi = hi > 32 ? 32 : hi;
+  if (hi <= lo) return 0u;
+  const unsigned upto = hi == 32 ? 0xffffffffu : (1u << hi) - 1u;
+  return upto & ~((1u << lo) - 1u);
+}
+
 __device__ __forceinline__ bool window_candidate(const float4* wbuf, int u0, int nt, int ck) {
   for (int u = u0; u < nt; ++u)
     if (in_window(wbuf[u].w, ck)) return true;
@@ -1408,10 +1418,14 @@ __global__ void __launch_bounds__(kBlock, 4) k_neighbour_lists(DevBatch b) {
         int base = s.cell_off + ((jr - 1) * s.ncd[0] + (ir - 1)) * s.ncd[2];
         int ub = __ldg(P.cell_start + base + klo - 1);
         int ue = __ldg(P.cell_start + base + khi);
+        // this lane's own window in the run, cells ck-1..ck+1: the slots the
+        // reference visits (CalcVarLength.f90's 27-cell block)
+        int wlo = 0, whi = 0;
         if (mine) {
-          // candidates of this lane's own window (the reference's loop count)
           int ml = ck > 1 ? ck - 1 : 1, mh = ck < s.ncd[2] ? ck + 1 : s.ncd[2];
-          cand += __ldg(P.cell_start + base + mh) - __ldg(P.cell_start + base + ml - 1);
+          wlo = __ldg(P.cell_start + base + ml - 1);
+          whi = __ldg(P.cell_start + base + mh);
+          cand += whi - wlo;
         }
         float Dx = (float)(gci - ir) * s.dcdf[0];
         float Dy = (DIM == 3) ? (float)(gcj - jr) * s.dcdf[1] : 0.f;
@@ -1440,21 +1454,22 @@ __global__ void __launch_bounds__(kBlock, 4) k_neighbour_lists(DevBatch b) {
             if (!trunc && window_candidate(wbuf, 0, nt, ck)) trunc = true;
             continue;
           }
-          // phase 2a (rare): resolve band hits -- outside the lane's window
-          // (the reference never visits those) or failing the FP64 test
-          // they are dropped; hitm then holds exactly the accepted ones
+          // only the lane's own window counts: the warp's union of runs
+          // reaches two z cells away from some lanes, and where the cell is
+          // narrower than 2h (CreaGrid rounds the cell count to nearest) a
+          // candidate there can lie within 2h without being the reference's
+          // neighbour
+          hitm &= window_mask(wlo - c0, whi - c0);
+          // phase 2a (rare): resolve band hits -- those failing the FP64
+          // test are dropped; hitm then holds exactly the accepted ones
           unsigned band = hitm & ~lom;
           while (band) {
             int u = __ffs(band) - 1;
             band &= band - 1;
-            bool keep = in_window(wbuf[u].w, ck);
-            if (keep) {
-              double4 xq = P.X[c0 + u], xi = P.X[p];
-              double r0 = xi.x - xq.x, r1 = xi.y - xq.y, r2 = xi.z - xq.z;
-              double rr = r0 * r0 + r1 * r1 + r2 * r2;
-              keep = !(rr > s.square_doubleh);
-            }
-            if (!keep) hitm &= ~(1u << u);
+            double4 xq = P.X[c0 + u], xi = P.X[p];
+            double r0 = xi.x - xq.x, r1 = xi.y - xq.y, r2 = xi.z - xq.z;
+            double rr = r0 * r0 + r1 * r1 + r2 * r2;
+            if (rr > s.square_doubleh) hitm &= ~(1u << u);
           }
           if (nacc + __popc(hitm) >= cap) {
             // reaching NMAXPARTJ in this tile (rare): accepted ones in
@@ -3460,32 +3475,40 @@ __global__ void k_to_caller(DevBatch b, double* x, double* v, double* rho, doubl
 
 template <int DIM>
 __global__ void k_dump_neighbours(DevBatch b, int nmaxj, int* counts, int* lists) {
+  // the stored lists the pair passes read, in caller indices, with the
+  // particle itself put back where the reference's visiting order has it
+  // (the lists leave it out): before the first entry past its own slot in
+  // its own column (the centre run).  It was accepted unless the NMAXPARTJ
+  // cap cut the list before it, in which case cnt reached the cap.
   __shared__ SimDev s;
   int cur = -1;
   const Particles& P = b.P;
+  constexpr unsigned kCentre = (DIM == 3) ? 4u : 1u;
   for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
     Tile tl = b.tiles[t];
     load_sim(s, b.sims, tl.sim, cur);
     int p = tl.start + threadIdx.x;
     if (threadIdx.x >= tl.count || p >= s.p_off + b.dyn[tl.sim].nag) continue;
-    double4 xi = P.X[p];
     size_t row = (size_t)s.p_off + P.I[p] - 1;
-    int ci = 0, cj = 0, ck = 0;
+    const int cnt = b.ncount[p];
+    const int* base = reinterpret_cast<const int*>(reinterpret_cast<const int4*>(b.nlist) + list_base4(p, b.list_cap4));
+    bool self = cnt < s.nmaxpartj;
     int n = 0;
-    bool stop = !particle_cell(s, xi.x, xi.y, xi.z, ci, cj, ck);
-    constexpr int NR = (DIM == 3) ? 9 : 3;
-    for (int r = 0; r < NR && !stop; ++r) {
-      int qb, qe;
-      neighbour_run<DIM>(s, P.cell_start, ci, cj, ck, r, qb, qe);
-      for (int q = qb; q < qe; ++q) {
-        if (n >= s.nmaxpartj) { stop = true; break; }
-        double4 xj = P.X[q];
-        double r0 = xi.x - xj.x, r1 = xi.y - xj.y, r2 = xi.z - xj.z;
-        double rr = r0 * r0 + r1 * r1 + r2 * r2;
-        if (rr > s.square_doubleh) continue;
-        if (n < nmaxj) lists[row * nmaxj + n] = P.I[q];
+    for (int k = 0; k < cnt; ++k) {
+      const unsigned e = (unsigned)base[(size_t)(k >> 2) * 128 + (k & 3)];
+      const unsigned run = e >> kSlotBits;
+      const int q = (int)(e & kSlotMask);
+      if (self && (run > kCentre || (run == kCentre && q > p))) {
+        if (n < nmaxj) lists[row * nmaxj + n] = P.I[p];
         n++;
+        self = false;
       }
+      if (n < nmaxj) lists[row * nmaxj + n] = P.I[q];
+      n++;
+    }
+    if (self) {
+      if (n < nmaxj) lists[row * nmaxj + n] = P.I[p];
+      n++;
     }
     counts[row] = n;
   }

@@ -40,7 +40,18 @@ CASES = {
     "dam_break_2d": lambda: cases.dam_break_2d(),
     "dam_break_3d_dx02": lambda: cases.dam_break_3d(dx=0.02),
     "random_box_20k": lambda: cases.random_box(n=20000, seed=11),
+    # CreaGrid rounds 13.96 cells up to 14: cells narrower than 2h, so two
+    # cells away in z a random particle can lie within 2h and still not be
+    # a neighbour (outside the 27-cell block)
+    "random_box_30k_narrow_cells": lambda: cases.random_box(n=30000, seed=12),
 }
+
+
+def test_narrow_cell_case_has_narrow_cells():
+    from sphera_b200 import slab
+    c = CASES["random_box_30k_narrow_cells"]()
+    lo, ncd, dcd = slab.whole_grid(c.params)
+    assert dcd < 2.0 * c.params.dx * c.params.trunc
 
 
 @pytest.mark.parametrize("name", list(CASES))
