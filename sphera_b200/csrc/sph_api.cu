@@ -247,7 +247,9 @@ int prepare_sim(const SphParams& prm, const SphGeometry& g, int cap, HostSim& hs
     double band = 2.0 * err;
     s.rr_lo = std::nextafter((float)(s.square_doubleh - band), 0.0f);
     s.rr_hi = std::nextafter((float)(s.square_doubleh + band), 3.0e38f);
-    s.pad_f = 0.0f;
+    // CreaGrid rounds the cell count to nearest, so a cell can be narrower
+    // than 2h; then the list pass masks every hit to the lane's window
+    s.narrow_z = s.dcd[2] < s.doubleh ? 1 : 0;
   }
   s.ioff = 0;
   if (cell_lo > 0) {

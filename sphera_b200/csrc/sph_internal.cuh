@@ -65,7 +65,7 @@ struct SimDev {
   double ktdelta;         // kernel-table step
   float dcdf[3];          // (float)dcd: cell origins differ by multiples of it
   float rr_lo, rr_hi;     // FP32 screening band around (2h)^2 (see sph_api.cu)
-  float pad_f;
+  int narrow_z;           // z cells narrower than 2h: a candidate two cells away can lie within 2h
   double kerneltab[kKtRows + 1][5];
 };
 

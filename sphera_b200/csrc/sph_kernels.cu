@@ -1256,11 +1256,12 @@ __device__ __forceinline__ float screen_rf(const float4& xj, float ax, float ay,
 
 // Screens the staged tile of nt candidates for one lane, branch-free: bit u
 // of hitm is set unless candidate u's FP32 r^2 exceeds rr_hi (a certain
-// rejection), bit u of lom when it is below rr_lo (a certain acceptance:
-// such a pair is closer than 2h <= dcd, so the candidate lies in the lane's
-// 3-cell window).  Hits are about one candidate in nine; the band cases
-// (hit, not low) are left to the caller.  Entries past nt are staged far
-// away and never hit, so the tile is screened in blocks of 8.
+// rejection), bit u of lom when it is below rr_lo (a certain acceptance of
+// the distance test; the caller still masks the lane's own 3-cell window,
+// which a candidate closer than 2h can lie outside where cells are narrower
+// than 2h).  Hits are about one candidate in nine; the band cases (hit, not
+// low) are left to the caller.  Entries past nt are staged far away and
+// never hit, so the tile is screened in blocks of 8.
 template <int DIM, bool REBASE>
 __device__ __forceinline__ void screen_tile(const float4* wbuf, int nt, float ax, float ay, float zi, float fz, int ck,
                                             float dz, float rr_lo, float rr_hi, unsigned& hitm, unsigned& lom) {
@@ -1455,21 +1456,27 @@ __global__ void __launch_bounds__(kBlock, 4) k_neighbour_lists(DevBatch b) {
             continue;
           }
           // only the lane's own window counts: the warp's union of runs
-          // reaches two z cells away from some lanes, and where the cell is
+          // reaches two z cells away from some lanes, and where the cells are
           // narrower than 2h (CreaGrid rounds the cell count to nearest) a
           // candidate there can lie within 2h without being the reference's
-          // neighbour
-          hitm &= window_mask(wlo - c0, whi - c0);
-          // phase 2a (rare): resolve band hits -- those failing the FP64
-          // test are dropped; hitm then holds exactly the accepted ones
+          // neighbour; with cells at least 2h wide such a candidate is never
+          // a hit below the band, and band hits are tested below
+          if (s.narrow_z) hitm &= window_mask(wlo - c0, whi - c0);
+          // phase 2a (rare): resolve band hits -- outside the lane's window
+          // (the reference never visits those) or failing the FP64 test
+          // they are dropped; hitm then holds exactly the accepted ones
           unsigned band = hitm & ~lom;
           while (band) {
             int u = __ffs(band) - 1;
             band &= band - 1;
-            double4 xq = P.X[c0 + u], xi = P.X[p];
-            double r0 = xi.x - xq.x, r1 = xi.y - xq.y, r2 = xi.z - xq.z;
-            double rr = r0 * r0 + r1 * r1 + r2 * r2;
-            if (rr > s.square_doubleh) hitm &= ~(1u << u);
+            bool keep = in_window(wbuf[u].w, ck);
+            if (keep) {
+              double4 xq = P.X[c0 + u], xi = P.X[p];
+              double r0 = xi.x - xq.x, r1 = xi.y - xq.y, r2 = xi.z - xq.z;
+              double rr = r0 * r0 + r1 * r1 + r2 * r2;
+              keep = !(rr > s.square_doubleh);
+            }
+            if (!keep) hitm &= ~(1u << u);
           }
           if (nacc + __popc(hitm) >= cap) {
             // reaching NMAXPARTJ in this tile (rare): accepted ones in

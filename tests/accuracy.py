@@ -9,6 +9,9 @@ Three device runs start from the oracle's initial state:
                (seeded): a control that shows how far any run that does not
                reproduce the oracle's floating-point sums bit for bit drifts
                from it;
+  * fp64_ic32  the same form from the initial state rounded to FP32 (x, v,
+               rho, p, m as an FP32 code would hold them): a control of the
+               size of the differences FP32 arithmetic brings, made once;
   * fp32c      the FP32-compensated form.
 
 The time step is adaptive (CFL on the largest speed), so the runs' clocks
@@ -108,9 +111,12 @@ def study(oracle_mod, dx, t_end=0.5, every=0.05, threads=0, perturb=1e-12, seed=
     x = case.state.x
     xp = x * (1.0 + perturb * rng.uniform(-1.0, 1.0, size=x.shape))
     st = case.state
+    r32 = lambda a: a.astype(np.float32).astype(np.float64)
     runs = {
         "fp64": _with_precision(case, abi.SPH_PREC_FP64),
         "fp64_pert": _with_precision(case, abi.SPH_PREC_FP64, abi.State(xp, st.v, st.rho, st.p, st.m)),
+        "fp64_ic32": _with_precision(case, abi.SPH_PREC_FP64,
+                                     abi.State(r32(st.x), r32(st.v), r32(st.rho), r32(st.p), r32(st.m))),
         "fp32c": _with_precision(case, abi.SPH_PREC_FP32C),
     }
     out = {"dx": dx, "particles": case.n, "t_end": t_end, "every": every, "oracle_seconds": oracle_s,
