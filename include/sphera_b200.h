@@ -277,10 +277,11 @@ int  sph_idle(SphHandle* h, int32_t* idle);
 /* Autotuner (no reference counterpart): sizes the persistent grid of the
  * neighbour-list, momentum, continuity and boundary kernels on the live
  * state by timing `reps` launches of each candidate (1 to 32 blocks per
- * SM) of variants that leave the state unchanged, and for the FP32c
- * momentum and continuity pair loops also picks their shape (0: lean, 3
- * and 5 blocks per SM; 1: a list chunk's neighbour records loaded
- * together, 2 and 3 blocks per SM), then rebuilds the step graph.
+ * SM) of variants that leave the state unchanged, and for the momentum
+ * and continuity pair loops also picks their shape (0: lean, one pair's
+ * records at a time; 1: several list entries' records loaded together --
+ * a list chunk's in the FP32c form, two entries' in the FP64 form), then
+ * rebuilds the step graph.  Without C1 in both forms.
  * grid_out (may be NULL; 7 entries) receives in [0..4] the chosen blocks
  * of lists, momentum, continuity, boundary find and integrals, in [5] and
  * [6] the momentum and continuity shapes.                                 */

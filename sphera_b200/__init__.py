@@ -210,7 +210,10 @@ class Simulation:
 
     def step_download(self, nsteps=1):
         """step(nsteps) then download(), the last step's x, v, m copied to
-        the host while that step finishes (sph_step_download)."""
+        the host while that step finishes (sph_step_download).  The buffers
+        here are pageable numpy arrays, so the results are the same but the
+        copy does not overlap the step; a caller that wants the overlap
+        passes page-locked buffers to the C ABI (as bench.py's e2e leg does)."""
         n = self.n
         st = abi.State.empty(n)
         _chk(lib().sph_step_download(self._h, int(nsteps), C.byref(st.struct)), "sph_step_download")

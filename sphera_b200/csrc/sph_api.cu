@@ -1573,9 +1573,9 @@ int sph_autotune(SphHandle* h, int32_t reps, int32_t* grid_out) {
     e = cudaMallocAsync(&keep_d, nb_bytes, q);
     if (e == cudaSuccess) e = cudaMemcpyAsync(keep_d, b.P.BD, nb_bytes, cudaMemcpyDeviceToDevice, q);
   }
-  // the FP32c momentum pair loop comes in two shapes (lean at 3 blocks per
-  // SM, or a list chunk's records loaded together at 2): both are timed
-  const bool two_shapes = h->precision == SPH_PREC_FP32C && !h->any_c1;
+  // the momentum and continuity pair loops come in two shapes (lean, or
+  // several list entries' records loaded together): both are timed
+  const bool two_shapes = !h->any_c1;
   int best_batch = b.mom_batch, best_cbatch = b.con_batch;
   for (int cls = 0; cls < kGridClasses && e == cudaSuccess; ++cls) {
     if (cls == kGridIntegrals && h->dim != 3) continue;

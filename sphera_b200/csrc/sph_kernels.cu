@@ -1677,7 +1677,11 @@ __global__ void __launch_bounds__(kBlock, 2) k_renormalisation(DevBatch b) {
 
 // C1: with input_any_t%C1_BE the pressure terms are renormalised with
 // B_ren_gradp (3D only).
-template <int DIM, bool FUSED, bool C1 = false>
+// BATCH (not with C1): two list entries' records are requested before the
+// first one's arithmetic, so the second pair's gathers wait behind the
+// first pair's FP64 divisions instead of after them; the terms are formed
+// and summed in the same order, so the results are the same bits.
+template <int DIM, bool FUSED, bool C1 = false, bool BATCH = false>
 __global__ void __launch_bounds__(kBlock, 2) k_momentum(DevBatch b) {
   __shared__ SimDev s;
   __shared__ double stpres[3][kBlock];   // the wall pressure term, kept out of the pair loop's registers
@@ -1750,17 +1754,11 @@ __global__ void __launch_bounds__(kBlock, 2) k_momentum(DevBatch b) {
     lr.init(b.nlist, p, b.list_cap4, cnt);
     const int nmax = __reduce_max_sync(0xffffffffu, (unsigned)cnt);
     prefetch_list_l2(b.nlist, p, b.list_cap4, nmax);
-    for (int k = 0; k < nmax; ++k) {
-      int e = lr.get(k);
-      if (k >= cnt) continue;
-      int q = e & kSlotMask;
-      double4 xj = P.X[q];
+    auto pair = [&](const double4& xj, const double4& vj, const double2& rpj) {
       double r0 = xi.x - xj.x, r1 = xi.y - xj.y, r2 = xi.z - xj.z;
       double rr = r0 * r0 + r1 * r1 + r2 * r2;
       double PK1, PK2, PK3;
       kernel_values(s, rr, PK1, PK2, PK3);
-      double4 vj = P.V[q];
-      double2 rpj = P.RP[q];
       double rhoj = rpj.x, pj = rpj.y, amassj = xj.w;
       double dv0 = vj.x - vi[0], dv1 = vj.y - vi[1], dv2 = vj.z - vi[2];
       // pressure gradient and ALE1 terms, inter_EqMoto.f90:195-221
@@ -1795,6 +1793,32 @@ __global__ void __launch_bounds__(kBlock, 2) k_momentum(DevBatch b) {
         }
         tv2 = tv2 + w2;
         rs2 = rs2 + w2;
+      }
+    };
+    if (BATCH) {
+      for (int k = 0; k < nmax; k += 2) {
+        const int e0 = lr.get(k);
+        const int e1 = k + 1 < nmax ? lr.get(k + 1) : 0;
+        const bool u0 = k < cnt, u1 = k + 1 < cnt;
+        double4 x0 = make_double4(0.0, 0.0, 0.0, 0.0), v0 = x0, x1 = x0, v1 = x0;
+        double2 p0 = make_double2(0.0, 0.0), p1 = p0;
+        if (u0) {
+          const int q = e0 & kSlotMask;
+          x0 = P.X[q]; v0 = P.V[q]; p0 = P.RP[q];
+        }
+        if (u1) {
+          const int q = e1 & kSlotMask;
+          x1 = P.X[q]; v1 = P.V[q]; p1 = P.RP[q];
+        }
+        if (u0) pair(x0, v0, p0);
+        if (u1) pair(x1, v1, p1);
+      }
+    } else {
+      for (int k = 0; k < nmax; ++k) {
+        int e = lr.get(k);
+        if (k >= cnt) continue;
+        int q = e & kSlotMask;
+        pair(P.X[q], P.V[q], P.RP[q]);
       }
     }
     double dtc = 1.0e300;
@@ -1973,7 +1997,9 @@ __device__ __forceinline__ double continuity_boundary_c1(const SimDev& s, const 
 // form, Continuity_Equation.f90:119-126,201-217 -- the whole velocity
 // gradient vectors are summed, and renormalised with B_ren_divu when
 // C1_divu is set; their trace equals the plain form's sum bit for bit.
-template <int DIM, bool FUSED, bool C1 = false>
+// BATCH (not with C1): two list entries' records requested before the
+// first one's arithmetic, as in k_momentum; the same sums.
+template <int DIM, bool FUSED, bool C1 = false, bool BATCH = false>
 __global__ void __launch_bounds__(kBlock, 2) k_continuity(DevBatch b) {
   __shared__ SimDev s;
   int cur = -1;
@@ -2003,16 +2029,11 @@ __global__ void __launch_bounds__(kBlock, 2) k_continuity(DevBatch b) {
     lr.init(b.nlist, p, b.list_cap4, cnt);
     const int nmax = __reduce_max_sync(0xffffffffu, (unsigned)cnt);
     prefetch_list_l2(b.nlist, p, b.list_cap4, nmax);
-    for (int k = 0; k < nmax; ++k) {
-      int e = lr.get(k);
-      if (k >= cnt) continue;
-      int q = e & kSlotMask;
-      double4 xj = P.X[q];
+    auto pair = [&](const double4& xj, const double4& vj) {
       double r0 = xi.x - xj.x, r1 = xi.y - xj.y, r2 = xi.z - xj.z;
       double rr = r0 * r0 + r1 * r1 + r2 * r2;
       double PK1, PK2, PK3;
       kernel_values(s, rr, PK1, PK2, PK3);
-      double4 vj = P.V[q];
       double c = rhoi * vj.w * PK1;     // rhoi * (amassj / rhoj) * PK1
       if (C1) {
         const double c0 = c * (vj.x - vi.x), c1 = c * (vj.y - vi.y), c2 = c * (vj.z - vi.z);
@@ -2029,6 +2050,31 @@ __global__ void __launch_bounds__(kBlock, 2) k_continuity(DevBatch b) {
         a1 = a1 + c * (vj.x - vi.x) * r0;
         if (DIM == 3) a2 = a2 + c * (vj.y - vi.y) * r1;
         a3 = a3 + c * (vj.z - vi.z) * r2;
+      }
+    };
+    if (BATCH) {
+      for (int k = 0; k < nmax; k += 2) {
+        const int e0 = lr.get(k);
+        const int e1 = k + 1 < nmax ? lr.get(k + 1) : 0;
+        const bool u0 = k < cnt, u1 = k + 1 < cnt;
+        double4 x0 = make_double4(0.0, 0.0, 0.0, 0.0), v0 = x0, x1 = x0, v1 = x0;
+        if (u0) {
+          const int q = e0 & kSlotMask;
+          x0 = P.X[q]; v0 = P.V[q];
+        }
+        if (u1) {
+          const int q = e1 & kSlotMask;
+          x1 = P.X[q]; v1 = P.V[q];
+        }
+        if (u0) pair(x0, v0);
+        if (u1) pair(x1, v1);
+      }
+    } else {
+      for (int k = 0; k < nmax; ++k) {
+        int e = lr.get(k);
+        if (k >= cnt) continue;
+        int q = e & kSlotMask;
+        pair(P.X[q], P.V[q]);
       }
     }
     if (active) {
@@ -3720,11 +3766,21 @@ void launch_momentum(const DevBatch& b, bool fused, cudaStream_t st) {
     if (fused) k_momentum<3, true, true><<<g, kBlock, 0, st>>>(b);
     else k_momentum<3, false, true><<<g, kBlock, 0, st>>>(b);
   } else if (b.dim == 3) {
-    if (fused) k_momentum<3, true><<<g, kBlock, 0, st>>>(b);
-    else k_momentum<3, false><<<g, kBlock, 0, st>>>(b);
+    if (b.mom_batch) {
+      if (fused) k_momentum<3, true, false, true><<<g, kBlock, 0, st>>>(b);
+      else k_momentum<3, false, false, true><<<g, kBlock, 0, st>>>(b);
+    } else {
+      if (fused) k_momentum<3, true><<<g, kBlock, 0, st>>>(b);
+      else k_momentum<3, false><<<g, kBlock, 0, st>>>(b);
+    }
   } else {
-    if (fused) k_momentum<2, true><<<g, kBlock, 0, st>>>(b);
-    else k_momentum<2, false><<<g, kBlock, 0, st>>>(b);
+    if (b.mom_batch) {
+      if (fused) k_momentum<2, true, false, true><<<g, kBlock, 0, st>>>(b);
+      else k_momentum<2, false, false, true><<<g, kBlock, 0, st>>>(b);
+    } else {
+      if (fused) k_momentum<2, true><<<g, kBlock, 0, st>>>(b);
+      else k_momentum<2, false><<<g, kBlock, 0, st>>>(b);
+    }
   }
 }
 
@@ -3799,11 +3855,21 @@ void launch_continuity(const DevBatch& b, bool fused, cudaStream_t st) {
     if (fused) k_continuity<3, true, true><<<g, kBlock, 0, st>>>(b);
     else k_continuity<3, false, true><<<g, kBlock, 0, st>>>(b);
   } else if (b.dim == 3) {
-    if (fused) k_continuity<3, true><<<g, kBlock, 0, st>>>(b);
-    else k_continuity<3, false><<<g, kBlock, 0, st>>>(b);
+    if (b.con_batch) {
+      if (fused) k_continuity<3, true, false, true><<<g, kBlock, 0, st>>>(b);
+      else k_continuity<3, false, false, true><<<g, kBlock, 0, st>>>(b);
+    } else {
+      if (fused) k_continuity<3, true><<<g, kBlock, 0, st>>>(b);
+      else k_continuity<3, false><<<g, kBlock, 0, st>>>(b);
+    }
   } else {
-    if (fused) k_continuity<2, true><<<g, kBlock, 0, st>>>(b);
-    else k_continuity<2, false><<<g, kBlock, 0, st>>>(b);
+    if (b.con_batch) {
+      if (fused) k_continuity<2, true, false, true><<<g, kBlock, 0, st>>>(b);
+      else k_continuity<2, false, false, true><<<g, kBlock, 0, st>>>(b);
+    } else {
+      if (fused) k_continuity<2, true><<<g, kBlock, 0, st>>>(b);
+      else k_continuity<2, false><<<g, kBlock, 0, st>>>(b);
+    }
   }
 }
 

@@ -35,8 +35,8 @@ struct DevBatch {
   int grid_blocks;         // blocks of the persistent particle kernels (default)
   int sms;                 // streaming multiprocessors of the device
   int grid[kGridClasses];  // autotuned blocks per kernel class (0 = grid_blocks)
-  int mom_batch;           // FP32c momentum pair loop: 1 = chunk records loaded together (autotuned)
-  int con_batch;           // the same for the FP32c continuity pair loop
+  int mom_batch;           // momentum pair loop: 1 = several entries' records loaded together (autotuned)
+  int con_batch;           // the same for the continuity pair loop
   int c1;                  // some simulation renormalises (C1_BE, 3D): P.BG (and P.BD) allocated
   int c1_divu;             // some simulation renormalises its velocity gradients (C1_divu)
 };

@@ -40,18 +40,31 @@ CASES = {
     "dam_break_2d": lambda: cases.dam_break_2d(),
     "dam_break_3d_dx02": lambda: cases.dam_break_3d(dx=0.02),
     "random_box_20k": lambda: cases.random_box(n=20000, seed=11),
-    # CreaGrid rounds 13.96 cells up to 14: cells narrower than 2h, so two
-    # cells away in z a random particle can lie within 2h and still not be
-    # a neighbour (outside the 27-cell block)
-    "random_box_30k_narrow_cells": lambda: cases.random_box(n=30000, seed=12),
+    # CreaGrid rounds 10.51 cells of 2h up to 11: cells 4.5% narrower than
+    # 2h, so a particle two cells away can lie within 2h and still not be a
+    # neighbour (outside the 27-cell block); this box has 42 such pairs
+    "random_box_11k_narrow_cells": lambda: cases.random_box(n=10800, seed=12),
 }
 
 
-def test_narrow_cell_case_has_narrow_cells():
+def test_narrow_cell_case_has_pairs_two_cells_apart():
+    """The narrow-cell case must hold pairs within 2h whose cells are two
+    apart (the ones the reference's 27-cell search never visits), or it
+    would not test the list pass's window mask."""
     from sphera_b200 import slab
-    c = CASES["random_box_30k_narrow_cells"]()
+    c = CASES["random_box_11k_narrow_cells"]()
+    h2 = 2.0 * c.params.dx * c.params.trunc
     lo, ncd, dcd = slab.whole_grid(c.params)
-    assert dcd < 2.0 * c.params.dx * c.params.trunc
+    assert dcd < 0.96 * h2
+    x = c.state.x
+    cell = np.ceil((x - lo) / dcd)            # a cube: the same grid in x, y, z
+    far = 0
+    for a in range(0, len(x), 256):
+        d = x[a:a + 256, None, :] - x[None, :, :]
+        near = np.einsum("ijk,ijk->ij", d, d) <= h2 * h2
+        apart = np.abs(cell[a:a + 256, None, :] - cell[None, :, :]).max(axis=2) >= 2
+        far += int((near & apart).sum())
+    assert far > 0
 
 
 @pytest.mark.parametrize("name", list(CASES))
