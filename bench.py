@@ -262,7 +262,12 @@ def run_ensemble(args, ws, rank, emit=True):
     cs = cases.ensemble_2d(n_sims=args.n_sims, dx=0.01, seed=0xC3 + rank, precision=abi.SPH_PREC_FP32C)
     b = Batch(cs)
     b.upload()
-    grids = b.autotune(reps=2)
+    if getattr(args, "shape", None) and len(args.shape.split(",")) == 7:
+        # a fixed launch configuration instead of the autotuner's choice
+        grids = dict(zip(__import__("sphera_b200")._SHAPE_KEYS, (int(t) for t in args.shape.split(","))))
+        b.set_launch_shape(grids)
+    else:
+        grids = b.autotune(reps=2)
     for i in range(len(cs)):
         b.set_end_time(i, args.t_end)
     n_total = sum(c.n for c in cs)
