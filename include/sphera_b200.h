@@ -141,7 +141,10 @@ typedef struct SphGeometry {
     const int32_t* side_zone;       /* [n_sides] zone id                              */
 } SphGeometry;
 
-/* Particle state in the caller's order (pg(1:n)). */
+/* Particle state in the caller's order (pg(1:n)).  The arrays may be host
+ * memory or device memory of the handle's device (as may the laminar-flag
+ * arrays of sph_replace_particles, sph_set_clock and sph_dump_laminar):
+ * copies take their direction from the pointers.                         */
 typedef struct SphState {
     int32_t n;
     double* x;                      /* [n][3] pg%coord                                */

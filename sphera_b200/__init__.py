@@ -120,6 +120,16 @@ def _set_launch_shape(h, shape):
     _chk(lib().sph_set_launch_shape(h, abi.iptr(g)), "sph_set_launch_shape")
 
 
+def _int_ptr(a):
+    """int32* of a numpy array or of a torch tensor (host or device), or NULL."""
+    if a is None:
+        return C.POINTER(C.c_int32)()
+    if type(a).__module__.startswith("torch"):
+        assert str(a.dtype) == "torch.int32" and a.is_contiguous()
+        return C.cast(a.data_ptr(), C.POINTER(C.c_int32))
+    return abi.iptr(np.ascontiguousarray(a, dtype=np.int32))
+
+
 class Simulation:
     """One simulation on the device (a one-entry batch of the C ABI)."""
 
@@ -143,9 +153,9 @@ class Simulation:
 
     def replace_particles(self, state, laminar=None):
         """A new particle set (and its laminar flags), the clock kept; the
-        search runs on it."""
-        lam = None if laminar is None else np.ascontiguousarray(laminar, dtype=np.int32)
-        _chk(lib().sph_replace_particles(self._h, C.byref(state.struct), abi.iptr(lam)), "sph_replace_particles")
+        search runs on it.  state and laminar may be host arrays or, for a
+        host that keeps them on the device, device tensors."""
+        _chk(lib().sph_replace_particles(self._h, C.byref(state.struct), _int_ptr(laminar)), "sph_replace_particles")
         self.n = state.n
 
     def set_time_step(self, dt):
@@ -335,6 +345,16 @@ class Simulation:
         f = np.zeros(self.n, np.int32)
         _chk(lib().sph_dump_laminar(self._h, abi.iptr(f)), "sph_dump_laminar")
         return f
+
+    def dump_laminar_into(self, flags):
+        """dump_laminar into a caller's int32 array or device tensor of n entries."""
+        _chk(lib().sph_dump_laminar(self._h, _int_ptr(flags)), "sph_dump_laminar")
+
+    def download_into(self, state):
+        """download() into a caller's state (abi.State or a state of device
+        tensors, n rows); returns the particle count."""
+        _chk(lib().sph_download(self._h, C.byref(state.struct)), "sph_download")
+        return state.struct.n
 
     def dump_renormalisation(self, divu=True):
         """B_ren_gradp and (divu) B_ren_divu in caller order, (n, 3, 3)."""

@@ -736,9 +736,9 @@ void enqueue_early_copy(SphHandle* h, cudaStream_t st, EarlyCopy& ec) {
   cudaError_t e = cudaGetLastError();
   const size_t o = h->sims[0].dev.p_off, n = (size_t)ec.n;
   SphState* sta = ec.state;
-  if (e == cudaSuccess && sta->x) e = cudaMemcpyAsync(sta->x, h->d_cx + 3 * o, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, q);
-  if (e == cudaSuccess && sta->v) e = cudaMemcpyAsync(sta->v, h->d_cv + 3 * o, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, q);
-  if (e == cudaSuccess && sta->m) e = cudaMemcpyAsync(sta->m, h->d_cm + o, sizeof(double) * n, cudaMemcpyDeviceToHost, q);
+  if (e == cudaSuccess && sta->x) e = cudaMemcpyAsync(sta->x, h->d_cx + 3 * o, sizeof(double) * 3 * n, cudaMemcpyDefault, q);
+  if (e == cudaSuccess && sta->v) e = cudaMemcpyAsync(sta->v, h->d_cv + 3 * o, sizeof(double) * 3 * n, cudaMemcpyDefault, q);
+  if (e == cudaSuccess && sta->m) e = cudaMemcpyAsync(sta->m, h->d_cm + o, sizeof(double) * n, cudaMemcpyDefault, q);
   ec.err = e;
 }
 
@@ -1002,17 +1002,22 @@ int create_batch(int nsims, const SphParams* params, const SphGeometry* geoms, c
   return SPH_OK;
 }
 
+// The caller's arrays may be host memory (pageable or page-locked) or
+// device memory of the handle's device: the copies take the direction from
+// the pointers (unified addressing), so a host that keeps its state on the
+// device (e.g. a slab exchange done with device tensors) never stages it
+// through the host.
 int upload_sim(SphHandle* h, int sim, const SphState* st) {
   if (!h || !st || sim < 0 || sim >= h->nsims) return SPH_ERR_INVALID_ARGUMENT;
   HostSim& hs = h->sims[sim];
   if (st->n < 0 || st->n > hs.cap || !st->x || !st->v || !st->rho || !st->p || !st->m) return SPH_ERR_INVALID_ARGUMENT;
   size_t o = hs.dev.p_off, n = st->n;
   cudaStream_t q = h->stream;
-  SPH_CUDA(cudaMemcpyAsync(h->d_cx + 3 * o, st->x, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, q));
-  SPH_CUDA(cudaMemcpyAsync(h->d_cv + 3 * o, st->v, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, q));
-  SPH_CUDA(cudaMemcpyAsync(h->d_crho + o, st->rho, sizeof(double) * n, cudaMemcpyHostToDevice, q));
-  SPH_CUDA(cudaMemcpyAsync(h->d_cp + o, st->p, sizeof(double) * n, cudaMemcpyHostToDevice, q));
-  SPH_CUDA(cudaMemcpyAsync(h->d_cm + o, st->m, sizeof(double) * n, cudaMemcpyHostToDevice, q));
+  SPH_CUDA(cudaMemcpyAsync(h->d_cx + 3 * o, st->x, sizeof(double) * 3 * n, cudaMemcpyDefault, q));
+  SPH_CUDA(cudaMemcpyAsync(h->d_cv + 3 * o, st->v, sizeof(double) * 3 * n, cudaMemcpyDefault, q));
+  SPH_CUDA(cudaMemcpyAsync(h->d_crho + o, st->rho, sizeof(double) * n, cudaMemcpyDefault, q));
+  SPH_CUDA(cudaMemcpyAsync(h->d_cp + o, st->p, sizeof(double) * n, cudaMemcpyDefault, q));
+  SPH_CUDA(cudaMemcpyAsync(h->d_cm + o, st->m, sizeof(double) * n, cudaMemcpyDefault, q));
   h->n_of[sim] = st->n;
   return SPH_OK;
 }
@@ -1129,14 +1134,14 @@ static int download_impl(SphHandle* h, int sim, SphState* state, double* acc, do
   size_t o = hs.dev.p_off;
   if (state) {
     state->n = n;
-    if (state->x) SPH_CUDA(cudaMemcpyAsync(state->x, h->d_cx + 3 * o, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, q));
-    if (state->v) SPH_CUDA(cudaMemcpyAsync(state->v, h->d_cv + 3 * o, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, q));
-    if (state->rho) SPH_CUDA(cudaMemcpyAsync(state->rho, h->d_crho + o, sizeof(double) * n, cudaMemcpyDeviceToHost, q));
-    if (state->p) SPH_CUDA(cudaMemcpyAsync(state->p, h->d_cp + o, sizeof(double) * n, cudaMemcpyDeviceToHost, q));
-    if (state->m) SPH_CUDA(cudaMemcpyAsync(state->m, h->d_cm + o, sizeof(double) * n, cudaMemcpyDeviceToHost, q));
+    if (state->x) SPH_CUDA(cudaMemcpyAsync(state->x, h->d_cx + 3 * o, sizeof(double) * 3 * n, cudaMemcpyDefault, q));
+    if (state->v) SPH_CUDA(cudaMemcpyAsync(state->v, h->d_cv + 3 * o, sizeof(double) * 3 * n, cudaMemcpyDefault, q));
+    if (state->rho) SPH_CUDA(cudaMemcpyAsync(state->rho, h->d_crho + o, sizeof(double) * n, cudaMemcpyDefault, q));
+    if (state->p) SPH_CUDA(cudaMemcpyAsync(state->p, h->d_cp + o, sizeof(double) * n, cudaMemcpyDefault, q));
+    if (state->m) SPH_CUDA(cudaMemcpyAsync(state->m, h->d_cm + o, sizeof(double) * n, cudaMemcpyDefault, q));
   }
-  if (acc) SPH_CUDA(cudaMemcpyAsync(acc, h->d_cacc + 3 * o, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, q));
-  if (dden) SPH_CUDA(cudaMemcpyAsync(dden, h->d_cdden + o, sizeof(double) * n, cudaMemcpyDeviceToHost, q));
+  if (acc) SPH_CUDA(cudaMemcpyAsync(acc, h->d_cacc + 3 * o, sizeof(double) * 3 * n, cudaMemcpyDefault, q));
+  if (dden) SPH_CUDA(cudaMemcpyAsync(dden, h->d_cdden + o, sizeof(double) * n, cudaMemcpyDefault, q));
   SPH_CUDA(cudaStreamSynchronize(q));
   return h->h_dyn[sim].status;
 }
@@ -1190,8 +1195,8 @@ int sph_step_download(SphHandle* h, int32_t nsteps, SphState* state) {
   launch_to_caller(h->db, nullptr, nullptr, h->d_crho, h->d_cp, nullptr, nullptr, nullptr, q);
   cudaError_t e = cudaGetLastError();
   const size_t o = h->sims[0].dev.p_off, n = (size_t)ec.n;
-  if (e == cudaSuccess && state->rho) e = cudaMemcpyAsync(state->rho, h->d_crho + o, sizeof(double) * n, cudaMemcpyDeviceToHost, q);
-  if (e == cudaSuccess && state->p) e = cudaMemcpyAsync(state->p, h->d_cp + o, sizeof(double) * n, cudaMemcpyDeviceToHost, q);
+  if (e == cudaSuccess && state->rho) e = cudaMemcpyAsync(state->rho, h->d_crho + o, sizeof(double) * n, cudaMemcpyDefault, q);
+  if (e == cudaSuccess && state->p) e = cudaMemcpyAsync(state->p, h->d_cp + o, sizeof(double) * n, cudaMemcpyDefault, q);
   cudaError_t e3 = cudaStreamSynchronize(h->stream3);
   if (e == cudaSuccess) e = ec.err;
   if (e == cudaSuccess) e = e3;
@@ -1263,7 +1268,7 @@ int sph_replace_particles(SphHandle* h, const SphState* state, const int32_t* la
   cudaStream_t q = h->stream;
   SPH_CUDA(cudaMemcpyAsync(h->d_dyn, h->h_dyn.data(), sizeof(SimDyn), cudaMemcpyHostToDevice, q));
   if (laminar && state->n > 0)
-    SPH_CUDA(cudaMemcpyAsync(h->d_ci1, laminar, sizeof(int32_t) * state->n, cudaMemcpyHostToDevice, q));
+    SPH_CUDA(cudaMemcpyAsync(h->d_ci1, laminar, sizeof(int32_t) * state->n, cudaMemcpyDefault, q));
   launch_init_from_caller(h->db, h->d_cx, h->d_cv, h->d_crho, h->d_cp, h->d_cm, q);
   sort_sequence(h, q);
   if (laminar && state->n > 0) launch_load_laminar(h->db, h->d_ci1, q);
@@ -1305,7 +1310,7 @@ int sph_set_clock(SphHandle* h, const SphClock* clock, const int32_t* laminar) {
   const int n = h->h_dyn[0].nag;
   cudaStream_t q = h->stream;
   if (laminar && n > 0)
-    SPH_CUDA(cudaMemcpyAsync(h->d_ci1, laminar, sizeof(int32_t) * n, cudaMemcpyHostToDevice, q));
+    SPH_CUDA(cudaMemcpyAsync(h->d_ci1, laminar, sizeof(int32_t) * n, cudaMemcpyDefault, q));
   launch_set_clock(h->db, clock->time, clock->step, clock->dt, clock->dt_prev, clock->dt_average,
                    laminar && n > 0 ? h->d_ci1 : nullptr, q);
   SPH_CUDA(cudaGetLastError());
@@ -1498,7 +1503,7 @@ int sph_dump_laminar(SphHandle* h, int32_t* flags) {
   cudaStream_t q = h->stream;
   launch_dump_laminar(h->db, h->d_ci1, q);
   SPH_CUDA(cudaGetLastError());
-  SPH_CUDA(cudaMemcpyAsync(flags, h->d_ci1, sizeof(int) * n, cudaMemcpyDeviceToHost, q));
+  SPH_CUDA(cudaMemcpyAsync(flags, h->d_ci1, sizeof(int) * n, cudaMemcpyDefault, q));
   return cuda_status(cudaStreamSynchronize(q));
 }
 

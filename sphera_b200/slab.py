@@ -47,6 +47,10 @@ from . import abi
 _REC = 11
 
 
+def _torch(a):
+    return type(a).__module__.startswith("torch")
+
+
 def whole_grid(params):
     """CreaGrid.f90:51-74 restated on the host (the device's own sequence of
     IEEE operations): x-extent origin, cell count and cell size."""
@@ -61,7 +65,11 @@ def whole_grid(params):
 
 
 def cell_x(x, lo, dcd):
-    """ParticleCellNumber.f90:52-62 in x: ceiling((x - extr) / dcd)."""
+    """ParticleCellNumber.f90:52-62 in x: ceiling((x - extr) / dcd), on numpy
+    arrays or torch tensors (the same correctly rounded FP64 operations)."""
+    if _torch(x):
+        import torch
+        return torch.ceil((x[:, 0] - lo) / dcd).to(torch.int64)
     return np.ceil((x[:, 0] - lo) / dcd).astype(np.int64)
 
 
@@ -83,19 +91,44 @@ def split_cells(ncd, nslabs, weights=None):
 def assemble(rec, ci, own, ncd):
     """The particle set of the slab owning x cells own = (a, b): its owned
     particles and the ghosts of cells a - 1 and b + 1, in increasing global
-    index.  rec: (n, _REC) records, ci their x cells.  Returns the rows and
-    the mask of owned rows."""
+    index.  rec: (n, _REC) records, ci their x cells (numpy or torch).
+    Returns the rows and the mask of owned rows."""
     a, b = own
     keep = (ci >= max(a - 1, 1)) & (ci <= min(b + 1, ncd))
     rows = rec[keep]
-    order = np.argsort(rows[:, 0], kind="stable")
+    if _torch(rows):
+        import torch
+        order = torch.argsort(rows[:, 0], stable=True)
+    else:
+        order = np.argsort(rows[:, 0], kind="stable")
     rows = rows[order]
     c = ci[keep][order]
     return rows, (c >= a) & (c <= b)
 
 
+class DeviceState:
+    """An SphState over torch tensors in the handle's device memory (the
+    library's copies take their direction from the pointers)."""
+
+    def __init__(self, x, v, rho, p, m):
+        self.x, self.v, self.rho, self.p, self.m = (t.contiguous() for t in (x, v, rho, p, m))
+        st = abi.SphState()
+        st.n = int(self.rho.shape[0])
+        for f in ("x", "v", "rho", "p", "m"):
+            setattr(st, f, abi.C.cast(getattr(self, f).data_ptr(), abi.C.POINTER(abi.C.c_double)))
+        self.struct = st
+
+    @property
+    def n(self):
+        return int(self.rho.shape[0])
+
+
 def records(gid, st, laminar=None):
-    out = np.empty((st.n, _REC))
+    if _torch(st.x):
+        import torch
+        out = torch.empty((st.n, _REC), dtype=torch.float64, device=st.x.device)
+    else:
+        out = np.empty((st.n, _REC))
     out[:, 0] = gid
     out[:, 1:4] = st.x
     out[:, 4:7] = st.v
@@ -107,33 +140,64 @@ def records(gid, st, laminar=None):
 
 
 def state_of(rows):
+    if _torch(rows):
+        return DeviceState(rows[:, 1:4], rows[:, 4:7], rows[:, 7], rows[:, 8], rows[:, 9])
     return abi.State(np.ascontiguousarray(rows[:, 1:4]), np.ascontiguousarray(rows[:, 4:7]),
                      np.ascontiguousarray(rows[:, 7]), np.ascontiguousarray(rows[:, 8]),
                      np.ascontiguousarray(rows[:, 9]))
 
 
 def laminar_of(rows):
+    if _torch(rows):
+        import torch
+        return rows[:, 10].to(torch.int32).contiguous()
     return np.ascontiguousarray(rows[:, 10], dtype=np.int32)
 
 
 class SlabEngine:
-    """The device side of one slab: a library handle over the slab's cells."""
+    """The device side of one slab: a library handle over the slab's cells.
+    With device=True its state crosses the C ABI as device tensors."""
 
-    def __init__(self, case, cells, capacity):
+    def __init__(self, case, cells, capacity, device=False):
         from . import Simulation
         self.sim = Simulation(params=case.params, geometry=case.geometry, capacity=capacity, cells=cells)
+        self.device = device
+
+    def _ready(self):
+        # device tensors are written by torch on its own stream; the
+        # library reads them on the handle's stream, so torch's work must
+        # be complete first (the library synchronises its own stream before
+        # it returns, so what it writes is complete for torch)
+        if self.device:
+            import torch
+            torch.cuda.current_stream().synchronize()
 
     def upload(self, st):
+        self._ready()
         self.sim.upload(st)
 
     def replace(self, st, laminar):
+        self._ready()
         self.sim.replace_particles(st, laminar)
 
     def download(self):
-        return self.sim.download()
+        if not self.device:
+            return self.sim.download()
+        import torch
+        n = self.sim.n
+        dev = torch.device("cuda", torch.cuda.current_device())
+        st = DeviceState(*(torch.empty(sh, dtype=torch.float64, device=dev)
+                           for sh in ((n, 3), (n, 3), (n,), (n,), (n,))))
+        self.sim.download_into(st)
+        return st
 
     def laminar(self):
-        return self.sim.dump_laminar()
+        if not self.device:
+            return self.sim.dump_laminar()
+        import torch
+        f = torch.empty(self.sim.n, dtype=torch.int32, device=torch.device("cuda", torch.cuda.current_device()))
+        self.sim.dump_laminar_into(f)
+        return f
 
     def momentum(self):
         self.sim.rhs_momentum(want=False)
@@ -156,10 +220,11 @@ class SlabEngine:
 
 
 class SlabRun:
-    """All slabs in one process; the exchanges gather the owned particles on
-    the host and rebuild every slab's set from them."""
+    """All slabs in one process; the exchanges gather the owned particles
+    and rebuild every slab's set from them -- on the host, or with
+    device=True as device tensors that cross the C ABI without a host copy."""
 
-    def __init__(self, case, nslabs=2, ranges=None, engine=SlabEngine, capacity=None):
+    def __init__(self, case, nslabs=2, ranges=None, engine=SlabEngine, capacity=None, device=False):
         self.case = case
         self.lo, self.ncd, self.dcd = whole_grid(case.params)
         st = case.state
@@ -168,8 +233,12 @@ class SlabRun:
             ranges = split_cells(self.ncd, nslabs, np.bincount(ci, minlength=self.ncd + 1)[1:])
         self.ranges = ranges
         cap = capacity or st.n
-        self.engines = [engine(case, (max(a - 1, 1), min(b + 1, self.ncd)), cap) for a, b in ranges]
+        kw = dict(device=True) if device else {}
+        self.engines = [engine(case, (max(a - 1, 1), min(b + 1, self.ncd)), cap, **kw) for a, b in ranges]
         self.rec = records(np.arange(st.n, dtype=np.float64), st)
+        if device:
+            import torch
+            self.rec = torch.from_numpy(self.rec).to(torch.device("cuda", torch.cuda.current_device()))
         self.n = st.n
         self.owned = [None] * len(ranges)
         sets = self._sets()
@@ -179,12 +248,14 @@ class SlabRun:
 
     def _sets(self):
         ci = cell_x(self.rec[:, 1:4], self.lo, self.dcd)
-        if np.any((ci < 1) | (ci > self.ncd)):
+        if bool(((ci < 1) | (ci > self.ncd)).any()):
             raise RuntimeError("a particle left the grid: slab runs do not remove particles")
         out = []
         for k, own in enumerate(self.ranges):
             rows, mask = assemble(self.rec, ci, own, self.ncd)
-            self.owned[k] = (rows[:, 0].astype(np.int64), mask)
+            gid = rows[:, 0]
+            gid = gid.long() if _torch(gid) else gid.astype(np.int64)
+            self.owned[k] = (gid, mask)
             out.append(rows)
         return out
 
@@ -214,15 +285,17 @@ class SlabRun:
             self._exchange()
             self._global_dt()
 
-    def state(self):
-        """The whole simulation's state in its original particle order."""
+    def _host_rec(self):
         self._gather()
-        return state_of(self.rec)
+        return self.rec.cpu().numpy() if _torch(self.rec) else self.rec
+
+    def state(self):
+        """The whole simulation's state in its original particle order (host arrays)."""
+        return state_of(self._host_rec())
 
     def laminar(self):
         """pg%laminar_flag of the whole simulation, original particle order."""
-        self._gather()
-        return laminar_of(self.rec)
+        return laminar_of(self._host_rec())
 
     def counts(self):
         return [int(m.sum()) for _, m in self.owned], [int((~m).sum()) for _, m in self.owned]
@@ -238,9 +311,13 @@ class DistributedSlabRun:
     r + 1 only, the owned particles in the cells next to the shared edge
     (the neighbour's ghosts) and those that crossed it (migrants); a step
     moves a particle far less than a cell, so no other rank is reached.  The
-    dt is an all-reduce (min)."""
+    dt is an all-reduce (min).  With device=True (an NCCL group, one GPU per
+    rank) the records stay in device tensors: the slab's state is read and
+    replaced through the C ABI with device pointers and the edge layers go
+    rank to rank with NCCL send/recv, never through the host; otherwise
+    (gloo) they are host arrays."""
 
-    def __init__(self, case, ranges, engine=SlabEngine, capacity=None, device=None):
+    def __init__(self, case, ranges, engine=SlabEngine, capacity=None, device=False):
         import torch.distributed as dist
         self.dist = dist
         self.rank, self.size = dist.get_rank(), dist.get_world_size()
@@ -254,42 +331,45 @@ class DistributedSlabRun:
         all_rec = records(np.arange(st.n, dtype=np.float64), st)
         ci = cell_x(st.x, self.lo, self.dcd)
         rows, mask = assemble(all_rec, ci, self.own, self.ncd)
-        self.rows, self.mask = rows, mask
         a, b = self.own
-        self.engine = engine(case, (max(a - 1, 1), min(b + 1, self.ncd)), capacity or st.n)
+        kw = dict(device=True) if device else {}
+        self.engine = engine(case, (max(a - 1, 1), min(b + 1, self.ncd)), capacity or st.n, **kw)
+        if device:
+            import torch
+            dev = torch.device("cuda", torch.cuda.current_device())
+            rows, mask = torch.from_numpy(rows).to(dev), torch.from_numpy(mask).to(dev)
+        self.rows, self.mask = rows, mask
         self.engine.upload(state_of(rows))
         self._global_dt()
 
-    def _tensor(self, arr):
-        import torch
-        t = torch.from_numpy(np.ascontiguousarray(arr))
-        return t.to(self.device) if self.device is not None else t
-
     def _trade(self, peer, send):
-        """Sends `send` rows to `peer` and returns the rows it sent back."""
+        """Sends `send` rows to `peer` and returns the rows it sent back
+        (tensors on the rows' device: NCCL moves device memory, gloo host)."""
         import torch
         dist = self.dist
-        cnt_out = self._tensor(np.array([send.shape[0]], dtype=np.int64))
-        cnt_in = self._tensor(np.zeros(1, dtype=np.int64))
+        dev = send.device if _torch(send) else torch.device("cpu")
+        payload = send if _torch(send) else torch.from_numpy(np.ascontiguousarray(send))
+        cnt_out = torch.tensor([payload.shape[0]], dtype=torch.int64, device=dev)
+        cnt_in = torch.zeros(1, dtype=torch.int64, device=dev)
         reqs = [dist.isend(cnt_out, peer), dist.irecv(cnt_in, peer)]
         for r in reqs:
             r.wait()
-        m = int(cnt_in.cpu().item())
-        buf_in = self._tensor(np.zeros((m, _REC)))
+        m = int(cnt_in.item())
+        buf_in = torch.empty((m, _REC), dtype=torch.float64, device=dev)
         reqs = []
-        if send.shape[0]:
-            reqs.append(dist.isend(self._tensor(send), peer))
+        if payload.shape[0]:
+            reqs.append(dist.isend(payload.contiguous(), peer))
         if m:
             reqs.append(dist.irecv(buf_in, peer))
         for r in reqs:
             r.wait()
-        return buf_in.cpu().numpy() if isinstance(buf_in, torch.Tensor) else buf_in
+        return buf_in if _torch(send) else buf_in.numpy()
 
     def _exchange(self):
         st = self.engine.download()
         mine = records(self.rows[:, 0], st, self.engine.laminar())[self.mask]   # my owned particles, updated
         ci = cell_x(mine[:, 1:4], self.lo, self.dcd)
-        if np.any((ci < 1) | (ci > self.ncd)):
+        if bool(((ci < 1) | (ci > self.ncd)).any()):
             raise RuntimeError("a particle left the grid: slab runs do not remove particles")
         a, b = self.own
         got = [mine]
@@ -298,20 +378,23 @@ class DistributedSlabRun:
         for peer, sel in ((self.rank - 1, ci <= a), (self.rank + 1, ci >= b)):
             if 0 <= peer < self.size:
                 got.append(self._trade(peer, mine[sel]))
-        allrec = np.vstack(got)
-        # a received row may be a ghost of mine that I also own no longer, or
-        # a duplicate of an owned row: keep one row per particle
-        _, first = np.unique(allrec[:, 0], return_index=True)
-        allrec = allrec[first]
+        if _torch(mine):
+            import torch
+            allrec = torch.cat(got)
+        else:
+            allrec = np.vstack(got)
+        # the ranks own disjoint particle sets, so every row is a distinct
+        # particle; assemble orders them by global index
         rows, mask = assemble(allrec, cell_x(allrec[:, 1:4], self.lo, self.dcd), self.own, self.ncd)
         self.rows, self.mask = rows, mask
         self.engine.replace(state_of(rows), laminar_of(rows))
 
     def _global_dt(self):
         import torch
-        t = self._tensor(np.array([self.engine.dt()]))
+        dev = torch.device("cuda", torch.cuda.current_device()) if self.device else torch.device("cpu")
+        t = torch.tensor([self.engine.dt()], dtype=torch.float64, device=dev)
         self.dist.all_reduce(t, op=self.dist.ReduceOp.MIN)
-        dt = float(t.cpu().item()) if isinstance(t, torch.Tensor) else float(t)
+        dt = float(t.item())
         self.engine.set_dt(dt)
         return dt
 
@@ -325,9 +408,10 @@ class DistributedSlabRun:
 
     def owned_records(self):
         """(global index, x, v, rho, p, m, laminar) rows of the particles this
-        rank owns."""
+        rank owns (host array)."""
         st = self.engine.download()
-        return records(self.rows[:, 0], st, self.engine.laminar())[self.mask]
+        r = records(self.rows[:, 0], st, self.engine.laminar())[self.mask]
+        return r.cpu().numpy() if _torch(r) else r
 
     def close(self):
         self.engine.close()

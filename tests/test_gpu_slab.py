@@ -55,13 +55,16 @@ def undivided(case, steps):
         return sim.download(), sim.diagnostics()
 
 
+@pytest.mark.parametrize("device", [False, True], ids=["host", "device"])
 @pytest.mark.parametrize("precision", [abi.SPH_PREC_FP64, abi.SPH_PREC_FP32C], ids=["fp64", "fp32c"])
 @pytest.mark.parametrize("name,nslabs,steps", [("dam_break_2d", 2, 60), ("dam_break_2d", 3, 60),
                                                ("dam_break_2d_laminar", 2, 60), ("dam_break_3d", 2, 60)])
-def test_slabs_are_the_undivided_run(name, nslabs, steps, precision):
+def test_slabs_are_the_undivided_run(name, nslabs, steps, precision, device):
+    """host: the exchanges go through host arrays; device: the records stay
+    in device tensors and cross the C ABI as device pointers."""
     case = make(name, precision)
     ref, _ = undivided(case, steps)
-    run = slab.SlabRun(case, nslabs=nslabs)
+    run = slab.SlabRun(case, nslabs=nslabs, device=device)
     try:
         owned0, _ = run.counts()
         run.step(steps)

@@ -177,6 +177,32 @@ def test_slab_run_is_the_undivided_run(nslabs):
     assert np.array_equal(got, ref)
 
 
+def test_torch_records_and_sets_equal_numpy():
+    """The device path's record handling (torch tensors; here on the CPU)
+    gives the numpy path's cells, sets, order and state columns exactly."""
+    import torch
+    case = moving_case()
+    lo, ncd, dcd = slab.whole_grid(case.params)
+    rng = np.random.Generator(np.random.PCG64(4))
+    lam = rng.integers(0, 2, case.n).astype(np.int32)
+    rec = slab.records(np.arange(case.n, dtype=np.float64), case.state, lam)
+    trec = torch.from_numpy(rec.copy())
+    ci, tci = slab.cell_x(rec[:, 1:4], lo, dcd), slab.cell_x(trec[:, 1:4], lo, dcd)
+    assert np.array_equal(ci, tci.numpy())
+    for own in slab.split_cells(ncd, 3, np.bincount(ci, minlength=ncd + 1)[1:]):
+        rows, mask = slab.assemble(rec, ci, own, ncd)
+        trows, tmask = slab.assemble(trec, tci, own, ncd)
+        assert np.array_equal(rows, trows.numpy()) and np.array_equal(mask, tmask.numpy())
+        st, tst = slab.state_of(rows), slab.state_of(trows)
+        for f in ("x", "v", "rho", "p", "m"):
+            assert np.array_equal(getattr(st, f), getattr(tst, f).numpy()), f
+        assert tst.struct.n == st.n
+        assert np.array_equal(slab.laminar_of(rows), slab.laminar_of(trows).numpy())
+    back = slab.records(trec[:, 0], slab.DeviceState(trec[:, 1:4], trec[:, 4:7], trec[:, 7], trec[:, 8],
+                                                      trec[:, 9]), trec[:, 10])
+    assert np.array_equal(back.numpy(), rec)
+
+
 def _free_port():
     s = socket.socket()
     s.bind(("127.0.0.1", 0))
