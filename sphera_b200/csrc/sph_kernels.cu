@@ -2227,6 +2227,64 @@ __device__ __forceinline__ void separation_f32(const SimDev& s, RunCursor<DIM>& 
   d2 = (ckf - xj.w) * dz + (xfi.z - xj.z);
 }
 
+// The closing of an FP32c momentum pass for particle p, from its nine pair
+// sums ms and its FP64 wall terms (zero without close faces): the laminar
+// flag (inter_EqMoto.f90:269-283), gravity, the elastic reaction, and in
+// the fused step the leapfrog update and the particle's CFL time.  One
+// function for both places a particle is closed (the finishing launch, and
+// the pair launch itself for particles without close faces), so the two
+// give the same bits.
+template <int DIM, bool FUSED>
+__device__ __forceinline__ void momentum_f32_close(const SimDev& s, const DevBatch& b, SimDyn* dyn, int p,
+                                                   const double* ms, double* tpres, const double* tdiss,
+                                                   const double* tvisc, const double* vi, double rhoi, double pi,
+                                                   int nb, int bstart, double& dtc) {
+  const Particles& P = b.P;
+  const double GI = (double)9.80665f;   // Static_allocation_module.f90:72, a default-REAL literal
+  const double* geff = dyn->geff;
+  double rs0 = ms[6], rs1 = ms[7], rs2 = ms[8];
+  tpres[0] = tpres[0] + ms[0];
+  tpres[1] = tpres[1] + ms[1];
+  tpres[2] = tpres[2] + ms[2];
+  int lam_new = 0;
+  if (s.kin_visc > 0.0) {
+    double absv_pres = sqrt(tpres[0] * tpres[0] + tpres[1] * tpres[1] + tpres[2] * tpres[2]) + GI;
+    double absv_morris = sqrt(rs0 * rs0 + rs1 * rs1 + rs2 * rs2);
+    double weight = 0.0;
+    if (absv_pres != 0.0) weight = absv_morris / absv_pres * 100.0;
+    lam_new = (weight > 5.0 || absv_pres == 0.0) ? 1 : 0;
+  }
+  double acc[3];
+  acc[0] = tpres[0] + (tdiss[0] + ms[3]) + (tvisc[0] + rs0) + geff[0];
+  acc[1] = tpres[1] + (tdiss[1] + ms[4]) + (tvisc[1] + rs1) + geff[1];
+  acc[2] = tpres[2] + (tdiss[2] + ms[5]) + (tvisc[2] + rs2) + geff[2];
+  const double4 xi = P.X[p];
+  if (nb > 0) {
+    double R[3];
+    const double xa[3] = {xi.x, xi.y, xi.z};
+    elastic_reaction<DIM>(s, b, nb, bstart, xa, vi, R);
+    for (int d = 0; d < 3; ++d) acc[d] = acc[d] + R[d];
+  }
+  if (FUSED) {
+    double dtvel = dyn->dtvel, dt = dyn->dt;
+    double vn[3];
+    for (int d = 0; d < 3; ++d) vn[d] = vi[d] + dtvel * acc[d];
+    P.X2[p] = make_double4(xi.x + dt * vn[0], xi.y + dt * vn[1], xi.z + dt * vn[2], xi.w);
+    P.V2[p] = make_double4(vn[0], vn[1], vn[2], rhoi);
+    if (P.VF2) P.VF2[p] = make_float4((float)vn[0], (float)vn[1], (float)vn[2], 0.f);
+    P.P2[p] = pi;
+    P.I2[p] = P.I[p];
+    P.L2[p] = (uint8_t)lam_new;
+    double U = sqrt(vn[0] * vn[0] + vn[1] * vn[1] + vn[2] * vn[2]);
+    // with velocity smoothing the CFL minimum is taken on the smoothed
+    // velocities (k_velocity_smoothing_apply), which also moves X2
+    if (!(s.teta_v > 1.0e-9)) dtc = s.cfl * 2.0 * s.h / (s.celerita + U);
+  } else {
+    P.ACC[p] = make_double4(acc[0], acc[1], acc[2], 0.0);
+    P.L[p] = (uint8_t)lam_new;
+  }
+}
+
 // Momentum, FP32c form, in two launches.  k_momentum_f32 holds only what
 // the pair loop needs -- the particle's FP32 values, the compensated sums,
 // the list chunk being read and the next one -- so that it runs at 3 blocks
@@ -2246,8 +2304,11 @@ __device__ __forceinline__ void separation_f32(const SimDev& s, RunCursor<DIM>& 
 // instead of one, at 2 blocks of 256 per SM (the registers they need); the
 // autotuner chooses it or the lean loop (3 blocks per SM) on the live
 // state.  Both sum the same terms in the same order: identical results.
+// fused (the whole step, not C1): a particle without close faces has no
+// FP64 wall terms, so this launch closes it at once (momentum_f32_close,
+// the finishing launch's own code) instead of passing its nine sums on.
 template <int DIM, bool C1 = false, bool BATCH = false>
-__global__ void __launch_bounds__(kBlock, (C1 || BATCH) ? 2 : 3) k_momentum_f32(DevBatch b) {
+__global__ void __launch_bounds__(kBlock, (C1 || BATCH) ? 2 : 3) k_momentum_f32(DevBatch b, int fused) {
   __shared__ SimDev s;
   int cur = -1;
   const Particles& P = b.P;
@@ -2369,7 +2430,25 @@ __global__ void __launch_bounds__(kBlock, (C1 || BATCH) ? 2 : 3) k_momentum_f32(
         cg0 = cg1 = cg2 = 0.f;
       }
     }
-    if (active) {
+    bool close_here = false;
+    if (!C1 && fused && active) close_here = P.bdt_count[p] == 0;
+    double dtc = 1.0e300;
+    if (close_here) {
+      const double ms[9] = {tp0.val(), tp1.val(), tp2.val(), td0.val(), td1.val(), td2.val(),
+                            tv0.val(), tv1.val(), tv2.val()};
+      double tpres[3] = {0, 0, 0};
+      const double tdiss[3] = {0, 0, 0}, tvisc[3] = {0, 0, 0};
+      const double4 v4 = P.V[p];
+      const double2 rp = P.RP[p];
+      const double vi[3] = {v4.x, v4.y, v4.z};
+      momentum_f32_close<DIM, true>(s, b, dyn, p, ms, tpres, tdiss, tvisc, vi, rp.x, rp.y, 0, 0, dtc);
+    }
+    if (!C1 && fused) {
+      const double m = warp_min(dtc);
+      if ((threadIdx.x & 31) == 0 && m < 1.0e300)
+        atomicMin(&dyn->dtmin_bits, (unsigned long long)__double_as_longlong(m));
+    }
+    if (active && !close_here) {
       double* o = P.MSUM + p;
       const size_t st = (size_t)P.total_slots;   // component-major: coalesced
       o[0] = tp0.val();
@@ -2398,7 +2477,6 @@ __global__ void __launch_bounds__(kBlock) k_momentum_f32_finish(DevBatch b) {
   __shared__ SimDev s;
   int cur = -1;
   const Particles& P = b.P;
-  const double GI = (double)9.80665f;   // Static_allocation_module.f90:72, a default-REAL literal
   for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
     Tile tl = b.tiles[t];
     load_sim(s, b.sims, tl.sim, cur);
@@ -2417,6 +2495,9 @@ __global__ void __launch_bounds__(kBlock) k_momentum_f32_finish(DevBatch b) {
       active = false;
     }
     double dtc = 1.0e300;
+    // in the fused step the pair launch has closed the particles without
+    // close faces already (k_momentum_f32)
+    if (FUSED && !C1 && active && P.bdt_count[p] == 0) active = false;
     if (active) {
       double ms[9];
       for (int c = 0; c < 9; ++c) ms[c] = P.MSUM[(size_t)c * P.total_slots + p];
@@ -2450,47 +2531,7 @@ __global__ void __launch_bounds__(kBlock) k_momentum_f32_finish(DevBatch b) {
         if (DIM == 3) me_boundary3d(s, b, nb, bstart, vi, rhoi, pi, lam, geff, tpres, tdiss, tvisc);
         else me_boundary2d(s, b, nb, bstart, vi, rhoi, pi, lam, geff, tpres, tdiss, tvisc);
       }
-      double rs0 = ms[6], rs1 = ms[7], rs2 = ms[8];
-      tpres[0] = tpres[0] + ms[0];
-      tpres[1] = tpres[1] + ms[1];
-      tpres[2] = tpres[2] + ms[2];
-      int lam_new = 0;
-      if (s.kin_visc > 0.0) {
-        double absv_pres = sqrt(tpres[0] * tpres[0] + tpres[1] * tpres[1] + tpres[2] * tpres[2]) + GI;
-        double absv_morris = sqrt(rs0 * rs0 + rs1 * rs1 + rs2 * rs2);
-        double weight = 0.0;
-        if (absv_pres != 0.0) weight = absv_morris / absv_pres * 100.0;
-        lam_new = (weight > 5.0 || absv_pres == 0.0) ? 1 : 0;
-      }
-      double acc[3];
-      acc[0] = tpres[0] + (tdiss[0] + ms[3]) + (tvisc[0] + rs0) + geff[0];
-      acc[1] = tpres[1] + (tdiss[1] + ms[4]) + (tvisc[1] + rs1) + geff[1];
-      acc[2] = tpres[2] + (tdiss[2] + ms[5]) + (tvisc[2] + rs2) + geff[2];
-      const double4 xi = P.X[p];
-      if (nb > 0) {
-        double R[3];
-        const double xa[3] = {xi.x, xi.y, xi.z};
-        elastic_reaction<DIM>(s, b, nb, bstart, xa, vi, R);
-        for (int d = 0; d < 3; ++d) acc[d] = acc[d] + R[d];
-      }
-      if (FUSED) {
-        double dtvel = dyn->dtvel, dt = dyn->dt;
-        double vn[3];
-        for (int d = 0; d < 3; ++d) vn[d] = vi[d] + dtvel * acc[d];
-        P.X2[p] = make_double4(xi.x + dt * vn[0], xi.y + dt * vn[1], xi.z + dt * vn[2], xi.w);
-        P.V2[p] = make_double4(vn[0], vn[1], vn[2], rhoi);
-        if (P.VF2) P.VF2[p] = make_float4((float)vn[0], (float)vn[1], (float)vn[2], 0.f);
-        P.P2[p] = pi;
-        P.I2[p] = P.I[p];
-        P.L2[p] = (uint8_t)lam_new;
-        double U = sqrt(vn[0] * vn[0] + vn[1] * vn[1] + vn[2] * vn[2]);
-        // with velocity smoothing the CFL minimum is taken on the smoothed
-        // velocities (k_velocity_smoothing_apply), which also moves X2
-        if (!(s.teta_v > 1.0e-9)) dtc = s.cfl * 2.0 * s.h / (s.celerita + U);
-      } else {
-        P.ACC[p] = make_double4(acc[0], acc[1], acc[2], 0.0);
-        P.L[p] = (uint8_t)lam_new;
-      }
+      momentum_f32_close<DIM, FUSED>(s, b, dyn, p, ms, tpres, tdiss, tvisc, vi, rhoi, pi, nb, bstart, dtc);
     }
     if (FUSED) {
       double m = warp_min(dtc);
@@ -3800,18 +3841,19 @@ void launch_momentum_f32(const DevBatch& b, bool fused, cudaStream_t st) {
   int g = blocks_for(b, kGridMomentum);
   int gf = blocks_for(b);
   c1_frontier_2d(b, true, st);
+  const int f = fused ? 1 : 0;
   if (b.dim == 3 && b.c1) {
-    k_momentum_f32<3, true><<<g, kBlock, 0, st>>>(b);
+    k_momentum_f32<3, true><<<g, kBlock, 0, st>>>(b, f);
     if (fused) k_momentum_f32_finish<3, true, true><<<gf, kBlock, 0, st>>>(b);
     else k_momentum_f32_finish<3, false, true><<<gf, kBlock, 0, st>>>(b);
   } else if (b.dim == 3) {
-    if (b.mom_batch) k_momentum_f32<3, false, true><<<g, kBlock, 0, st>>>(b);
-    else k_momentum_f32<3><<<g, kBlock, 0, st>>>(b);
+    if (b.mom_batch) k_momentum_f32<3, false, true><<<g, kBlock, 0, st>>>(b, f);
+    else k_momentum_f32<3><<<g, kBlock, 0, st>>>(b, f);
     if (fused) k_momentum_f32_finish<3, true><<<gf, kBlock, 0, st>>>(b);
     else k_momentum_f32_finish<3, false><<<gf, kBlock, 0, st>>>(b);
   } else {
-    if (b.mom_batch) k_momentum_f32<2, false, true><<<g, kBlock, 0, st>>>(b);
-    else k_momentum_f32<2><<<g, kBlock, 0, st>>>(b);
+    if (b.mom_batch) k_momentum_f32<2, false, true><<<g, kBlock, 0, st>>>(b, f);
+    else k_momentum_f32<2><<<g, kBlock, 0, st>>>(b, f);
     if (fused) k_momentum_f32_finish<2, true><<<gf, kBlock, 0, st>>>(b);
     else k_momentum_f32_finish<2, false><<<gf, kBlock, 0, st>>>(b);
   }
