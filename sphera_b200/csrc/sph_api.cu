@@ -13,9 +13,23 @@
 #include <new>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "../../include/sphera_b200.h"
 #include "sph_internal.cuh"
 #include "sph_launch.h"
+
+// NVTX ranges around the entry points, named after the reference routines
+// they stand in for, so a profiler's timeline reads like time_step_loop.f90
+// (header-only; without a profiler attached a range costs a branch).
+namespace {
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange&) = delete;
+  NvtxRange& operator=(const NvtxRange&) = delete;
+};
+}  // namespace
 
 namespace sph {
 
@@ -1101,12 +1115,14 @@ int sph_idle(SphHandle* h, int32_t* idle) {
 }
 
 int sph_upload(SphHandle* h, const SphState* state) {
+  NvtxRange range_("sph_upload: IC (OrdGrid1, CalcVarLength, ComputeBoundaryDataTab, time_step_duration)");
   if (!h || h->nsims != 1) return SPH_ERR_INVALID_ARGUMENT;
   SPH_TRY(upload_sim(h, 0, state));
   return initialise(h);
 }
 
 int sph_batch_upload(SphHandle* h, int32_t nsims, const SphState* states) {
+  NvtxRange range_("sph_batch_upload: IC of every simulation");
   if (!h || nsims != h->nsims || !states) return SPH_ERR_INVALID_ARGUMENT;
   for (int s = 0; s < nsims; ++s) SPH_TRY(upload_sim(h, s, &states[s]));
   return initialise(h);
@@ -1164,6 +1180,7 @@ static void fill_info(SphHandle* h, int sim, SphStepInfo* info) {
 }
 
 int sph_step(SphHandle* h, int32_t nsteps, SphStepInfo* info) {
+  NvtxRange range_("sph_step: time_step_loop");
   if (!h || !h->uploaded || nsteps < 0) return SPH_ERR_INVALID_ARGUMENT;
   SPH_TRY(build_graph(h));
   for (int s = 0; s < nsteps; ++s) SPH_CUDA(cudaGraphLaunch(h->graph, h->stream));
@@ -1178,6 +1195,7 @@ int sph_step(SphHandle* h, int32_t nsteps, SphStepInfo* info) {
 // pass still run (see enqueue_early_copy).  The last step is launched
 // without the graph so that the copy can start inside it.
 int sph_step_download(SphHandle* h, int32_t nsteps, SphState* state) {
+  NvtxRange range_("sph_step_download: time_step_loop + pg(:) to the host");
   if (!h || !h->uploaded || h->nsims != 1 || nsteps < 0 || !state) return SPH_ERR_INVALID_ARGUMENT;
   if (nsteps == 0) return download_impl(h, 0, state, nullptr, nullptr);
   SPH_TRY(build_graph(h));
@@ -1208,6 +1226,7 @@ int sph_step_download(SphHandle* h, int32_t nsteps, SphState* state) {
 
 // Enqueue steps without waiting (the caller synchronises through sph_sync).
 int sph_step_async(SphHandle* h, int32_t nsteps) {
+  NvtxRange range_("sph_step_async: time_step_loop (enqueued)");
   if (!h || !h->uploaded || nsteps < 0) return SPH_ERR_INVALID_ARGUMENT;
   SPH_TRY(build_graph(h));
   for (int s = 0; s < nsteps; ++s) SPH_CUDA(cudaGraphLaunch(h->graph, h->stream));
@@ -1260,6 +1279,7 @@ int sph_create_slab(const SphParams* params, const SphGeometry* geometry, int32_
 // neighbour lists and ComputeBoundaryDataTab on it (the search of
 // time_step_loop.f90:286-324), no time-step evaluation.
 int sph_replace_particles(SphHandle* h, const SphState* state, const int32_t* laminar) {
+  NvtxRange range_("sph_replace_particles: OrdGrid1, CalcVarLength, ComputeBoundaryDataTab");
   if (!h || !h->uploaded || h->nsims != 1 || !state) return SPH_ERR_INVALID_ARGUMENT;
   if (h->any_c1) return SPH_ERR_UNSUPPORTED;
   SPH_TRY(read_dyn(h));
@@ -1343,6 +1363,7 @@ int sph_get_diagnostics(SphHandle* h, SphDiagnostics* diag) {
 
 // ---------------------------------------------------------------- fine-grained
 int sph_time_step_duration(SphHandle* h, double* dt_out) {
+  NvtxRange range_("time_step_duration");
   if (!h || !h->uploaded) return SPH_ERR_INVALID_ARGUMENT;
   SPH_TRY(sync_dyn(h));
   if (dt_out) *dt_out = h->h_dyn[0].dt;
@@ -1350,6 +1371,7 @@ int sph_time_step_duration(SphHandle* h, double* dt_out) {
 }
 
 int sph_rhs_momentum(SphHandle* h, double* acc_out) {
+  NvtxRange range_("RHS_momentum_equation");
   if (!h || !h->uploaded) return SPH_ERR_INVALID_ARGUMENT;
   momentum_pass(h, false, h->stream);
   SPH_CUDA(cudaGetLastError());
@@ -1358,6 +1380,7 @@ int sph_rhs_momentum(SphHandle* h, double* acc_out) {
 }
 
 int sph_leapfrog_momentum(SphHandle* h) {
+  NvtxRange range_("Leapfrog_momentum");
   if (!h || !h->uploaded) return SPH_ERR_INVALID_ARGUMENT;
   launch_leapfrog_momentum(h->db, h->stream);
   if (h->any_teta_v) launch_velocity_smoothing(h->db, false, h->precision == SPH_PREC_FP32C, h->stream);
@@ -1367,6 +1390,7 @@ int sph_leapfrog_momentum(SphHandle* h) {
 }
 
 int sph_leapfrog_trajectories(SphHandle* h) {
+  NvtxRange range_("Leapfrog_trajectories");
   if (!h || !h->uploaded) return SPH_ERR_INVALID_ARGUMENT;
   launch_leapfrog_trajectories(h->db, h->stream);
   SPH_CUDA(cudaGetLastError());
@@ -1374,6 +1398,7 @@ int sph_leapfrog_trajectories(SphHandle* h) {
 }
 
 int sph_ord_grid(SphHandle* h) {
+  NvtxRange range_("OrdGrid1 + CalcVarLength");
   if (!h || !h->uploaded) return SPH_ERR_INVALID_ARGUMENT;
   launch_stage(h->db, h->stream);
   sort_sequence(h, h->stream);
@@ -1383,6 +1408,7 @@ int sph_ord_grid(SphHandle* h) {
 }
 
 int sph_boundary_data_tab(SphHandle* h) {
+  NvtxRange range_("ComputeBoundaryDataTab");
   if (!h || !h->uploaded) return SPH_ERR_INVALID_ARGUMENT;
   launch_boundary(h->db, h->stream);
   SPH_CUDA(cudaGetLastError());
@@ -1390,6 +1416,7 @@ int sph_boundary_data_tab(SphHandle* h) {
 }
 
 int sph_continuity(SphHandle* h, double* dden_out) {
+  NvtxRange range_("SASPH_continuity + Continuity_Equation");
   if (!h || !h->uploaded) return SPH_ERR_INVALID_ARGUMENT;
   continuity_pass(h, false, h->stream);
   SPH_CUDA(cudaGetLastError());
@@ -1398,6 +1425,7 @@ int sph_continuity(SphHandle* h, double* dden_out) {
 }
 
 int sph_leapfrog_continuity(SphHandle* h) {
+  NvtxRange range_("Leapfrog_continuity");
   if (!h || !h->uploaded) return SPH_ERR_INVALID_ARGUMENT;
   launch_leapfrog_continuity(h->db, h->stream);
   refresh_copies(h, h->stream);
@@ -1406,6 +1434,7 @@ int sph_leapfrog_continuity(SphHandle* h) {
 }
 
 int sph_eos(SphHandle* h) {
+  NvtxRange range_("EoS_fluid_loop + time_step_duration");
   if (!h || !h->uploaded) return SPH_ERR_INVALID_ARGUMENT;
   launch_eos(h->db, h->stream);
   if (h->any_teta_p) launch_pressure_smoothing(h->db, h->precision == SPH_PREC_FP32C, h->stream);
@@ -1420,6 +1449,7 @@ int sph_eos(SphHandle* h) {
 // fluid_global_quantities.f90:59-72 for simulation `sim` (out[8]) or, with
 // sim = -1, for every simulation of the handle (out[nsims][8]).
 int sph_global_quantities(SphHandle* h, int32_t sim, double* out) {
+  NvtxRange range_("fluid_global_quantities");
   if (!h || !h->uploaded || !out || sim < -1 || sim >= h->nsims) return SPH_ERR_INVALID_ARGUMENT;
   cudaStream_t q = h->stream;
   launch_global_quantities(h->db, h->d_gq_part, h->d_gq_out, q);
@@ -1557,6 +1587,7 @@ int sph_set_launch_shape(SphHandle* h, const int32_t* shape) {
 }
 
 int sph_autotune(SphHandle* h, int32_t reps, int32_t* grid_out) {
+  NvtxRange range_("sph_autotune");
   if (!h || !h->uploaded || reps <= 0) return SPH_ERR_INVALID_ARGUMENT;
   cudaStream_t q = h->stream;
   DevBatch& b = h->db;
