@@ -474,10 +474,8 @@ def main():
                     help="partial smoothing coefficient TetaP = TetaV of the dam-break workload (0: off)")
     ap.add_argument("--c1", action="store_true",
                     help="dam break with the 1st-order consistency renormalisation (C1_BE and C1_divu, "
-                         "invB_det_thresh 1e-3); FP64 form only")
+                         "invB_det_thresh 1e-3), in the forms --forms names")
     args = ap.parse_args()
-    if args.c1 and args.forms != "fp64":
-        ap.error("--c1 runs in the FP64 form only: add --forms fp64")
     args.warmup = max(3, args.warmup)
     if args.t_end is None:
         args.t_end = 0.3 if args.workload == "serving" else 0.5

@@ -193,6 +193,13 @@ typedef struct SphHandle SphHandle;
 /* Life cycle                                                              */
 /* ---------------------------------------------------------------------- */
 
+/* The device (0-based) the calling thread's next sph_create,
+ * sph_batch_create or sph_create_slab builds its handle on.  A handle keeps
+ * its device: every call on it runs there and gives the caller's current
+ * device back on return, so one host thread may drive handles on several
+ * GPUs.                                                                    */
+int  sph_select_device(int32_t device);
+
 /* Builds the grid (CreaGrid.f90:51-74), the boundary geometry
  * (DefineLocalSystemVersors.f90, GridCellBoundaryFacesIntersections3D.f90 /
  * DefineBoundarySideGeometry2D.f90) and the IC integral tables

@@ -91,6 +91,7 @@ def lib():
         "sph_replace_particles": ([vp, C.POINTER(abi.SphState), ip], C.c_int),
         "sph_set_time_step": ([vp, C.c_double], C.c_int),
         "sph_get_clock": ([vp, C.POINTER(abi.SphClock)], C.c_int),
+        "sph_select_device": ([C.c_int32], C.c_int),
         "sph_set_clock": ([vp, C.POINTER(abi.SphClock), ip], C.c_int),
     }
     for name, (args, res) in sig.items():
@@ -392,10 +393,20 @@ def measure_fp32_peak():
     return t.value
 
 
-class Batch:
-    """Several independent simulations advanced by the same launches."""
+def select_device(device):
+    """The device the next Simulation / Batch of this thread is built on
+    (sph_select_device); a handle keeps its device afterwards."""
+    _chk(lib().sph_select_device(int(device)), "sph_select_device")
 
-    def __init__(self, cases):
+
+class Batch:
+    """Several independent simulations advanced by the same launches;
+    device: the GPU to build it on (default: the thread's current one)."""
+
+    def __init__(self, cases, device=None):
+        if device is not None:
+            select_device(device)
+        self.device = device
         self.cases = list(cases)
         n = len(self.cases)
         self._params = (abi.SphParams * n)(*[c.params for c in self.cases])

@@ -650,6 +650,27 @@ struct SphHandle {
   size_t device_bytes = 0;          // bytes of the arrays below `owned`
   bool dry = false;                 // size the arrays only (sph_memory_required)
 };
+// Every entry point that takes a handle runs on the handle's device and
+// gives the caller's current device back on return, so a host may hold
+// handles on several devices (one per GPU of a node) in one thread.
+namespace {
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(const SphHandle* h) {
+    if (!h) return;
+    int cur = -1;
+    if (cudaGetDevice(&cur) != cudaSuccess) { cudaGetLastError(); return; }
+    if (cur != h->device && cudaSetDevice(h->device) == cudaSuccess) prev = cur;
+    else cudaGetLastError();
+  }
+  ~DeviceGuard() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+  DeviceGuard(const DeviceGuard&) = delete;
+  DeviceGuard& operator=(const DeviceGuard&) = delete;
+};
+}  // namespace
+
 
 namespace {
 
@@ -1076,6 +1097,7 @@ int sph_batch_create(int32_t nsims, const SphParams* params, const SphGeometry* 
 }
 
 void sph_destroy(SphHandle* h) {
+  DeviceGuard dev_guard_(h);
   if (!h) return;
   if (h->stream) cudaStreamSynchronize(h->stream);
   if (h->graph) cudaGraphExecDestroy(h->graph);
@@ -1104,6 +1126,7 @@ int sph_memory_required(int32_t nsims, const SphParams* params, const SphGeometr
 }
 
 int sph_idle(SphHandle* h, int32_t* idle) {
+  DeviceGuard dev_guard_(h);
   if (!h || !idle) return SPH_ERR_INVALID_ARGUMENT;
   cudaError_t e = cudaStreamQuery(h->stream);
   if (e == cudaErrorNotReady) {
@@ -1115,6 +1138,7 @@ int sph_idle(SphHandle* h, int32_t* idle) {
 }
 
 int sph_upload(SphHandle* h, const SphState* state) {
+  DeviceGuard dev_guard_(h);
   NvtxRange range_("sph_upload: IC (OrdGrid1, CalcVarLength, ComputeBoundaryDataTab, time_step_duration)");
   if (!h || h->nsims != 1) return SPH_ERR_INVALID_ARGUMENT;
   SPH_TRY(upload_sim(h, 0, state));
@@ -1122,6 +1146,7 @@ int sph_upload(SphHandle* h, const SphState* state) {
 }
 
 int sph_batch_upload(SphHandle* h, int32_t nsims, const SphState* states) {
+  DeviceGuard dev_guard_(h);
   NvtxRange range_("sph_batch_upload: IC of every simulation");
   if (!h || nsims != h->nsims || !states) return SPH_ERR_INVALID_ARGUMENT;
   for (int s = 0; s < nsims; ++s) SPH_TRY(upload_sim(h, s, &states[s]));
@@ -1129,6 +1154,7 @@ int sph_batch_upload(SphHandle* h, int32_t nsims, const SphState* states) {
 }
 
 int sph_batch_set_end_time(SphHandle* h, int32_t sim, double t_end) {
+  DeviceGuard dev_guard_(h);
   if (!h || sim < 0 || sim >= h->nsims || !h->uploaded) return SPH_ERR_INVALID_ARGUMENT;
   SPH_CUDA(cudaMemcpyAsync(&h->d_dyn[sim].t_end, &t_end, sizeof(double), cudaMemcpyHostToDevice, h->stream));
   return cuda_status(cudaStreamSynchronize(h->stream));
@@ -1163,11 +1189,15 @@ static int download_impl(SphHandle* h, int sim, SphState* state, double* acc, do
 }
 
 int sph_download(SphHandle* h, SphState* state) {
+  DeviceGuard dev_guard_(h);
   if (!h || h->nsims != 1 || !state) return SPH_ERR_INVALID_ARGUMENT;
   return download_impl(h, 0, state, nullptr, nullptr);
 }
 
-int sph_batch_download(SphHandle* h, int32_t sim, SphState* state) { return download_impl(h, sim, state, nullptr, nullptr); }
+int sph_batch_download(SphHandle* h, int32_t sim, SphState* state) {
+  DeviceGuard dev_guard_(h);
+  return download_impl(h, sim, state, nullptr, nullptr);
+}
 
 static void fill_info(SphHandle* h, int sim, SphStepInfo* info) {
   const SimDyn& d = h->h_dyn[sim];
@@ -1180,6 +1210,7 @@ static void fill_info(SphHandle* h, int sim, SphStepInfo* info) {
 }
 
 int sph_step(SphHandle* h, int32_t nsteps, SphStepInfo* info) {
+  DeviceGuard dev_guard_(h);
   NvtxRange range_("sph_step: time_step_loop");
   if (!h || !h->uploaded || nsteps < 0) return SPH_ERR_INVALID_ARGUMENT;
   SPH_TRY(build_graph(h));
@@ -1195,6 +1226,7 @@ int sph_step(SphHandle* h, int32_t nsteps, SphStepInfo* info) {
 // pass still run (see enqueue_early_copy).  The last step is launched
 // without the graph so that the copy can start inside it.
 int sph_step_download(SphHandle* h, int32_t nsteps, SphState* state) {
+  DeviceGuard dev_guard_(h);
   NvtxRange range_("sph_step_download: time_step_loop + pg(:) to the host");
   if (!h || !h->uploaded || h->nsims != 1 || nsteps < 0 || !state) return SPH_ERR_INVALID_ARGUMENT;
   if (nsteps == 0) return download_impl(h, 0, state, nullptr, nullptr);
@@ -1226,6 +1258,7 @@ int sph_step_download(SphHandle* h, int32_t nsteps, SphState* state) {
 
 // Enqueue steps without waiting (the caller synchronises through sph_sync).
 int sph_step_async(SphHandle* h, int32_t nsteps) {
+  DeviceGuard dev_guard_(h);
   NvtxRange range_("sph_step_async: time_step_loop (enqueued)");
   if (!h || !h->uploaded || nsteps < 0) return SPH_ERR_INVALID_ARGUMENT;
   SPH_TRY(build_graph(h));
@@ -1234,11 +1267,13 @@ int sph_step_async(SphHandle* h, int32_t nsteps) {
 }
 
 int sph_sync(SphHandle* h) {
+  DeviceGuard dev_guard_(h);
   if (!h) return SPH_ERR_INVALID_ARGUMENT;
   return sync_dyn(h);
 }
 
 int sph_batch_info(SphHandle* h, int32_t sim, SphStepInfo* info, int32_t* frozen) {
+  DeviceGuard dev_guard_(h);
   if (!h || sim < 0 || sim >= h->nsims || !info) return SPH_ERR_INVALID_ARGUMENT;
   SPH_TRY(sync_dyn(h));
   fill_info(h, sim, info);
@@ -1252,6 +1287,7 @@ void* sph_stream(SphHandle* h) { return h ? (void*)h->stream : nullptr; }
 // fatal status.  A member's failure is reported in status[], not as the
 // call's result, so a server can retire it and keep the others running.
 int sph_batch_status(SphHandle* h, int32_t* frozen, double* time, int32_t* steps, int32_t* status) {
+  DeviceGuard dev_guard_(h);
   if (!h) return SPH_ERR_INVALID_ARGUMENT;
   SPH_TRY(read_dyn(h));
   for (int s = 0; s < h->nsims; ++s) {
@@ -1261,6 +1297,16 @@ int sph_batch_status(SphHandle* h, int32_t* frozen, double* time, int32_t* steps
     if (status) status[s] = h->h_dyn[s].status;
   }
   return SPH_OK;
+}
+
+// The device the next sph_create / sph_batch_create / sph_create_slab of
+// this host thread builds its handle on (cudaSetDevice); every call on a
+// handle then runs on the handle's own device whatever the current one.
+int sph_select_device(int32_t device) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) { cudaGetLastError(); return SPH_ERR_NO_DEVICE; }
+  if (device < 0 || device >= n) return SPH_ERR_INVALID_ARGUMENT;
+  return cuda_status(cudaSetDevice(device));
 }
 
 // ------------------------------------------------------------------- slabs
@@ -1279,6 +1325,7 @@ int sph_create_slab(const SphParams* params, const SphGeometry* geometry, int32_
 // neighbour lists and ComputeBoundaryDataTab on it (the search of
 // time_step_loop.f90:286-324), no time-step evaluation.
 int sph_replace_particles(SphHandle* h, const SphState* state, const int32_t* laminar) {
+  DeviceGuard dev_guard_(h);
   NvtxRange range_("sph_replace_particles: OrdGrid1, CalcVarLength, ComputeBoundaryDataTab");
   if (!h || !h->uploaded || h->nsims != 1 || !state) return SPH_ERR_INVALID_ARGUMENT;
   if (h->any_c1) return SPH_ERR_UNSUPPORTED;
@@ -1299,6 +1346,7 @@ int sph_replace_particles(SphHandle* h, const SphState* state, const int32_t* la
 }
 
 int sph_set_time_step(SphHandle* h, double dt) {
+  DeviceGuard dev_guard_(h);
   if (!h || !h->uploaded || !(dt > 0.0)) return SPH_ERR_INVALID_ARGUMENT;
   for (int s = 0; s < h->nsims; ++s)
     if (h->sims[s].prm.pesodt != 0.0) return SPH_ERR_UNSUPPORTED;
@@ -1309,6 +1357,7 @@ int sph_set_time_step(SphHandle* h, double dt) {
 
 // ------------------------------------------------------------- checkpoint
 int sph_get_clock(SphHandle* h, SphClock* clock) {
+  DeviceGuard dev_guard_(h);
   if (!h || !h->uploaded || h->nsims != 1 || !clock) return SPH_ERR_INVALID_ARGUMENT;
   SPH_TRY(sync_dyn(h));
   const SimDyn& d = h->h_dyn[0];
@@ -1322,6 +1371,7 @@ int sph_get_clock(SphHandle* h, SphClock* clock) {
 }
 
 int sph_set_clock(SphHandle* h, const SphClock* clock, const int32_t* laminar) {
+  DeviceGuard dev_guard_(h);
   if (!h || !h->uploaded || h->nsims != 1 || !clock) return SPH_ERR_INVALID_ARGUMENT;
   if (h->any_c1) return SPH_ERR_UNSUPPORTED;
   if (!(clock->dt > 0.0) || !(clock->dt_prev > 0.0) || clock->step < 0 || !(clock->time >= 0.0))
@@ -1340,12 +1390,14 @@ int sph_set_clock(SphHandle* h, const SphClock* clock, const int32_t* laminar) {
 // Stops simulation `sim` from the next enqueued launch on (stream-ordered,
 // no wait): it freezes with status SPH_CANCELLED and keeps its state.
 int sph_batch_cancel(SphHandle* h, int32_t sim) {
+  DeviceGuard dev_guard_(h);
   if (!h || !h->uploaded || sim < 0 || sim >= h->nsims) return SPH_ERR_INVALID_ARGUMENT;
   launch_cancel(h->db, sim, h->stream);
   return cuda_status(cudaGetLastError());
 }
 
 int sph_get_diagnostics(SphHandle* h, SphDiagnostics* diag) {
+  DeviceGuard dev_guard_(h);
   if (!h || !diag) return SPH_ERR_INVALID_ARGUMENT;
   int st = sync_dyn(h);
   const SimDyn& d = h->h_dyn[0];
@@ -1363,6 +1415,7 @@ int sph_get_diagnostics(SphHandle* h, SphDiagnostics* diag) {
 
 // ---------------------------------------------------------------- fine-grained
 int sph_time_step_duration(SphHandle* h, double* dt_out) {
+  DeviceGuard dev_guard_(h);
   NvtxRange range_("time_step_duration");
   if (!h || !h->uploaded) return SPH_ERR_INVALID_ARGUMENT;
   SPH_TRY(sync_dyn(h));
@@ -1371,6 +1424,7 @@ int sph_time_step_duration(SphHandle* h, double* dt_out) {
 }
 
 int sph_rhs_momentum(SphHandle* h, double* acc_out) {
+  DeviceGuard dev_guard_(h);
   NvtxRange range_("RHS_momentum_equation");
   if (!h || !h->uploaded) return SPH_ERR_INVALID_ARGUMENT;
   momentum_pass(h, false, h->stream);
@@ -1380,6 +1434,7 @@ int sph_rhs_momentum(SphHandle* h, double* acc_out) {
 }
 
 int sph_leapfrog_momentum(SphHandle* h) {
+  DeviceGuard dev_guard_(h);
   NvtxRange range_("Leapfrog_momentum");
   if (!h || !h->uploaded) return SPH_ERR_INVALID_ARGUMENT;
   launch_leapfrog_momentum(h->db, h->stream);
@@ -1390,6 +1445,7 @@ int sph_leapfrog_momentum(SphHandle* h) {
 }
 
 int sph_leapfrog_trajectories(SphHandle* h) {
+  DeviceGuard dev_guard_(h);
   NvtxRange range_("Leapfrog_trajectories");
   if (!h || !h->uploaded) return SPH_ERR_INVALID_ARGUMENT;
   launch_leapfrog_trajectories(h->db, h->stream);
@@ -1398,6 +1454,7 @@ int sph_leapfrog_trajectories(SphHandle* h) {
 }
 
 int sph_ord_grid(SphHandle* h) {
+  DeviceGuard dev_guard_(h);
   NvtxRange range_("OrdGrid1 + CalcVarLength");
   if (!h || !h->uploaded) return SPH_ERR_INVALID_ARGUMENT;
   launch_stage(h->db, h->stream);
@@ -1408,6 +1465,7 @@ int sph_ord_grid(SphHandle* h) {
 }
 
 int sph_boundary_data_tab(SphHandle* h) {
+  DeviceGuard dev_guard_(h);
   NvtxRange range_("ComputeBoundaryDataTab");
   if (!h || !h->uploaded) return SPH_ERR_INVALID_ARGUMENT;
   launch_boundary(h->db, h->stream);
@@ -1416,6 +1474,7 @@ int sph_boundary_data_tab(SphHandle* h) {
 }
 
 int sph_continuity(SphHandle* h, double* dden_out) {
+  DeviceGuard dev_guard_(h);
   NvtxRange range_("SASPH_continuity + Continuity_Equation");
   if (!h || !h->uploaded) return SPH_ERR_INVALID_ARGUMENT;
   continuity_pass(h, false, h->stream);
@@ -1425,6 +1484,7 @@ int sph_continuity(SphHandle* h, double* dden_out) {
 }
 
 int sph_leapfrog_continuity(SphHandle* h) {
+  DeviceGuard dev_guard_(h);
   NvtxRange range_("Leapfrog_continuity");
   if (!h || !h->uploaded) return SPH_ERR_INVALID_ARGUMENT;
   launch_leapfrog_continuity(h->db, h->stream);
@@ -1434,6 +1494,7 @@ int sph_leapfrog_continuity(SphHandle* h) {
 }
 
 int sph_eos(SphHandle* h) {
+  DeviceGuard dev_guard_(h);
   NvtxRange range_("EoS_fluid_loop + time_step_duration");
   if (!h || !h->uploaded) return SPH_ERR_INVALID_ARGUMENT;
   launch_eos(h->db, h->stream);
@@ -1449,6 +1510,7 @@ int sph_eos(SphHandle* h) {
 // fluid_global_quantities.f90:59-72 for simulation `sim` (out[8]) or, with
 // sim = -1, for every simulation of the handle (out[nsims][8]).
 int sph_global_quantities(SphHandle* h, int32_t sim, double* out) {
+  DeviceGuard dev_guard_(h);
   NvtxRange range_("fluid_global_quantities");
   if (!h || !h->uploaded || !out || sim < -1 || sim >= h->nsims) return SPH_ERR_INVALID_ARGUMENT;
   cudaStream_t q = h->stream;
@@ -1461,6 +1523,7 @@ int sph_global_quantities(SphHandle* h, int32_t sim, double* out) {
 
 // ---------------------------------------------------------------- verification
 int sph_dump_grid(SphHandle* h, int32_t* cella, int32_t* icont, int32_t* npartord) {
+  DeviceGuard dev_guard_(h);
   if (!h || !h->uploaded || h->nsims != 1) return SPH_ERR_INVALID_ARGUMENT;
   SPH_TRY(sync_dyn(h));
   int n = h->h_dyn[0].nag;
@@ -1488,6 +1551,7 @@ int sph_dump_grid(SphHandle* h, int32_t* cella, int32_t* icont, int32_t* npartor
 }
 
 int sph_dump_neighbours(SphHandle* h, int32_t nmaxj, int32_t* counts, int32_t* lists) {
+  DeviceGuard dev_guard_(h);
   if (!h || !h->uploaded || h->nsims != 1 || nmaxj <= 0 || !counts || !lists) return SPH_ERR_INVALID_ARGUMENT;
   SPH_TRY(sync_dyn(h));
   int n = h->h_dyn[0].nag;
@@ -1505,6 +1569,7 @@ int sph_dump_neighbours(SphHandle* h, int32_t nmaxj, int32_t* counts, int32_t* l
 }
 
 int sph_dump_boundary(SphHandle* h, int32_t max_per, int32_t* ncb, int32_t* clobonum, double* values) {
+  DeviceGuard dev_guard_(h);
   if (!h || !h->uploaded || h->nsims != 1 || max_per <= 0 || !ncb || !clobonum || !values) return SPH_ERR_INVALID_ARGUMENT;
   SPH_TRY(sync_dyn(h));
   int n = h->h_dyn[0].nag;
@@ -1527,6 +1592,7 @@ int sph_dump_boundary(SphHandle* h, int32_t max_per, int32_t* ncb, int32_t* clob
 }
 
 int sph_dump_laminar(SphHandle* h, int32_t* flags) {
+  DeviceGuard dev_guard_(h);
   if (!h || !h->uploaded || h->nsims != 1 || !flags) return SPH_ERR_INVALID_ARGUMENT;
   SPH_TRY(sync_dyn(h));
   int n = h->h_dyn[0].nag;
@@ -1538,6 +1604,7 @@ int sph_dump_laminar(SphHandle* h, int32_t* flags) {
 }
 
 int sph_dump_renormalisation(SphHandle* h, double* b_gradp, double* b_divu) {
+  DeviceGuard dev_guard_(h);
   if (!h || !h->uploaded || h->nsims != 1 || !h->any_c1) return SPH_ERR_INVALID_ARGUMENT;
   if (b_divu && !h->any_c1_divu) return SPH_ERR_INVALID_ARGUMENT;
   SPH_TRY(sync_dyn(h));
@@ -1569,6 +1636,7 @@ int sph_dump_renormalisation(SphHandle* h, double* b_gradp, double* b_divu) {
 // Applies a launch configuration (sph_autotune's output, or a chosen one):
 // blocks per kernel class (0 = the default) and the two pair-loop shapes.
 int sph_set_launch_shape(SphHandle* h, const int32_t* shape) {
+  DeviceGuard dev_guard_(h);
   if (!h || !shape) return SPH_ERR_INVALID_ARGUMENT;
   for (int c = 0; c < kGridClasses; ++c)
     if (shape[c] < 0) return SPH_ERR_INVALID_ARGUMENT;
@@ -1587,6 +1655,7 @@ int sph_set_launch_shape(SphHandle* h, const int32_t* shape) {
 }
 
 int sph_autotune(SphHandle* h, int32_t reps, int32_t* grid_out) {
+  DeviceGuard dev_guard_(h);
   NvtxRange range_("sph_autotune");
   if (!h || !h->uploaded || reps <= 0) return SPH_ERR_INVALID_ARGUMENT;
   cudaStream_t q = h->stream;
@@ -1683,6 +1752,7 @@ int sph_autotune(SphHandle* h, int32_t reps, int32_t* grid_out) {
 //   ms[4] continuity + Leapfrog_continuity + EoS
 //   ms[5] time_step_duration closing
 int sph_profile_phases(SphHandle* h, int32_t nsteps, double* ms) {
+  DeviceGuard dev_guard_(h);
   if (!h || !h->uploaded || nsteps <= 0 || !ms) return SPH_ERR_INVALID_ARGUMENT;
   cudaEvent_t ev[7];
   for (int i = 0; i < 7; ++i)
@@ -1721,6 +1791,7 @@ int sph_profile_phases(SphHandle* h, int32_t nsteps, double* ms) {
 // Candidates tested and pairs accepted (incl. the particle itself) by the
 // neighbour-list pass: c[0], c[1]; c[2..3] are reserved (zero).
 int sph_get_counters(SphHandle* h, uint64_t* c, int32_t reset) {
+  DeviceGuard dev_guard_(h);
   if (!h || !c) return SPH_ERR_INVALID_ARGUMENT;
   unsigned long long t[4];
   SPH_CUDA(cudaMemcpyAsync(t, h->d_counters, sizeof(t), cudaMemcpyDeviceToHost, h->stream));

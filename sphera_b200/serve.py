@@ -34,6 +34,12 @@ its only clean stop is the kill file (time_step_loop.f90:485-487); here:
   allocation the budget did not foresee) reports its requests failed with
   that code and returns their bytes.
 
+Several GPUs (``devices``): each has its own budget; a group is formed for,
+and built on, the device with the most free bytes (the head of the queue
+waits only while it fits on none), so requests spread over the node's GPUs
+as memory frees up.  A handle keeps its device (every library call runs
+there), so one host thread drives all of them.
+
 Every kernel treats each member of a group independently, so a request's
 result does not depend on what else is admitted: it equals the same
 request run alone, bit for bit.
@@ -66,6 +72,7 @@ class Result:
     cancelled: bool = False
     status: int = 0
     group: int = -1
+    device: object = None
 
     @property
     def time_to_result(self):
@@ -83,6 +90,7 @@ class _Group:
     requests: list
     bytes: int
     done: list = field(default_factory=list)
+    device: object = None
 
 
 def _kind(case):
@@ -95,31 +103,46 @@ def _default_sizer(cases):
     return memory_required(cases)
 
 
-def _default_factory(cases):
+def _default_factory(cases, device=None):
     from . import Batch
-    return Batch(cases)
+    return Batch(cases, device=device)
 
 
 class Server:
     """Admits requests by HBM budget and advances them concurrently.
 
-    hbm_budget: bytes of device memory the admitted groups may hold.
+    hbm_budget: bytes of device memory the admitted groups may hold, per
+        device.
+    devices: the GPUs to serve on (default: the thread's current one); the
+        factory is then called as factory(cases, device).
     chunk: steps enqueued per group between two status reads.
     keep_state: download each result's state (the request's answer).
     """
 
-    def __init__(self, hbm_budget, chunk=32, keep_state=True, sizer=None, factory=None, clock=None):
+    def __init__(self, hbm_budget, chunk=32, keep_state=True, sizer=None, factory=None, clock=None,
+                 devices=None):
         self.budget = int(hbm_budget)
+        self.devices = list(devices) if devices else [None]
         self.chunk = int(chunk)
         self.keep_state = keep_state
         self.sizer = sizer or _default_sizer
         self.factory = factory or _default_factory
         self.clock = clock or time.perf_counter
-        self.used = 0
-        self.peak_used = 0
+        self.used_by = {d: 0 for d in self.devices}
+        self.peak_by = {d: 0 for d in self.devices}
         self.groups_formed = 0
         self.max_concurrent = 0
         self._cancel = set()
+
+    @property
+    def used(self):
+        """Bytes the admitted groups hold, over all devices."""
+        return sum(self.used_by.values())
+
+    @property
+    def peak_used(self):
+        """The largest bytes any one device held at once."""
+        return max(self.peak_by.values())
 
     def cancel(self, rid):
         """Withdraws request `rid`: taken out of the queue if it waits, frozen
@@ -127,16 +150,19 @@ class Server:
         self._cancel.add(rid)
 
     def _admit(self, waiting, now, results):
-        """Forms one group from the head of the queue (FIFO, no overtaking)."""
+        """Forms one group from the head of the queue (FIFO, no overtaking)
+        for the device with the most free bytes."""
+        dev = min(self.devices, key=lambda d: (self.used_by[d], self.devices.index(d)))
+        used = self.used_by[dev]
         group, need = [], 0
         while waiting:
             if group and _kind(waiting[0].case) != _kind(group[0].case):
                 break                  # a batch holds one dim and precision
             cand = group + [waiting[0]]
             b = self.sizer([r.case for r in cand])
-            if self.used + b > self.budget:
-                if not group and self.used == 0:
-                    # larger than the whole budget: it can never run
+            if used + b > self.budget:
+                if not group and b > self.budget:
+                    # larger than a whole device's budget: it can never run
                     r = waiting.popleft()
                     results[r.rid].rejected = True
                     continue
@@ -148,7 +174,8 @@ class Server:
         gid = self.groups_formed
         self.groups_formed += 1
         try:
-            batch = self.factory([r.case for r in group])
+            cases = [r.case for r in group]
+            batch = self.factory(cases) if self.devices == [None] else self.factory(cases, dev)
         except RuntimeError as e:
             self._fail_group(group, gid, getattr(e, "code", -1), now, results)
             return None
@@ -170,9 +197,10 @@ class Server:
         for r in group:
             results[r.rid].admitted = now
             results[r.rid].group = gid
-        self.used += need
-        self.peak_used = max(self.peak_used, self.used)
-        g = _Group(gid, batch, group, need, [False] * len(group))
+            results[r.rid].device = dev
+        self.used_by[dev] += need
+        self.peak_by[dev] = max(self.peak_by[dev], self.used_by[dev])
+        g = _Group(gid, batch, group, need, [False] * len(group), dev)
         batch.step_async(self.chunk)
         return g
 
@@ -251,7 +279,7 @@ class Server:
                     res.finished = self.clock() - t0
                 if all(g.done):
                     g.batch.close()
-                    self.used -= g.bytes
+                    self.used_by[g.device] -= g.bytes
                     active.remove(g)
                 else:
                     g.batch.step_async(self.chunk)

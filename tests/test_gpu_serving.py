@@ -73,3 +73,18 @@ def test_memory_required_matches_allocation():
     b.close()
     # the pool rounds allocations up; the stream and graph add a little
     assert need <= used <= need * 1.25 + (64 << 20)
+
+
+def test_served_on_an_explicit_device_list():
+    """devices=[0]: the groups are built with sph_select_device and every
+    call on them runs on their device; the results are those run alone.
+    (Every GPU call here has one GPU; the spreading over several devices is
+    tested on the CPU with stand-in groups.)"""
+    reqs = _requests()[:3]
+    srv = Server(1 << 34, chunk=16, devices=[0])
+    res = srv.run(reqs)
+    for r in reqs:
+        got = res[r.rid]
+        assert got.completed and got.device == 0
+        st, steps = _alone(r)
+        assert got.steps == steps and np.array_equal(got.state.x, st.x)

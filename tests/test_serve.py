@@ -232,3 +232,53 @@ def test_cancel_while_queued_and_while_running():
     for rid in (1, 2, 3, 4):
         assert res[rid].completed and res[rid].steps == _steps_alone(reqs[rid])
     assert srv.used == 0
+
+
+def _server_on(devices, budget):
+    made = []
+
+    def sizer(cases):
+        return sum(c.nbytes for c in cases)
+
+    def factory(cases, device):
+        b = FakeBatch(cases)
+        b.device = device
+        made.append(b)
+        return b
+
+    srv = Server(budget, chunk=4, keep_state=False, sizer=sizer, factory=factory, clock=FakeClock(),
+                 devices=devices)
+    return srv, made
+
+
+def test_requests_spread_over_devices_by_free_bytes():
+    """Two GPUs with a budget each: a group goes to the device with the
+    most free bytes, each device stays within its budget, both are used,
+    and every request finishes with the steps it takes alone."""
+    FakeBatch.live = []
+    srv, made = _server_on(["gpu0", "gpu1"], 1000)
+    reqs = _requests()
+    for q in reqs:
+        q.arrival = 0.0
+    res = srv.run(reqs, poll=0.0)
+    assert all(r.completed for r in res.values())
+    for q in reqs:
+        assert res[q.rid].steps == _steps_alone(q)
+        assert res[q.rid].device == next(b.device for b in made if q.case in b.cases)
+    # 300 + 500 + 200 fill gpu0; 800 + 100 go to the empty gpu1 at once
+    assert res[0].device == res[1].device == res[2].device == "gpu0"
+    assert res[3].device == res[4].device == "gpu1"
+    assert res[3].admitted == res[0].admitted
+    assert {b.device for b in made} == {"gpu0", "gpu1"}
+    assert srv.peak_by["gpu0"] <= 1000 and srv.peak_by["gpu1"] <= 1000
+    assert srv.used == 0 and all(b.closed for b in made)
+
+
+def test_request_larger_than_one_device_is_rejected():
+    FakeBatch.live = []
+    srv, _ = _server_on(["gpu0", "gpu1"], 1000)
+    reqs = _requests()
+    reqs[2].case.nbytes = 1500        # fits in the two budgets together, in neither alone
+    res = srv.run(reqs, poll=0.0)
+    assert res[2].rejected
+    assert all(res[i].completed for i in range(len(reqs)) if i != 2)
