@@ -483,6 +483,15 @@ int  sph_get_counters(SphHandle* h, uint64_t* c, int32_t reset);
  * or FP32 when fp32 != 0.                                                 */
 int  sph_measure_fp64_peak(double* tflops);
 int  sph_measure_fma_peak(int32_t fp32, double* tflops);
+/* Self-check of the kernels' exact FP64 division: the FP64 passes divide by
+ * a shared or constant divisor b through its correctly rounded reciprocal
+ * and two remainder corrections (Markstein's method), which must give the
+ * IEEE quotient a / b bit for bit.  Compares it with a / b on count
+ * generated operand pairs (seeded; random, near-all-ones divisors, quotients
+ * next to rounding midpoints, zero dividends, the kernels' own ranges) on
+ * the current device; *mismatches receives the number that differ and
+ * first_bad (may be NULL) the operands a, b of one of them.               */
+int  sph_check_division(uint64_t count, uint64_t seed, uint64_t* mismatches, double* first_bad);
 
 #ifdef __cplusplus
 }

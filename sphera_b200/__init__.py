@@ -77,6 +77,7 @@ def lib():
         "sph_get_counters": ([vp, C.POINTER(C.c_uint64), C.c_int32], C.c_int),
         "sph_measure_fp64_peak": ([dp], C.c_int),
         "sph_measure_fma_peak": ([C.c_int32, dp], C.c_int),
+        "sph_check_division": ([C.c_uint64, C.c_uint64, C.POINTER(C.c_uint64), dp], C.c_int),
         "sph_autotune": ([vp, C.c_int32, ip], C.c_int),
         "sph_batch_status": ([vp, ip, dp, ip, ip], C.c_int),
         "sph_batch_cancel": ([vp, C.c_int32], C.c_int),
@@ -391,6 +392,16 @@ def measure_fp32_peak():
     t = C.c_double()
     _chk(lib().sph_measure_fma_peak(1, C.byref(t)), "sph_measure_fma_peak")
     return t.value
+
+
+def check_division(count, seed=0x5EED):
+    """The kernels' exact FP64 division against the IEEE a / b on count
+    generated operand pairs (sph_check_division): (mismatches, (a, b) of one
+    mismatch or None)."""
+    n = C.c_uint64()
+    first = (C.c_double * 2)()
+    _chk(lib().sph_check_division(int(count), int(seed), C.byref(n), first), "sph_check_division")
+    return int(n.value), ((first[0], first[1]) if n.value else None)
 
 
 def select_device(device):

@@ -276,6 +276,11 @@ int prepare_sim(const SphParams& prm, const SphGeometry& g, int cap, HostSim& hs
   s.ncells = (int)ncells;
   // ComputeKernelTable.f90:58-71
   s.ktdelta = 2.0 / kKtRows;
+  // correctly rounded reciprocals (IEEE division on the host) for the
+  // kernels' exact divisions by these constants (div_rn)
+  s.rcp_h = 1.0 / s.h;
+  s.rcp_squareh = 1.0 / s.squareh;
+  s.rcp_ktdelta = 1.0 / s.ktdelta;
   for (int nr = 0; nr <= kKtRows; ++nr) {
     double rob = s.ktdelta * nr;
     s.kerneltab[nr][0] = rob;
@@ -1839,5 +1844,39 @@ int sph_measure_fma_peak(int32_t fp32, double* tflops) {
 }
 
 int sph_measure_fp64_peak(double* tflops) { return sph_measure_fma_peak(0, tflops); }
+
+// The kernels' exact division (div_rn) against the IEEE division on count
+// generated operand pairs of the current device.
+int sph_check_division(uint64_t count, uint64_t seed, uint64_t* mismatches, double* first_bad) {
+  if (!mismatches) return SPH_ERR_INVALID_ARGUMENT;
+  int dev = 0, sms = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
+    cudaGetLastError();
+    return SPH_ERR_NO_DEVICE;
+  }
+  unsigned long long* bad = nullptr;
+  double* first = nullptr;
+  SPH_TRY(dalloc(&bad, 2));
+  if (dalloc(&first, 2) != SPH_OK) { cudaFree(bad); return SPH_ERR_ALLOC; }
+  unsigned long long hb[2] = {0, 0};
+  double hf[2] = {0.0, 0.0};
+  cudaError_t e = cudaMemset(bad, 0, sizeof(hb));
+  if (e == cudaSuccess) e = cudaMemset(first, 0, sizeof(hf));
+  if (e == cudaSuccess) {
+    launch_check_division(count, seed, bad, first, sms * 8, 0);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpy(hb, bad, sizeof(hb), cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) e = cudaMemcpy(hf, first, sizeof(hf), cudaMemcpyDeviceToHost);
+  cudaFree(bad);
+  cudaFree(first);
+  if (e != cudaSuccess) return cuda_status(e);
+  *mismatches = hb[0];
+  if (first_bad) {
+    first_bad[0] = hf[0];
+    first_bad[1] = hf[1];
+  }
+  return SPH_OK;
+}
 
 }  // extern "C"

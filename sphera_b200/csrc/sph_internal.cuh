@@ -63,6 +63,7 @@ struct SimDev {
   double c1_w1a, c1_w1b, c1_w2;  // grad_W_sub.f90 factors 1/(pi h^3), 3/(4 pi h^3), 15/(64 pi h^3)
   double zpmin;           // 0.05 h, ComputeBoundaryVolumeIntegrals_P0.f90
   double ktdelta;         // kernel-table step
+  double rcp_h, rcp_squareh, rcp_ktdelta;  // RN(1/h), RN(1/h^2), RN(1/ktdelta): divisors of div_rn
   float dcdf[3];          // (float)dcd: cell origins differ by multiples of it
   float rr_lo, rr_hi;     // FP32 screening band around (2h)^2 (see sph_api.cu)
   int narrow_z;           // z cells narrower than 2h: a candidate two cells away can lie within 2h

@@ -84,11 +84,33 @@ __device__ __forceinline__ void neighbour_run(const SimDev& s, const int* __rest
 }
 
 // Kernel values of CalcVarLength.f90:242-269 for an accepted pair.
+// a / b rounded to nearest, bit for bit what the IEEE division a / b gives,
+// from y = RN(1/b) (a constant's reciprocal formed on the host, or
+// __drcp_rn(b) once for a divisor that several divisions share).  The
+// method is Markstein's (P. Markstein, IBM J. Res. Dev. 34(1), 1990; the
+// theorem in Muller et al., Handbook of Floating-Point Arithmetic, on
+// division with a fused multiply-add): if y is within half an ulp of 1/b
+// and q within one ulp of a/b, the remainder r = a - b q is exact and
+// RN(q + r y) = RN(a/b).  q0 = RN(a y) can be up to 1.5 ulp off, so one
+// correction first brings it within half an ulp plus O(2^-105) relative
+// (q1), and the second is the theorem's step.  A zero remainder means the
+// current q is the exact quotient and is kept as it is (so a zero a keeps
+// its sign, which q + 0 y would lose).  Domain: a, b finite, b != 0, and no
+// quotient or remainder in the subnormal range -- true of every caller
+// (lengths, densities and smoothing lengths of a physical state).
+__device__ __forceinline__ double div_rn(double a, double b, double y) {
+  const double q0 = __dmul_rn(a, y);
+  const double r0 = __fma_rn(-b, q0, a);
+  const double q1 = r0 == 0.0 ? q0 : __fma_rn(r0, y, q0);
+  const double r1 = __fma_rn(-b, q1, a);
+  return r1 == 0.0 ? q1 : __fma_rn(r1, y, q1);
+}
+
 __device__ __forceinline__ void kernel_values(const SimDev& s, double rijtemp2, double& PK1, double& PK2,
                                               double& PK3) {
   double rijtemp = sqrt(rijtemp2);
-  double rij_su_h = rijtemp / s.h;
-  double rij_su_h_quad = rijtemp2 / s.squareh;
+  double rij_su_h = div_rn(rijtemp, s.h, s.rcp_h);
+  double rij_su_h_quad = div_rn(rijtemp2, s.squareh, s.rcp_squareh);
   int index_rij_su_h = (int)rij_su_h;
   double denom = 1.0 / (rijtemp + s.eta);
   PK1 = 0.0;
@@ -134,13 +156,13 @@ __device__ __forceinline__ void block_count2(unsigned long long* counters, int a
 __device__ __forceinline__ void interpolate_table(const SimDev& s, double xval, double* iv) {
   double deltaX = s.ktdelta;
   double xval0 = s.kerneltab[0][0];
-  int nr0 = (int)((xval - xval0) / deltaX);
+  int nr0 = (int)div_rn(xval - xval0, deltaX, s.rcp_ktdelta);
   if (nr0 <= 0) {
     for (int c = 0; c < 4; ++c) iv[c] = s.kerneltab[0][c + 1];
   } else if (nr0 >= kKtRows) {
     for (int c = 0; c < 4; ++c) iv[c] = s.kerneltab[kKtRows][c + 1];
   } else {
-    double csi = (xval - s.kerneltab[nr0][0]) / deltaX;
+    double csi = div_rn(xval - s.kerneltab[nr0][0], deltaX, s.rcp_ktdelta);
     for (int c = 0; c < 4; ++c)
       iv[c] = s.kerneltab[nr0][c + 1] + csi * (s.kerneltab[nr0 + 1][c + 1] - s.kerneltab[nr0][c + 1]);
   }
@@ -509,7 +531,7 @@ __device__ void face_integrals(const SimDev& s, const double* __restrict__ bit, 
         if (!ft.inside(px0, px1)) continue;
         double d0 = px0 - L0, d1 = px1 - L1, d2 = 0.0 - L2;
         double dist = sqrt(d0 * d0 + d1 * d1 + d2 * d2);
-        double rob = dist / s.h;
+        double rob = div_rn(dist, s.h, s.rcp_h);
         if (fabs(rob - robpre) > 1.0e-3) {
           double iv[4];
           interpolate_table(s, rob, iv);
@@ -820,7 +842,7 @@ __global__ void __launch_bounds__(kBlock) k_boundary2d(DevBatch b) {
             alfa_k = alfa_k + dalfa;
             double sa = sin(alfa_k), ca = cos(alfa_k);
             double rb = ypb / ca;
-            double rob = rb / s.h;
+            double rob = div_rn(rb, s.h, s.rcp_h);
             double mult = s.h * j2_wro2(rob) * dalfa;
             D0 = D0 + sa * mult;
             D1 = D1 - ca * mult;
@@ -1557,7 +1579,9 @@ __global__ void __launch_bounds__(kBlock, 4) k_neighbour_lists(DevBatch b) {
 // them as they are.  The frontier terms are added by the momentum (first
 // step) and continuity passes, which also invert.  One sqrt and the
 // division r / h are shared by the range test and both gradients; the
-// constant factors come from the host (SimDev::c1_w*).
+// constant factors come from the host (SimDev::c1_w*).  The pair's twelve
+// divisions by |r| and rho_j go through one correctly rounded reciprocal
+// of each (div_rn: the IEEE quotients, bit for bit).
 // The 2D SA-SPH frontier terms of the renormalisation matrices, -RN IntWdV
 // per close side (AddBoundaryContribution_to_CE2D.f90:81-94 for both
 // matrices in every continuity pass; AddBoundaryContributions_to_ME2D.f90:
@@ -1642,27 +1666,28 @@ __global__ void __launch_bounds__(kBlock, 2) k_renormalisation(DevBatch b) {
       double4 xj = P.X[q];
       double r[3] = {xj.x - xi.x, xj.y - xi.y, xj.z - xi.z};
       double abs_r = sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
-      double qh = abs_r / s.h;
+      double qh = div_rn(abs_r, s.h, s.rcp_h);
       if ((int)qh >= 2 || abs_r < s.h * 1.0e-6) continue;
       const double mj = xj.w, rhoj = P.RP[q].x;
       const double w = 2.0 - qh;
       double go[3];
       // anti-cluster kernel (q <= 2 here)
-      double t = -(3.0 * (w * w) * s.c1_w2) / s.h;
+      const double rcp_r = __drcp_rn(abs_r), rcp_rhoj = __drcp_rn(rhoj);
+      double t = div_rn(-(3.0 * (w * w) * s.c1_w2), s.h, s.rcp_h);
       for (int c = 0; c < 3; ++c) {
-        double gw = t * r[c] / abs_r;
+        double gw = div_rn(t * r[c], abs_r, rcp_r);
         if (DIM == 2) gw = gw * s.h * 4.0 / 3.0;
-        go[c] = gw * mj / rhoj;
+        go[c] = div_rn(gw * mj, rhoj, rcp_rhoj);
       }
       for (int c = 0; c < 3; ++c)
         for (int kk = 0; kk < 3; ++kk) Bg[3 * kk + c] = Bg[3 * kk + c] + r[c] * go[kk];
       if (divu) {
         // beta-spline (q < 2 here)
-        t = (qh <= 1.0 ? s.c1_w1a * (9.0 / 4.0 * (qh * qh) - 3.0 * qh) : -(s.c1_w1b * (w * w))) / s.h;
+        t = div_rn(qh <= 1.0 ? s.c1_w1a * (9.0 / 4.0 * (qh * qh) - 3.0 * qh) : -(s.c1_w1b * (w * w)), s.h, s.rcp_h);
         for (int c = 0; c < 3; ++c) {
-          double gw = t * r[c] / abs_r;
+          double gw = div_rn(t * r[c], abs_r, rcp_r);
           if (DIM == 2) gw = gw * s.h * 10.0 / 7.0;
-          go[c] = gw * mj / rhoj;
+          go[c] = div_rn(gw * mj, rhoj, rcp_rhoj);
         }
         for (int c = 0; c < 3; ++c)
           for (int kk = 0; kk < 3; ++kk) Bd[3 * kk + c] = Bd[3 * kk + c] + r[c] * go[kk];
@@ -1748,6 +1773,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_momentum(DevBatch b) {
     double tv0 = tvisc[0], tv1 = tvisc[1], tv2 = tvisc[2];
     double rs0 = 0, rs1 = 0, rs2 = 0;
     const double celt = s.celerita + s.celerita;
+    const double rcp_rhoi = __drcp_rn(rhoi);
     const bool morris = s.kin_visc > 1.0e-12;
     const double nu = s.kin_visc;
     ListPrefetcher lr;
@@ -1762,11 +1788,14 @@ __global__ void __launch_bounds__(kBlock, 2) k_momentum(DevBatch b) {
       double rhoj = rpj.x, pj = rpj.y, amassj = xj.w;
       double dv0 = vj.x - vi[0], dv1 = vj.y - vi[1], dv2 = vj.z - vi[2];
       // pressure gradient and ALE1 terms, inter_EqMoto.f90:195-221
-      double alpha = (pj - pi) / (rhoi * rhoj);
+      // the two divisions by rho_i rho_j and the one by rho_i share correctly
+      // rounded reciprocals (div_rn: the IEEE quotients, bit for bit)
+      const double rr_ij = rhoi * rhoj, rcp_rr = __drcp_rn(rr_ij);
+      double alpha = div_rn(pj - pi, rr_ij, rcp_rr);
       tp0 = tp0 + -(amassj * alpha * r0 * PK3);
       if (DIM == 3) tp1 = tp1 + -(amassj * alpha * r1 * PK3);
       tp2 = tp2 + -(amassj * alpha * r2 * PK3);
-      double alpha2 = (pi * (rhoj / rhoi + 1.0) + pj * (rhoi / rhoj - 1.0)) / (rhoi * rhoj);
+      double alpha2 = div_rn(pi * (div_rn(rhoj, rhoi, rcp_rhoi) + 1.0) + pj * (rhoi / rhoj - 1.0), rr_ij, rcp_rr);
       al0 = al0 - amassj * alpha2 * r0 * PK3;
       if (DIM == 3) al1 = al1 - amassj * alpha2 * r1 * PK3;
       al2 = al2 - amassj * alpha2 * r2 * PK3;
@@ -2755,8 +2784,8 @@ __global__ void k_refresh_f32(DevBatch b) {
 // PartKernel(4) of CalcVarLength.f90:241-268: the kernel value W = wu coefke.
 __device__ __forceinline__ double kernel_w(const SimDev& s, double rr) {
   double r = sqrt(rr);
-  double q = r / s.h;
-  double q2 = rr / s.squareh;
+  double q = div_rn(r, s.h, s.rcp_h);
+  double q2 = div_rn(rr, s.squareh, s.rcp_squareh);
   int idx = (int)q;
   if (idx >= 2) return 0.0;
   double wu = 0.666666667 + q2 * (q * 0.5 - 1.0);
@@ -3719,6 +3748,78 @@ double launch_fp64_probe(double* sink, int blocks, cudaStream_t st) {
   const int iters = 4096;
   k_fp64_probe<<<blocks, 256, 0, st>>>(sink, iters);
   return 2.0 * 8.0 * iters * 256.0 * blocks;
+}
+
+// Self-check of div_rn against the IEEE division a / b on generated
+// operands (SplitMix64 of the seed and the operand index).  Five kinds, by
+// index mod 5: random signs, significands and exponents in [-64, 63];
+// divisors whose significands are within 255 units of all ones; quotients
+// within a few units of 2^-106 relative of a rounding midpoint of a random
+// quotient (a = RN(b q + b ulp(q)/2)); a zero dividend of either sign; and
+// the ranges of the kernels' operands (1e-6 to 1e3 over 1e-3 to 2e3).
+__device__ __forceinline__ unsigned long long splitmix64(unsigned long long z) {
+  z += 0x9e3779b97f4a7c15ull;
+  z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+  z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+  return z ^ (z >> 31);
+}
+
+__device__ __forceinline__ double compose_double(unsigned long long frac, int exp, unsigned sign) {
+  const unsigned long long bits = ((unsigned long long)(sign & 1u) << 63) |
+                                  ((unsigned long long)(exp + 1023) << 52) | (frac & ((1ull << 52) - 1));
+  return __longlong_as_double((long long)bits);
+}
+
+// bad[0] counts mismatches, bad[1] flags that first[] holds one's operands.
+__global__ void __launch_bounds__(256) k_check_division(unsigned long long n, unsigned long long seed,
+                                                        unsigned long long* bad, double* first) {
+  const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
+  unsigned long long nbad = 0;
+  for (unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const unsigned long long u1 = splitmix64(seed ^ (2 * i)), u2 = splitmix64(seed ^ (2 * i + 1));
+    const int e1 = (int)((u1 >> 52) & 127) - 64, e2 = (int)((u2 >> 52) & 127) - 64;
+    double a, b;
+    switch ((int)(i % 5)) {
+      case 0:
+        a = compose_double(u1, e1, (unsigned)(u1 >> 63));
+        b = compose_double(u2, e2, (unsigned)(u2 >> 63));
+        break;
+      case 1:
+        a = compose_double(u1, e1, (unsigned)(u1 >> 63));
+        b = compose_double(((1ull << 52) - 1) - (u2 & 255), e2 & 15, (unsigned)(u2 >> 63));
+        break;
+      case 2: {
+        const double q = compose_double(u1, e1 & 31, 0);
+        const double half_ulp = compose_double(0, (e1 & 31) - 53, 0);
+        b = compose_double(u2, e2 & 31, (unsigned)(u2 >> 63));
+        a = __fma_rn(b, half_ulp, __dmul_rn(b, q));
+        break;
+      }
+      case 3:
+        a = (u1 & 1) ? -0.0 : 0.0;
+        b = compose_double(u2, e2, (unsigned)(u2 >> 63));
+        break;
+      default:
+        a = compose_double(u1, (int)((u1 >> 52) % 30) - 20, (unsigned)(u1 >> 63));
+        b = compose_double(u2, (int)((u2 >> 52) % 21) - 10, 0);
+        break;
+    }
+    const double ref = a / b;
+    const double got = div_rn(a, b, __drcp_rn(b));
+    if (__double_as_longlong(ref) != __double_as_longlong(got)) {
+      ++nbad;
+      if (atomicCAS(bad + 1, 0ull, 1ull) == 0ull) {   // the first mismatch found keeps its operands
+        first[0] = a;
+        first[1] = b;
+      }
+    }
+  }
+  if (nbad) atomicAdd(bad, nbad);
+}
+
+void launch_check_division(unsigned long long n, unsigned long long seed, unsigned long long* bad, double* first,
+                           int blocks, cudaStream_t st) {
+  k_check_division<<<blocks, 256, 0, st>>>(n, seed, bad, first);
 }
 
 // ==========================================================================

@@ -96,6 +96,8 @@ void launch_dump_laminar(const DevBatch& b, int* flags, cudaStream_t st);
 void launch_global_quantities(const DevBatch& b, double2* part, double* out, cudaStream_t st);
 // FP64 FMA throughput probe: returns flops per launch
 double launch_fp64_probe(double* sink, int blocks, cudaStream_t st);
+void launch_check_division(unsigned long long n, unsigned long long seed, unsigned long long* bad, double* first,
+                           int blocks, cudaStream_t st);
 double launch_fp32_probe(float* sink, int blocks, cudaStream_t st);
 
 }  // namespace sph
