@@ -392,6 +392,23 @@ int prepare_sim(const SphParams& prm, const SphGeometry& g, int cap, HostSim& hs
       D.laminar_no_slip_check = z.laminar_no_slip_check;
       D.zone_type = z.type;
     }
+    // The boundary quadrature's ring shortcut (face_integrals) needs the
+    // computed distances of one ring's points to agree to far better than
+    // its 1e-6 margin.  They differ by rounding only, about 2^-49 |L| / h in
+    // rob, L the particle's local coordinates: bounded by the grid box's
+    // corner farthest from the face's reference vertex.
+    double lmax = 0.0;
+    for (int f = 0; f < g.n_faces; ++f)
+      for (int c = 0; c < 8; ++c) {
+        double d2 = 0.0;
+        for (int d = 0; d < 3; ++d) {
+          const double corner = s.extr_lo[d] + (((c >> d) & 1) ? s.dcd[d] * s.ncd[d] : 0.0);
+          const double u = corner - hs.faces[f].GXref[d];
+          d2 += u * u;
+        }
+        lmax = std::max(lmax, std::sqrt(d2));
+      }
+    s.ring_skip = (lmax <= 1.0e6 * s.h) ? 1 : 0;
     // CompleteBoundaries3D.f90: BFaceList ordered by zone
     std::vector<int> bface;
     for (int nt = 1; nt <= g.n_zones; ++nt)

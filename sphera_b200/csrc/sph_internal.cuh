@@ -67,6 +67,7 @@ struct SimDev {
   float dcdf[3];          // (float)dcd: cell origins differ by multiples of it
   float rr_lo, rr_hi;     // FP32 screening band around (2h)^2 (see sph_api.cu)
   int narrow_z;           // z cells narrower than 2h: a candidate two cells away can lie within 2h
+  int ring_skip;          // boundary quadrature: a ring's later points skip the refresh test (see face_integrals)
   double kerneltab[kKtRows + 1][5];
 };
 

@@ -522,6 +522,14 @@ __device__ void face_integrals(const SimDev& s, const double* __restrict__ bit, 
       double lpj2 = L2 + zp;
       if (!(lpj2 <= 0.0)) continue;       // the whole ring lies above the face plane
       double tsegnato = L2 / (L2 - lpj2);
+      // The points of a ring share their polar angle, so their distances to
+      // the particle differ by rounding only (s.ring_skip bounds that far
+      // below 1e-6 in rob).  After the ring's first inside point the
+      // refresh test |rob - robpre| > 1e-3 is therefore false for every
+      // later point -- unless the first point missed the threshold by less
+      // than 1e-6, when the ring is tested point by point.  Skipping the
+      // test skips its distance, square root and division.
+      bool test_all = !s.ring_skip, first = true;
       for (int q = 0; q < 32; ++q) {
         const double* row = row0 + q * 7;
         double lpj0 = L0 + row[0];
@@ -529,18 +537,23 @@ __device__ void face_integrals(const SimDev& s, const double* __restrict__ bit, 
         double px0 = L0 + (lpj0 - L0) * tsegnato;
         double px1 = L1 + (lpj1 - L1) * tsegnato;
         if (!ft.inside(px0, px1)) continue;
-        double d0 = px0 - L0, d1 = px1 - L1, d2 = 0.0 - L2;
-        double dist = sqrt(d0 * d0 + d1 * d1 + d2 * d2);
-        double rob = div_rn(dist, s.h, s.rcp_h);
-        if (fabs(rob - robpre) > 1.0e-3) {
-          double iv[4];
-          interpolate_table(s, rob, iv);
-          double da = row[3];
-          J0 = iv[0] * da;
-          J1 = iv[1] * da;
-          J2 = iv[2] * da;
-          J3 = iv[3] * da;
-          robpre = rob;
+        if (first || test_all) {
+          double d0 = px0 - L0, d1 = px1 - L1, d2 = 0.0 - L2;
+          double dist = sqrt(d0 * d0 + d1 * d1 + d2 * d2);
+          double rob = div_rn(dist, s.h, s.rcp_h);
+          const double gap = fabs(rob - robpre);
+          if (first && !(gap > 1.0e-3) && gap > 1.0e-3 - 1.0e-6) test_all = true;
+          first = false;
+          if (gap > 1.0e-3) {
+            double iv[4];
+            interpolate_table(s, rob, iv);
+            double da = row[3];
+            J0 = iv[0] * da;
+            J1 = iv[1] * da;
+            J2 = iv[2] * da;
+            J3 = iv[3] * da;
+            robpre = rob;
+          }
         }
         double r0 = row[4], r1 = row[5], r2 = row[6];
         double RZ2 = r2 * r2;

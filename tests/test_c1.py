@@ -162,3 +162,20 @@ def test_c1_matrices_memory():
     assert g - base >= 72 * slots
     assert gd - g >= 72 * slots
     assert memory_required([only_divu]) == base
+
+
+@pytest.mark.parametrize("thresh,blows_up", [(1.0e-3, True), (0.614, False)])
+def test_oracle_dam_break_stability_depends_on_the_threshold(oracle_lib, thresh, blows_up):
+    """The reference's input template warns that C1_BE is unstable when
+    invB_det_thresh is too small; its tutorials with C1_BE use 0.614.  The 3D
+    dam break at dx 0.02 shows both: at 1e-3 the time step collapses within
+    300 steps (to about 5e-9 s), at 0.614 it stays at its initial size."""
+    case = c1_case(dx=0.02, thresh=thresh)
+    o = oracle_lib.Oracle(case, nthreads=8)
+    o.prepare()
+    dt0 = o.dt
+    o.step(300)
+    if blows_up:
+        assert o.dt < 1.0e-3 * dt0
+    else:
+        assert o.dt > 0.5 * dt0 and o.removed == 0

@@ -181,3 +181,24 @@ def test_2d_needs_a_positive_threshold():
     with pytest.raises(SphError) as e:
         Simulation(case)
     assert e.value.code == abi.SPH_ERR_INVALID_ARGUMENT
+
+
+@pytest.mark.parametrize("precision,thresh,blows_up", [(abi.SPH_PREC_FP64, 1.0e-3, True),
+                                                       (abi.SPH_PREC_FP64, 0.614, False),
+                                                       (abi.SPH_PREC_FP32C, 0.614, False)])
+def test_dam_break_stability_depends_on_the_threshold(precision, thresh, blows_up):
+    """As in the oracle (tests/test_c1.py): at invB_det_thresh 1e-3 the 3D
+    dam break at dx 0.02 blows up within 300 steps (the time step collapses;
+    the FP64 form follows the oracle), at the reference tutorials' 0.614 it
+    keeps its time step and every particle, in both forms."""
+    case = c1_case(dx=0.02, thresh=thresh, precision=precision)
+    sim = Simulation(case)
+    sim.upload(case.state)
+    dt0 = sim.clock()["dt"]
+    sim.step(300)
+    dt = sim.clock()["dt"]
+    if blows_up:
+        assert dt < 1.0e-3 * dt0
+    else:
+        assert dt > 0.5 * dt0
+        assert sim.diagnostics().removed_out_of_grid == 0
