@@ -229,6 +229,8 @@ int prepare_sim(const SphParams& prm, const SphGeometry& g, int cap, HostSim& hs
     s.dcd[d] = dextr / s.ncd[d];
   }
   if (s.dim == 2) s.ncd[1] = 1;
+  // IEEE reciprocals of the cell sizes: particle_cell divides by them exactly (div_rn)
+  for (int d = 0; d < 3; ++d) s.rcp_dcd[d] = s.dcd[d] > 0.0 ? 1.0 / s.dcd[d] : 0.0;
   // FP32 screening copies (k_rank_permute): the offset f of a particle from
   // the origin o of its cell, in FP32.  A candidate difference is formed as
   // D + (f_i - f_j) with D = (float)(cell index difference * dcd), which is

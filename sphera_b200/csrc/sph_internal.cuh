@@ -64,6 +64,7 @@ struct SimDev {
   double zpmin;           // 0.05 h, ComputeBoundaryVolumeIntegrals_P0.f90
   double ktdelta;         // kernel-table step
   double rcp_h, rcp_squareh, rcp_ktdelta;  // RN(1/h), RN(1/h^2), RN(1/ktdelta): divisors of div_rn
+  double rcp_dcd[3];      // RN(1/dcd): particle_cell's divisions
   float dcdf[3];          // (float)dcd: cell origins differ by multiples of it
   float rr_lo, rr_hi;     // FP32 screening band around (2h)^2 (see sph_api.cu)
   int narrow_z;           // z cells narrower than 2h: a candidate two cells away can lie within 2h

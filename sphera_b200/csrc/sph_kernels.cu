@@ -41,11 +41,33 @@ __device__ __forceinline__ void load_sim(SimDev& dst, const SimDev* src, int sim
 
 // ParticleCellNumber.f90:52-62 + CellNumber.f90:53-59: 1-based (i,j,k),
 // false if outside the grid.
+// a / b rounded to nearest, bit for bit what the IEEE division a / b gives,
+// from y = RN(1/b) (a constant's reciprocal formed on the host, or
+// __drcp_rn(b) once for a divisor that several divisions share).  The
+// method is Markstein's (P. Markstein, IBM J. Res. Dev. 34(1), 1990; the
+// theorem in Muller et al., Handbook of Floating-Point Arithmetic, on
+// division with a fused multiply-add): if y is within half an ulp of 1/b
+// and q within one ulp of a/b, the remainder r = a - b q is exact and
+// RN(q + r y) = RN(a/b).  q0 = RN(a y) can be up to 1.5 ulp off, so one
+// correction first brings it within half an ulp plus O(2^-105) relative
+// (q1), and the second is the theorem's step.  A zero remainder means the
+// current q is the exact quotient and is kept as it is (so a zero a keeps
+// its sign, which q + 0 y would lose).  Domain: a, b finite, b != 0, and no
+// quotient or remainder in the subnormal range -- true of every caller
+// (lengths, densities and smoothing lengths of a physical state).
+__device__ __forceinline__ double div_rn(double a, double b, double y) {
+  const double q0 = __dmul_rn(a, y);
+  const double r0 = __fma_rn(-b, q0, a);
+  const double q1 = r0 == 0.0 ? q0 : __fma_rn(r0, y, q0);
+  const double r1 = __fma_rn(-b, q1, a);
+  return r1 == 0.0 ? q1 : __fma_rn(r1, y, q1);
+}
+
 __device__ __forceinline__ bool particle_cell(const SimDev& s, double x, double y, double z, int& i, int& j,
                                               int& k) {
-  double ci = ceil((x - s.extr_lo[0]) / s.dcd[0]) - (double)s.ioff;   // exact: whole numbers
-  double ck = ceil((z - s.extr_lo[2]) / s.dcd[2]);
-  double cj = (s.dim == 3) ? ceil((y - s.extr_lo[1]) / s.dcd[1]) : 1.0;
+  double ci = ceil(div_rn(x - s.extr_lo[0], s.dcd[0], s.rcp_dcd[0])) - (double)s.ioff;   // exact: whole numbers
+  double ck = ceil(div_rn(z - s.extr_lo[2], s.dcd[2], s.rcp_dcd[2]));
+  double cj = (s.dim == 3) ? ceil(div_rn(y - s.extr_lo[1], s.dcd[1], s.rcp_dcd[1])) : 1.0;
   if (!(ci >= 1.0 && ci <= (double)s.ncd[0] && cj >= 1.0 && cj <= (double)s.ncd[1] && ck >= 1.0 &&
         ck <= (double)s.ncd[2]))
     return false;
@@ -84,28 +106,6 @@ __device__ __forceinline__ void neighbour_run(const SimDev& s, const int* __rest
 }
 
 // Kernel values of CalcVarLength.f90:242-269 for an accepted pair.
-// a / b rounded to nearest, bit for bit what the IEEE division a / b gives,
-// from y = RN(1/b) (a constant's reciprocal formed on the host, or
-// __drcp_rn(b) once for a divisor that several divisions share).  The
-// method is Markstein's (P. Markstein, IBM J. Res. Dev. 34(1), 1990; the
-// theorem in Muller et al., Handbook of Floating-Point Arithmetic, on
-// division with a fused multiply-add): if y is within half an ulp of 1/b
-// and q within one ulp of a/b, the remainder r = a - b q is exact and
-// RN(q + r y) = RN(a/b).  q0 = RN(a y) can be up to 1.5 ulp off, so one
-// correction first brings it within half an ulp plus O(2^-105) relative
-// (q1), and the second is the theorem's step.  A zero remainder means the
-// current q is the exact quotient and is kept as it is (so a zero a keeps
-// its sign, which q + 0 y would lose).  Domain: a, b finite, b != 0, and no
-// quotient or remainder in the subnormal range -- true of every caller
-// (lengths, densities and smoothing lengths of a physical state).
-__device__ __forceinline__ double div_rn(double a, double b, double y) {
-  const double q0 = __dmul_rn(a, y);
-  const double r0 = __fma_rn(-b, q0, a);
-  const double q1 = r0 == 0.0 ? q0 : __fma_rn(r0, y, q0);
-  const double r1 = __fma_rn(-b, q1, a);
-  return r1 == 0.0 ? q1 : __fma_rn(r1, y, q1);
-}
-
 __device__ __forceinline__ void kernel_values(const SimDev& s, double rijtemp2, double& PK1, double& PK2,
                                               double& PK3) {
   double rijtemp = sqrt(rijtemp2);
