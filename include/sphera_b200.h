@@ -211,7 +211,10 @@ void sph_destroy(SphHandle* h);
 
 /* Uploads pg(1:n) and performs the IC part of time_step_loop.f90:82-173:
  * OrdGrid1, neighbour search, ComputeBoundaryDataTab and the IC
- * time_step_duration.  v doubles as pg%var.                               */
+ * time_step_duration.  v doubles as pg%var.  x and m are copied first; the
+ * sort, the neighbour search and the boundary data run on them while v,
+ * rho and p are still being copied (with page-locked buffers; pageable ones
+ * give the same results without the overlap).                            */
 int  sph_upload(SphHandle* h, const SphState* state);
 /* Copies pg(1:n) back in the caller's order (after removals, the
  * reference's swap-with-last order).  Any of x, v, rho, p, m may be NULL.  */
@@ -290,8 +293,10 @@ int  sph_idle(SphHandle* h, int32_t* idle);
  * SM) of variants that leave the state unchanged, and for the momentum
  * and continuity pair loops also picks their shape (0: lean, one pair's
  * records at a time; 1: several list entries' records loaded together --
- * a list chunk's in the FP32c form, two entries' in the FP64 form), then
- * rebuilds the step graph.  Without C1 in both forms.
+ * a list chunk's in the FP32c form, two entries' in the FP64 form; 2, FP32c
+ * momentum only: 1 with two entries' terms computed on paired FP32
+ * instructions, the same bits), then rebuilds the step graph.  Without C1
+ * in both forms.
  * grid_out (may be NULL; 7 entries) receives in [0..4] the chosen blocks
  * of lists, momentum, continuity, boundary find and integrals, in [5] and
  * [6] the momentum and continuity shapes.                                 */

@@ -628,8 +628,10 @@ struct SphHandle {
   cudaStream_t stream = nullptr;
   cudaStream_t stream2 = nullptr;   // the boundary pass beside the lists (step graph)
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
-  cudaStream_t stream3 = nullptr;   // sph_step_download: x, v, m to the host beside the step's end
+  cudaStream_t stream3 = nullptr;   // sph_step_download: x, v, m to the host beside the step's end;
+                                    // an upload: v, rho, p to the device beside the IC's search
   cudaEvent_t ev_sorted = nullptr;
+  cudaEvent_t ev_pos = nullptr, ev_rest = nullptr;   // an upload's two halves
   int nsims = 0;
   int dim = 3;
   int precision = SPH_PREC_FP64;
@@ -1066,24 +1068,56 @@ int create_batch(int nsims, const SphParams* params, const SphGeometry* geoms, c
 // the pointers (unified addressing), so a host that keeps its state on the
 // device (e.g. a slab exchange done with device tensors) never stages it
 // through the host.
-int upload_sim(SphHandle* h, int sim, const SphState* st) {
+// The positions and masses of simulation `sim` (what the sort needs), on
+// the handle's stream.
+int upload_positions(SphHandle* h, int sim, const SphState* st) {
   if (!h || !st || sim < 0 || sim >= h->nsims) return SPH_ERR_INVALID_ARGUMENT;
   HostSim& hs = h->sims[sim];
   if (st->n < 0 || st->n > hs.cap || !st->x || !st->v || !st->rho || !st->p || !st->m) return SPH_ERR_INVALID_ARGUMENT;
   size_t o = hs.dev.p_off, n = st->n;
   cudaStream_t q = h->stream;
   SPH_CUDA(cudaMemcpyAsync(h->d_cx + 3 * o, st->x, sizeof(double) * 3 * n, cudaMemcpyDefault, q));
-  SPH_CUDA(cudaMemcpyAsync(h->d_cv + 3 * o, st->v, sizeof(double) * 3 * n, cudaMemcpyDefault, q));
-  SPH_CUDA(cudaMemcpyAsync(h->d_crho + o, st->rho, sizeof(double) * n, cudaMemcpyDefault, q));
-  SPH_CUDA(cudaMemcpyAsync(h->d_cp + o, st->p, sizeof(double) * n, cudaMemcpyDefault, q));
   SPH_CUDA(cudaMemcpyAsync(h->d_cm + o, st->m, sizeof(double) * n, cudaMemcpyDefault, q));
   h->n_of[sim] = st->n;
   return SPH_OK;
 }
 
-// IC of all simulations: sort, boundary data, IC time step.
-int initialise(SphHandle* h) {
-  cudaStream_t q = h->stream;
+// Its velocities, densities and pressures, on stream q (after
+// upload_positions has checked the state).
+int upload_rest(SphHandle* h, int sim, const SphState* st, cudaStream_t q) {
+  size_t o = h->sims[sim].dev.p_off, n = st->n;
+  SPH_CUDA(cudaMemcpyAsync(h->d_cv + 3 * o, st->v, sizeof(double) * 3 * n, cudaMemcpyDefault, q));
+  SPH_CUDA(cudaMemcpyAsync(h->d_crho + o, st->rho, sizeof(double) * n, cudaMemcpyDefault, q));
+  SPH_CUDA(cudaMemcpyAsync(h->d_cp + o, st->p, sizeof(double) * n, cudaMemcpyDefault, q));
+  return SPH_OK;
+}
+
+int upload_sim(SphHandle* h, int sim, const SphState* st) {
+  SPH_TRY(upload_positions(h, sim, st));
+  return upload_rest(h, sim, st, h->stream);
+}
+
+// The third stream and its events, made on first use.
+int ensure_stream3(SphHandle* h) {
+  if (h->stream3) return SPH_OK;
+  SPH_CUDA(cudaStreamCreateWithFlags(&h->stream3, cudaStreamNonBlocking));
+  SPH_CUDA(cudaEventCreateWithFlags(&h->ev_sorted, cudaEventDisableTiming));
+  SPH_CUDA(cudaEventCreateWithFlags(&h->ev_pos, cudaEventDisableTiming));
+  SPH_CUDA(cudaEventCreateWithFlags(&h->ev_rest, cudaEventDisableTiming));
+  return SPH_OK;
+}
+
+// Upload and IC of all simulations: sort, lists, boundary data, IC time
+// step.  The positions and masses go first, and the sort, the lists and the
+// boundary data run on them while the velocities, densities and pressures
+// are still being copied (stream 3); those are gathered into the sorted
+// order once both the copy and the sort are done, before the renormalisation
+// matrices and the time step that read them.  The boundary pass runs beside
+// the lists, as in the step.  The same results as one stream in sequence.
+int upload_and_initialise(SphHandle* h, const SphState* states) {
+  SPH_TRY(ensure_stream3(h));
+  cudaStream_t q = h->stream, q3 = h->stream3;
+  for (int s = 0; s < h->nsims; ++s) SPH_TRY(upload_positions(h, s, &states[s]));
   for (int s = 0; s < h->nsims; ++s) {
     std::memset(&h->h_dyn[s], 0, sizeof(SimDyn));
     h->h_dyn[s].nag = h->n_of[s];
@@ -1092,10 +1126,29 @@ int initialise(SphHandle* h) {
   }
   std::memset(&h->h_dyn[h->nsims], 0, sizeof(SimDyn));
   SPH_CUDA(cudaMemcpyAsync(h->d_dyn, h->h_dyn.data(), sizeof(SimDyn) * (h->nsims + 1), cudaMemcpyHostToDevice, q));
-  launch_init_from_caller(h->db, h->d_cx, h->d_cv, h->d_crho, h->d_cp, h->d_cm, q);
-  sort_sequence(h, q);
-  launch_boundary(h->db, q);
-  lists_pass(h, q);
+  launch_init_positions(h->db, h->d_cx, h->d_cm, q);
+  SPH_CUDA(cudaEventRecord(h->ev_pos, q));
+  SPH_CUDA(cudaStreamWaitEvent(q3, h->ev_pos, 0));
+  for (int s = 0; s < h->nsims; ++s) SPH_TRY(upload_rest(h, s, &states[s], q3));
+  launch_init_rest(h->db, h->d_cv, h->d_crho, h->d_cp, q3);
+  launch_sort_reset(h->db, q);
+  launch_bin(h->db, KeyKind::Sort, q);
+  launch_removal(h->db, q);
+  launch_scan(h->db, h->P.cell_start, q);
+  launch_place(h->db, q);
+  launch_rank_permute_positions(h->db, q);
+  SPH_CUDA(cudaEventRecord(h->ev_sorted, q));
+  SPH_CUDA(cudaStreamWaitEvent(q3, h->ev_sorted, 0));
+  launch_rank_permute_rest(h->db, q3);
+  SPH_CUDA(cudaEventRecord(h->ev_rest, q3));
+  SPH_CUDA(cudaEventRecord(h->ev_fork, q));
+  SPH_CUDA(cudaStreamWaitEvent(h->stream2, h->ev_fork, 0));
+  launch_boundary(h->db, h->stream2);
+  SPH_CUDA(cudaEventRecord(h->ev_join, h->stream2));
+  launch_neighbour_lists(h->db, q);
+  SPH_CUDA(cudaStreamWaitEvent(q, h->ev_join, 0));
+  SPH_CUDA(cudaStreamWaitEvent(q, h->ev_rest, 0));
+  if (h->any_c1) launch_renormalisation(h->db, q);
   launch_dt_reduce(h->db, q);
   launch_finalize(h->db, 0, q);
   SPH_CUDA(cudaGetLastError());
@@ -1136,6 +1189,8 @@ void sph_destroy(SphHandle* h) {
     cudaStreamDestroy(h->stream3);
   }
   if (h->ev_sorted) cudaEventDestroy(h->ev_sorted);
+  if (h->ev_pos) cudaEventDestroy(h->ev_pos);
+  if (h->ev_rest) cudaEventDestroy(h->ev_rest);
   if (h->ev_fork) cudaEventDestroy(h->ev_fork);
   if (h->ev_join) cudaEventDestroy(h->ev_join);
   cudaGetLastError();
@@ -1164,17 +1219,15 @@ int sph_idle(SphHandle* h, int32_t* idle) {
 int sph_upload(SphHandle* h, const SphState* state) {
   DeviceGuard dev_guard_(h);
   NvtxRange range_("sph_upload: IC (OrdGrid1, CalcVarLength, ComputeBoundaryDataTab, time_step_duration)");
-  if (!h || h->nsims != 1) return SPH_ERR_INVALID_ARGUMENT;
-  SPH_TRY(upload_sim(h, 0, state));
-  return initialise(h);
+  if (!h || h->nsims != 1 || !state) return SPH_ERR_INVALID_ARGUMENT;
+  return upload_and_initialise(h, state);
 }
 
 int sph_batch_upload(SphHandle* h, int32_t nsims, const SphState* states) {
   DeviceGuard dev_guard_(h);
   NvtxRange range_("sph_batch_upload: IC of every simulation");
   if (!h || nsims != h->nsims || !states) return SPH_ERR_INVALID_ARGUMENT;
-  for (int s = 0; s < nsims; ++s) SPH_TRY(upload_sim(h, s, &states[s]));
-  return initialise(h);
+  return upload_and_initialise(h, states);
 }
 
 int sph_batch_set_end_time(SphHandle* h, int32_t sim, double t_end) {
@@ -1255,10 +1308,7 @@ int sph_step_download(SphHandle* h, int32_t nsteps, SphState* state) {
   if (!h || !h->uploaded || h->nsims != 1 || nsteps < 0 || !state) return SPH_ERR_INVALID_ARGUMENT;
   if (nsteps == 0) return download_impl(h, 0, state, nullptr, nullptr);
   SPH_TRY(build_graph(h));
-  if (!h->stream3) {
-    SPH_CUDA(cudaStreamCreateWithFlags(&h->stream3, cudaStreamNonBlocking));
-    SPH_CUDA(cudaEventCreateWithFlags(&h->ev_sorted, cudaEventDisableTiming));
-  }
+  SPH_TRY(ensure_stream3(h));
   for (int s = 0; s + 1 < nsteps; ++s) SPH_CUDA(cudaGraphLaunch(h->graph, h->stream));
   // rows to copy early: the count the host last read back, which the steps
   // enqueued since can only have lowered (removals), so no wait is needed
@@ -1664,7 +1714,7 @@ int sph_set_launch_shape(SphHandle* h, const int32_t* shape) {
   if (!h || !shape) return SPH_ERR_INVALID_ARGUMENT;
   for (int c = 0; c < kGridClasses; ++c)
     if (shape[c] < 0) return SPH_ERR_INVALID_ARGUMENT;
-  if (shape[kGridClasses] < 0 || shape[kGridClasses] > 1 || shape[kGridClasses + 1] < 0 ||
+  if (shape[kGridClasses] < 0 || shape[kGridClasses] > 2 || shape[kGridClasses + 1] < 0 ||
       shape[kGridClasses + 1] > 1)
     return SPH_ERR_INVALID_ARGUMENT;
   SPH_CUDA(cudaStreamSynchronize(h->stream));
@@ -1703,18 +1753,21 @@ int sph_autotune(SphHandle* h, int32_t reps, int32_t* grid_out) {
     if (e == cudaSuccess) e = cudaMemcpyAsync(keep_d, b.P.BD, nb_bytes, cudaMemcpyDeviceToDevice, q);
   }
   // the momentum and continuity pair loops come in two shapes (lean, or
-  // several list entries' records loaded together): both are timed
+  // several list entries' records loaded together), the FP32c momentum loop
+  // in a third (batched, two entries' terms on paired FP32 instructions):
+  // all are timed
   const bool two_shapes = !h->any_c1;
+  const int mom_shapes = h->precision == SPH_PREC_FP32C ? 3 : 2;
   int best_batch = b.mom_batch, best_cbatch = b.con_batch;
   for (int cls = 0; cls < kGridClasses && e == cudaSuccess; ++cls) {
     if (cls == kGridIntegrals && h->dim != 3) continue;
     float best = 1e30f;
     int best_g = 0;
-    const int nshapes = ((cls == kGridMomentum || cls == kGridContinuity) && two_shapes) ? 2 : 1;
+    const int nshapes = !two_shapes ? 1 : cls == kGridMomentum ? mom_shapes : cls == kGridContinuity ? 2 : 1;
     for (int cand = 0; cand < nshapes * 6; ++cand) {
       const int m = mult[cand % 6];
-      if (nshapes == 2 && cls == kGridMomentum) b.mom_batch = cand / 6;
-      if (nshapes == 2 && cls == kGridContinuity) b.con_batch = cand / 6;
+      if (nshapes > 1 && cls == kGridMomentum) b.mom_batch = cand / 6;
+      if (nshapes > 1 && cls == kGridContinuity) b.con_batch = cand / 6;
       int g = b.sms * m;
       b.grid[cls] = g;
       auto run = [&]() {
@@ -1736,8 +1789,8 @@ int sph_autotune(SphHandle* h, int32_t reps, int32_t* grid_out) {
       if (ms < best) {
         best = ms;
         best_g = g;
-        if (nshapes == 2 && cls == kGridMomentum) best_batch = b.mom_batch;
-        if (nshapes == 2 && cls == kGridContinuity) best_cbatch = b.con_batch;
+        if (nshapes > 1 && cls == kGridMomentum) best_batch = b.mom_batch;
+        if (nshapes > 1 && cls == kGridContinuity) best_cbatch = b.con_batch;
       }
     }
     b.grid[cls] = best_g;

@@ -417,6 +417,16 @@ __global__ void k_place(DevBatch b, const int* __restrict__ cstart, int use_scra
 
 // Rank inside the cell by caller index (OrdGrid1.f90:100-105 stable
 // scatter) and gather the scratch record into the sorted state.
+// PART selects what is gathered: kPermuteAll everything (the step); the IC
+// of an upload splits it in two so that the velocities, densities and
+// pressures can still be on their way from the host while the lists and
+// the boundary data are built from the sorted positions:
+// kPermutePositions gathers x, m, the caller index and the laminar flag and
+// keeps each slot's destination in P.slot (free once k_place has run);
+// kPermuteRest gathers the rest through it.
+constexpr int kPermuteAll = 0, kPermutePositions = 1, kPermuteRest = 2;
+
+template <int PART>
 __global__ void k_rank_permute(DevBatch b) {
   __shared__ SimDev s;
   int cur = -1;
@@ -426,29 +436,38 @@ __global__ void k_rank_permute(DevBatch b) {
     load_sim(s, b.sims, tl.sim, cur);
     if (threadIdx.x >= tl.count) continue;
     int d = tl.start + threadIdx.x;
-    int key = P.tmp_key[d];
-    int myid = P.tmp_id[d];
     int fin = d;
-    if (key != s.cell_off + s.ncells) {
-      int cs = P.cell_start[key], ce = P.cell_start[key + 1];
-      int rank = 0;
-      for (int q = cs; q < ce; ++q) rank += (P.tmp_id[q] < myid) ? 1 : 0;
-      fin = cs + rank;
+    if (PART == kPermuteRest) {
+      fin = P.slot[d];
+    } else {
+      int key = P.tmp_key[d];
+      int myid = P.tmp_id[d];
+      if (key != s.cell_off + s.ncells) {
+        int cs = P.cell_start[key], ce = P.cell_start[key + 1];
+        int rank = 0;
+        for (int q = cs; q < ce; ++q) rank += (P.tmp_id[q] < myid) ? 1 : 0;
+        fin = cs + rank;
+      }
+      P.I[fin] = myid;
+      if (PART == kPermutePositions) P.slot[d] = fin;
     }
     int src = P.tmp_src[d];
     double4 x = P.X2[src];
-    double4 v = P.V2[src];
-    P.X[fin] = x;
-    P.XF[fin] = screening_copy(s, x);
-    double vol = x.w / v.w;
-    double pr = P.P2[src];
-    P.V[fin] = make_double4(v.x, v.y, v.z, vol);
-    P.RP[fin] = make_double2(v.w, pr);
-    P.VF[fin] = make_float4((float)v.x, (float)v.y, (float)v.z, (float)vol);
-    P.RF[fin] = make_float4((float)v.w, (float)(pr / (v.w * v.w)), (float)x.w, 0.f);
-    P.RM[fin] = make_float2((float)v.w, (float)(pr / (v.w * v.w)));
-    P.I[fin] = myid;
-    P.L[fin] = P.L2[src];
+    if (PART != kPermuteRest) {
+      P.X[fin] = x;
+      P.XF[fin] = screening_copy(s, x);
+      P.L[fin] = P.L2[src];
+    }
+    if (PART != kPermutePositions) {
+      double4 v = P.V2[src];
+      double vol = x.w / v.w;
+      double pr = P.P2[src];
+      P.V[fin] = make_double4(v.x, v.y, v.z, vol);
+      P.RP[fin] = make_double2(v.w, pr);
+      P.VF[fin] = make_float4((float)v.x, (float)v.y, (float)v.z, (float)vol);
+      P.RF[fin] = make_float4((float)v.w, (float)(pr / (v.w * v.w)), (float)x.w, 0.f);
+      P.RM[fin] = make_float2((float)v.w, (float)(pr / (v.w * v.w)));
+    }
   }
 }
 
@@ -2349,8 +2368,11 @@ __device__ __forceinline__ void momentum_f32_close(const SimDev& s, const DevBat
 // fused (the whole step, not C1): a particle without close faces has no
 // FP64 wall terms, so this launch closes it at once (momentum_f32_close,
 // the finishing launch's own code) instead of passing its nine sums on.
-template <int DIM, bool C1 = false, bool BATCH = false>
+// PAIRED (with BATCH, not C1): two list entries' terms on Blackwell's paired
+// FP32 instructions (pair2), the same bits as two calls of `pair`.
+template <int DIM, bool C1 = false, bool BATCH = false, bool PAIRED = false>
 __global__ void __launch_bounds__(kBlock, (C1 || BATCH) ? 2 : 3) k_momentum_f32(DevBatch b, int fused) {
+  static_assert(!PAIRED || (BATCH && !C1), "the paired loop is a batched, non-C1 shape");
   __shared__ SimDev s;
   int cur = -1;
   const Particles& P = b.P;
@@ -2436,6 +2458,83 @@ __global__ void __launch_bounds__(kBlock, (C1 || BATCH) ? 2 : 3) k_momentum_f32(
         cv2 = fmaf(vf, dv2, cv2);
       }
     };
+    // `pair` for entries ea, eb on paired instructions: every half rounds as
+    // the scalar instruction does (x - y as fma(y, -1, x), one rounding
+    // either way; products and sums in the scalar code's association, no
+    // contraction), the special-function values, the cubic spline's branch
+    // and the accumulations stay scalar, ea's accumulated before eb's.
+    auto pair2 = [&](int ea, int eb, const float4& xa, const float4& va, const float2& ra, const float4& xb,
+                     const float4& vb, const float2& rb) {
+      const float2 m1 = make_float2(-1.f, -1.f);
+      rc.update(s, (int)((unsigned)ea >> kSlotBits));
+      const float dxa = rc.Dx, dya = rc.Dy;
+      rc.update(s, (int)((unsigned)eb >> kSlotBits));
+      const float2 Dx = make_float2(dxa, rc.Dx), Dy = make_float2(dya, rc.Dy);
+      const float2 d0 = __fadd2_rn(Dx, __ffma2_rn(make_float2(xa.x, xb.x), m1, make_float2(xfi.x, xfi.x)));
+      const float2 d1 = (DIM == 3) ? __fadd2_rn(Dy, __ffma2_rn(make_float2(xa.y, xb.y), m1, make_float2(xfi.y, xfi.y)))
+                                   : make_float2(0.f, 0.f);
+      const float2 dk = __ffma2_rn(make_float2(xa.w, xb.w), m1, make_float2(ckf, ckf));
+      const float2 d2 = __fadd2_rn(__fmul2_rn(dk, make_float2(dz, dz)),
+                                   __ffma2_rn(make_float2(xa.z, xb.z), m1, make_float2(xfi.z, xfi.z)));
+      const float2 rr = __ffma2_rn(d2, d2, __ffma2_rn(d1, d1, __fmul2_rn(d0, d0)));
+      // kernel_values_f32
+      const float2 rq = make_float2(fmaxf(rr.x, 1.0e-30f), fmaxf(rr.y, 1.0e-30f));
+      const float2 r = __fmul2_rn(rq, make_float2(rsqrt_approx(rq.x), rsqrt_approx(rq.y)));
+      const float2 q = __fmul2_rn(r, make_float2(fc.hinv, fc.hinv));
+      const float2 q2 = __fmul2_rn(rr, make_float2(fc.h2inv, fc.h2inv));
+      const float2 a = __fadd2_rn(r, make_float2(fc.eta, fc.eta));
+      const float2 bq = __fadd2_rn(rr, make_float2(fc.eta2, fc.eta2));
+      const float2 ab = __fmul2_rn(a, bq);
+      const float2 inv = make_float2(rcp_approx(ab.x), rcp_approx(ab.y));
+      const float2 denom = __fmul2_rn(bq, inv);
+      const float2 glo = __ffma2_rn(make_float2(1.5f, 1.5f), q2, __fmul2_rn(make_float2(-2.0f, -2.0f), q));
+      const float2 ghi = __ffma2_rn(make_float2(-0.5f, -0.5f), q2,
+                                    __ffma2_rn(make_float2(2.0f, 2.0f), q, make_float2(-2.0f, -2.0f)));
+      const float2 g = make_float2(q.x < 1.0f ? glo.x : ghi.x, q.y < 1.0f ? glo.y : ghi.y);
+      const float2 gw = __ffma2_rn(make_float2(12.0f, 12.0f), q,
+                                   __ffma2_rn(make_float2(-3.0f, -3.0f), q2, make_float2(-12.0f, -12.0f)));
+      const float2 PK1 = __fmul2_rn(__fmul2_rn(g, make_float2(fc.ke, fc.ke)), denom);
+      const float2 PK2 = __fmul2_rn(PK1, __fmul2_rn(a, inv));
+      const float2 PK3 = __fmul2_rn(__fmul2_rn(gw, make_float2(fc.kacl, fc.kacl)), denom);
+      const float2 mj = __fmul2_rn(make_float2(ra.x, rb.x), make_float2(va.w, vb.w));
+      // pressure: pf = -t
+      const float2 t = __fmul2_rn(__fmul2_rn(mj, __fadd2_rn(make_float2(Pi, Pi), make_float2(ra.y, rb.y))), PK3);
+      // viscosity
+      const float2 dv0 = __ffma2_rn(make_float2(vix, vix), m1, make_float2(va.x, vb.x));
+      const float2 dv1 = __ffma2_rn(make_float2(viy, viy), m1, make_float2(va.y, vb.y));
+      const float2 dv2 = __ffma2_rn(make_float2(viz, viz), m1, make_float2(va.z, vb.z));
+      const float2 rsum = __fadd2_rn(make_float2(rhof, rhof), make_float2(ra.x, rb.x));
+      const float2 bm = __ffma2_rn(make_float2(fc.nu, fc.nu), rsum, make_float2(1.0e-3f, 1.0e-3f));
+      const float2 rb2 = __fmul2_rn(rsum, bm);
+      const float2 iv = make_float2(rcp_approx(rb2.x), rcp_approx(rb2.y));
+      // vr = -u; df = -w
+      const float2 u = __ffma2_rn(dv2, d2, __ffma2_rn(dv1, d1, __fmul2_rn(dv0, d0)));
+      const float2 w = __fmul2_rn(
+          __fmul2_rn(__fmul2_rn(mj, __fmul2_rn(make_float2(fc.amon, fc.amon), __fmul2_rn(bm, iv))), u), PK2);
+      cp0 = fmaf(-t.x, d0.x, cp0);
+      if (DIM == 3) cp1 = fmaf(-t.x, d1.x, cp1);
+      cp2 = fmaf(-t.x, d2.x, cp2);
+      cd0 = fmaf(-w.x, d0.x, cd0);
+      if (DIM == 3) cd1 = fmaf(-w.x, d1.x, cd1);
+      cd2 = fmaf(-w.x, d2.x, cd2);
+      cp0 = fmaf(-t.y, d0.y, cp0);
+      if (DIM == 3) cp1 = fmaf(-t.y, d1.y, cp1);
+      cp2 = fmaf(-t.y, d2.y, cp2);
+      cd0 = fmaf(-w.y, d0.y, cd0);
+      if (DIM == 3) cd1 = fmaf(-w.y, d1.y, cd1);
+      cd2 = fmaf(-w.y, d2.y, cd2);
+      if (morris) {
+        // vf = -z
+        const float2 z = __fmul2_rn(
+            __fmul2_rn(__fmul2_rn(__fmul2_rn(mj, make_float2(fc.nu4, fc.nu4)), __fmul2_rn(rsum, iv)), PK2), rr);
+        cv0 = fmaf(-z.x, dv0.x, cv0);
+        if (DIM == 3) cv1 = fmaf(-z.x, dv1.x, cv1);
+        cv2 = fmaf(-z.x, dv2.x, cv2);
+        cv0 = fmaf(-z.y, dv0.y, cv0);
+        if (DIM == 3) cv1 = fmaf(-z.y, dv1.y, cv1);
+        cv2 = fmaf(-z.y, dv2.y, cv2);
+      }
+    };
     for (int c = 0; c < nchmax; ++c) {
       const int4 ch = nxt;
       if (c + 1 < nch) nxt = __ldg(lbase + (size_t)(c + 1) * 32);
@@ -2449,10 +2548,17 @@ __global__ void __launch_bounds__(kBlock, (C1 || BATCH) ? 2 : 3) k_momentum_f32(
         if (rem > 1) { x1 = __ldg(P.XF + q1); v1 = __ldg(P.VF + q1); r1 = __ldg(P.RM + q1); }
         if (rem > 2) { x2 = __ldg(P.XF + q2); v2 = __ldg(P.VF + q2); r2 = __ldg(P.RM + q2); }
         if (rem > 3) { x3 = __ldg(P.XF + q3); v3 = __ldg(P.VF + q3); r3 = __ldg(P.RM + q3); }
-        pair(ch.x, x0, v0, r0);
-        if (rem > 1) pair(ch.y, x1, v1, r1);
-        if (rem > 2) pair(ch.z, x2, v2, r2);
-        if (rem > 3) pair(ch.w, x3, v3, r3);
+        if (PAIRED) {
+          if (rem > 1) pair2(ch.x, ch.y, x0, v0, r0, x1, v1, r1);
+          else pair(ch.x, x0, v0, r0);
+          if (rem > 3) pair2(ch.z, ch.w, x2, v2, r2, x3, v3, r3);
+          else if (rem > 2) pair(ch.z, x2, v2, r2);
+        } else {
+          pair(ch.x, x0, v0, r0);
+          if (rem > 1) pair(ch.y, x1, v1, r1);
+          if (rem > 2) pair(ch.z, x2, v2, r2);
+          if (rem > 3) pair(ch.w, x3, v3, r3);
+        }
       } else {
         auto one = [&](int e) {
           const int q = e & kSlotMask;
@@ -3585,6 +3691,48 @@ __global__ void k_init_from_caller(DevBatch b, const double* x, const double* v,
   }
 }
 
+// k_init_from_caller in two halves, for an upload whose positions and
+// masses arrive first: the positions half also marks each slot's caller
+// index (0 = empty), and the rest half fills a slot's velocity, density and
+// pressure where that mark is set.  The rest half does not read the particle
+// count, which the removal pass of the concurrent sort may be lowering.
+__global__ void k_init_positions(DevBatch b, const double* x, const double* m) {
+  __shared__ SimDev s;
+  int cur = -1;
+  const Particles& P = b.P;
+  for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
+    Tile tl = b.tiles[t];
+    load_sim(s, b.sims, tl.sim, cur);
+    if (threadIdx.x >= tl.count) continue;
+    int q = tl.start + threadIdx.x;
+    int i = q - s.p_off;
+    if (i < b.dyn[tl.sim].nag) {
+      P.X2[q] = make_double4(x[3 * (size_t)q], x[3 * (size_t)q + 1], x[3 * (size_t)q + 2], m[q]);
+      P.I2[q] = i + 1;
+    } else {
+      P.X2[q] = make_double4(0, 0, 0, 0);
+      P.I2[q] = 0;
+    }
+    P.L2[q] = 0;
+  }
+}
+
+__global__ void k_init_rest(DevBatch b, const double* v, const double* rho, const double* p) {
+  const Particles& P = b.P;
+  for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
+    Tile tl = b.tiles[t];
+    if (threadIdx.x >= tl.count) continue;
+    int q = tl.start + threadIdx.x;
+    if (P.I2[q] != 0) {
+      P.V2[q] = make_double4(v[3 * (size_t)q], v[3 * (size_t)q + 1], v[3 * (size_t)q + 2], rho[q]);
+      P.P2[q] = p[q];
+    } else {
+      P.V2[q] = make_double4(0, 0, 0, 1.0);
+      P.P2[q] = 0.0;
+    }
+  }
+}
+
 __global__ void k_to_caller(DevBatch b, double* x, double* v, double* rho, double* p, double* m, double* acc,
                             double* dden) {
   __shared__ SimDev s;
@@ -3888,7 +4036,15 @@ void launch_place(const DevBatch& b, cudaStream_t st) {
 }
 
 void launch_rank_permute(const DevBatch& b, cudaStream_t st) {
-  k_rank_permute<<<blocks_for(b), kBlock, 0, st>>>(b);
+  k_rank_permute<kPermuteAll><<<blocks_for(b), kBlock, 0, st>>>(b);
+}
+
+void launch_rank_permute_positions(const DevBatch& b, cudaStream_t st) {
+  k_rank_permute<kPermutePositions><<<blocks_for(b), kBlock, 0, st>>>(b);
+}
+
+void launch_rank_permute_rest(const DevBatch& b, cudaStream_t st) {
+  k_rank_permute<kPermuteRest><<<blocks_for(b), kBlock, 0, st>>>(b);
 }
 
 void launch_rank_reference(const DevBatch& b, const int* cell_start_ref, int* npartord, cudaStream_t st) {
@@ -3961,12 +4117,14 @@ void launch_momentum_f32(const DevBatch& b, bool fused, cudaStream_t st) {
     if (fused) k_momentum_f32_finish<3, true, true><<<gf, kBlock, 0, st>>>(b);
     else k_momentum_f32_finish<3, false, true><<<gf, kBlock, 0, st>>>(b);
   } else if (b.dim == 3) {
-    if (b.mom_batch) k_momentum_f32<3, false, true><<<g, kBlock, 0, st>>>(b, f);
+    if (b.mom_batch == 2) k_momentum_f32<3, false, true, true><<<g, kBlock, 0, st>>>(b, f);
+    else if (b.mom_batch) k_momentum_f32<3, false, true><<<g, kBlock, 0, st>>>(b, f);
     else k_momentum_f32<3><<<g, kBlock, 0, st>>>(b, f);
     if (fused) k_momentum_f32_finish<3, true><<<gf, kBlock, 0, st>>>(b);
     else k_momentum_f32_finish<3, false><<<gf, kBlock, 0, st>>>(b);
   } else {
-    if (b.mom_batch) k_momentum_f32<2, false, true><<<g, kBlock, 0, st>>>(b, f);
+    if (b.mom_batch == 2) k_momentum_f32<2, false, true, true><<<g, kBlock, 0, st>>>(b, f);
+    else if (b.mom_batch) k_momentum_f32<2, false, true><<<g, kBlock, 0, st>>>(b, f);
     else k_momentum_f32<2><<<g, kBlock, 0, st>>>(b, f);
     if (fused) k_momentum_f32_finish<2, true><<<gf, kBlock, 0, st>>>(b);
     else k_momentum_f32_finish<2, false><<<gf, kBlock, 0, st>>>(b);
@@ -4072,6 +4230,12 @@ void launch_finalize(const DevBatch& b, int mode, cudaStream_t st) {
 void launch_init_from_caller(const DevBatch& b, const double* x, const double* v, const double* rho,
                              const double* p, const double* m, cudaStream_t st) {
   k_init_from_caller<<<blocks_for(b), kBlock, 0, st>>>(b, x, v, rho, p, m);
+}
+void launch_init_positions(const DevBatch& b, const double* x, const double* m, cudaStream_t st) {
+  k_init_positions<<<blocks_for(b), kBlock, 0, st>>>(b, x, m);
+}
+void launch_init_rest(const DevBatch& b, const double* v, const double* rho, const double* p, cudaStream_t st) {
+  k_init_rest<<<blocks_for(b), kBlock, 0, st>>>(b, v, rho, p);
 }
 void launch_to_caller(const DevBatch& b, double* x, double* v, double* rho, double* p, double* m, double* acc,
                       double* dden, cudaStream_t st) {

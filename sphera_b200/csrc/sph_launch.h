@@ -35,7 +35,8 @@ struct DevBatch {
   int grid_blocks;         // blocks of the persistent particle kernels (default)
   int sms;                 // streaming multiprocessors of the device
   int grid[kGridClasses];  // autotuned blocks per kernel class (0 = grid_blocks)
-  int mom_batch;           // momentum pair loop: 1 = several entries' records loaded together (autotuned)
+  int mom_batch;           // momentum pair loop: 1 = several entries' records loaded together, 2 = the same
+                           // with two entries' terms on paired FP32 instructions (FP32c; autotuned)
   int con_batch;           // the same for the continuity pair loop
   int c1;                  // some simulation renormalises (C1_BE, 3D): P.BG (and P.BD) allocated
   int c1_divu;             // some simulation renormalises its velocity gradients (C1_divu)
@@ -52,6 +53,9 @@ void launch_sort_reset(const DevBatch& b, cudaStream_t st);
 void upload_bit2d(const double* tab, cudaStream_t st);
 void launch_place(const DevBatch& b, cudaStream_t st);
 void launch_rank_permute(const DevBatch& b, cudaStream_t st);
+// the IC of an upload: positions first (destinations kept in P.slot), then the rest
+void launch_rank_permute_positions(const DevBatch& b, cudaStream_t st);
+void launch_rank_permute_rest(const DevBatch& b, cudaStream_t st);
 void launch_rank_reference(const DevBatch& b, const int* cell_start_ref, int* npartord, cudaStream_t st);
 // neighbour lists (CalcVarLength replacement)
 void launch_neighbour_lists(const DevBatch& b, cudaStream_t st);
@@ -84,6 +88,8 @@ void launch_set_clock(const DevBatch& b, double time, int step, double dt, doubl
 // host <-> device in caller order
 void launch_init_from_caller(const DevBatch& b, const double* x, const double* v, const double* rho,
                              const double* p, const double* m, cudaStream_t st);
+void launch_init_positions(const DevBatch& b, const double* x, const double* m, cudaStream_t st);
+void launch_init_rest(const DevBatch& b, const double* v, const double* rho, const double* p, cudaStream_t st);
 void launch_to_caller(const DevBatch& b, double* x, double* v, double* rho, double* p, double* m,
                       double* acc, double* dden, cudaStream_t st);
 // verification
