@@ -470,7 +470,7 @@ def main():
     ap.add_argument("--autotune", type=int, default=1, help="size the persistent grids on the live state first")
     ap.add_argument("--shape", default=None,
                     help="force the FP32c momentum,continuity pair-loop shapes, e.g. 1,1 (0 lean, 1 batched "
-                         "loads, 2 momentum only: batched, paired FP32), or all seven values sph_autotune chooses")
+                         "loads, 2 batched with paired FP32 arithmetic), or all seven values sph_autotune chooses")
     ap.add_argument("--teta", type=float, default=0.0,
                     help="partial smoothing coefficient TetaP = TetaV of the dam-break workload (0: off)")
     ap.add_argument("--c1", action="store_true",

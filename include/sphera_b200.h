@@ -294,7 +294,7 @@ int  sph_idle(SphHandle* h, int32_t* idle);
  * and continuity pair loops also picks their shape (0: lean, one pair's
  * records at a time; 1: several list entries' records loaded together --
  * a list chunk's in the FP32c form, two entries' in the FP64 form; 2, FP32c
- * momentum only: 1 with two entries' terms computed on paired FP32
+ * form only: 1 with two entries' terms computed on paired FP32
  * instructions, the same bits), then rebuilds the step graph.  Without C1
  * in both forms.
  * grid_out (may be NULL; 7 entries) receives in [0..4] the chosen blocks

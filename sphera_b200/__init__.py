@@ -298,7 +298,7 @@ class Simulation:
     def autotune(self, reps=3):
         """Sizes the persistent grids of the pair, list and boundary kernels
         and picks the pair loops' shapes (0 lean, 1 batched record loads,
-        2 for the FP32c momentum loop: batched with paired FP32 arithmetic)."""
+        2 in the FP32c form: batched with paired FP32 arithmetic)."""
         return _autotune(self._h, reps)
 
     def set_launch_shape(self, shape):

@@ -1715,7 +1715,7 @@ int sph_set_launch_shape(SphHandle* h, const int32_t* shape) {
   for (int c = 0; c < kGridClasses; ++c)
     if (shape[c] < 0) return SPH_ERR_INVALID_ARGUMENT;
   if (shape[kGridClasses] < 0 || shape[kGridClasses] > 2 || shape[kGridClasses + 1] < 0 ||
-      shape[kGridClasses + 1] > 1)
+      shape[kGridClasses + 1] > 2)
     return SPH_ERR_INVALID_ARGUMENT;
   SPH_CUDA(cudaStreamSynchronize(h->stream));
   for (int c = 0; c < kGridClasses; ++c) h->db.grid[c] = shape[c];
@@ -1753,17 +1753,17 @@ int sph_autotune(SphHandle* h, int32_t reps, int32_t* grid_out) {
     if (e == cudaSuccess) e = cudaMemcpyAsync(keep_d, b.P.BD, nb_bytes, cudaMemcpyDeviceToDevice, q);
   }
   // the momentum and continuity pair loops come in two shapes (lean, or
-  // several list entries' records loaded together), the FP32c momentum loop
-  // in a third (batched, two entries' terms on paired FP32 instructions):
-  // all are timed
+  // several list entries' records loaded together), the FP32c loops in a
+  // third (batched, two entries' terms on paired FP32 instructions): all
+  // are timed
   const bool two_shapes = !h->any_c1;
-  const int mom_shapes = h->precision == SPH_PREC_FP32C ? 3 : 2;
+  const int pair_shapes = h->precision == SPH_PREC_FP32C ? 3 : 2;
   int best_batch = b.mom_batch, best_cbatch = b.con_batch;
   for (int cls = 0; cls < kGridClasses && e == cudaSuccess; ++cls) {
     if (cls == kGridIntegrals && h->dim != 3) continue;
     float best = 1e30f;
     int best_g = 0;
-    const int nshapes = !two_shapes ? 1 : cls == kGridMomentum ? mom_shapes : cls == kGridContinuity ? 2 : 1;
+    const int nshapes = (two_shapes && (cls == kGridMomentum || cls == kGridContinuity)) ? pair_shapes : 1;
     for (int cand = 0; cand < nshapes * 6; ++cand) {
       const int m = mult[cand % 6];
       if (nshapes > 1 && cls == kGridMomentum) b.mom_batch = cand / 6;

@@ -2701,8 +2701,11 @@ __global__ void __launch_bounds__(kBlock) k_momentum_f32_finish(DevBatch b) {
 // 119-126,201-217); the others of the batch sum as without it.
 // BATCH (not with DIVU): a list chunk's eight neighbour records requested
 // before the chunk's arithmetic, at 3 blocks per SM; the same sums.
-template <int DIM, bool DIVU = false, bool BATCH = false>
+// PAIRED (with BATCH): two entries' terms on paired FP32 instructions
+// (contrib2), the same bits as two calls of `contrib`.
+template <int DIM, bool DIVU = false, bool BATCH = false, bool PAIRED = false>
 __global__ void __launch_bounds__(kBlock, DIVU ? 2 : (BATCH ? 3 : 5)) k_continuity_f32(DevBatch b) {
+  static_assert(!PAIRED || (BATCH && !DIVU), "the paired loop is a batched, non-C1 shape");
   __shared__ SimDev s;
   int cur = -1;
   const Particles& P = b.P;
@@ -2750,6 +2753,43 @@ __global__ void __launch_bounds__(kBlock, DIVU ? 2 : (BATCH ? 3 : 5)) k_continui
         float c = rhof * vj.w * PK1;
         part = fmaf(c, fmaf(vj.z - viz, d2, fmaf(vj.y - viy, d1, (vj.x - vix) * d0)), part);
       };
+      // contrib for entries ea, eb on paired instructions (each half rounds
+      // as the scalar instruction; x - y as fma(y, -1, x)), ea's term
+      // accumulated before eb's
+      auto contrib2 = [&](int ea, int eb, const float4& xa, const float4& va, const float4& xb, const float4& vb) {
+        const float2 m1 = make_float2(-1.f, -1.f);
+        rc.update(s, (int)((unsigned)ea >> kSlotBits));
+        const float dxa = rc.Dx, dya = rc.Dy;
+        rc.update(s, (int)((unsigned)eb >> kSlotBits));
+        const float2 Dx = make_float2(dxa, rc.Dx), Dy = make_float2(dya, rc.Dy);
+        const float2 d0 = __fadd2_rn(Dx, __ffma2_rn(make_float2(xa.x, xb.x), m1, make_float2(xfi.x, xfi.x)));
+        const float2 d1 = (DIM == 3)
+                              ? __fadd2_rn(Dy, __ffma2_rn(make_float2(xa.y, xb.y), m1, make_float2(xfi.y, xfi.y)))
+                              : make_float2(0.f, 0.f);
+        const float2 dk = __ffma2_rn(make_float2(xa.w, xb.w), m1, make_float2(ckf, ckf));
+        const float2 d2 = __fadd2_rn(__fmul2_rn(dk, make_float2(dz, dz)),
+                                     __ffma2_rn(make_float2(xa.z, xb.z), m1, make_float2(xfi.z, xfi.z)));
+        const float2 rr = __ffma2_rn(d2, d2, __ffma2_rn(d1, d1, __fmul2_rn(d0, d0)));
+        // kernel_pk1_f32
+        const float2 rq = make_float2(fmaxf(rr.x, 1.0e-30f), fmaxf(rr.y, 1.0e-30f));
+        const float2 r = __fmul2_rn(rq, make_float2(rsqrt_approx(rq.x), rsqrt_approx(rq.y)));
+        const float2 q = __fmul2_rn(r, make_float2(fc.hinv, fc.hinv));
+        const float2 q2 = __fmul2_rn(rr, make_float2(fc.h2inv, fc.h2inv));
+        const float2 glo = __ffma2_rn(make_float2(1.5f, 1.5f), q2, __fmul2_rn(make_float2(-2.0f, -2.0f), q));
+        const float2 ghi = __ffma2_rn(make_float2(-0.5f, -0.5f), q2,
+                                      __ffma2_rn(make_float2(2.0f, 2.0f), q, make_float2(-2.0f, -2.0f)));
+        const float2 g = make_float2(q.x < 1.0f ? glo.x : ghi.x, q.y < 1.0f ? glo.y : ghi.y);
+        const float2 ra = __fadd2_rn(r, make_float2(fc.eta, fc.eta));
+        const float2 PK1 = __fmul2_rn(__fmul2_rn(g, make_float2(fc.ke, fc.ke)),
+                                      make_float2(rcp_approx(ra.x), rcp_approx(ra.y)));
+        const float2 c = __fmul2_rn(__fmul2_rn(make_float2(rhof, rhof), make_float2(va.w, vb.w)), PK1);
+        const float2 dv0 = __ffma2_rn(make_float2(vix, vix), m1, make_float2(va.x, vb.x));
+        const float2 dv1 = __ffma2_rn(make_float2(viy, viy), m1, make_float2(va.y, vb.y));
+        const float2 dv2 = __ffma2_rn(make_float2(viz, viz), m1, make_float2(va.z, vb.z));
+        const float2 u = __ffma2_rn(dv2, d2, __ffma2_rn(dv1, d1, __fmul2_rn(dv0, d0)));
+        part = fmaf(c.x, u.x, part);
+        part = fmaf(c.y, u.y, part);
+      };
       const int nch = (cnt + 3) >> 2, nchmax = (nmax + 3) >> 2;
       const int4* lbase = reinterpret_cast<const int4*>(b.nlist) + list_base4(p, b.list_cap4);
       int4 nxt = nch > 0 ? __ldg(lbase) : make_int4(0, 0, 0, 0);
@@ -2764,10 +2804,17 @@ __global__ void __launch_bounds__(kBlock, DIVU ? 2 : (BATCH ? 3 : 5)) k_continui
         if (rem > 1) { x1 = __ldg(P.XF + q1); v1 = __ldg(P.VF + q1); }
         if (rem > 2) { x2 = __ldg(P.XF + q2); v2 = __ldg(P.VF + q2); }
         if (rem > 3) { x3 = __ldg(P.XF + q3); v3 = __ldg(P.VF + q3); }
-        contrib(ch.x, x0, v0);
-        if (rem > 1) contrib(ch.y, x1, v1);
-        if (rem > 2) contrib(ch.z, x2, v2);
-        if (rem > 3) contrib(ch.w, x3, v3);
+        if (PAIRED) {
+          if (rem > 1) contrib2(ch.x, ch.y, x0, v0, x1, v1);
+          else contrib(ch.x, x0, v0);
+          if (rem > 3) contrib2(ch.z, ch.w, x2, v2, x3, v3);
+          else if (rem > 2) contrib(ch.z, x2, v2);
+        } else {
+          contrib(ch.x, x0, v0);
+          if (rem > 1) contrib(ch.y, x1, v1);
+          if (rem > 2) contrib(ch.z, x2, v2);
+          if (rem > 3) contrib(ch.w, x3, v3);
+        }
         sum.add(part);
         part = 0.f;
       }
@@ -4134,8 +4181,10 @@ void launch_momentum_f32(const DevBatch& b, bool fused, cudaStream_t st) {
 void launch_continuity_f32_pairs(const DevBatch& b, cudaStream_t st) {
   int g = blocks_for(b, kGridContinuity);
   if (b.dim == 3 && b.c1_divu) k_continuity_f32<3, true><<<g, kBlock, 0, st>>>(b);
+  else if (b.dim == 3 && b.con_batch == 2) k_continuity_f32<3, false, true, true><<<g, kBlock, 0, st>>>(b);
   else if (b.dim == 3 && b.con_batch) k_continuity_f32<3, false, true><<<g, kBlock, 0, st>>>(b);
   else if (b.dim == 3) k_continuity_f32<3><<<g, kBlock, 0, st>>>(b);
+  else if (b.con_batch == 2) k_continuity_f32<2, false, true, true><<<g, kBlock, 0, st>>>(b);
   else if (b.con_batch) k_continuity_f32<2, false, true><<<g, kBlock, 0, st>>>(b);
   else k_continuity_f32<2><<<g, kBlock, 0, st>>>(b);
 }

@@ -37,7 +37,7 @@ struct DevBatch {
   int grid[kGridClasses];  // autotuned blocks per kernel class (0 = grid_blocks)
   int mom_batch;           // momentum pair loop: 1 = several entries' records loaded together, 2 = the same
                            // with two entries' terms on paired FP32 instructions (FP32c; autotuned)
-  int con_batch;           // the same for the continuity pair loop
+  int con_batch;           // the same for the continuity pair loop (0, 1, 2)
   int c1;                  // some simulation renormalises (C1_BE, 3D): P.BG (and P.BD) allocated
   int c1_divu;             // some simulation renormalises its velocity gradients (C1_divu)
 };

@@ -1,5 +1,5 @@
 """Launch shapes change no result: the pair loops' shapes (lean, several
-list entries' records loaded together, and for the FP32c momentum loop the
+list entries' records loaded together, and in the FP32c form the
 batched one on paired FP32 instructions) and any persistent grid give
 the same state bit for bit, in both forms, for a single simulation and for
 a batch; in the FP64 form every shape stays on the oracle."""
@@ -14,7 +14,8 @@ SHAPES = [dict(momentum_shape=0, continuity_shape=0),
           dict(momentum_shape=1, continuity_shape=0),
           dict(momentum_shape=0, continuity_shape=1),
           dict(momentum_shape=1, continuity_shape=1, lists=148, momentum=296, continuity=592),
-          dict(momentum_shape=2, continuity_shape=1)]
+          dict(momentum_shape=2, continuity_shape=1),
+          dict(momentum_shape=2, continuity_shape=2)]
 
 
 @pytest.mark.parametrize("precision", [abi.SPH_PREC_FP32C, abi.SPH_PREC_FP64], ids=["fp32c", "fp64"])
@@ -43,7 +44,7 @@ def test_autotune_reports_the_shapes_and_keeps_results():
     a = Batch(cs)
     a.upload()
     got = a.autotune(reps=1)
-    assert got["momentum_shape"] in (0, 1, 2) and got["continuity_shape"] in (0, 1)
+    assert got["momentum_shape"] in (0, 1, 2) and got["continuity_shape"] in (0, 1, 2)
     a.step(20)
     b = Batch(cs)
     b.upload()
