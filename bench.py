@@ -452,7 +452,7 @@ def main():
     ap.add_argument("--min-seconds", type=float, default=2.0,
                     help="repeat the timed window of --steps replays until this much device time is timed")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--e2e-steps", type=int, default=10)
+    ap.add_argument("--e2e-steps", type=int, default=30)
     ap.add_argument("--cpu-steps", type=int, default=3)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-extras", action="store_true",

@@ -265,27 +265,40 @@ __global__ void k_bin(DevBatch b) {
   __shared__ SimDev s;
   int cur = -1;
   const Particles& P = b.P;
+  const int lane = threadIdx.x & 31;
   for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
     Tile tl = b.tiles[t];
     load_sim(s, b.sims, tl.sim, cur);
-    if (threadIdx.x >= tl.count) continue;
+    const bool valid = threadIdx.x < tl.count;
     int p = tl.start + threadIdx.x;
-    SimDyn* dyn = b.dyn + tl.sim;
-    int nag = dyn->nag;
-    int key = s.cell_off + s.ncells;  // removal bin
-    if (p < s.p_off + nag) {
-      double4 x = (KIND == KeyKind::Sort) ? P.X2[p] : P.X[p];
-      int i, j, k;
-      if (particle_cell(s, x.x, x.y, x.z, i, j, k)) {
-        key = s.cell_off + ((KIND == KeyKind::Sort) ? cell_key_local(s, i, j, k)
-                                                     : ((k - 1) * s.ncd[1] + (j - 1)) * s.ncd[0] + (i - 1));
-      } else if (KIND == KeyKind::Sort) {
-        atomicAdd(&dyn->n_out, 1);
-        P.out_flag[s.p_off + P.I2[p] - 1] = 1;
+    int key = -1;
+    if (valid) {
+      SimDyn* dyn = b.dyn + tl.sim;
+      int nag = dyn->nag;
+      key = s.cell_off + s.ncells;  // removal bin
+      if (p < s.p_off + nag) {
+        double4 x = (KIND == KeyKind::Sort) ? P.X2[p] : P.X[p];
+        int i, j, k;
+        if (particle_cell(s, x.x, x.y, x.z, i, j, k)) {
+          key = s.cell_off + ((KIND == KeyKind::Sort) ? cell_key_local(s, i, j, k)
+                                                       : ((k - 1) * s.ncd[1] + (j - 1)) * s.ncd[0] + (i - 1));
+        } else if (KIND == KeyKind::Sort) {
+          atomicAdd(&dyn->n_out, 1);
+          P.out_flag[s.p_off + P.I2[p] - 1] = 1;
+        }
       }
+      P.key[p] = key;
     }
-    P.key[p] = key;
-    P.slot[p] = atomicAdd(P.cell_count + key, 1);
+    // the lanes of a warp that bin into one cell (the last sort's order
+    // keeps most of a warp in one or two) take their slots with one atomic;
+    // a slot only has to be unique within its cell (the placement is ranked
+    // by caller index afterwards)
+    const unsigned peers = __match_any_sync(0xffffffffu, key);
+    const int leader = __ffs(peers) - 1;
+    int base = 0;
+    if (valid && lane == leader) base = atomicAdd(P.cell_count + key, __popc(peers));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (valid) P.slot[p] = base + __popc(peers & ((1u << lane) - 1u));
   }
 }
 
