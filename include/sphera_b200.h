@@ -235,7 +235,8 @@ int  sph_sync(SphHandle* h);
  * keeps the state in its own memory between steps (time_step_loop.f90 with
  * pg(:) on the CPU).  The positions, velocities and masses of the last
  * step are copied to the host while that step's neighbour search, boundary
- * data and continuity pass still run.  The buffers must hold the particle
+ * data and continuity pass still run (copied again after the step when a
+ * particle left the grid in it, which renumbers the rest).  The buffers must hold the particle
  * count before the call, as the host last saw it (sph_upload, or the last
  * call that returned a count); state->n returns the count after it (lower
  * after out-of-grid removals; rows from there on are unspecified).  The

@@ -632,6 +632,7 @@ struct SphHandle {
                                     // an upload: v, rho, p to the device beside the IC's search
   cudaEvent_t ev_sorted = nullptr;
   cudaEvent_t ev_pos = nullptr, ev_rest = nullptr;   // an upload's two halves
+  cudaEvent_t ev_moved = nullptr;   // sph_step_download: the last step's momentum pass done
   int nsims = 0;
   int dim = 3;
   int precision = SPH_PREC_FP64;
@@ -778,11 +779,13 @@ void refresh_copies(SphHandle* h, cudaStream_t st) {
 }
 
 // The early half of sph_step_download: positions, velocities and masses
-// are final once a step's sort has run (the passes after it write only
-// rho, p and their FP32 copies), so their scatter to caller order and their
-// copy to the host run on a third stream beside the lists, boundary and
-// continuity passes.  n rows are copied: the count before the step, which
-// removals can only lower.
+// are final once a step's momentum pass (and velocity smoothing) has run
+// (the passes after it write only rho, p and their FP32 copies, and the
+// sort only reorders), so their scatter to caller order, from the step's
+// record, and their copy to the host run on a third stream beside the sort,
+// lists, boundary and continuity passes.  n rows are copied: the count
+// before the step, which removals can only lower.  A removal in the step
+// renumbers particles: the caller then copies again from the sorted state.
 struct EarlyCopy {
   SphState* state;
   int n;
@@ -790,10 +793,10 @@ struct EarlyCopy {
 };
 
 void enqueue_early_copy(SphHandle* h, cudaStream_t st, EarlyCopy& ec) {
-  cudaEventRecord(h->ev_sorted, st);
-  cudaStreamWaitEvent(h->stream3, h->ev_sorted, 0);
+  cudaEventRecord(h->ev_moved, st);
+  cudaStreamWaitEvent(h->stream3, h->ev_moved, 0);
   cudaStream_t q = h->stream3;
-  launch_to_caller(h->db, h->d_cx, h->d_cv, nullptr, nullptr, h->d_cm, nullptr, nullptr, q);
+  launch_scratch_to_caller(h->db, h->d_cx, h->d_cv, h->d_cm, q);
   cudaError_t e = cudaGetLastError();
   const size_t o = h->sims[0].dev.p_off, n = (size_t)ec.n;
   SphState* sta = ec.state;
@@ -813,8 +816,8 @@ void enqueue_early_copy(SphHandle* h, cudaStream_t st, EarlyCopy& ec) {
 void step_sequence(SphHandle* h, cudaStream_t st, EarlyCopy* early = nullptr) {
   momentum_pass(h, true, st);
   if (h->any_teta_v) launch_velocity_smoothing(h->db, true, h->precision == SPH_PREC_FP32C, st);
-  sort_sequence(h, st);
   if (early) enqueue_early_copy(h, st, *early);
+  sort_sequence(h, st);
   cudaEventRecord(h->ev_fork, st);
   cudaStreamWaitEvent(h->stream2, h->ev_fork, 0);
   launch_boundary(h->db, h->stream2);
@@ -1104,6 +1107,7 @@ int ensure_stream3(SphHandle* h) {
   SPH_CUDA(cudaEventCreateWithFlags(&h->ev_sorted, cudaEventDisableTiming));
   SPH_CUDA(cudaEventCreateWithFlags(&h->ev_pos, cudaEventDisableTiming));
   SPH_CUDA(cudaEventCreateWithFlags(&h->ev_rest, cudaEventDisableTiming));
+  SPH_CUDA(cudaEventCreateWithFlags(&h->ev_moved, cudaEventDisableTiming));
   return SPH_OK;
 }
 
@@ -1191,6 +1195,7 @@ void sph_destroy(SphHandle* h) {
   if (h->ev_sorted) cudaEventDestroy(h->ev_sorted);
   if (h->ev_pos) cudaEventDestroy(h->ev_pos);
   if (h->ev_rest) cudaEventDestroy(h->ev_rest);
+  if (h->ev_moved) cudaEventDestroy(h->ev_moved);
   if (h->ev_fork) cudaEventDestroy(h->ev_fork);
   if (h->ev_join) cudaEventDestroy(h->ev_join);
   cudaGetLastError();
@@ -1299,8 +1304,8 @@ int sph_step(SphHandle* h, int32_t nsteps, SphStepInfo* info) {
 
 // nsteps steps, then the state in caller order, as sph_step followed by
 // sph_download, with the last step's positions, velocities and masses
-// copied to the host while that step's lists, boundary data and continuity
-// pass still run (see enqueue_early_copy).  The last step is launched
+// copied to the host while that step's sort, lists, boundary data and
+// continuity pass still run (see enqueue_early_copy).  The last step is launched
 // without the graph so that the copy can start inside it.
 int sph_step_download(SphHandle* h, int32_t nsteps, SphState* state) {
   DeviceGuard dev_guard_(h);
@@ -1327,6 +1332,17 @@ int sph_step_download(SphHandle* h, int32_t nsteps, SphState* state) {
   SPH_TRY(sync_dyn(h));
   if (e != cudaSuccess) return cuda_status(e);
   state->n = h->h_dyn[0].nag;
+  if (state->n != ec.n && (state->x || state->v || state->m)) {
+    // particles were removed (and renumbered): the rows again, from the
+    // sorted state in the final numbering
+    launch_to_caller(h->db, h->d_cx, h->d_cv, nullptr, nullptr, h->d_cm, nullptr, nullptr, q);
+    SPH_CUDA(cudaGetLastError());
+    const size_t m = (size_t)state->n;
+    if (state->x) SPH_CUDA(cudaMemcpyAsync(state->x, h->d_cx + 3 * o, sizeof(double) * 3 * m, cudaMemcpyDefault, q));
+    if (state->v) SPH_CUDA(cudaMemcpyAsync(state->v, h->d_cv + 3 * o, sizeof(double) * 3 * m, cudaMemcpyDefault, q));
+    if (state->m) SPH_CUDA(cudaMemcpyAsync(state->m, h->d_cm + o, sizeof(double) * m, cudaMemcpyDefault, q));
+    SPH_CUDA(cudaStreamSynchronize(q));
+  }
   return SPH_OK;
 }
 

@@ -3817,6 +3817,32 @@ __global__ void k_to_caller(DevBatch b, double* x, double* v, double* rho, doubl
   }
 }
 
+// Positions, velocities and masses of a fused step's record (X2, V2, I2 in
+// the last sort's slot order, written by the momentum pass and final from
+// then on) to caller order, before the step's own sort has run.  Slots are
+// those below the particle count; the sort's removal pass may lower that
+// count concurrently, in which case the caller redoes this copy from the
+// sorted state (the removal renumbers particles).
+__global__ void k_scratch_to_caller(DevBatch b, double* x, double* v, double* m) {
+  __shared__ SimDev s;
+  int cur = -1;
+  const Particles& P = b.P;
+  for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
+    Tile tl = b.tiles[t];
+    load_sim(s, b.sims, tl.sim, cur);
+    int q = tl.start + threadIdx.x;
+    if (threadIdx.x >= tl.count || q >= s.p_off + b.dyn[tl.sim].nag) continue;
+    const int id = P.I2[q];
+    if (id <= 0) continue;
+    const size_t o = (size_t)s.p_off + id - 1;
+    const double4 xx = P.X2[q];
+    const double4 vv = P.V2[q];
+    x[3 * o] = xx.x; x[3 * o + 1] = xx.y; x[3 * o + 2] = xx.z;
+    v[3 * o] = vv.x; v[3 * o + 1] = vv.y; v[3 * o + 2] = vv.z;
+    m[o] = xx.w;
+  }
+}
+
 template <int DIM>
 __global__ void k_dump_neighbours(DevBatch b, int nmaxj, int* counts, int* lists) {
   // the stored lists the pair passes read, in caller indices, with the
@@ -4292,6 +4318,9 @@ void launch_finalize(const DevBatch& b, int mode, cudaStream_t st) {
 void launch_init_from_caller(const DevBatch& b, const double* x, const double* v, const double* rho,
                              const double* p, const double* m, cudaStream_t st) {
   k_init_from_caller<<<blocks_for(b), kBlock, 0, st>>>(b, x, v, rho, p, m);
+}
+void launch_scratch_to_caller(const DevBatch& b, double* x, double* v, double* m, cudaStream_t st) {
+  k_scratch_to_caller<<<blocks_for(b), kBlock, 0, st>>>(b, x, v, m);
 }
 void launch_init_positions(const DevBatch& b, const double* x, const double* m, cudaStream_t st) {
   k_init_positions<<<blocks_for(b), kBlock, 0, st>>>(b, x, m);

@@ -89,6 +89,8 @@ void launch_set_clock(const DevBatch& b, double time, int step, double dt, doubl
 void launch_init_from_caller(const DevBatch& b, const double* x, const double* v, const double* rho,
                              const double* p, const double* m, cudaStream_t st);
 void launch_init_positions(const DevBatch& b, const double* x, const double* m, cudaStream_t st);
+// a fused step's x, v, m from its momentum record (before its sort) to caller order
+void launch_scratch_to_caller(const DevBatch& b, double* x, double* v, double* m, cudaStream_t st);
 void launch_init_rest(const DevBatch& b, const double* v, const double* rho, const double* p, cudaStream_t st);
 void launch_to_caller(const DevBatch& b, double* x, double* v, double* rho, double* p, double* m,
                       double* acc, double* dden, cudaStream_t st);
