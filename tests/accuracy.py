@@ -1,5 +1,5 @@
 """Accuracy study of the device forms against the FP64 oracle on the
-3D dam break, on the north star's schedule: fields compared every 0.05 s
+3D dam break: fields compared every 0.05 s
 up to 0.5 s of physical time.
 
 Three device runs start from the oracle's initial state:

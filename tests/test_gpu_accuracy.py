@@ -1,4 +1,4 @@
-"""The FP32-compensated form against the FP64 oracle on the north star's
+"""The FP32-compensated form against the FP64 oracle on the accuracy
 schedule: the 3D dam break compared every 0.05 s up to 0.5 s of physical
 time (tests/accuracy.py), with three FP64 controls: the plain FP64 form,
 the FP64 form from positions perturbed by 1e-12, and the FP64 form from the
@@ -22,8 +22,8 @@ are:
   * the FP64 global sums: the mass exactly conserved by every run, and the
     FP32c volume within the same factor of the controls' drift.
 
-The default case is dx = 0.02 m (13,500 particles).  The full-size study of
-the north star, dx = 0.01 m (108,000 particles, about six minutes of the
+The default case is dx = 0.02 m (13,500 particles).  The full-size study,
+dx = 0.01 m (108,000 particles, about six minutes of the
 oracle on 16 host threads), runs when SPH_ACCURACY_FULL=1; either writes its
 record as JSON to $SPH_ACCURACY_OUT when that is set.
 """

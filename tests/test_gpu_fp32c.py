@@ -1,6 +1,6 @@
 """The FP32-compensated form against the FP64 oracle.
 
-Tolerances (the north-star bar for this form): density and velocity fields
+Tolerances (the accuracy bar of this form): density and velocity fields
 within 1e-3 relative L2 of the FP64 oracle; per-step rates on an identical
 state within 1e-5 relative L2 (FP32 pair arithmetic with compensated sums);
 neighbour sets identical to the FP64 form (the distance test is decided

@@ -1,6 +1,6 @@
 """GPU parity of the FP64 path against the oracle, through the C ABI.
 
-Bars:
+Bars (the parity contract of the FP64 form):
   * cell indices (pg%cella), Icont, NPartOrd and neighbour lists: bit-exact;
   * drho/dt and dv/dt on an identical state: relative L2 error <= 1e-12
     per field (normwise, because drho/dt nearly cancels in hydrostatic
