@@ -725,6 +725,10 @@ def run_step_bench(args, ws, rank, local):
         # passes, + 1 for the renormalisation matrices
         "gpu_launches": ((KERNELS_PER_STEP if fp32c else KERNELS_PER_STEP_FP64)
                          + (4 if args.teta > 0 else 0) + (1 if args.c1 else 0)) * args.steps,
+        # the line's figures are one window's (the median); every window launches as many
+        "gpu_launches_all_windows": ((KERNELS_PER_STEP if fp32c else KERNELS_PER_STEP_FP64)
+                                     + (4 if args.teta > 0 else 0) + (1 if args.c1 else 0))
+                                    * args.steps * head["windows"],
         "clocks": head["clocks"],
         "cpu_baseline": cpu,
     }
